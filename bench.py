@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""PISO steps/s of the Taylor-Hood P2/P1 tetrahedral Navier-Stokes step on B200.
+
+Workload (one "step" = one pisoStep): cylinder L=30, R=2 along x, ~1M tets (16 disk rings x 217
+axial prism layers -> 999,936 tets, N2 = 1,378,515 P2 nodes, nv = 178,106 pressure DOFs),
+rho = 1060, nu = 0.004, dt = 0.01, parabolic inlet u_x = 2*0.5*(1 - r^2/4), no-slip wall, p = 0
+outlet, FP64, CG pressure and batched BiCGSTAB momentum to 1e-10 relative residual, from rest.
+The mesh is synthetic (the reference meshes with TetGen, which is not available here).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cfsa|reference]
+
+Multi-GPU (torchrun, one rank per GPU): the step does not shard in this build, every rank runs
+an independent replica ("replicas only"); value = all ranks' steps / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "cell-fluid-structure-analysis_b200"
+sys.path.insert(0, str(PKG))
+
+METRIC = "PISO steps/s at 1M tets (FP64 GPU step)"
+UNIT = "steps/s"
+GEOM = dict(length=30.0, radius=2.0, rings=16, layers=217)
+FLUID = (1060.0, 0.004)
+DT = 0.01
+TOL = 1e-10
+MAXIT = (5000, 50000)
+INLET_PEAK = 2 * 0.5
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cfsa", choices=["cfsa", "reference"])
+    ap.add_argument("--rings", type=int, default=GEOM["rings"])
+    ap.add_argument("--layers", type=int, default=GEOM["layers"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-budget-s", type=float, default=120.0,
+                    help="cap on the timed CPU work of --impl reference")
+    return ap.parse_args()
+
+
+def workload_desc(m, rings, layers):
+    nv, nt, ne, _, _ = m.sizes
+    return {
+        "workload": f"cylinder L=30 R=2, {nt} tets ({rings} rings x {layers} layers), "
+                    f"N2={nv + ne} P2 nodes, nv={nv}; FP64 PISO, CG pressure + batched BiCGSTAB "
+                    f"momentum to 1e-10, parabolic inlet peak 1.0, rho 1060, nu 0.004, dt 0.01",
+        "tets": nt, "p2_nodes": nv + ne, "pressure_dofs": nv,
+        "velocity_dofs": 3 * (nv + ne),
+        "l2": "no flush: momentum operator ~0.5 GB and M ~0.3 GB stream through the 126 MB L2 every step",
+    }
+
+
+def make_mesh(cf, rings, layers):
+    m = cf.Mesh.cylinder(GEOM["length"], GEOM["radius"], rings, layers)
+    m.setupBoundaryConditions((1.0, 0.0, 0.0), 1.0)
+    return m
+
+
+def make_solver(cf, m):
+    s = cf.NavierStokesSolver()
+    s.setKrylovTolerances(TOL, TOL)
+    s.setMaxIterations(*MAXIT)
+    s.setPressureSolver(cf.KRYLOV_CG)
+    s.setDt(DT)
+    s.initialize(m, cf.Fluid(*FLUID))  # from rest; inlet set after initialize (CLI order)
+    profile = cf.parabolic_inlet(m.nodePositions(), INLET_PEAK, GEOM["radius"])
+    s.setInletVelocityProfile(profile)
+    return s, profile
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self, indices):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                if int(f[0]) not in indices:
+                    continue
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_table():
+    p = ROOT / "profiles" / "dram_traffic.json"
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
+def cpu_baseline(xyz, tets, profile, n_threads):
+    """Oracle port (test infrastructure) timed on the host cores: the 2nd step from rest of the
+    same workload (setup and the 1st step untimed)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    cores = po.set_threads(n_threads)
+    o = po.Oracle(xyz, tets)
+    o.set_fluid(*FLUID)
+    o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=1)
+    o.initialize()
+    o.set_inlet(profile)
+    if o.piso_step() != 0:
+        return None
+    t = time.perf_counter()
+    code = o.piso_step()
+    dt = time.perf_counter() - t
+    return {"value": (1.0 / dt) if code == 0 else 0.0, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"1 PISO step (2nd from rest) of the {len(tets)}-tet workload, {dt:.2f} s, "
+                      f"FP64 oracle with OpenMP on {cores} threads"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import cfsa_b200 as cf  # mesh generation only (host C++), no device work
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    cores = po.set_threads(os.cpu_count() or 1)
+    m = make_mesh(cf, args.rings, args.layers)
+    xyz, tets = m.vertices(), m.tets()
+    profile = cf.parabolic_inlet(m.nodePositions(), INLET_PEAK, GEOM["radius"])
+    o = po.Oracle(xyz, tets)
+    o.set_fluid(*FLUID)
+    o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=1)
+    o.initialize()
+    o.set_inlet(profile)
+    for _ in range(max(1, min(args.warmup, 3))):
+        o.piso_step()
+    done, t0 = 0, time.perf_counter()
+    while done < args.steps:
+        if o.piso_step() != 0:
+            break
+        done += 1
+        if time.perf_counter() - t0 > args.reference_budget_s:
+            break
+    el = time.perf_counter() - t0
+    value = done / el if el > 0 else 0.0
+    sample = (f"{done} of {args.steps} requested PISO steps after {max(1, min(args.warmup, 3))} warm-up "
+              f"steps, FP64 oracle port with OpenMP on {cores} threads, capped at "
+              f"{args.reference_budget_s:.0f} s of timed work")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": done, "warmup": max(1, min(args.warmup, 3)),
+            "ms_per_step": 1e3 * el / max(done, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic: procedural cylinder mesh",
+            "config": workload_desc(m, args.rings, args.layers),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    import cfsa_b200 as cf
+
+    m = make_mesh(cf, args.rings, args.layers)
+    s, profile = make_solver(cf, m)
+    nv, nt, ne, _, _ = m.sizes
+    N2 = nv + ne
+
+    ok, done = s.pisoSteps(max(args.warmup, 3))
+    if not ok:
+        raise SystemExit(f"warm-up failed after {done} steps: {s.stats()}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    clocks = ClockSampler()
+    barrier()
+    if rank == 0:
+        clocks.start()
+    ok, done = s.pisoSteps(args.steps)  # device-timed with CUDA events on the solver's stream
+    st = s.stats()
+    barrier()
+    clk = clocks.stop(set(range(world))) if rank == 0 else None
+    if not ok:
+        raise SystemExit(f"timed steps failed after {done} steps: {st}")
+    ms_total = st["last_step_ms"]
+    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1e3)
+
+    # end to end through the public API with host buffers: per step upload the inlet profile
+    # (H2D), pisoStep, read back u and p (D2H)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.setInletVelocityProfile(profile)
+        if not s.pisoStep():
+            raise SystemExit("e2e step failed")
+        u = s.getVelocity()
+        p = s.getPressure()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps / float(te.item())
+
+    # roofline of the step's SpMV kernels on live data (CUDA events on the solver's stream)
+    peak, peak_kind = measured_peak()
+    traffic = traffic_table()
+    kernels = {}
+    for name, which, per_step in (("momentum_spmv_3rhs", cf.KERNEL_MOMENTUM_SPMV, 2 * st["krylov_iters"][0]),
+                                  ("pressure_cg_spmv", cf.KERNEL_PRESSURE_SPMV, st["krylov_iters"][1])):
+        ms, by = s.profileKernel(which, 50)
+        gbs = by / (ms * 1e-3) / 1e9
+        kernels[name] = {"avg_ms": ms, "alg_bytes": by, "achieved_gbs": gbs,
+                         "launches_timed_region": int(per_step),
+                         "time_share_est": None, "traffic": traffic.get(name)}
+    total_ms = ms_max
+    for k in kernels.values():
+        k["time_share_est"] = k["avg_ms"] * k["launches_timed_region"] / total_ms
+    dom_name = max(kernels, key=lambda k: kernels[k]["time_share_est"])
+    dom = kernels[dom_name]
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": dom["achieved_gbs"], "peak": peak,
+                "unit": "GB/s", "frac": dom["achieved_gbs"] / peak, "peak_kind": peak_kind,
+                "traffic": dom["traffic"]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(m.vertices(), m.tets(), profile, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: procedural cylinder mesh (TetGen unavailable), random-free",
+            "config": dict(workload_desc(m, args.rings, args.layers), parallelism=f"replicas x{world}"),
+            "dof_updates_per_s": value * (3 * N2 + nv),
+            "krylov_iters_per_step": [st["krylov_iters"][0] / args.steps, st["krylov_iters"][1] / args.steps],
+            "gpu_launches": int(st["kernel_launches"]),
+            "roofline": roofline, "kernels": kernels,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(profile.nbytes),
+                    "d2h_bytes_per_step": int(u.nbytes + p.nbytes)},
+            "cpu_baseline": cpu, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,1334 @@
+// Host side of the C ABI declared in include/cfsa_ns.h: device memory, set-up (adjacency,
+// patterns, SELL layout, assembly), the step sequence and its CUDA-graph capture.
+//
+// One PISO step is captured once into a CUDA graph whose two Krylov loops are conditional
+// WHILE nodes: the last reduction kernel of each iteration decides on the device whether the
+// loop continues, so a step (or a batch of steps) runs with no host round trip.
+#include "cfsa_ns.h"
+#include "ns_kernels.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+using namespace cfsa;
+
+namespace {
+
+struct Sell {
+  int *sptr = nullptr, *col = nullptr, *len = nullptr, *perm = nullptr, *posmap = nullptr;
+  int nrows = 0, nrows_pad = 0, nslices = 0;
+  int64_t nentries = 0;
+  SellView view() const { return SellView{sptr, col, len, perm, nrows_pad}; }
+};
+
+struct CudaError {
+  std::string msg;
+};
+
+#define CK(call)                                                                               \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess)                                                                     \
+      throw CudaError{std::string(#call) + ": " + cudaGetErrorString(e_)};                     \
+  } while (0)
+
+inline unsigned int blocks_for(int64_t n) { return (unsigned int)((n + kBlock - 1) / kBlock); }
+
+}  // namespace
+
+struct cfsa_ns {
+  int device = 0;
+  cudaStream_t stream = nullptr, body_stream = nullptr;
+  std::string err;
+  std::vector<void *> allocs;
+
+  int64_t nv = 0, ne = 0, N2 = 0, nt = 0, nbf = 0;
+  double density = 1000, viscosity = 0.001;
+  double dt = 1e-4, tol_mom = 1e-6, tol_p = 1e-8;
+  int maxit_mom = 1000, maxit_p = 1000, ncorr = 1;
+  double relax_u = 1.0, relax_p = 1.0;
+  int outlet_type = CFSA_OUTLET_DIRICHLET;
+  double outlet_pressure = 0.0;
+  int ref_node = -1;
+  int krylov = CFSA_KRYLOV_CG;
+  int precision = CFSA_PRECISION_FP64;
+  double time = 0.0;
+  int64_t steps = 0;
+  float last_ms = 0.f;
+
+  std::vector<signed char> h_bc;  // [N2]
+  std::vector<double> h_inlet;    // [3][N2]
+  std::vector<int> h_rp2, h_rp1;
+
+  // mesh
+  double *xyz = nullptr, *vol = nullptr, *grad = nullptr;
+  int *tnode = nullptr;
+  signed char *bc = nullptr;
+  int *adj_ptr = nullptr, *adj = nullptr;
+  // P2 operators
+  int *rp2 = nullptr, *ci2 = nullptr, *rows2 = nullptr, *dpos2 = nullptr;
+  int64_t nnz2 = 0;
+  double *Mv = nullptr, *Kv = nullptr, *Ms = nullptr, *At = nullptr, *diagA = nullptr, *invA = nullptr;
+  Sell s2;
+  // P1 operators
+  int *rp1 = nullptr, *ci1 = nullptr, *rows1 = nullptr, *dpos1 = nullptr;
+  int64_t nnz1 = 0;
+  double *Gv = nullptr, *Lv = nullptr, *Ls = nullptr, *Lt = nullptr, *diagL = nullptr, *invL = nullptr;
+  Sell s1;
+  double *invm = nullptr;
+  // fields
+  double *u = nullptr, *ustar = nullptr, *p = nullptr, *pc = nullptr, *inlet = nullptr;
+  // work
+  double *ct = nullptr, *divt = nullptr;
+  double *wb = nullptr, *wr = nullptr, *wr0 = nullptr, *wp = nullptr, *wv = nullptr, *ws = nullptr,
+         *wt = nullptr;  // [3][N2]
+  double *pb = nullptr, *pr = nullptr, *pz = nullptr, *pp = nullptr, *pq = nullptr, *ps = nullptr,
+         *pt = nullptr, *pv = nullptr;  // [nv]
+  double *stash = nullptr;
+  // boundary faces
+  int *fverts = nullptr, *ftet = nullptr, *vf_ptr = nullptr, *vf = nullptr;
+  double *fnormal = nullptr, *farea = nullptr, *fshear = nullptr, *fpress = nullptr, *fout = nullptr;
+  // solver states
+  BicgState *bs_mom = nullptr, *bs_p = nullptr;
+  CgState *cs = nullptr;
+  DevStatus *st = nullptr, *st_free = nullptr;
+  Reduce red{};
+  DevStatus *h_st = nullptr;
+  BicgState *h_bs = nullptr;
+  CgState *h_cs = nullptr;
+  double *h_stage = nullptr;  // pinned [3][N2] staging for host transfers
+  BicgState *bs_prof = nullptr;
+  CgState *cs_prof = nullptr;
+  int64_t batch_launches = 0;
+  int64_t batch_iters[2] = {0, 0};
+  int launches_per_step = 0;  // kernels of one step outside the Krylov loop bodies
+
+  bool mom_dirty = true, poisson_dirty = true, graph_dirty = true;
+  bool use_graph = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  template <class T>
+  T *dalloc(size_t count) {
+    void *ptr = nullptr;
+    if (count == 0) count = 1;
+    CK(cudaMalloc(&ptr, count * sizeof(T)));
+    allocs.push_back(ptr);
+    return static_cast<T *>(ptr);
+  }
+  template <class T>
+  T *dupload(const std::vector<T> &h) {
+    T *d = dalloc<T>(h.size());
+    if (!h.empty()) CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    return d;
+  }
+
+  ~cfsa_ns() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void *ptr : allocs) cudaFree(ptr);
+    if (h_st) cudaFreeHost(h_st);
+    if (h_bs) cudaFreeHost(h_bs);
+    if (h_cs) cudaFreeHost(h_cs);
+    if (h_stage) cudaFreeHost(h_stage);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (body_stream) cudaStreamDestroy(body_stream);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  // ------------------------------------------------------------------ set-up
+  void build_sell(int n, const std::vector<int> &rp, Sell &S, const int *d_rp, const int *d_ci) {
+    S.nrows = n;
+    S.nrows_pad = (n + kSellC - 1) / kSellC * kSellC;
+    S.nslices = S.nrows_pad / kSellC;
+    std::vector<int> perm(S.nrows_pad, -1), len(S.nrows_pad, 0);
+    std::vector<int> idx;
+    for (int w0 = 0; w0 < n; w0 += kSellSigma) {
+      const int w1 = std::min(n, w0 + kSellSigma);
+      idx.resize(w1 - w0);
+      std::iota(idx.begin(), idx.end(), w0);
+      std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+        return (rp[a + 1] - rp[a]) > (rp[b + 1] - rp[b]);
+      });
+      for (int k = 0; k < w1 - w0; ++k) {
+        perm[w0 + k] = idx[k];
+        len[w0 + k] = rp[idx[k] + 1] - rp[idx[k]];
+      }
+    }
+    std::vector<int> sptr(S.nslices + 1, 0);
+    for (int s = 0; s < S.nslices; ++s) {
+      int w = 0;
+      for (int k = 0; k < kSellC; ++k) w = std::max(w, len[s * kSellC + k]);
+      sptr[s + 1] = sptr[s] + w * kSellC;
+    }
+    S.nentries = sptr[S.nslices];
+    S.perm = dupload(perm);
+    S.len = dupload(len);
+    S.sptr = dupload(sptr);
+    S.col = dalloc<int>((size_t)S.nentries);
+    CK(cudaMemsetAsync(S.col, 0, (size_t)S.nentries * sizeof(int), stream));
+    S.posmap = dalloc<int>((size_t)rp[n]);
+    k_sell_fill<<<blocks_for(S.nrows_pad), kBlock, 0, stream>>>(S.nrows_pad, S.sptr, S.perm, S.len,
+                                                                d_rp, d_ci, S.col, S.posmap);
+    CK(cudaGetLastError());
+  }
+
+  void build_pattern(bool p2, int nrows, std::vector<int> &h_rp, int *&d_rp, int *&d_ci,
+                     int64_t &nnz, int *d_err) {
+    int *counts = dalloc<int>(nrows);
+    const unsigned int g = (unsigned int)((nrows + 7) / 8);
+    if (p2)
+      k_pattern<true><<<g, kBlock, 0, stream>>>(nrows, (int)nt, adj_ptr, adj, tnode, counts, nullptr,
+                                                nullptr, d_err);
+    else
+      k_pattern<false><<<g, kBlock, 0, stream>>>(nrows, (int)nt, adj_ptr, adj, tnode, counts,
+                                                 nullptr, nullptr, d_err);
+    CK(cudaGetLastError());
+    std::vector<int> hc(nrows);
+    CK(cudaMemcpyAsync(hc.data(), counts, nrows * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (herr) throw CudaError{"sparsity pattern: node " + std::to_string(herr - 1) +
+                              " has more than " + std::to_string(kPatternCap) + " candidate columns"};
+    h_rp.assign(nrows + 1, 0);
+    int64_t acc = 0;
+    for (int i = 0; i < nrows; ++i) {
+      acc += hc[i];
+      if (acc > 0x7fffffffLL) throw CudaError{"matrix has more than 2^31 nonzeros"};
+      h_rp[i + 1] = (int)acc;
+    }
+    nnz = acc;
+    d_rp = dupload(h_rp);
+    d_ci = dalloc<int>((size_t)nnz);
+    if (p2)
+      k_pattern<true><<<g, kBlock, 0, stream>>>(nrows, (int)nt, adj_ptr, adj, tnode, nullptr, d_rp,
+                                                d_ci, d_err);
+    else
+      k_pattern<false><<<g, kBlock, 0, stream>>>(nrows, (int)nt, adj_ptr, adj, tnode, nullptr, d_rp,
+                                                 d_ci, d_err);
+    CK(cudaGetLastError());
+  }
+
+  void setup(const cfsa_mesh_view *m, const cfsa_fluid *f) {
+    CK(cudaGetDevice(&device));
+    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    nv = m->nv;
+    nt = m->nt;
+    ne = m->ne;
+    N2 = nv + ne;
+    density = f->density;
+    viscosity = f->viscosity;
+    if (N2 > 0x7fffffffLL / 3 || nt * 16 > 0x7fffffffLL) throw CudaError{"mesh too large for 32-bit indices"};
+    // host-side node table (SoA) and boundary tags
+    std::vector<int> h_tnode((size_t)nt * 10);
+    for (int64_t t = 0; t < nt; ++t) {
+      for (int a = 0; a < 4; ++a) {
+        const int v = m->tets[4 * t + a];
+        if (v < 0 || v >= nv) throw CudaError{"tet references a vertex out of range"};
+        h_tnode[(size_t)a * nt + t] = v;
+      }
+      for (int e = 0; e < 6; ++e) {
+        const int id = m->tet_edges[6 * t + e];
+        if (id < 0 || id >= ne) throw CudaError{"tet references an edge node out of range"};
+        h_tnode[(size_t)(4 + e) * nt + t] = (int)nv + id;
+      }
+    }
+    h_bc.assign((size_t)N2, (signed char)BC_UNDEFINED);
+    for (int64_t i = 0; i < nv; ++i) h_bc[i] = m->p1_bc ? m->p1_bc[i] : BC_UNDEFINED;
+    for (int64_t k = 0; k < ne; ++k) h_bc[nv + k] = m->p2_bc ? m->p2_bc[k] : BC_UNDEFINED;
+    // node -> incident tets, ascending tet order; entry = tet*16 + local node index
+    std::vector<int> h_adj_ptr((size_t)N2 + 1, 0), h_adj((size_t)nt * 10);
+    for (int64_t t = 0; t < nt; ++t)
+      for (int l = 0; l < 10; ++l) h_adj_ptr[h_tnode[(size_t)l * nt + t] + 1]++;
+    for (int64_t i = 0; i < N2; ++i) h_adj_ptr[i + 1] += h_adj_ptr[i];
+    {
+      std::vector<int> fill(h_adj_ptr.begin(), h_adj_ptr.end() - 1);
+      for (int64_t t = 0; t < nt; ++t)
+        for (int l = 0; l < 10; ++l) h_adj[fill[h_tnode[(size_t)l * nt + t]]++] = (int)(t * 16 + l);
+    }
+    std::vector<double> h_xyz(m->vertices, m->vertices + 3 * nv);
+    xyz = dupload(h_xyz);
+    tnode = dupload(h_tnode);
+    bc = dupload(h_bc);
+    adj_ptr = dupload(h_adj_ptr);
+    adj = dupload(h_adj);
+    vol = dalloc<double>(nt);
+    grad = dalloc<double>((size_t)nt * 12);
+    k_geometry<<<blocks_for(nt), kBlock, 0, stream>>>((int)nt, xyz, tnode, vol, grad);
+    CK(cudaGetLastError());
+    int *d_err = dalloc<int>(1);
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+    build_pattern(true, (int)N2, h_rp2, rp2, ci2, nnz2, d_err);
+    build_pattern(false, (int)nv, h_rp1, rp1, ci1, nnz1, d_err);
+    rows2 = dalloc<int>((size_t)nnz2);
+    rows1 = dalloc<int>((size_t)nnz1);
+    dpos2 = dalloc<int>((size_t)N2);
+    dpos1 = dalloc<int>((size_t)nv);
+    k_row_of_slot<<<blocks_for(N2), kBlock, 0, stream>>>((int)N2, rp2, rows2);
+    k_row_of_slot<<<blocks_for(nv), kBlock, 0, stream>>>((int)nv, rp1, rows1);
+    k_diag_pos<<<blocks_for(N2), kBlock, 0, stream>>>((int)N2, rp2, ci2, dpos2);
+    k_diag_pos<<<blocks_for(nv), kBlock, 0, stream>>>((int)nv, rp1, ci1, dpos1);
+    CK(cudaGetLastError());
+    build_sell((int)N2, h_rp2, s2, rp2, ci2);
+    build_sell((int)nv, h_rp1, s1, rp1, ci1);
+    Mv = dalloc<double>((size_t)nnz2);
+    Kv = dalloc<double>((size_t)nnz2);
+    Ms = dalloc<double>((size_t)s2.nentries);
+    At = dalloc<double>((size_t)s2.nentries);
+    CK(cudaMemsetAsync(Ms, 0, (size_t)s2.nentries * sizeof(double), stream));
+    CK(cudaMemsetAsync(At, 0, (size_t)s2.nentries * sizeof(double), stream));
+    diagA = dalloc<double>(N2);
+    invA = dalloc<double>(N2);
+    Gv = dalloc<double>((size_t)nnz1 * 3);
+    Lv = dalloc<double>((size_t)nnz1);
+    Ls = dalloc<double>((size_t)s1.nentries);
+    Lt = dalloc<double>((size_t)s1.nentries);
+    CK(cudaMemsetAsync(Ls, 0, (size_t)s1.nentries * sizeof(double), stream));
+    CK(cudaMemsetAsync(Lt, 0, (size_t)s1.nentries * sizeof(double), stream));
+    diagL = dalloc<double>(nv);
+    invL = dalloc<double>(nv);
+    invm = dalloc<double>(N2);
+    // fields and work
+    const size_t n3 = (size_t)3 * N2;
+    u = dalloc<double>(n3);
+    ustar = dalloc<double>(n3);
+    inlet = dalloc<double>(n3);
+    p = dalloc<double>(nv);
+    pc = dalloc<double>(nv);
+    for (double **w : {&wb, &wr, &wr0, &wp, &wv, &ws, &wt}) *w = dalloc<double>(n3);
+    for (double **w : {&pb, &pr, &pz, &pp, &pq, &ps, &pt, &pv}) *w = dalloc<double>(nv);
+    ct = dalloc<double>((size_t)nt * 3);
+    divt = dalloc<double>(nt);
+    stash = dalloc<double>(1);
+    for (double *w : {u, ustar, inlet}) CK(cudaMemsetAsync(w, 0, n3 * sizeof(double), stream));
+    CK(cudaMemsetAsync(p, 0, nv * sizeof(double), stream));
+    CK(cudaMemsetAsync(pc, 0, nv * sizeof(double), stream));
+    h_inlet.assign(n3, 0.0);
+    // reductions and states
+    const int64_t maxrows = std::max<int64_t>({(int64_t)s2.nrows_pad, nt, N2});
+    red.partials = dalloc<double>((size_t)(blocks_for(maxrows) + 1) * kMaxRed);
+    red.counter = dalloc<unsigned int>(1);
+    CK(cudaMemsetAsync(red.counter, 0, sizeof(unsigned int), stream));
+    bs_mom = dalloc<BicgState>(1);
+    bs_p = dalloc<BicgState>(1);
+    cs = dalloc<CgState>(1);
+    st = dalloc<DevStatus>(1);
+    st_free = dalloc<DevStatus>(1);
+    CK(cudaMemsetAsync(bs_mom, 0, sizeof(BicgState), stream));
+    CK(cudaMemsetAsync(bs_p, 0, sizeof(BicgState), stream));
+    CK(cudaMemsetAsync(cs, 0, sizeof(CgState), stream));
+    CK(cudaMemsetAsync(st, 0, sizeof(DevStatus), stream));
+    CK(cudaMemsetAsync(st_free, 0, sizeof(DevStatus), stream));
+    CK(cudaMallocHost(&h_st, sizeof(DevStatus)));
+    CK(cudaMallocHost(&h_bs, 2 * sizeof(BicgState)));
+    CK(cudaMallocHost(&h_cs, sizeof(CgState)));
+    CK(cudaMallocHost(&h_stage, n3 * sizeof(double)));
+    bs_prof = dalloc<BicgState>(1);
+    cs_prof = dalloc<CgState>(1);
+    // boundary faces
+    nbf = m->nbf;
+    if (nbf > 0) {
+      std::vector<int> hv(m->bface_verts, m->bface_verts + 3 * nbf), ht(m->bface_tet, m->bface_tet + nbf);
+      std::vector<double> hn(m->bface_normal, m->bface_normal + 3 * nbf), ha(m->bface_area, m->bface_area + nbf);
+      std::vector<int> hvp((size_t)nv + 1, 0), hvf((size_t)nbf * 3);
+      for (int64_t fi = 0; fi < nbf; ++fi)
+        for (int k = 0; k < 3; ++k) {
+          if (hv[3 * fi + k] < 0 || hv[3 * fi + k] >= nv) throw CudaError{"boundary face vertex out of range"};
+          hvp[hv[3 * fi + k] + 1]++;
+        }
+      for (int64_t i = 0; i < nv; ++i) hvp[i + 1] += hvp[i];
+      std::vector<int> fill(hvp.begin(), hvp.end() - 1);
+      for (int64_t fi = 0; fi < nbf; ++fi)
+        for (int k = 0; k < 3; ++k) hvf[fill[hv[3 * fi + k]]++] = (int)fi;
+      fverts = dupload(hv);
+      ftet = dupload(ht);
+      fnormal = dupload(hn);
+      farea = dupload(ha);
+      vf_ptr = dupload(hvp);
+      vf = dupload(hvf);
+      fshear = dalloc<double>((size_t)nbf * 3);
+      fpress = dalloc<double>((size_t)nbf * 3);
+    }
+    fout = dalloc<double>((size_t)nv * 3);
+    assemble();
+    if (const char *e = std::getenv("CFSA_NO_GRAPH")) use_graph = (std::atoi(e) == 0);
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  // buildMassMatrix + buildStiffnessMatrix + buildGradientMatrices + buildPoissonMatrix
+  void assemble() {
+    k_geometry<<<blocks_for(nt), kBlock, 0, stream>>>((int)nt, xyz, tnode, vol, grad);
+    k_assemble_p2<<<blocks_for(N2), kBlock, 0, stream>>>((int)N2, (int)nt, density, 1.0 / viscosity,
+                                                         adj_ptr, adj, tnode, vol, grad, rp2, ci2, Mv, Kv);
+    k_assemble_p1<<<blocks_for(nv), kBlock, 0, stream>>>((int)nv, (int)nt, nnz1, adj_ptr, adj, tnode,
+                                                         vol, grad, rp1, ci1, Gv, Lv);
+    k_lumped_mass<<<blocks_for(N2), kBlock, 0, stream>>>((int)N2, rp2, Mv, invm);
+    CK(cudaGetLastError());
+    mom_dirty = poisson_dirty = true;
+  }
+
+  void ensure_operators() {
+    if (mom_dirty) {
+      k_momentum_diag<<<blocks_for(N2), kBlock, 0, stream>>>((int)N2, dt, dpos2, Mv, Kv, bc, diagA, invA);
+      k_momentum_sell<<<blocks_for(nnz2), kBlock, 0, stream>>>(nnz2, dt, s2.posmap, rows2, ci2, Mv, Kv,
+                                                               bc, invA, At, Ms);
+      CK(cudaGetLastError());
+      mom_dirty = false;
+    }
+    if (poisson_dirty) {
+      k_poisson_diag<<<blocks_for(nv), kBlock, 0, stream>>>((int)nv, outlet_type, ref_node, dpos1, Lv,
+                                                            bc, diagL, invL);
+      k_poisson_sell<<<blocks_for(nnz1), kBlock, 0, stream>>>(nnz1, outlet_type, ref_node, s1.posmap,
+                                                              rows1, ci1, Lv, bc, invL, Ls, Lt);
+      CK(cudaGetLastError());
+      poisson_dirty = false;
+    }
+  }
+
+  // ------------------------------------------------------------------ Krylov loops
+  // Appends a WHILE conditional node to the graph being captured on `stream`; its body (one
+  // Krylov iteration) is captured from `body` on body_stream. Returns the handle.
+  template <class Body>
+  void capture_while(Body body) {
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(stream, &cst, nullptr, &g, &deps, &ndeps));
+    if (cst != cudaStreamCaptureStatusActive) throw CudaError{"stream is not capturing"};
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
+    CK(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(body_stream, bodyg, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeRelaxed));
+    body(body_stream, h, 1);
+    cudaGraph_t out = nullptr;
+    CK(cudaStreamEndCapture(body_stream, &out));
+  }
+
+  // Eager loop: enqueue iterations in growing chunks and poll the active flag in between.
+  template <class Body, class ActiveFn>
+  void eager_while(Body body, ActiveFn active_of, int maxit) {
+    int done = 0, chunk = 2;
+    while (done <= maxit) {
+      for (int k = 0; k < chunk; ++k) body(stream, (cudaGraphConditionalHandle)0, 0);
+      done += chunk;
+      if (!active_of()) break;
+      chunk = std::min(chunk * 2, 64);
+    }
+  }
+
+  template <int NC>
+  void bicg_body(BicgArgs a, cudaStream_t s, int nrows_pad, int n) {
+    const unsigned int gs = blocks_for(nrows_pad), gp = blocks_for(n);
+    k_bicg_p<NC><<<gs, kBlock, 0, s>>>(a);
+    k_bicg_v<NC><<<gs, kBlock, 0, s>>>(a);
+    k_bicg_s<NC><<<gp, kBlock, 0, s>>>(a);
+    k_bicg_t<NC><<<gs, kBlock, 0, s>>>(a);
+    k_bicg_xr<NC><<<gp, kBlock, 0, s>>>(a);
+  }
+
+  bool poll_bicg(const BicgState *d) {
+    CK(cudaMemcpyAsync(h_bs, d, sizeof(BicgState), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    return h_bs->active != 0;
+  }
+  bool poll_cg() {
+    CK(cudaMemcpyAsync(h_cs, cs, sizeof(CgState), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    return h_cs->active != 0;
+  }
+
+  BicgArgs momentum_args() {
+    BicgArgs a{};
+    a.S = s2.view();
+    a.At = At;
+    a.diagA = diagA;
+    a.invA = invA;
+    a.b = wb;
+    a.x = ustar;
+    a.r = wr;
+    a.r0 = wr0;
+    a.pk = wp;
+    a.v = wv;
+    a.s = ws;
+    a.t = wt;
+    a.n = (int)N2;
+    a.bs = bs_mom;
+    a.red = red;
+    a.st = st;
+    a.slot = 0;
+    return a;
+  }
+
+  // ------------------------------------------------------------------ step phases
+  void enqueue_momentum(bool capture) {
+    k_tet_conv<<<blocks_for(nt), kBlock, 0, stream>>>((int)nt, N2, tnode, grad, u, ct, st);
+    MomentumRhsArgs m{};
+    m.S = s2.view();
+    m.Ms = Ms;
+    m.G = CsrView{rp1, ci1};
+    m.Gv = Gv;
+    m.nnz1 = nnz1;
+    m.adj_ptr = adj_ptr;
+    m.adj = adj;
+    m.vol = vol;
+    m.ct = ct;
+    m.bc = bc;
+    m.inlet = inlet;
+    m.u = u;
+    m.p = p;
+    m.dt = dt;
+    m.tol = tol_mom;
+    m.n = (int)N2;
+    m.nv = (int)nv;
+    m.nt = (int)nt;
+    m.maxit = maxit_mom;
+    m.b = wb;
+    m.x = ustar;
+    m.r = wr;
+    m.r0 = wr0;
+    m.pk = wp;
+    m.v = wv;
+    m.bs = bs_mom;
+    m.st = st;
+    m.red = red;
+    k_momentum_rhs<<<blocks_for(s2.nrows_pad), kBlock, 0, stream>>>(m);
+    CK(cudaGetLastError());
+    BicgArgs a = momentum_args();
+    auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
+      BicgArgs b = a;
+      b.cond = h;
+      b.use_cond = use;
+      bicg_body<3>(b, s, s2.nrows_pad, (int)N2);
+    };
+    if (capture)
+      capture_while(body);
+    else
+      eager_while(body, [&] { return poll_bicg(bs_mom); }, maxit_mom);
+    k_check_bicg<<<1, 1, 0, stream>>>(bs_mom, 3, 0, st);
+    CK(cudaGetLastError());
+  }
+
+  void enqueue_pressure_solve(bool capture) {
+    k_tet_div<<<blocks_for(nt), kBlock, 0, stream>>>((int)nt, N2, tnode, grad, ustar, divt, st);
+    PressureRhsArgs a{};
+    a.adj_ptr = adj_ptr;
+    a.adj = adj;
+    a.vol = vol;
+    a.divt = divt;
+    a.bc = bc;
+    a.invL = invL;
+    a.dt = dt;
+    a.tol = tol_p;
+    a.outlet_pressure = outlet_pressure;
+    a.nv = (int)nv;
+    a.outlet_type = outlet_type;
+    a.ref_node = ref_node;
+    a.maxit = maxit_p;
+    a.krylov = (krylov == CFSA_KRYLOV_BICGSTAB) ? 1 : 0;
+    a.b = pb;
+    a.x = pc;
+    a.r = pr;
+    a.z_or_r0 = pz;
+    a.pk = pp;
+    a.v = pv;
+    a.cs = cs;
+    a.bs = bs_p;
+    a.st = st;
+    a.red = red;
+    k_pressure_rhs<<<blocks_for(nv), kBlock, 0, stream>>>(a);
+    CK(cudaGetLastError());
+    if (krylov == CFSA_KRYLOV_BICGSTAB) {
+      BicgArgs b{};
+      b.S = s1.view();
+      b.At = Lt;
+      b.diagA = diagL;
+      b.invA = invL;
+      b.b = pb;
+      b.x = pc;
+      b.r = pr;
+      b.r0 = pz;
+      b.pk = pp;
+      b.v = pv;
+      b.s = ps;
+      b.t = pt;
+      b.n = (int)nv;
+      b.bs = bs_p;
+      b.red = red;
+      b.st = st;
+      b.slot = 1;
+      auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
+        BicgArgs c = b;
+        c.cond = h;
+        c.use_cond = use;
+        bicg_body<1>(c, s, s1.nrows_pad, (int)nv);
+      };
+      if (capture)
+        capture_while(body);
+      else
+        eager_while(body, [&] { return poll_bicg(bs_p); }, maxit_p);
+      k_check_bicg<<<1, 1, 0, stream>>>(bs_p, 1, 1, st);
+    } else {
+      CgArgs c{};
+      c.S = s1.view();
+      c.Ls = Ls;
+      c.invL = invL;
+      c.x = pc;
+      c.r = pr;
+      c.z = pz;
+      c.pk = pp;
+      c.q = pq;
+      c.n = (int)nv;
+      c.cs = cs;
+      c.red = red;
+      c.st = st;
+      auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
+        CgArgs d = c;
+        d.cond = h;
+        d.use_cond = use;
+        k_cg_q<<<blocks_for(s1.nrows_pad), kBlock, 0, s>>>(d);
+        k_cg_xr<<<blocks_for(nv), kBlock, 0, s>>>(d);
+        k_cg_p<<<blocks_for(nv), kBlock, 0, s>>>(d);
+      };
+      if (capture)
+        capture_while(body);
+      else
+        eager_while(body, [&] { return poll_cg(); }, maxit_p);
+      k_check_cg<<<1, 1, 0, stream>>>(cs, st);
+    }
+    CK(cudaGetLastError());
+  }
+
+  void enqueue_pressure_update() {
+    k_pressure_update<<<blocks_for(nv), kBlock, 0, stream>>>((int)nv, relax_p, outlet_type,
+                                                             outlet_pressure, bc, pc, p, st);
+    if (ref_node >= 0 && ref_node < nv) {
+      k_pressure_stash<<<1, 1, 0, stream>>>(ref_node, p, stash, st);
+      k_pressure_normalize<<<blocks_for(nv), kBlock, 0, stream>>>((int)nv, stash, p, st);
+    }
+    CK(cudaGetLastError());
+  }
+
+  void enqueue_correct() {
+    CorrectArgs c{};
+    c.G = CsrView{rp1, ci1};
+    c.Gv = Gv;
+    c.nnz1 = nnz1;
+    c.invm = invm;
+    c.pc = pc;
+    c.ustar = ustar;
+    c.inlet = inlet;
+    c.bc = bc;
+    c.dt = dt;
+    c.relax_u = relax_u;
+    c.n = (int)N2;
+    c.nv = (int)nv;
+    c.u = u;
+    c.st = st;
+    k_correct_velocity<<<blocks_for(N2), kBlock, 0, stream>>>(c);
+    CK(cudaGetLastError());
+  }
+
+  void enqueue_finish() {
+    FinishArgs f{};
+    f.bc = bc;
+    f.inlet = inlet;
+    f.u = u;
+    f.ustar = ustar;
+    f.p = p;
+    f.pc = pc;
+    f.n = (int)N2;
+    f.nv = (int)nv;
+    f.st = st;
+    f.red = red;
+    k_finish_step<<<blocks_for(N2), kBlock, 0, stream>>>(f);
+    CK(cudaGetLastError());
+  }
+
+  // pisoStep (ncorr correctors) or simpleStep (one corrector). The 2nd and later correctors of
+  // the reference solve the identical system again (the divergence is always that of u*), so
+  // their pressure correction is the first one's; only the p update and u correction repeat.
+  void enqueue_step(bool capture, bool simple) {
+    enqueue_momentum(capture);
+    const int nc = simple ? 1 : ncorr;
+    const bool normalize = (ref_node >= 0 && ref_node < nv);
+    for (int c = 0; c < nc; ++c) {
+      if (c == 0) enqueue_pressure_solve(capture);
+      enqueue_pressure_update();
+      enqueue_correct();
+    }
+    enqueue_finish();
+    // tet_conv, momentum_rhs, check, [tet_div, pressure_rhs, check], per corrector
+    // update (+ stash + normalize) and correct, finish
+    launches_per_step = 3 + (nc > 0 ? 3 : 0) + nc * (2 + (normalize ? 2 : 0)) + 1;
+  }
+
+  void ensure_graph() {
+    if (!graph_dirty && graph_exec) return;
+    if (graph_exec) {
+      CK(cudaGraphExecDestroy(graph_exec));
+      graph_exec = nullptr;
+    }
+    if (graph) {
+      CK(cudaGraphDestroy(graph));
+      graph = nullptr;
+    }
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+    try {
+      enqueue_step(true, false);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CK(cudaStreamEndCapture(stream, &graph));
+    CK(cudaGraphInstantiate(&graph_exec, graph, 0));
+    graph_dirty = false;
+  }
+
+  void reset_status() { CK(cudaMemsetAsync(st, 0, sizeof(DevStatus), stream)); }
+
+  int finish_batch(int launched_steps) {
+    CK(cudaMemcpyAsync(h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+    CK(cudaEventSynchronize(ev1));
+    CK(cudaStreamSynchronize(stream));
+    CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
+    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : 3;
+    batch_launches = (int64_t)launched_steps * launches_per_step + 5 * (int64_t)h_st->body_runs[0] +
+                     pressure_body * (int64_t)h_st->body_runs[1];
+    batch_iters[0] = (int64_t)h_st->iters[0];
+    batch_iters[1] = (int64_t)h_st->iters[1];
+    for (int64_t k = 0; k < h_st->steps_done; ++k) time += dt;
+    steps += h_st->steps_done;
+    return h_st->code;
+  }
+
+  int run_steps(int n, int *n_done, bool simple) {
+    ensure_operators();
+    reset_status();
+    int launched = 0;
+    if (use_graph && !simple) {
+      ensure_graph();
+      CK(cudaEventRecord(ev0, stream));
+      for (int k = 0; k < n; ++k) CK(cudaGraphLaunch(graph_exec, stream));
+      launched = n;
+      CK(cudaEventRecord(ev1, stream));
+    } else {
+      CK(cudaEventRecord(ev0, stream));
+      for (int k = 0; k < n; ++k) {
+        enqueue_step(false, simple);
+        ++launched;
+        CK(cudaMemcpyAsync(h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        if (h_st->halt) break;
+      }
+      CK(cudaEventRecord(ev1, stream));
+    }
+    const int code = finish_batch(launched);
+    if (n_done) *n_done = h_st->steps_done;
+    return code;
+  }
+
+  // [N2][3] host layout <-> component-major device layout through pinned staging.
+  void download_vec3(const double *d, double *out) {
+    CK(cudaMemcpyAsync(h_stage, d, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    const double *hx = h_stage, *hy = h_stage + N2, *hz = h_stage + 2 * N2;
+    for (int64_t i = 0; i < N2; ++i) {
+      out[3 * i] = hx[i];
+      out[3 * i + 1] = hy[i];
+      out[3 * i + 2] = hz[i];
+    }
+  }
+  void upload_vec3(const double *in, double *d) {
+    CK(cudaStreamSynchronize(stream));  // staging may still feed an earlier copy
+    double *hx = h_stage, *hy = h_stage + N2, *hz = h_stage + 2 * N2;
+    for (int64_t i = 0; i < N2; ++i) {
+      hx[i] = in[3 * i];
+      hy[i] = in[3 * i + 1];
+      hz[i] = in[3 * i + 2];
+    }
+    CK(cudaMemcpyAsync(d, h_stage, (size_t)3 * N2 * sizeof(double), cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  // Kernel timing on the live data with private Krylov states (solver state untouched).
+  void profile_kernel(int which, int iters, double *avg_ms, double *alg_bytes) {
+    ensure_operators();
+    CK(cudaStreamSynchronize(stream));
+    if (which == CFSA_KERNEL_MOMENTUM_SPMV) {
+      BicgState hs{};
+      hs.active = 7;
+      hs.ncomp = 3;
+      for (int c = 0; c < 3; ++c) hs.rho[c] = 1.0;
+      CK(cudaMemcpyAsync(bs_prof, &hs, sizeof(hs), cudaMemcpyHostToDevice, stream));
+      BicgArgs a = momentum_args();
+      a.bs = bs_prof;
+      a.st = nullptr;
+      a.v = ws;  // scratch output
+      const unsigned int g = blocks_for(s2.nrows_pad);
+      k_bicg_v<3><<<g, kBlock, 0, stream>>>(a);  // warm-up
+      CK(cudaEventRecord(ev0, stream));
+      for (int k = 0; k < iters; ++k) k_bicg_v<3><<<g, kBlock, 0, stream>>>(a);
+      CK(cudaEventRecord(ev1, stream));
+      *alg_bytes = 12.0 * (double)nnz2 + 8.0 * s2.nrows_pad + 4.0 * (s2.nslices + 1) + 72.0 * (double)N2;
+    } else if (which == CFSA_KERNEL_PRESSURE_SPMV) {
+      CgState hc{};
+      hc.active = 1;
+      hc.absnew = 1.0;
+      CK(cudaMemcpyAsync(cs_prof, &hc, sizeof(hc), cudaMemcpyHostToDevice, stream));
+      CgArgs c{};
+      c.S = s1.view();
+      c.Ls = Ls;
+      c.invL = invL;
+      c.x = pc;
+      c.r = pr;
+      c.z = pz;
+      c.pk = pp;
+      c.q = ps;  // scratch output
+      c.n = (int)nv;
+      c.cs = cs_prof;
+      c.red = red;
+      c.st = nullptr;
+      const unsigned int g = blocks_for(s1.nrows_pad);
+      k_cg_q<<<g, kBlock, 0, stream>>>(c);
+      CK(cudaEventRecord(ev0, stream));
+      for (int k = 0; k < iters; ++k) k_cg_q<<<g, kBlock, 0, stream>>>(c);
+      CK(cudaEventRecord(ev1, stream));
+      *alg_bytes = 12.0 * (double)nnz1 + 8.0 * s1.nrows_pad + 4.0 * (s1.nslices + 1) + 16.0 * (double)nv;
+    } else {
+      throw CudaError{"unknown kernel id"};
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    *avg_ms = (double)ms / (double)std::max(1, iters);
+  }
+};
+
+namespace {
+
+int fail(cfsa_ns *h, int code, const std::string &msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+template <class F>
+int guarded(cfsa_ns *h, F &&f) {
+  try {
+    return f();
+  } catch (const CudaError &e) {
+    return fail(h, CFSA_CUDA_ERROR, e.msg);
+  } catch (const std::bad_alloc &) {
+    return fail(h, CFSA_CUDA_ERROR, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(h, CFSA_BAD_ARG, e.what());
+  }
+}
+
+std::string g_create_error;
+
+}  // namespace
+
+extern "C" {
+
+int cfsa_ns_create(const cfsa_mesh_view *mesh, const cfsa_fluid *fluid, cfsa_ns **out) {
+  if (!mesh || !fluid || !out || mesh->nv <= 0 || mesh->nt <= 0 || mesh->ne < 0 || !mesh->vertices ||
+      !mesh->tets || !mesh->tet_edges) {
+    g_create_error = "cfsa_ns_create: bad arguments";
+    return CFSA_BAD_ARG;
+  }
+  if (!(fluid->viscosity > 0.0) || !(fluid->density > 0.0)) {
+    g_create_error = "cfsa_ns_create: density and viscosity must be positive";
+    return CFSA_BAD_ARG;
+  }
+  cfsa_ns *h = new (std::nothrow) cfsa_ns();
+  if (!h) return CFSA_CUDA_ERROR;
+  int code = guarded(h, [&] {
+    h->setup(mesh, fluid);
+    return CFSA_OK;
+  });
+  if (code != CFSA_OK) {
+    g_create_error = h->err;
+    delete h;
+    *out = nullptr;
+    return code;
+  }
+  *out = h;
+  return CFSA_OK;
+}
+
+void cfsa_ns_destroy(cfsa_ns *h) { delete h; }
+
+const char *cfsa_ns_last_error(const cfsa_ns *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int cfsa_ns_sizes(const cfsa_ns *h, int64_t out[4]) {
+  if (!h || !out) return CFSA_BAD_ARG;
+  out[0] = h->nv;
+  out[1] = h->ne;
+  out[2] = h->N2;
+  out[3] = h->nt;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_dt(cfsa_ns *h, double dt) {
+  if (!h) return CFSA_BAD_ARG;
+  if (!(dt > 0.0)) return fail(h, CFSA_BAD_ARG, "dt must be positive");
+  if (dt != h->dt) h->mom_dirty = h->graph_dirty = true;
+  h->dt = dt;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_tolerances(cfsa_ns *h, double momentum, double pressure) {
+  if (!h) return CFSA_BAD_ARG;
+  if (!(momentum > 0.0) || !(pressure > 0.0)) return fail(h, CFSA_BAD_ARG, "tolerances must be positive");
+  h->tol_mom = momentum;
+  h->tol_p = pressure;
+  h->graph_dirty = true;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_max_iterations(cfsa_ns *h, int momentum, int pressure) {
+  if (!h) return CFSA_BAD_ARG;
+  if (momentum < 1 || pressure < 1) return fail(h, CFSA_BAD_ARG, "iteration caps must be >= 1");
+  h->maxit_mom = momentum;
+  h->maxit_p = pressure;
+  h->graph_dirty = true;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_num_corrections(cfsa_ns *h, int n) {
+  if (!h) return CFSA_BAD_ARG;
+  if (n < 0) return fail(h, CFSA_BAD_ARG, "number of corrections must be >= 0");
+  h->ncorr = n;
+  h->graph_dirty = true;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_relaxation(cfsa_ns *h, double relax_u, double relax_p) {
+  if (!h) return CFSA_BAD_ARG;
+  h->relax_u = relax_u;
+  h->relax_p = relax_p;
+  h->graph_dirty = true;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_outlet(cfsa_ns *h, int outlet_type, double outlet_pressure) {
+  if (!h) return CFSA_BAD_ARG;
+  if (outlet_type < 0 || outlet_type > 2) return fail(h, CFSA_BAD_ARG, "bad outlet type");
+  h->outlet_type = outlet_type;
+  h->outlet_pressure = outlet_pressure;
+  h->poisson_dirty = h->graph_dirty = true;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_reference_node(cfsa_ns *h, int node) {
+  if (!h) return CFSA_BAD_ARG;
+  h->ref_node = node;
+  h->poisson_dirty = h->graph_dirty = true;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_inlet_uniform(cfsa_ns *h, const double u[3]) {
+  if (!h || !u) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    for (int c = 0; c < 3; ++c)
+      std::fill(h->h_inlet.begin() + (size_t)c * h->N2, h->h_inlet.begin() + (size_t)(c + 1) * h->N2, u[c]);
+    CK(cudaMemcpyAsync(h->inlet, h->h_inlet.data(), h->h_inlet.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u) {
+  if (!h || !u) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    for (int64_t i = 0; i < h->N2; ++i)
+      for (int c = 0; c < 3; ++c) h->h_inlet[(size_t)c * h->N2 + i] = u[3 * i + c];
+    CK(cudaMemcpyAsync(h->inlet, h->h_inlet.data(), h->h_inlet.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov) {
+  if (!h) return CFSA_BAD_ARG;
+  if (krylov != CFSA_KRYLOV_CG && krylov != CFSA_KRYLOV_BICGSTAB)
+    return fail(h, CFSA_BAD_ARG, "unknown Krylov method");
+  h->krylov = krylov;
+  h->graph_dirty = true;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_precision(cfsa_ns *h, int precision) {
+  if (!h) return CFSA_BAD_ARG;
+  if (precision != CFSA_PRECISION_FP64)
+    return fail(h, CFSA_UNSUPPORTED, "only CFSA_PRECISION_FP64 is available in this build");
+  h->precision = precision;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_viscosity(cfsa_ns *h, double viscosity) {
+  if (!h) return CFSA_BAD_ARG;
+  if (!(viscosity > 0.0)) return fail(h, CFSA_BAD_ARG, "viscosity must be positive");
+  return guarded(h, [&] {
+    h->viscosity = viscosity;
+    h->assemble();
+    h->graph_dirty = true;
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_initialize_fields(cfsa_ns *h) {
+  if (!h) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    const size_t n3 = (size_t)3 * h->N2;
+    std::vector<double> u0(n3, 0.0);
+    for (int64_t i = 0; i < h->N2; ++i)
+      if (h->h_bc[i] == BC_INLET)
+        for (int c = 0; c < 3; ++c) u0[(size_t)c * h->N2 + i] = h->h_inlet[(size_t)c * h->N2 + i];
+    CK(cudaMemcpyAsync(h->u, u0.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->ustar, 0, n3 * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(h->p, 0, h->nv * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(h->pc, 0, h->nv * sizeof(double), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->time = 0.0;
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_assemble(cfsa_ns *h) {
+  if (!h) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    h->assemble();
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_update_vertices(cfsa_ns *h, const double *xyz) {
+  if (!h || !xyz) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    CK(cudaMemcpyAsync(h->xyz, xyz, (size_t)3 * h->nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    h->assemble();
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_update_boundary_tags(cfsa_ns *h, const int8_t *p1_bc, const int8_t *p2_bc) {
+  if (!h) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    if (p1_bc)
+      for (int64_t i = 0; i < h->nv; ++i) h->h_bc[i] = p1_bc[i];
+    if (p2_bc)
+      for (int64_t k = 0; k < h->ne; ++k) h->h_bc[h->nv + k] = p2_bc[k];
+    CK(cudaMemcpyAsync(h->bc, h->h_bc.data(), h->h_bc.size(), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->mom_dirty = h->poisson_dirty = h->graph_dirty = true;
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_piso_steps(cfsa_ns *h, int n, int *n_done) {
+  if (!h) return CFSA_BAD_ARG;
+  if (n < 0) return fail(h, CFSA_BAD_ARG, "negative step count");
+  return guarded(h, [&] {
+    const int code = h->run_steps(n, n_done, false);
+    if (code != CFSA_OK) h->err = "step failed with status " + std::to_string(code);
+    return code;
+  });
+}
+
+int cfsa_ns_piso_step(cfsa_ns *h) { return cfsa_ns_piso_steps(h, 1, nullptr); }
+
+int cfsa_ns_simple_step(cfsa_ns *h) {
+  if (!h) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    const int code = h->run_steps(1, nullptr, true);
+    if (code != CFSA_OK) h->err = "step failed with status " + std::to_string(code);
+    return code;
+  });
+}
+
+int cfsa_ns_momentum_predictor(cfsa_ns *h) {
+  if (!h) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    h->ensure_operators();
+    h->reset_status();
+    h->enqueue_momentum(false);
+    CK(cudaMemcpyAsync(h->h_st, h->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return h->h_st->code;
+  });
+}
+
+int cfsa_ns_pressure_poisson(cfsa_ns *h) {
+  if (!h) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    h->ensure_operators();
+    h->reset_status();
+    h->enqueue_pressure_solve(false);
+    h->enqueue_pressure_update();
+    CK(cudaMemcpyAsync(h->h_st, h->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return h->h_st->code;
+  });
+}
+
+int cfsa_ns_correct_velocity(cfsa_ns *h) {
+  if (!h) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    h->reset_status();
+    h->enqueue_correct();
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_get_velocity(cfsa_ns *h, double *u) {
+  if (!h || !u) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    h->download_vec3(h->u, u);
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_get_velocity_star(cfsa_ns *h, double *u) {
+  if (!h || !u) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    h->download_vec3(h->ustar, u);
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_get_pressure(cfsa_ns *h, double *p) {
+  if (!h || !p) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    CK(cudaMemcpyAsync(p, h->p, h->nv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_get_pressure_correction(cfsa_ns *h, double *p) {
+  if (!h || !p) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    CK(cudaMemcpyAsync(p, h->pc, h->nv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_set_fields(cfsa_ns *h, const double *u, const double *p) {
+  if (!h) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    if (u) h->upload_vec3(u, h->u);
+    if (p) {
+      CK(cudaMemcpyAsync(h->p, p, h->nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+    }
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_get_time(const cfsa_ns *h, double *t) {
+  if (!h || !t) return CFSA_BAD_ARG;
+  *t = h->time;
+  return CFSA_OK;
+}
+
+int cfsa_ns_get_stats(const cfsa_ns *hc, cfsa_ns_stats *s) {
+  if (!hc || !s) return CFSA_BAD_ARG;
+  cfsa_ns *h = const_cast<cfsa_ns *>(hc);
+  return guarded(h, [&] {
+    CK(cudaMemcpyAsync(h->h_bs, h->bs_mom, sizeof(BicgState), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_bs + 1, h->bs_p, sizeof(BicgState), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_cs, h->cs, sizeof(CgState), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    std::memset(s, 0, sizeof(*s));
+    for (int c = 0; c < 3; ++c) {
+      s->momentum_iters[c] = h->h_bs[0].iters[c];
+      const double b2 = h->h_bs[0].bnorm2[c];
+      s->momentum_residual[c] = b2 > 0 ? std::sqrt(h->h_bs[0].rnorm2[c] / b2) : 0.0;
+    }
+    if (h->krylov == CFSA_KRYLOV_BICGSTAB) {
+      s->pressure_iters = h->h_bs[1].iters[0];
+      const double b2 = h->h_bs[1].bnorm2[0];
+      s->pressure_residual = b2 > 0 ? std::sqrt(h->h_bs[1].rnorm2[0] / b2) : 0.0;
+    } else {
+      s->pressure_iters = h->h_cs->iters;
+      const double b2 = h->h_cs->bnorm2;
+      s->pressure_residual = b2 > 0 ? std::sqrt(h->h_cs->rnorm2 / b2) : 0.0;
+    }
+    s->steps = h->steps;
+    s->time = h->time;
+    s->last_step_ms = h->last_ms;
+    s->nnz_p2 = h->nnz2;
+    s->nnz_p1 = h->nnz1;
+    s->kernel_launches = h->batch_launches;
+    s->krylov_iters[0] = h->batch_iters[0];
+    s->krylov_iters[1] = h->batch_iters[1];
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_compute_divergence(cfsa_ns *h, const double *u, double *div) {
+  if (!h || !u || !div) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    h->upload_vec3(u, h->wb);
+    k_tet_div<<<blocks_for(h->nt), kBlock, 0, h->stream>>>((int)h->nt, h->N2, h->tnode, h->grad, h->wb,
+                                                           h->divt, h->st_free);
+    k_gather_div<<<blocks_for(h->nv), kBlock, 0, h->stream>>>((int)h->nv, h->adj_ptr, h->adj, h->vol,
+                                                              h->divt, h->pb);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(div, h->pb, h->nv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_compute_advection(cfsa_ns *h, double *conv) {
+  if (!h || !conv) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    k_tet_conv<<<blocks_for(h->nt), kBlock, 0, h->stream>>>((int)h->nt, h->N2, h->tnode, h->grad, h->u,
+                                                            h->ct, h->st_free);
+    k_gather_conv<<<blocks_for(h->N2), kBlock, 0, h->stream>>>((int)h->N2, (int)h->nt, h->adj_ptr, h->adj,
+                                                               h->vol, h->ct, h->wb);
+    CK(cudaGetLastError());
+    h->download_vec3(h->wb, conv);
+    return CFSA_OK;
+  });
+}
+
+static int face_forces(cfsa_ns *h, double *out, int which) {
+  if (!h || !out) return CFSA_BAD_ARG;
+  if (h->nbf <= 0) return fail(h, CFSA_BAD_ARG, "mesh view carried no boundary faces");
+  return guarded(h, [&] {
+    k_face_forces<<<blocks_for(h->nbf), kBlock, 0, h->stream>>>(
+        (int)h->nbf, (int)h->nt, h->N2, h->viscosity, h->fverts, h->ftet, h->fnormal, h->farea, h->tnode,
+        h->grad, h->u, h->p, h->fshear, h->fpress);
+    std::vector<double> a((size_t)3 * h->nv), b((size_t)3 * h->nv);
+    if (which == 0 || which == 2) {
+      k_face_gather<<<blocks_for(h->nv), kBlock, 0, h->stream>>>((int)h->nv, h->vf_ptr, h->vf, h->fpress,
+                                                                 h->fout);
+      CK(cudaMemcpyAsync(a.data(), h->fout, a.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+    }
+    if (which == 1 || which == 2) {
+      k_face_gather<<<blocks_for(h->nv), kBlock, 0, h->stream>>>((int)h->nv, h->vf_ptr, h->vf, h->fshear,
+                                                                 h->fout);
+      CK(cudaMemcpyAsync(b.data(), h->fout, b.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+    }
+    CK(cudaGetLastError());
+    for (size_t k = 0; k < a.size(); ++k)
+      out[k] = (which == 0) ? a[k] : (which == 1) ? b[k] : a[k] + b[k];
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_compute_pressure_forces(cfsa_ns *h, double *out) { return face_forces(h, out, 0); }
+int cfsa_ns_compute_shear_stress(cfsa_ns *h, double *out) { return face_forces(h, out, 1); }
+int cfsa_ns_compute_total_fluid_forces(cfsa_ns *h, double *out) { return face_forces(h, out, 2); }
+
+int cfsa_ns_get_matrix_size(cfsa_ns *h, int which, int64_t *nrows, int64_t *nnz) {
+  if (!h || !nrows || !nnz) return CFSA_BAD_ARG;
+  if (which < 0 || which > 7) return fail(h, CFSA_BAD_ARG, "unknown matrix id");
+  const bool p2 = (which == CFSA_MAT_MASS || which == CFSA_MAT_STIFFNESS || which == CFSA_MAT_MOMENTUM);
+  *nrows = p2 ? h->N2 : h->nv;
+  *nnz = p2 ? h->nnz2 : h->nnz1;
+  return CFSA_OK;
+}
+
+int cfsa_ns_get_matrix(cfsa_ns *h, int which, int64_t *rowptr, int32_t *cols, double *vals) {
+  if (!h || !rowptr || !cols || !vals) return CFSA_BAD_ARG;
+  if (which < 0 || which > 7) return fail(h, CFSA_BAD_ARG, "unknown matrix id");
+  return guarded(h, [&] {
+    const bool p2 = (which == CFSA_MAT_MASS || which == CFSA_MAT_STIFFNESS || which == CFSA_MAT_MOMENTUM);
+    const int64_t n = p2 ? h->N2 : h->nv, nnz = p2 ? h->nnz2 : h->nnz1;
+    const std::vector<int> &rp = p2 ? h->h_rp2 : h->h_rp1;
+    for (int64_t i = 0; i <= n; ++i) rowptr[i] = rp[i];
+    CK(cudaMemcpyAsync(cols, p2 ? h->ci2 : h->ci1, nnz * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    auto get = [&](const double *d, double *o) {
+      CK(cudaMemcpyAsync(o, d, nnz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    };
+    std::vector<double> tmp;
+    switch (which) {
+      case CFSA_MAT_MASS: get(h->Mv, vals); break;
+      case CFSA_MAT_STIFFNESS: get(h->Kv, vals); break;
+      case CFSA_MAT_GRAD_X: get(h->Gv, vals); break;
+      case CFSA_MAT_GRAD_Y: get(h->Gv + h->nnz1, vals); break;
+      case CFSA_MAT_GRAD_Z: get(h->Gv + 2 * h->nnz1, vals); break;
+      case CFSA_MAT_POISSON: get(h->Lv, vals); break;
+      case CFSA_MAT_MOMENTUM:
+        tmp.resize(nnz);
+        get(h->Mv, vals);
+        get(h->Kv, tmp.data());
+        break;
+      case CFSA_MAT_POISSON_BC: get(h->Lv, vals); break;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    if (which == CFSA_MAT_MOMENTUM) {
+      for (int64_t i = 0; i < n; ++i)
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+          double a = vals[k] / h->dt + tmp[k];
+          if (cols[k] == i && (h->h_bc[i] == BC_INLET || h->h_bc[i] == BC_WALL)) a += kMomentumPenalty;
+          vals[k] = a;
+        }
+    } else if (which == CFSA_MAT_POISSON_BC) {
+      for (int64_t i = 0; i < n; ++i)
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+          if (cols[k] == i && ((h->outlet_type == 1 && i == h->ref_node) ||
+                               (h->outlet_type == 0 && h->h_bc[i] == BC_OUTLET)))
+            vals[k] += kPoissonPenalty;
+    }
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_get_inv_lumped_mass(cfsa_ns *h, double *out) {
+  if (!h || !out) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    CK(cudaMemcpyAsync(out, h->invm, h->N2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+}  // extern "C"
+
+extern "C" int cfsa_ns_profile_kernel(cfsa_ns *h, int which, int iters, double *avg_ms,
+                                      double *alg_bytes) {
+  if (!h || !avg_ms || !alg_bytes || iters < 1) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    h->profile_kernel(which, iters, avg_ms, alg_bytes);
+    return CFSA_OK;
+  });
+}

@@ -1,0 +1,130 @@
+// Device-side data structures and helpers shared by the Navier-Stokes kernels.
+//
+// Layouts in HBM (all device arrays are owned by the solver handle):
+//   * tet data is structure-of-arrays so that per-tet kernels load with unit stride:
+//     tet_node[l*nt + t] (l = 0..3 vertices, 4..9 P2 nodes nv+edge_id), vol[t],
+//     grad[k*nt + t] (k = 3*a + c: component c of the gradient of vertex a);
+//   * vector fields are component-major: u[c*N2 + i];
+//   * every operator is held in CSR (ascending columns, the assembly format) and, for the
+//     operators used inside Krylov loops, in SELL-32 (slices of 32 rows, entries of a slice
+//     stored column-major, rows sorted by length inside windows of 256 rows). One thread owns
+//     one row and sums its entries in ascending column order, which is the summation order of
+//     the CSR (and of the reference's Eigen products), so SELL and CSR products agree bit for bit.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cfsa {
+
+constexpr int kBlock = 256;
+constexpr int kSellC = 32;
+constexpr int kSellSigma = 256;
+constexpr int kMaxRed = 8;  // values per block partial
+constexpr double kMomentumPenalty = 1e10;  // NavierStokes.cpp:463
+constexpr double kPoissonPenalty = 1e12;   // NavierStokes.cpp:611,619
+
+enum : int { BC_WALL = 0, BC_INLET = 1, BC_OUTLET = 2, BC_INTERNAL = 3, BC_UNDEFINED = 4 };
+
+// Krylov per-component status
+enum : int { KS_RUNNING = 0, KS_CONVERGED = 1, KS_MAXIT = 2, KS_BREAKDOWN = 3 };
+
+struct SellView {
+  const int *sptr;  // [nslices+1] entry offset of each slice
+  const int *col;   // [nentries]
+  const int *len;   // [nrows_pad] row length
+  const int *perm;  // [nrows_pad] original row, -1 for padding rows
+  int nrows_pad;
+};
+
+struct CsrView {
+  const int *rp;
+  const int *ci;
+};
+
+// Batched BiCGSTAB state (up to 3 right-hand sides sharing one matrix).
+struct BicgState {
+  double rho[3], alpha[3], omega[3], beta[3];
+  double bnorm2[3], tol2[3], r0norm2[3], rnorm2[3];
+  int iters[3], status[3];
+  int active;   // bit c: component c still iterating
+  int restart;  // bit c: component c restarts next iteration
+  int maxit;
+  int ncomp;
+};
+
+struct CgState {
+  double absnew, alpha, beta, bnorm2, tol2, rnorm2;
+  int iters, status, active, maxit;
+};
+
+struct DevStatus {
+  int halt;        // nonzero: remaining work of this batch is skipped
+  int code;        // first failure (CFSA_* code), 0 if none
+  int steps_done;  // completed steps in this batch
+  int nan;         // NaN flag of the current step
+  unsigned long long body_runs[2];  // Krylov loop bodies executed: [0] momentum, [1] pressure
+  unsigned long long iters[2];      // Krylov iterations completed: [0] momentum (max over rhs), [1] pressure
+};
+
+struct Reduce {
+  double *partials;       // [gridDim.x * kMaxRed]
+  unsigned int *counter;  // one ticket counter
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic grid reduction of NV doubles per thread. Every block writes its partial;
+// the last block to arrive (ticket counter) sums the partials in block order and returns true
+// with the totals in `out` (valid in all threads of that block). Other blocks return false.
+template <int NV>
+__device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&out)[NV]) {
+  __shared__ double sm[NV][kBlock / 32];
+  __shared__ bool last;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double w = warp_sum(v[j]);
+    if (lane == 0) sm[j][warp] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double s = 0.0;
+      for (int w = 0; w < nwarps; ++w) s += sm[j][w];
+      red.partials[(size_t)blockIdx.x * kMaxRed + j] = s;
+    }
+    __threadfence();
+    const unsigned int ticket = atomicAdd(red.counter, 1u);
+    last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double s = 0.0;
+    for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+      s += __ldcg(&red.partials[(size_t)b * kMaxRed + j]);
+    s = warp_sum(s);
+    if (lane == 0) sm[j][warp] = s;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double s = 0.0;
+    for (int w = 0; w < nwarps; ++w) s += sm[j][w];
+    out[j] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *red.counter = 0u;
+  return true;
+}
+
+}  // namespace cfsa

@@ -1,0 +1,1129 @@
+// CUDA kernels of the P2/P1 PISO step (sm_100a, FP64 path).
+//
+// Every kernel that mirrors an element loop of the reference keeps the reference's arithmetic
+// order (this translation unit is compiled with -fmad=false, so a*b+c rounds twice as on the
+// host) and replaces the scatter "out[node] += contribution, tets in order" with a gather over
+// the node's incident tets in ascending tet order. The sums therefore come out bit-identical to
+// the reference's element loops while needing no atomics.
+#pragma once
+
+#include "ns_common.cuh"
+
+namespace cfsa {
+
+// ------------------------------------------------------------------------------------------
+// Geometry: Mesh::computeGeometry volume and Mesh::computeShapeFunctionGradients
+// (src/Mesh/Mesh.cpp:455, 590-614).
+__global__ void k_geometry(int nt, const double *__restrict__ xyz, const int *__restrict__ tnode,
+                           double *__restrict__ vol, double *__restrict__ grad) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  double P[4][3];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int v = tnode[(size_t)a * nt + t];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) P[a][c] = xyz[3 * (size_t)v + c];
+  }
+  auto sub = [](const double *x, const double *y, double *o) {
+    o[0] = x[0] - y[0];
+    o[1] = x[1] - y[1];
+    o[2] = x[2] - y[2];
+  };
+  auto cross = [](const double *x, const double *y, double *o) {
+    o[0] = x[1] * y[2] - x[2] * y[1];
+    o[1] = x[2] * y[0] - x[0] * y[2];
+    o[2] = x[0] * y[1] - x[1] * y[0];
+  };
+  auto dot = [](const double *x, const double *y) { return (x[0] * y[0] + x[1] * y[1]) + x[2] * y[2]; };
+  double ba[3], ca[3], da[3], cr[3];
+  sub(P[1], P[0], ba);
+  sub(P[2], P[0], ca);
+  sub(P[3], P[0], da);
+  cross(ba, ca, cr);
+  vol[t] = fabs(dot(cr, da) / 6.0);
+  double e23[3];
+  cross(ca, da, e23);
+  const double inv6v = 1.0 / dot(ba, e23);
+  double g[4][3], x1[3], x2[3];
+  sub(P[3], P[1], x1);
+  sub(P[2], P[1], x2);
+  cross(x1, x2, g[0]);
+  cross(ca, da, g[1]);  // (p2-p0) x (p3-p0)
+  sub(P[3], P[0], x1);
+  sub(P[1], P[0], x2);
+  cross(x1, x2, g[2]);
+  cross(ba, ca, g[3]);  // (p1-p0) x (p2-p0)
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) grad[(size_t)(3 * a + c) * nt + t] = inv6v * g[a][c];
+}
+
+// ------------------------------------------------------------------------------------------
+// Sparsity patterns. One warp per row: candidates are the nodes of the row's incident tets
+// (all 10 for the P2 pattern, the 4 vertices for the P1 pattern); duplicates are dropped and
+// the survivors are ranked to produce ascending column indices.
+constexpr int kPatternCap = 1024;  // candidates per row held in shared memory
+
+template <bool P2>
+__global__ void k_pattern(int nrows, int nt, const int *__restrict__ adj_ptr,
+                          const int *__restrict__ adj, const int *__restrict__ tnode,
+                          int *__restrict__ counts, const int *__restrict__ rp,
+                          int *__restrict__ ci, int *__restrict__ err) {
+  __shared__ int cand[kBlock / 32][kPatternCap];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (row >= nrows) return;
+  const int nloc = P2 ? 10 : 4;
+  const int beg = adj_ptr[row], end = adj_ptr[row + 1];
+  const int ncand = (end - beg) * nloc;
+  if (ncand > kPatternCap) {
+    if (lane == 0) atomicExch(err, row + 1);
+    return;
+  }
+  int *cw = cand[warp];
+  for (int q = lane; q < ncand; q += 32) {
+    const int e = adj[beg + q / nloc] >> 4;  // tet id
+    cw[q] = tnode[(size_t)(q % nloc) * nt + e];
+  }
+  __syncwarp();
+  // pass 1: bit j of `dup` marks candidate lane + 32*j as a repeat of an earlier candidate
+  unsigned int dup = 0u;
+  for (int j = 0; j * 32 < ncand; ++j) {
+    const int q = j * 32 + lane;
+    if (q < ncand) {
+      const int c = cw[q];
+      for (int k = 0; k < q; ++k)
+        if (cw[k] == c) {
+          dup |= 1u << j;
+          break;
+        }
+    }
+  }
+  __syncwarp();
+  // pass 2: repeats are replaced by INT_MAX so that only distinct values remain comparable
+  for (int j = 0; j * 32 < ncand; ++j) {
+    const int q = j * 32 + lane;
+    if (q < ncand && ((dup >> j) & 1u)) cw[q] = 0x7fffffff;
+  }
+  __syncwarp();
+  int nuniq = 0;
+  for (int j = 0; j * 32 < ncand; ++j) {
+    const int q = j * 32 + lane;
+    const bool first = (q < ncand) && !((dup >> j) & 1u);
+    if (counts == nullptr && first) {
+      const int c = cw[q];
+      int rank = 0;  // number of distinct candidates smaller than c
+      for (int k = 0; k < ncand; ++k) rank += (cw[k] < c);
+      ci[rp[row] + rank] = c;
+    }
+    nuniq += __popc(__ballot_sync(0xffffffffu, first));
+  }
+  if (counts != nullptr && lane == 0) counts[row] = nuniq;
+}
+
+__device__ __forceinline__ int find_col(const int *__restrict__ ci, int beg, int end, int c) {
+  int lo = beg, hi = end - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ci[mid] < c)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void node_grad(const double *__restrict__ grad, int nt, int t, int l,
+                                          double g[3]) {
+  // P1: grad phi_l; P2 edge node: grad phi_a + grad phi_b (NavierStokes.cpp:194)
+  constexpr int ev[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+  if (l < 4) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g[c] = grad[(size_t)(3 * l + c) * nt + t];
+  } else {
+    const int a = ev[l - 4][0], b = ev[l - 4][1];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      g[c] = grad[(size_t)(3 * a + c) * nt + t] + grad[(size_t)(3 * b + c) * nt + t];
+  }
+}
+
+// P2 mass and stiffness, one thread per row, incident tets in ascending order
+// (buildMassMatrix NavierStokes.cpp:247-285, buildStiffnessMatrix :159-218).
+__global__ void k_assemble_p2(int nrows, int nt, double density, double mu,
+                              const int *__restrict__ adj_ptr, const int *__restrict__ adj,
+                              const int *__restrict__ tnode, const double *__restrict__ vol,
+                              const double *__restrict__ grad, const int *__restrict__ rp,
+                              const int *__restrict__ ci, double *__restrict__ Mv,
+                              double *__restrict__ Kv) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= nrows) return;
+  const int beg = rp[row], end = rp[row + 1];
+  for (int k = beg; k < end; ++k) {
+    Mv[k] = 0.0;
+    Kv[k] = 0.0;
+  }
+  for (int q = adj_ptr[row]; q < adj_ptr[row + 1]; ++q) {
+    const int t = adj[q] >> 4, li = adj[q] & 15;
+    const double V = vol[t];
+    const double mass = density * V;
+    double gi[3];
+    node_grad(grad, nt, t, li, gi);
+    for (int lj = 0; lj < 10; ++lj) {
+      const int col = tnode[(size_t)lj * nt + t];
+      const int slot = find_col(ci, beg, end, col);
+      double m;
+      if (li < 4 && lj < 4)
+        m = (li == lj) ? mass / 10.0 : mass / 20.0;
+      else if (li >= 4 && lj >= 4)
+        m = (li == lj) ? mass / 15.0 : mass / 60.0;
+      else
+        m = mass / 30.0;
+      double gj[3];
+      node_grad(grad, nt, t, lj, gj);
+      const double d = (gi[0] * gj[0] + gi[1] * gj[1]) + gi[2] * gj[2];
+      Mv[slot] += m;
+      Kv[slot] += mu * V * d;
+    }
+  }
+}
+
+// P1 gradient and Poisson matrices (buildGradientMatrices NavierStokes.cpp:91-120,
+// buildPoissonMatrix :331-349). G is stored as three consecutive nnz1 blocks (x, y, z).
+__global__ void k_assemble_p1(int nrows, int nt, int64_t nnz1, const int *__restrict__ adj_ptr,
+                              const int *__restrict__ adj, const int *__restrict__ tnode,
+                              const double *__restrict__ vol, const double *__restrict__ grad,
+                              const int *__restrict__ rp, const int *__restrict__ ci,
+                              double *__restrict__ Gv, double *__restrict__ Lv) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= nrows) return;
+  const int beg = rp[row], end = rp[row + 1];
+  for (int k = beg; k < end; ++k) {
+    Gv[k] = 0.0;
+    Gv[nnz1 + k] = 0.0;
+    Gv[2 * nnz1 + k] = 0.0;
+    Lv[k] = 0.0;
+  }
+  for (int q = adj_ptr[row]; q < adj_ptr[row + 1]; ++q) {
+    const int t = adj[q] >> 4, li = adj[q] & 15;
+    if (li >= 4) continue;
+    const double V = vol[t];
+    double gi[3];
+    node_grad(grad, nt, t, li, gi);
+    for (int lj = 0; lj < 4; ++lj) {
+      const int col = tnode[(size_t)lj * nt + t];
+      const int slot = find_col(ci, beg, end, col);
+      double gj[3];
+      node_grad(grad, nt, t, lj, gj);
+      const double contrib = V / 4.0;
+      Gv[slot] += contrib * gj[0];
+      Gv[nnz1 + slot] += contrib * gj[1];
+      Gv[2 * nnz1 + slot] += contrib * gj[2];
+      Lv[slot] += V * ((gi[0] * gj[0] + gi[1] * gj[1]) + gi[2] * gj[2]);
+    }
+  }
+}
+
+// 1/rowsum(M) with the reference's 1e-14 guard (NavierStokes.cpp:293-306).
+__global__ void k_lumped_mass(int n, const int *__restrict__ rp, const double *__restrict__ Mv,
+                              double *__restrict__ invm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) s += Mv[k] * 1.0;
+  invm[i] = (fabs(s) > 1e-14) ? 1.0 / s : 1.0;
+}
+
+__global__ void k_diag_pos(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                           int *__restrict__ dpos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int pos = -1;
+  for (int k = rp[i]; k < rp[i + 1]; ++k)
+    if (ci[k] == i) pos = k;
+  dpos[i] = pos;
+}
+
+// SELL layout: column indices and the CSR slot -> SELL position map.
+__global__ void k_sell_fill(int nrows_pad, const int *__restrict__ sptr, const int *__restrict__ perm,
+                            const int *__restrict__ len, const int *__restrict__ rp,
+                            const int *__restrict__ ci, int *__restrict__ scol,
+                            int *__restrict__ posmap) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrows_pad) return;
+  const int i = perm[r];
+  if (i < 0) return;
+  const int base = sptr[r >> 5] + (r & 31);
+  const int b = rp[i];
+  for (int k = 0; k < len[r]; ++k) {
+    scol[base + k * kSellC] = ci[b + k];
+    posmap[b + k] = base + k * kSellC;
+  }
+}
+
+__global__ void k_scatter_vals(int64_t nnz, const int *__restrict__ posmap,
+                               const double *__restrict__ src, double *__restrict__ dst) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nnz) dst[posmap[k]] = src[k];
+}
+
+// Momentum operator A = M/dt + K + 1e10 on Inlet/Wall diagonals (NavierStokes.cpp:460-495).
+__global__ void k_momentum_diag(int n, double dt, const int *__restrict__ dpos,
+                                const double *__restrict__ Mv, const double *__restrict__ Kv,
+                                const signed char *__restrict__ bc, double *__restrict__ diagA,
+                                double *__restrict__ invA) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k = dpos[i];
+  double d = Mv[k] / dt + Kv[k];
+  if (bc[i] == BC_INLET || bc[i] == BC_WALL) d += kMomentumPenalty;
+  diagA[i] = d;
+  invA[i] = (d != 0.0) ? 1.0 / d : 1.0;
+}
+
+// Right-preconditioned momentum operator At = A * diag(invA) in SELL layout, and M in SELL.
+__global__ void k_momentum_sell(int64_t nnz, double dt, const int *__restrict__ posmap,
+                                const int *__restrict__ rows, const int *__restrict__ ci,
+                                const double *__restrict__ Mv, const double *__restrict__ Kv,
+                                const signed char *__restrict__ bc,
+                                const double *__restrict__ invA, double *__restrict__ At,
+                                double *__restrict__ Ms) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nnz) return;
+  const int i = rows[k], j = ci[k];
+  double a = Mv[k] / dt + Kv[k];
+  if (i == j && (bc[i] == BC_INLET || bc[i] == BC_WALL)) a += kMomentumPenalty;
+  const int pos = posmap[k];
+  At[pos] = a * invA[j];
+  Ms[pos] = Mv[k];
+}
+
+__global__ void k_row_of_slot(int n, const int *__restrict__ rp, int *__restrict__ rows) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) rows[k] = i;
+}
+
+// Poisson operator with the outlet / reference penalty (NavierStokes.cpp:604-626) in SELL
+// layout: Ls = Lbc (for CG), Lt = Lbc * diag(invL) (for BiCGSTAB); diagonal inverse invL.
+__global__ void k_poisson_diag(int n, int outlet_type, int ref_node, const int *__restrict__ dpos,
+                               const double *__restrict__ Lv, const signed char *__restrict__ bc,
+                               double *__restrict__ diagL, double *__restrict__ invL) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double d = Lv[dpos[i]];
+  if ((outlet_type == 1 && i == ref_node) || (outlet_type == 0 && bc[i] == BC_OUTLET))
+    d += kPoissonPenalty;
+  diagL[i] = d;
+  invL[i] = (d != 0.0) ? 1.0 / d : 1.0;
+}
+
+__global__ void k_poisson_sell(int64_t nnz, int outlet_type, int ref_node,
+                               const int *__restrict__ posmap, const int *__restrict__ rows,
+                               const int *__restrict__ ci, const double *__restrict__ Lv,
+                               const signed char *__restrict__ bc,
+                               const double *__restrict__ invL, double *__restrict__ Ls,
+                               double *__restrict__ Lt) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nnz) return;
+  const int i = rows[k], j = ci[k];
+  double a = Lv[k];
+  if (i == j && ((outlet_type == 1 && i == ref_node) || (outlet_type == 0 && bc[i] == BC_OUTLET)))
+    a += kPoissonPenalty;
+  const int pos = posmap[k];
+  Ls[pos] = a;
+  Lt[pos] = a * invL[j];
+}
+
+// ------------------------------------------------------------------------------------------
+// Per-tet convection vector c_t = grad(u) * u_mean over P1 vertex velocities
+// (computeAdvectionRHS NavierStokes.cpp:550-567).
+__global__ void k_tet_conv(int nt, int64_t n2, const int *__restrict__ tnode,
+                           const double *__restrict__ grad, const double *__restrict__ u,
+                           double *__restrict__ ct, const DevStatus *__restrict__ st) {
+  if (st->halt) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  double uv[4][3];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int v = tnode[(size_t)a * nt + t];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) uv[a][c] = u[c * n2 + v];
+  }
+  double ue[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ue[c] = ue[c] + 0.25 * uv[a][c];
+  double gu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    double g[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) g[b] = grad[(size_t)(3 * j + b) * nt + t];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) gu[a][b] += uv[j][a] * g[b];
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    ct[(size_t)a * nt + t] = (gu[a][0] * ue[0] + gu[a][1] * ue[1]) + gu[a][2] * ue[2];
+}
+
+// Per-tet divergence tr(grad u) over P1 vertex velocities (computeDivergence
+// NavierStokes.cpp:684-693).
+__global__ void k_tet_div(int nt, int64_t n2, const int *__restrict__ tnode,
+                          const double *__restrict__ grad, const double *__restrict__ u,
+                          double *__restrict__ divt, const DevStatus *__restrict__ st) {
+  if (st && st->halt) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  double d[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int v = tnode[(size_t)j * nt + t];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) d[a] += u[a * n2 + v] * grad[(size_t)(3 * j + a) * nt + t];
+  }
+  divt[t] = (d[0] + d[1]) + d[2];
+}
+
+// Convection gather: conv_i = -sum_t w_t c_t, w = V/4 (vertex) or V/24 (edge node)
+// (NavierStokes.cpp:571-580), tets ascending.
+__device__ __forceinline__ void gather_conv(int i, int nt, const int *__restrict__ adj_ptr,
+                                            const int *__restrict__ adj,
+                                            const double *__restrict__ vol,
+                                            const double *__restrict__ ct, double acc[3]) {
+  acc[0] = acc[1] = acc[2] = 0.0;
+  for (int q = adj_ptr[i]; q < adj_ptr[i + 1]; ++q) {
+    const int t = adj[q] >> 4, l = adj[q] & 15;
+    const double w = (l < 4) ? vol[t] / 4.0 : vol[t] / 24.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[c] = acc[c] - w * ct[(size_t)c * nt + t];
+  }
+}
+
+// Divergence gather onto P1 vertices: div_i = sum_t (V/4) d_t (NavierStokes.cpp:696-698).
+__device__ __forceinline__ double gather_div(int i, const int *__restrict__ adj_ptr,
+                                             const int *__restrict__ adj,
+                                             const double *__restrict__ vol,
+                                             const double *__restrict__ divt) {
+  double s = 0.0;
+  for (int q = adj_ptr[i]; q < adj_ptr[i + 1]; ++q) {
+    const int t = adj[q] >> 4;
+    s += (vol[t] / 4.0) * divt[t];
+  }
+  return s;
+}
+
+__global__ void k_gather_conv(int n, int nt, const int *__restrict__ adj_ptr,
+                              const int *__restrict__ adj, const double *__restrict__ vol,
+                              const double *__restrict__ ct, double *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double acc[3];
+  gather_conv(i, nt, adj_ptr, adj, vol, ct, acc);
+  for (int c = 0; c < 3; ++c) out[(size_t)c * n + i] = acc[c];
+}
+
+__global__ void k_gather_div(int nv, const int *__restrict__ adj_ptr, const int *__restrict__ adj,
+                             const double *__restrict__ vol, const double *__restrict__ divt,
+                             double *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  out[i] = gather_div(i, adj_ptr, adj, vol, divt);
+}
+
+// ------------------------------------------------------------------------------------------
+// Momentum right-hand side (NavierStokes.cpp:429-495) for the three components, fused with the
+// initialisation of the batched BiCGSTAB (x0 = 0, r = r0 = b, p = v = 0).
+struct MomentumRhsArgs {
+  SellView S;
+  const double *Ms;  // M in SELL layout
+  CsrView G;         // P1 pattern
+  const double *Gv;  // [3][nnz1]
+  int64_t nnz1;
+  const int *adj_ptr, *adj;
+  const double *vol, *ct;
+  const signed char *bc;
+  const double *inlet;  // [3][N2]
+  const double *u, *p;
+  double dt, tol;
+  int n, nv, nt, maxit;
+  double *b, *x, *r, *r0, *pk, *v;
+  BicgState *bs;
+  DevStatus *st;
+  Reduce red;
+};
+
+__global__ void k_momentum_rhs(MomentumRhsArgs A) {
+  if (A.st->halt) return;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double part[3] = {0.0, 0.0, 0.0};
+  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  if (i >= 0) {
+    const int64_t n = A.n;
+    const int base = A.S.sptr[r >> 5] + (r & 31), len = A.S.len[r];
+    double mu[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < len; ++k) {
+      const int pos = base + k * kSellC;
+      const int c = A.S.col[pos];
+      const double m = A.Ms[pos];
+      mu[0] += m * A.u[c];
+      mu[1] += m * A.u[n + c];
+      mu[2] += m * A.u[2 * n + c];
+    }
+    double b[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) b[c] = 0.0 + mu[c] / A.dt;
+    if (i < A.nv) {
+      double gp[3] = {0.0, 0.0, 0.0};
+      for (int k = A.G.rp[i]; k < A.G.rp[i + 1]; ++k) {
+        const double pj = A.p[A.G.ci[k]];
+        gp[0] += A.Gv[k] * pj;
+        gp[1] += A.Gv[A.nnz1 + k] * pj;
+        gp[2] += A.Gv[2 * A.nnz1 + k] * pj;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) b[c] -= gp[c];
+    }
+    double conv[3];
+    gather_conv(i, A.nt, A.adj_ptr, A.adj, A.vol, A.ct, conv);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) b[c] += conv[c];
+    const int bcv = A.bc[i];
+    if (bcv == BC_INLET || bcv == BC_WALL) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double up = (bcv == BC_INLET) ? A.inlet[c * n + i] : 0.0;
+        b[c] += kMomentumPenalty * up;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t o = c * n + i;
+      A.b[o] = b[c];
+      A.x[o] = 0.0;
+      A.r[o] = b[c];
+      A.r0[o] = b[c];
+      A.pk[o] = 0.0;
+      A.v[o] = 0.0;
+      part[c] = b[c] * b[c];
+    }
+  }
+  double tot[3];
+  if (grid_reduce<3>(part, A.red, tot) && threadIdx.x == 0) {
+    BicgState *s = A.bs;
+    s->active = 0;
+    s->restart = 0;
+    s->maxit = A.maxit;
+    s->ncomp = 3;
+    for (int c = 0; c < 3; ++c) {
+      s->bnorm2[c] = tot[c];
+      s->r0norm2[c] = tot[c];
+      s->rnorm2[c] = tot[c];
+      s->tol2[c] = A.tol * A.tol * tot[c];
+      s->rho[c] = s->alpha[c] = s->omega[c] = 1.0;
+      s->beta[c] = 0.0;
+      s->iters[c] = 0;
+      if (isnan(tot[c])) {
+        s->status[c] = KS_BREAKDOWN;
+      } else if (tot[c] == 0.0 || tot[c] <= s->tol2[c]) {
+        s->status[c] = KS_CONVERGED;
+      } else {
+        s->status[c] = KS_RUNNING;
+        s->active |= 1 << c;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Batched right-Jacobi-preconditioned BiCGSTAB on At = A diag(1/diag(A)); x is kept in the
+// original variables (x += alpha*D^-1 p + omega*D^-1 s). NC right-hand sides share At.
+struct BicgArgs {
+  SellView S;
+  const double *At;
+  const double *diagA;  // diag(A), for the restart residual
+  const double *invA;
+  const double *b;
+  double *x, *r, *r0, *pk, *v, *s, *t;
+  int n;
+  BicgState *bs;
+  Reduce red;
+  cudaGraphConditionalHandle cond;
+  int use_cond;
+  DevStatus *st;  // launch counters
+  int slot;       // 0 momentum, 1 pressure
+};
+
+template <int NC>
+__device__ __forceinline__ void sell_spmv_row(const SellView &S, const double *__restrict__ val,
+                                              const double *__restrict__ x, int64_t n, int r,
+                                              double acc[NC]) {
+  const int base = S.sptr[r >> 5] + (r & 31), len = S.len[r];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+  for (int k = 0; k < len; ++k) {
+    const int pos = base + k * kSellC;
+    const int j = S.col[pos];
+    const double a = val[pos];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] += a * x[c * n + j];
+  }
+}
+
+// K1: p = r + beta (p - omega v); on restart: r = b - A x, r0 = r, p = r, rho = |r|^2.
+template <int NC>
+__global__ void k_bicg_p(BicgArgs A) {
+  const int active = A.bs->active;
+  if (!active) return;
+  const int restart = A.bs->restart;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  const int64_t n = A.n;
+  double part[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) part[c] = 0.0;
+  if (i >= 0) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      if (!((active >> c) & 1)) continue;
+      const int64_t o = c * n + i;
+      if ((restart >> c) & 1) {
+        const int base = A.S.sptr[r >> 5] + (r & 31), len = A.S.len[r];
+        double acc = 0.0;
+        for (int k = 0; k < len; ++k) {
+          const int pos = base + k * kSellC;
+          const int j = A.S.col[pos];
+          acc += A.At[pos] * (A.diagA[j] * A.x[c * n + j]);
+        }
+        const double ri = A.b[o] - acc;
+        A.r[o] = ri;
+        A.r0[o] = ri;
+        A.pk[o] = ri;
+        part[c] = ri * ri;
+      } else {
+        const double beta = A.bs->beta[c], omega = A.bs->omega[c];
+        A.pk[o] = A.r[o] + beta * (A.pk[o] - omega * A.v[o]);
+      }
+    }
+  }
+  if (restart) {
+    double tot[NC];
+    if (grid_reduce<NC>(part, A.red, tot) && threadIdx.x == 0) {
+      for (int c = 0; c < NC; ++c)
+        if ((restart >> c) & 1) {
+          A.bs->rho[c] = tot[c];
+          A.bs->r0norm2[c] = tot[c];
+        }
+      A.bs->restart = 0;
+    }
+  }
+}
+
+// K2: v = At p, alpha = rho / (r0 . v)
+template <int NC>
+__global__ void k_bicg_v(BicgArgs A) {
+  const int active = A.bs->active;
+  if (!active) return;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  const int64_t n = A.n;
+  double part[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) part[c] = 0.0;
+  if (i >= 0) {
+    double acc[NC];
+    sell_spmv_row<NC>(A.S, A.At, A.pk, n, r, acc);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      if (!((active >> c) & 1)) continue;
+      const int64_t o = c * n + i;
+      A.v[o] = acc[c];
+      part[c] = A.r0[o] * acc[c];
+    }
+  }
+  double tot[NC];
+  if (grid_reduce<NC>(part, A.red, tot) && threadIdx.x == 0) {
+    for (int c = 0; c < NC; ++c) {
+      if (!((active >> c) & 1)) continue;
+      if (tot[c] == 0.0) {
+        A.bs->status[c] = KS_BREAKDOWN;
+        A.bs->active &= ~(1 << c);
+      } else {
+        A.bs->alpha[c] = A.bs->rho[c] / tot[c];
+      }
+    }
+  }
+}
+
+// K3: s = r - alpha v
+template <int NC>
+__global__ void k_bicg_s(BicgArgs A) {
+  const int active = A.bs->active;
+  if (!active) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const int64_t n = A.n;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    if (!((active >> c) & 1)) continue;
+    const int64_t o = c * n + i;
+    A.s[o] = A.r[o] - A.bs->alpha[c] * A.v[o];
+  }
+}
+
+// K4: t = At s, omega = (t . s) / (t . t) (0 when t . t == 0)
+template <int NC>
+__global__ void k_bicg_t(BicgArgs A) {
+  const int active = A.bs->active;
+  if (!active) return;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  const int64_t n = A.n;
+  double part[2 * NC];
+#pragma unroll
+  for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
+  if (i >= 0) {
+    double acc[NC];
+    sell_spmv_row<NC>(A.S, A.At, A.s, n, r, acc);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      if (!((active >> c) & 1)) continue;
+      const int64_t o = c * n + i;
+      A.t[o] = acc[c];
+      part[c] = acc[c] * acc[c];
+      part[NC + c] = acc[c] * A.s[o];
+    }
+  }
+  double tot[2 * NC];
+  if (grid_reduce<2 * NC>(part, A.red, tot) && threadIdx.x == 0) {
+    for (int c = 0; c < NC; ++c) {
+      if (!((active >> c) & 1)) continue;
+      A.bs->omega[c] = (tot[c] > 0.0) ? tot[NC + c] / tot[c] : 0.0;
+    }
+  }
+}
+
+// K5: x += alpha D^-1 p + omega D^-1 s, r = s - omega t; convergence test and next beta.
+template <int NC>
+__global__ void k_bicg_xr(BicgArgs A) {
+  const int active = A.bs->active;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[A.slot] += 1;
+  if (!active) {
+    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0);
+    return;
+  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n = A.n;
+  double part[2 * NC];
+#pragma unroll
+  for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
+  if (i < A.n) {
+    const double dinv = A.invA[i];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      if (!((active >> c) & 1)) continue;
+      const int64_t o = c * n + i;
+      const double alpha = A.bs->alpha[c], omega = A.bs->omega[c];
+      const double y = dinv * A.pk[o];
+      const double z = dinv * A.s[o];
+      A.x[o] += alpha * y + omega * z;
+      const double ri = A.s[o] - omega * A.t[o];
+      A.r[o] = ri;
+      part[c] = ri * ri;
+      part[NC + c] = A.r0[o] * ri;
+    }
+  }
+  double tot[2 * NC];
+  if (grid_reduce<2 * NC>(part, A.red, tot) && threadIdx.x == 0) {
+    BicgState *s = A.bs;
+    const double eps = 2.220446049250313e-16;
+    for (int c = 0; c < NC; ++c) {
+      if (!((active >> c) & 1)) continue;
+      s->iters[c] += 1;
+      s->rnorm2[c] = tot[c];
+      if (isnan(tot[c]) || isnan(tot[NC + c])) {
+        s->status[c] = KS_BREAKDOWN;
+        s->active &= ~(1 << c);
+      } else if (tot[c] <= s->tol2[c]) {
+        s->status[c] = KS_CONVERGED;
+        s->active &= ~(1 << c);
+      } else if (s->iters[c] >= s->maxit) {
+        s->status[c] = KS_MAXIT;
+        s->active &= ~(1 << c);
+      } else if (s->omega[c] == 0.0) {
+        s->status[c] = KS_BREAKDOWN;
+        s->active &= ~(1 << c);
+      } else {
+        const double rho_new = tot[NC + c];
+        if (fabs(rho_new) < eps * eps * s->r0norm2[c]) {
+          s->restart |= 1 << c;
+        } else {
+          s->beta[c] = (rho_new / s->rho[c]) * (s->alpha[c] / s->omega[c]);
+          s->rho[c] = rho_new;
+        }
+      }
+    }
+    if (A.use_cond) cudaGraphSetConditional(A.cond, s->active ? 1u : 0u);
+  }
+}
+
+// After a Krylov loop: record a failure and halt the rest of the batch (pisoStep returns false
+// right after a failed solve, NavierStokes.cpp:387-398).
+__global__ void k_check_bicg(const BicgState *__restrict__ bs, int ncomp, int slot, DevStatus *st) {
+  if (st->halt) return;
+  int code = 0, it = 0;
+  for (int c = 0; c < ncomp; ++c) it = max(it, bs->iters[c]);
+  st->iters[slot] += (unsigned long long)it;
+  for (int c = 0; c < ncomp; ++c) {
+    if (bs->status[c] == KS_MAXIT && code == 0) code = 1;
+    if (bs->status[c] == KS_BREAKDOWN && code == 0) code = 2;
+  }
+  if (code) {
+    st->code = code;
+    st->halt = 1;
+  }
+}
+
+__global__ void k_check_cg(const CgState *__restrict__ cs, DevStatus *st) {
+  if (st->halt) return;
+  st->iters[1] += (unsigned long long)cs->iters;
+  int code = 0;
+  if (cs->status == KS_MAXIT) code = 1;
+  if (cs->status == KS_BREAKDOWN) code = 2;
+  if (code) {
+    st->code = code;
+    st->halt = 1;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Pressure Poisson right-hand side b = -div(u*)/dt + penalty * p_out on Dirichlet outlet nodes
+// (NavierStokes.cpp:590-626), fused with the Krylov initialisation (CG or BiCGSTAB, x0 = 0).
+struct PressureRhsArgs {
+  const int *adj_ptr, *adj;
+  const double *vol, *divt;
+  const signed char *bc;
+  const double *invL;
+  double dt, tol, outlet_pressure;
+  int nv, outlet_type, ref_node, maxit, krylov;  // krylov: 0 CG, 1 BiCGSTAB
+  double *b, *x, *r, *z_or_r0, *pk, *v;
+  CgState *cs;
+  BicgState *bs;
+  DevStatus *st;
+  Reduce red;
+};
+
+__global__ void k_pressure_rhs(PressureRhsArgs A) {
+  if (A.st->halt) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double part[2] = {0.0, 0.0};
+  if (i < A.nv) {
+    const double d = gather_div(i, A.adj_ptr, A.adj, A.vol, A.divt);
+    double b = -d / A.dt;
+    if (A.outlet_type == 1) {
+      if (i == A.ref_node) b += kPoissonPenalty * 0.0;
+    } else if (A.outlet_type == 0) {
+      if (A.bc[i] == BC_OUTLET) b += kPoissonPenalty * A.outlet_pressure;
+    }
+    A.b[i] = b;
+    A.x[i] = 0.0;
+    A.r[i] = b;
+    if (A.krylov == 0) {
+      const double z = A.invL[i] * b;
+      A.z_or_r0[i] = z;
+      A.pk[i] = z;
+      part[1] = b * z;
+    } else {
+      A.z_or_r0[i] = b;
+      A.pk[i] = 0.0;
+      A.v[i] = 0.0;
+    }
+    part[0] = b * b;
+  }
+  double tot[2];
+  if (grid_reduce<2>(part, A.red, tot) && threadIdx.x == 0) {
+    const double tol2 = A.tol * A.tol * tot[0];
+    const bool bad = isnan(tot[0]);
+    const bool done = bad || (tot[0] == 0.0 || tot[0] <= tol2);
+    const int final_status = bad ? KS_BREAKDOWN : KS_CONVERGED;
+    if (A.krylov == 0) {
+      CgState *c = A.cs;
+      c->bnorm2 = tot[0];
+      c->rnorm2 = tot[0];
+      c->tol2 = tol2;
+      c->absnew = tot[1];
+      c->iters = 0;
+      c->maxit = A.maxit;
+      c->status = done ? final_status : KS_RUNNING;
+      c->active = done ? 0 : 1;
+    } else {
+      BicgState *s = A.bs;
+      s->ncomp = 1;
+      s->maxit = A.maxit;
+      s->restart = 0;
+      s->bnorm2[0] = s->r0norm2[0] = s->rnorm2[0] = tot[0];
+      s->tol2[0] = tol2;
+      s->rho[0] = s->alpha[0] = s->omega[0] = 1.0;
+      s->beta[0] = 0.0;
+      s->iters[0] = 0;
+      s->status[0] = done ? final_status : KS_RUNNING;
+      s->active = done ? 0 : 1;
+    }
+  }
+}
+
+// Jacobi-preconditioned CG (Hestenes-Stiefel) on the SPD Poisson operator.
+struct CgArgs {
+  SellView S;
+  const double *Ls;
+  const double *invL;
+  double *x, *r, *z, *pk, *q;
+  int n;
+  CgState *cs;
+  Reduce red;
+  cudaGraphConditionalHandle cond;
+  int use_cond;
+  DevStatus *st;  // launch counters
+};
+
+// C1: q = L p, alpha = absnew / (p . q)
+__global__ void k_cg_q(CgArgs A) {
+  if (!A.cs->active) return;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  double part[1] = {0.0};
+  if (i >= 0) {
+    double acc[1];
+    sell_spmv_row<1>(A.S, A.Ls, A.pk, A.n, r, acc);
+    A.q[i] = acc[0];
+    part[0] = A.pk[i] * acc[0];
+  }
+  double tot[1];
+  if (grid_reduce<1>(part, A.red, tot) && threadIdx.x == 0) {
+    if (tot[0] == 0.0) {
+      A.cs->status = KS_BREAKDOWN;
+      A.cs->active = 0;
+    } else {
+      A.cs->alpha = A.cs->absnew / tot[0];
+    }
+  }
+}
+
+// C2: x += alpha p, r -= alpha q, z = D^-1 r; convergence test, beta = (r.z)_new / (r.z)_old
+__global__ void k_cg_xr(CgArgs A) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[1] += 1;
+  if (!A.cs->active) {
+    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0);
+    return;
+  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double part[2] = {0.0, 0.0};
+  if (i < A.n) {
+    const double alpha = A.cs->alpha;
+    A.x[i] += alpha * A.pk[i];
+    const double ri = A.r[i] - alpha * A.q[i];
+    A.r[i] = ri;
+    const double zi = A.invL[i] * ri;
+    A.z[i] = zi;
+    part[0] = ri * ri;
+    part[1] = ri * zi;
+  }
+  double tot[2];
+  if (grid_reduce<2>(part, A.red, tot) && threadIdx.x == 0) {
+    CgState *c = A.cs;
+    c->iters += 1;
+    c->rnorm2 = tot[0];
+    if (isnan(tot[0]) || isnan(tot[1])) {
+      c->status = KS_BREAKDOWN;
+      c->active = 0;
+    } else if (tot[0] <= c->tol2) {
+      c->status = KS_CONVERGED;
+      c->active = 0;
+    } else if (c->iters >= c->maxit) {
+      c->status = KS_MAXIT;
+      c->active = 0;
+    } else {
+      c->beta = tot[1] / c->absnew;
+      c->absnew = tot[1];
+    }
+    if (A.use_cond) cudaGraphSetConditional(A.cond, c->active ? 1u : 0u);
+  }
+}
+
+// C3: p = z + beta p
+__global__ void k_cg_p(CgArgs A) {
+  if (!A.cs->active) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  A.pk[i] = A.z[i] + A.cs->beta * A.pk[i];
+}
+
+// ------------------------------------------------------------------------------------------
+// p += relax_p p'; Dirichlet outlet reset (NavierStokes.cpp:652-662, reinforcePressureBCs
+// :1011-1024). The pressure correction p' is the Krylov solution.
+__global__ void k_pressure_update(int nv, double relax_p, int outlet_type, double outlet_pressure,
+                                  const signed char *__restrict__ bc, const double *__restrict__ pc,
+                                  double *__restrict__ p, const DevStatus *__restrict__ st) {
+  if (st->halt) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  double v = p[i] + relax_p * pc[i];
+  if (outlet_type == 0 && bc[i] == BC_OUTLET) v = outlet_pressure;
+  p[i] = v;
+}
+
+// normalizePressire (NavierStokes.cpp:804-813): p -= p[ref] (ref value stashed first).
+__global__ void k_pressure_stash(int ref, const double *__restrict__ p, double *__restrict__ stash,
+                                 const DevStatus *__restrict__ st) {
+  if (st->halt) return;
+  *stash = p[ref];
+}
+__global__ void k_pressure_normalize(int nv, const double *__restrict__ stash,
+                                     double *__restrict__ p, const DevStatus *__restrict__ st) {
+  if (st->halt) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  p[i] -= *stash;
+}
+
+// correctVelocity (NavierStokes.cpp:702-771).
+struct CorrectArgs {
+  CsrView G;
+  const double *Gv;
+  int64_t nnz1;
+  const double *invm, *pc, *ustar, *inlet;
+  const signed char *bc;
+  double dt, relax_u;
+  int n, nv;
+  double *u;
+  const DevStatus *st;
+};
+
+__global__ void k_correct_velocity(CorrectArgs A) {
+  if (A.st->halt) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const int64_t n = A.n;
+  const int bcv = A.bc[i];
+  double out[3];
+  if (bcv == BC_INLET) {
+    for (int c = 0; c < 3; ++c) out[c] = A.inlet[c * n + i];
+  } else if (bcv == BC_WALL) {
+    out[0] = out[1] = out[2] = 0.0;
+  } else if (i < A.nv && A.invm[i] > 1e-14) {
+    double g[3] = {0.0, 0.0, 0.0};
+    for (int k = A.G.rp[i]; k < A.G.rp[i + 1]; ++k) {
+      const double pj = A.pc[A.G.ci[k]];
+      g[0] += A.Gv[k] * pj;
+      g[1] += A.Gv[A.nnz1 + k] * pj;
+      g[2] += A.Gv[2 * A.nnz1 + k] * pj;
+    }
+    const double f = -A.dt * A.invm[i];
+    for (int c = 0; c < 3; ++c) out[c] = A.ustar[c * n + i] + A.relax_u * (f * g[c]);
+  } else {
+    for (int c = 0; c < 3; ++c) out[c] = A.ustar[c * n + i];
+  }
+  for (int c = 0; c < 3; ++c) A.u[c * n + i] = out[c];
+}
+
+// End of step: reenforceVelocityBCs (NavierStokes.cpp:815-839) and hasNans
+// (NavierStokes.hpp:116-138) over u, u*, p, p'; records the step in the status.
+struct FinishArgs {
+  const signed char *bc;
+  const double *inlet;
+  double *u;
+  const double *ustar, *p, *pc;
+  int n, nv;
+  DevStatus *st;
+  Reduce red;
+};
+
+__global__ void k_finish_step(FinishArgs A) {
+  if (A.st->halt) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double part[1] = {0.0};
+  if (i < A.n) {
+    const int64_t n = A.n;
+    const int bcv = A.bc[i];
+    bool nan = false;
+    for (int c = 0; c < 3; ++c) {
+      double ui = A.u[c * n + i];
+      if (bcv == BC_INLET) {
+        ui = A.inlet[c * n + i];
+        A.u[c * n + i] = ui;
+      } else if (bcv == BC_WALL) {
+        ui = 0.0;
+        A.u[c * n + i] = ui;
+      }
+      nan |= isnan(ui) || isnan(A.ustar[c * n + i]);
+    }
+    if (i < A.nv) nan |= isnan(A.p[i]) || isnan(A.pc[i]);
+    part[0] = nan ? 1.0 : 0.0;
+  }
+  double tot[1];
+  if (grid_reduce<1>(part, A.red, tot) && threadIdx.x == 0) {
+    A.st->steps_done += 1;
+    if (tot[0] > 0.0) {
+      A.st->nan = 1;
+      if (A.st->code == 0) A.st->code = 3;
+      A.st->halt = 1;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Boundary-face forces (computePressureForces / computeShearStress, NavierStokes.cpp:841-944):
+// per-face force, then a per-vertex gather over the vertex's boundary faces in face order.
+__global__ void k_face_forces(int nbf, int nt, int64_t n2, double mu, const int *__restrict__ fverts,
+                              const int *__restrict__ ftet, const double *__restrict__ fnormal,
+                              const double *__restrict__ farea, const int *__restrict__ tnode,
+                              const double *__restrict__ grad, const double *__restrict__ u,
+                              const double *__restrict__ p, double *__restrict__ fshear,
+                              double *__restrict__ fpress) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nbf) return;
+  const double nx = fnormal[3 * f], ny = fnormal[3 * f + 1], nz = fnormal[3 * f + 2];
+  const double area = farea[f];
+  double fp = 0.0;
+  for (int k = 0; k < 3; ++k) fp += p[fverts[3 * f + k]];
+  fp /= 3.0;
+  fpress[3 * f] = -fp * nx * area;
+  fpress[3 * f + 1] = -fp * ny * area;
+  fpress[3 * f + 2] = -fp * nz * area;
+  const int t = ftet[f];
+  double gu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int a = 0; a < 4; ++a) {
+    const int v = tnode[(size_t)a * nt + t];
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y) gu[x][y] += u[x * n2 + v] * grad[(size_t)(3 * a + y) * nt + t];
+  }
+  const double nrm[3] = {nx, ny, nz};
+  for (int x = 0; x < 3; ++x) {
+    double tr = 0.0;
+    double tau[3];
+    for (int y = 0; y < 3; ++y) tau[y] = 2.0 * mu * (0.5 * (gu[x][y] + gu[y][x]));
+    tr = (tau[0] * nrm[0] + tau[1] * nrm[1]) + tau[2] * nrm[2];
+    fshear[3 * f + x] = tr * area;
+  }
+}
+
+__global__ void k_face_gather(int nv, const int *__restrict__ vf_ptr, const int *__restrict__ vf,
+                              const double *__restrict__ fval, double *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  double a[3] = {0.0, 0.0, 0.0};
+  for (int q = vf_ptr[i]; q < vf_ptr[i + 1]; ++q) {
+    const int f = vf[q];
+    for (int c = 0; c < 3; ++c) a[c] += fval[3 * f + c] * (1.0 / 3.0);
+  }
+  for (int c = 0; c < 3; ++c) out[3 * i + c] = a[c];
+}
+
+}  // namespace cfsa

@@ -1,0 +1,192 @@
+/*
+ * cfsa_ns.h — C ABI of the B200 (sm_100a) Taylor-Hood P2/P1 Navier-Stokes PISO solver.
+ *
+ * This is the thin layer between the C++ NavierStokesSolver facade and the CUDA kernels.
+ * Plain pointers and sizes only; host arrays in, host arrays out. Each entry point cites the
+ * member of the reference's NavierStokesSolver (include/FEM/NavierStokes.hpp,
+ * src/FEM/NavierStokes.cpp of sudo-shaka/Cell-Fluid-Structure-Analysis) that it replaces.
+ *
+ * Layouts (the reference's): velocity fields are [N2][3] doubles with the nv P1 vertices
+ * first and the ne P2 edge nodes after them (N2 = nv + ne); pressure fields are [nv] doubles.
+ *
+ * Errors: every call returns a status code; the reference's bool returns map to
+ * status == CFSA_OK. cfsa_ns_last_error(h) gives the message of the last failure.
+ * Threading: one handle drives one CUDA stream on the device current at create time; a handle
+ * is not thread-safe, distinct handles are independent.
+ */
+#ifndef CFSA_NS_H
+#define CFSA_NS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CFSA_OK 0
+#define CFSA_NOT_CONVERGED 1   /* a Krylov solve hit its iteration cap */
+#define CFSA_BREAKDOWN 2       /* a Krylov solve broke down (zero denominator) */
+#define CFSA_NAN 3             /* hasNans() after the step */
+#define CFSA_CUDA_ERROR 4
+#define CFSA_BAD_ARG 5
+#define CFSA_NOT_INITIALIZED 6
+#define CFSA_UNSUPPORTED 7
+
+/* FluidBCType values (include/FEM/NavierStokes.hpp:13-19) */
+#define CFSA_BC_WALL 0
+#define CFSA_BC_INLET 1
+#define CFSA_BC_OUTLET 2
+#define CFSA_BC_INTERNAL 3
+#define CFSA_BC_UNDEFINED 4
+
+/* OutletType values (include/FEM/NavierStokes.hpp:21-25) */
+#define CFSA_OUTLET_DIRICHLET 0
+#define CFSA_OUTLET_NEUMANN 1
+
+/* pressure Krylov method: the reference uses BiCGSTAB (src/FEM/NavierStokes.cpp:633); the
+ * Poisson matrix with penalty rows is SPD, so CG is offered and is the default here. */
+#define CFSA_KRYLOV_CG 0
+#define CFSA_KRYLOV_BICGSTAB 1
+
+/* arithmetic of the Krylov solves */
+#define CFSA_PRECISION_FP64 0
+#define CFSA_PRECISION_MIXED 1 /* FP32 inner Krylov inside FP64 defect correction */
+
+/* matrix ids for cfsa_ns_get_matrix */
+#define CFSA_MAT_MASS 0       /* M  (buildMassMatrix, NavierStokes.cpp:227-310) */
+#define CFSA_MAT_STIFFNESS 1  /* K  (buildStiffnessMatrix, NavierStokes.cpp:135-225) */
+#define CFSA_MAT_GRAD_X 2     /* Gx (buildGradientMatrices, NavierStokes.cpp:70-133) */
+#define CFSA_MAT_GRAD_Y 3
+#define CFSA_MAT_GRAD_Z 4
+#define CFSA_MAT_POISSON 5    /* L  (buildPoissonMatrix, NavierStokes.cpp:316-356) */
+#define CFSA_MAT_MOMENTUM 6   /* M/dt + K + 1e10 on Inlet/Wall diagonals (NavierStokes.cpp:460-495) */
+#define CFSA_MAT_POISSON_BC 7 /* L + 1e12 on outlet / reference diagonals (NavierStokes.cpp:604-626) */
+
+typedef struct cfsa_ns cfsa_ns;
+
+/* Mesh as the solver reads it (Mesh accessors used by NavierStokes.cpp). */
+typedef struct {
+  int64_t nv, nt, ne;
+  const double *vertices;   /* [nv][3] */
+  const int32_t *tets;      /* [nt][4] P1 vertex ids */
+  const int32_t *tet_edges; /* [nt][6] edge-node ids 0..ne-1, local edges 01,02,03,12,13,23 */
+  const int8_t *p1_bc;      /* [nv] FluidBCType */
+  const int8_t *p2_bc;      /* [ne] FluidBCType */
+  int64_t nbf;              /* boundary faces (for forces and shear); may be 0 */
+  const int32_t *bface_verts; /* [nbf][3] */
+  const int32_t *bface_tet;   /* [nbf] owning tet */
+  const double *bface_normal; /* [nbf][3] */
+  const double *bface_area;   /* [nbf] */
+} cfsa_mesh_view;
+
+typedef struct {
+  double density;
+  double viscosity;
+} cfsa_fluid;
+
+typedef struct {
+  int32_t momentum_iters[3];  /* last step, per velocity component */
+  int32_t pressure_iters;     /* last corrector solve */
+  double momentum_residual[3];/* ||r||/||b|| at exit */
+  double pressure_residual;
+  int32_t momentum_outer[3];  /* defect-correction sweeps (mixed precision), else 0 */
+  int32_t pressure_outer;
+  int64_t steps;              /* PISO/SIMPLE steps taken since create */
+  double time;                /* simulated time */
+  double last_step_ms;        /* device time of the last stepping call, all its steps (CUDA events) */
+  int64_t nnz_p2, nnz_p1;     /* matrix sizes */
+  int64_t kernel_launches;    /* device kernels launched by the last stepping call */
+  int64_t krylov_iters[2];    /* Krylov iterations in the last stepping call: momentum, pressure */
+} cfsa_ns_stats;
+
+/* kernel ids for cfsa_ns_profile_kernel */
+#define CFSA_KERNEL_MOMENTUM_SPMV 0 /* 3-right-hand-side SELL product of the momentum BiCGSTAB */
+#define CFSA_KERNEL_PRESSURE_SPMV 1 /* SELL product of the pressure CG */
+
+/* NavierStokesSolver::initialize (include/FEM/NavierStokes.hpp:91-92; NavierStokes.cpp:10-68):
+ * uploads the mesh, builds the CSR patterns, assembles M, K, G, L on the device and zeroes the
+ * fields. The inlet value in effect at create time is zero (as in the reference's CLI path);
+ * call cfsa_ns_initialize_fields after setting the inlet to reproduce initialize() with a
+ * preset inlet. */
+int cfsa_ns_create(const cfsa_mesh_view *mesh, const cfsa_fluid *fluid, cfsa_ns **out);
+void cfsa_ns_destroy(cfsa_ns *h);
+const char *cfsa_ns_last_error(const cfsa_ns *h);
+
+/* Sizes: out[0..3] = nv, ne, N2, nt. */
+int cfsa_ns_sizes(const cfsa_ns *h, int64_t out[4]);
+
+/* ---- setters (include/FEM/NavierStokes.hpp:166-186) ---- */
+int cfsa_ns_set_dt(cfsa_ns *h, double dt);                                /* setDt */
+int cfsa_ns_set_tolerances(cfsa_ns *h, double momentum, double pressure); /* setTolerance (routed) */
+int cfsa_ns_set_max_iterations(cfsa_ns *h, int momentum, int pressure);   /* NavierStokes.cpp:499,634 */
+int cfsa_ns_set_num_corrections(cfsa_ns *h, int n);                        /* setNumberOfCorrections */
+int cfsa_ns_set_relaxation(cfsa_ns *h, double relax_u, double relax_p);    /* setRelaxU / setRelaxP */
+int cfsa_ns_set_outlet(cfsa_ns *h, int outlet_type, double outlet_pressure); /* setOutletType/Pressure */
+int cfsa_ns_set_reference_node(cfsa_ns *h, int node);                      /* setReferencePressureNode */
+int cfsa_ns_set_inlet_uniform(cfsa_ns *h, const double u[3]);             /* setMeanInletVelocity */
+int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u /*[N2][3]*/);   /* new: per-node inlet */
+int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov);                   /* new: CG or BiCGSTAB */
+int cfsa_ns_set_precision(cfsa_ns *h, int precision);                      /* new: FP64 or mixed */
+/* Fluid viscosity; stiffness (scaled by 1/viscosity, NavierStokes.cpp:153) is re-assembled. */
+int cfsa_ns_set_viscosity(cfsa_ns *h, double viscosity);
+
+/* initialize() field set-up (NavierStokes.cpp:22-46): zero fields, inlet nodes take the current
+ * inlet value, time reset to 0. */
+int cfsa_ns_initialize_fields(cfsa_ns *h);
+
+/* build_sparse_matrices (include/FEM/NavierStokes.hpp:97-102): re-assemble M, K, G, L on the
+ * device from the current vertex coordinates (patterns are reused). */
+int cfsa_ns_assemble(cfsa_ns *h);
+/* Mesh motion (Mesh::updateGeometry, include/Mesh/Mesh.hpp:98-101): new vertex coordinates
+ * [nv][3]; re-assembles. */
+int cfsa_ns_update_vertices(cfsa_ns *h, const double *xyz);
+/* New boundary tags (coupled BC remapping, src/Numerics/CoupledSolver.cpp:113-129). */
+int cfsa_ns_update_boundary_tags(cfsa_ns *h, const int8_t *p1_bc, const int8_t *p2_bc);
+
+/* ---- stepping ---- */
+int cfsa_ns_piso_step(cfsa_ns *h);                          /* pisoStep, NavierStokes.cpp:374-414 */
+int cfsa_ns_piso_steps(cfsa_ns *h, int n, int *n_done);     /* n x pisoStep, one sync at the end */
+int cfsa_ns_simple_step(cfsa_ns *h);                        /* simpleStep, NavierStokes.cpp:968-1009 */
+int cfsa_ns_momentum_predictor(cfsa_ns *h);                 /* solveMomentumPredictor, :416-524 */
+int cfsa_ns_pressure_poisson(cfsa_ns *h);                   /* solvePressurePoisson, :586-668 */
+int cfsa_ns_correct_velocity(cfsa_ns *h);                   /* correctVelocity, :702-771 */
+
+/* ---- fields ---- */
+int cfsa_ns_get_velocity(cfsa_ns *h, double *u /*[N2][3]*/);          /* getVelocity */
+int cfsa_ns_get_velocity_star(cfsa_ns *h, double *u /*[N2][3]*/);
+int cfsa_ns_get_pressure(cfsa_ns *h, double *p /*[nv]*/);             /* getPressure */
+int cfsa_ns_get_pressure_correction(cfsa_ns *h, double *p /*[nv]*/);
+int cfsa_ns_set_fields(cfsa_ns *h, const double *u /*[N2][3] or NULL*/, const double *p /*[nv] or NULL*/);
+int cfsa_ns_get_time(const cfsa_ns *h, double *t);                    /* getTime */
+int cfsa_ns_get_stats(const cfsa_ns *h, cfsa_ns_stats *s);
+
+/* ---- operators ---- */
+/* computeDivergence (NavierStokes.cpp:670-700) of a host velocity field. */
+int cfsa_ns_compute_divergence(cfsa_ns *h, const double *u /*[N2][3]*/, double *div /*[nv]*/);
+/* computeAdvectionRHS (NavierStokes.cpp:526-584) of the current velocity. */
+int cfsa_ns_compute_advection(cfsa_ns *h, double *conv /*[N2][3]*/);
+/* computeShearStress / computePressureForces / computeTotalFluidForces (NavierStokes.cpp:841-965)
+ * of the current fields; outputs [nv][3]. Requires boundary faces in the mesh view. */
+int cfsa_ns_compute_shear_stress(cfsa_ns *h, double *out);
+int cfsa_ns_compute_pressure_forces(cfsa_ns *h, double *out);
+int cfsa_ns_compute_total_fluid_forces(cfsa_ns *h, double *out);
+
+/* ---- matrices (CSR, ascending columns) ---- */
+int cfsa_ns_get_matrix_size(cfsa_ns *h, int which, int64_t *nrows, int64_t *nnz);
+int cfsa_ns_get_matrix(cfsa_ns *h, int which, int64_t *rowptr, int32_t *cols, double *vals);
+/* 1/rowsum(M) (NavierStokes.cpp:290-306) */
+int cfsa_ns_get_inv_lumped_mass(cfsa_ns *h, double *out /*[N2]*/);
+
+/* ---- diagnostics (no counterpart in the reference) ---- */
+/* Times `iters` back-to-back launches of one step kernel on the handle's stream with CUDA events,
+ * on the current device data, without touching the solver state. avg_ms: mean duration of one
+ * launch; alg_bytes: algorithmic bytes one launch must move (matrix values and column indices,
+ * row metadata, each vector element read or written once). */
+int cfsa_ns_profile_kernel(cfsa_ns *h, int which, int iters, double *avg_ms, double *alg_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFSA_NS_H */

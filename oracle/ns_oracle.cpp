@@ -1,0 +1,1057 @@
+// ============================================================================================
+// ORACLE — TEST INFRASTRUCTURE ONLY. Not part of the product path.
+//
+// A plain FP64 CPU restatement of the reference's Taylor-Hood P2/P1 PISO Navier-Stokes path
+// (sudo-shaka/Cell-Fluid-Structure-Analysis):
+//   * mesh processing: src/Mesh/Mesh.cpp:448-677 (geometry, faces in std::map order, P1
+//     gradients, P2 edge numbering with std::map) and the boundary tagging of
+//     src/Mesh/Mesh.cpp:325-417 with include/Mesh/Mesh.hpp:198-215;
+//   * assembly of M, K, Gx/Gy/Gz, L: src/FEM/NavierStokes.cpp:70-356 (triplets summed in
+//     insertion order, as Eigen::SparseMatrix::setFromTriplets does);
+//   * pisoStep / simpleStep and their phases: src/FEM/NavierStokes.cpp:374-771, 804-839,
+//     968-1024; boundary forces: src/FEM/NavierStokes.cpp:841-965.
+// The Krylov solvers restate the published algorithms (BiCGSTAB: van der Vorst 1992, right
+// Jacobi preconditioning; CG: Hestenes-Stiefel with Jacobi preconditioning) with the stopping
+// rule ||r|| <= tol*||b||, zero initial guess and an iteration cap; Eigen's sources were not
+// consulted (Eigen is not installed here).
+//
+// PARITY UNPINNED: the reference cannot be compiled in this environment (Eigen, yaml-cpp and
+// TetGen are absent) and it ships no tests, fixtures or golden vectors, so this restatement
+// could not be checked against outputs of the reference itself. It is cross-checked against an
+// independent numpy restatement and against analytic element identities in tests/.
+//
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load this library.
+// Extensions relative to the reference (each documented in the C API below): per-node inlet
+// profile, routing of the Krylov tolerances and iteration caps, CG for the pressure solve.
+// ============================================================================================
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <numeric>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+struct V3 {
+  double x = 0, y = 0, z = 0;
+  V3() = default;
+  V3(double a, double b, double c) : x(a), y(b), z(c) {}
+  double operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+  double &operator[](int i) { return i == 0 ? x : (i == 1 ? y : z); }
+  V3 operator+(const V3 &o) const { return {x + o.x, y + o.y, z + o.z}; }
+  V3 operator-(const V3 &o) const { return {x - o.x, y - o.y, z - o.z}; }
+  V3 operator-() const { return {-x, -y, -z}; }
+  V3 operator*(double s) const { return {x * s, y * s, z * s}; }
+  V3 operator/(double s) const { return {x / s, y / s, z / s}; }
+  double dot(const V3 &o) const { return (x * o.x + y * o.y) + z * o.z; }
+  V3 cross(const V3 &o) const { return {y * o.z - z * o.y, z * o.x - x * o.z, x * o.y - y * o.x}; }
+  double norm() const { return std::sqrt(dot(*this)); }
+  V3 normalized() const {
+    double n = norm();
+    return n > 0 ? (*this) / n : *this;
+  }
+};
+inline V3 operator*(double s, const V3 &a) { return a * s; }
+
+enum BC { kWall = 0, kInlet = 1, kOutlet = 2, kInternal = 3, kUndefined = 4 };
+enum Outlet { kDirichlet = 0, kNeumann = 1, kOutletUndefined = 2 };
+
+constexpr int kLocalFaces[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
+constexpr int kEdgeVerts[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+
+struct OTet {
+  double volume = 0;
+  int v[4] = {0, 0, 0, 0};
+  V3 centroid;
+};
+struct OFace {
+  int tet_a = -1, tet_b = -1, fa = -1, fb = -1;
+  double area = 0;
+  int v[3] = {0, 0, 0};
+  V3 normal, center;
+};
+
+struct Triplet {
+  int r, c;
+  double v;
+};
+
+struct CSR {
+  int64_t n = 0;
+  std::vector<int64_t> rowptr;
+  std::vector<int> col;
+  std::vector<double> val;
+  int64_t nnz() const { return (int64_t)col.size(); }
+};
+
+// setFromTriplets semantics: entries (r,c) summed in triplet insertion order; row-major CSR
+// with ascending columns.
+CSR from_triplets(int64_t n, const std::vector<Triplet> &trips) {
+  CSR A;
+  A.n = n;
+  std::vector<int64_t> cnt(n + 1, 0);
+  for (const auto &t : trips) cnt[t.r + 1]++;
+  for (int64_t i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
+  std::vector<int64_t> order(trips.size());
+  {
+    std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+    for (size_t k = 0; k < trips.size(); ++k) order[fill[trips[k].r]++] = (int64_t)k;
+  }
+  A.rowptr.assign(n + 1, 0);
+  std::vector<int> cols;
+  std::vector<double> vals;
+  cols.reserve(trips.size() / 2);
+  vals.reserve(trips.size() / 2);
+  std::vector<int64_t> seg;
+  for (int64_t i = 0; i < n; ++i) {
+    seg.assign(order.begin() + cnt[i], order.begin() + cnt[i + 1]);
+    std::stable_sort(seg.begin(), seg.end(),
+                     [&](int64_t a, int64_t b) { return trips[a].c < trips[b].c; });
+    size_t k = 0;
+    while (k < seg.size()) {
+      const int c = trips[seg[k]].c;
+      double s = trips[seg[k]].v;
+      size_t e = k + 1;
+      while (e < seg.size() && trips[seg[e]].c == c) {
+        s += trips[seg[e]].v;
+        ++e;
+      }
+      cols.push_back(c);
+      vals.push_back(s);
+      k = e;
+    }
+    A.rowptr[i + 1] = (int64_t)cols.size();
+  }
+  A.col.swap(cols);
+  A.val.swap(vals);
+  return A;
+}
+
+void spmv(const CSR &A, const double *x, double *y) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < A.n; ++i) {
+    double s = 0.0;
+    for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) s += A.val[k] * x[A.col[k]];
+    y[i] = s;
+  }
+}
+
+// Deterministic dot product: fixed 4096-element chunks summed sequentially, chunk partials
+// summed in order. The result does not depend on the number of threads.
+double dot(const double *a, const double *b, int64_t n) {
+  const int64_t C = 4096;
+  const int64_t nch = (n + C - 1) / C;
+  std::vector<double> part(nch > 0 ? nch : 1, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < nch; ++c) {
+    double s = 0.0;
+    const int64_t e = std::min(n, (c + 1) * C);
+    for (int64_t i = c * C; i < e; ++i) s += a[i] * b[i];
+    part[c] = s;
+  }
+  double s = 0.0;
+  for (int64_t c = 0; c < nch; ++c) s += part[c];
+  return s;
+}
+
+struct SolveInfo {
+  int iters = 0;
+  double rel_res = 0;
+  bool converged = false;
+};
+
+// Right-Jacobi-preconditioned BiCGSTAB, zero initial guess, stop when ||r||^2 <= tol^2 ||b||^2.
+// On near-breakdown (|rho| < eps^2 ||r0||^2) it restarts from the true residual with p = r.
+SolveInfo bicgstab(const CSR &A, const std::vector<double> &b, std::vector<double> &x, double tol,
+                   int maxit) {
+  const int64_t n = A.n;
+  SolveInfo info;
+  std::vector<double> invdiag(n, 1.0);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k)
+      if (A.col[k] == i) invdiag[i] = (A.val[k] != 0.0) ? 1.0 / A.val[k] : 1.0;
+  x.assign(n, 0.0);
+  const double bnorm2 = dot(b.data(), b.data(), n);
+  if (std::isnan(bnorm2)) return info;  // NaN right-hand side: not converged
+  if (bnorm2 == 0.0) {
+    info.converged = true;
+    return info;
+  }
+  std::vector<double> r(b), r0(b), p(n, 0.0), v(n, 0.0), y(n), s(n), z(n), t(n);
+  double r0norm2 = bnorm2;
+  double rho = 1.0, alpha = 1.0, w = 1.0;
+  const double tol2 = tol * tol * bnorm2;
+  const double eps = std::numeric_limits<double>::epsilon();
+  double rn2 = bnorm2;
+  int i = 0;
+  while (rn2 > tol2 && i < maxit) {
+    const double rho_old = rho;
+    rho = dot(r0.data(), r.data(), n);
+    bool restart = std::fabs(rho) < eps * eps * r0norm2;
+    double beta;
+    if (restart) {
+      spmv(A, x.data(), t.data());
+      for (int64_t k = 0; k < n; ++k) r[k] = b[k] - t[k];
+      r0 = r;
+      rho = r0norm2 = dot(r.data(), r.data(), n);
+      beta = 0.0;
+    } else {
+      beta = (rho / rho_old) * (alpha / w);
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < n; ++k) {
+      p[k] = r[k] + beta * (p[k] - w * v[k]);
+      y[k] = invdiag[k] * p[k];
+    }
+    spmv(A, y.data(), v.data());
+    const double r0v = dot(r0.data(), v.data(), n);
+    if (r0v == 0.0) break;  // breakdown: reported as not converged
+    alpha = rho / r0v;
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < n; ++k) {
+      s[k] = r[k] - alpha * v[k];
+      z[k] = invdiag[k] * s[k];
+    }
+    spmv(A, z.data(), t.data());
+    const double tt = dot(t.data(), t.data(), n);
+    w = (tt > 0.0) ? dot(t.data(), s.data(), n) / tt : 0.0;
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < n; ++k) {
+      x[k] += alpha * y[k] + w * z[k];
+      r[k] = s[k] - w * t[k];
+    }
+    rn2 = dot(r.data(), r.data(), n);
+    ++i;
+    if (std::isnan(rn2)) break;         // NaN residual: reported as not converged
+    if (w == 0.0 && rn2 > tol2) break;  // breakdown: reported as not converged
+  }
+  info.iters = i;
+  info.rel_res = std::sqrt(rn2 / bnorm2);
+  info.converged = rn2 <= tol2;
+  return info;
+}
+
+// Jacobi-preconditioned CG, zero initial guess, same stopping rule.
+SolveInfo cg(const CSR &A, const std::vector<double> &b, std::vector<double> &x, double tol,
+             int maxit) {
+  const int64_t n = A.n;
+  SolveInfo info;
+  std::vector<double> invdiag(n, 1.0);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k)
+      if (A.col[k] == i) invdiag[i] = (A.val[k] != 0.0) ? 1.0 / A.val[k] : 1.0;
+  x.assign(n, 0.0);
+  const double bnorm2 = dot(b.data(), b.data(), n);
+  if (bnorm2 == 0.0) {
+    info.converged = true;
+    return info;
+  }
+  if (std::isnan(bnorm2)) return info;  // NaN right-hand side: not converged
+  const double thr = tol * tol * bnorm2;
+  std::vector<double> r(b), z(n), p(n), q(n);
+  double rn2 = bnorm2;
+  int i = 0;
+  if (rn2 > thr) {
+    for (int64_t k = 0; k < n; ++k) z[k] = invdiag[k] * r[k];
+    p = z;
+    double absnew = dot(r.data(), z.data(), n);
+    while (i < maxit) {
+      spmv(A, p.data(), q.data());
+      const double pq = dot(p.data(), q.data(), n);
+      if (pq == 0.0) break;  // breakdown: reported as not converged
+      const double alpha = absnew / pq;
+#pragma omp parallel for schedule(static)
+      for (int64_t k = 0; k < n; ++k) {
+        x[k] += alpha * p[k];
+        r[k] -= alpha * q[k];
+      }
+      rn2 = dot(r.data(), r.data(), n);
+      ++i;
+      if (rn2 <= thr || std::isnan(rn2)) break;
+#pragma omp parallel for schedule(static)
+      for (int64_t k = 0; k < n; ++k) z[k] = invdiag[k] * r[k];
+      const double absold = absnew;
+      absnew = dot(r.data(), z.data(), n);
+      const double beta = absnew / absold;
+#pragma omp parallel for schedule(static)
+      for (int64_t k = 0; k < n; ++k) p[k] = z[k] + beta * p[k];
+    }
+  }
+  info.iters = i;
+  info.rel_res = std::sqrt(rn2 / bnorm2);
+  info.converged = rn2 <= thr;
+  return info;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Oracle {
+  // ---- mesh (src/Mesh/Mesh.cpp restatement) ----
+  std::vector<V3> vertices, edge_nodes;
+  std::vector<OTet> tets;
+  std::vector<OFace> faces;
+  std::vector<std::array<V3, 4>> grads;
+  std::map<std::pair<int, int>, int> edge_map;
+  std::vector<std::array<int, 6>> tet_edges;
+  std::vector<int> p1bc, p2bc;
+  size_t nv = 0, ne = 0, nt = 0, N2 = 0;
+
+  // ---- solver (src/FEM/NavierStokes.cpp restatement) ----
+  double density = 1000, viscosity = 0.001;
+  double dt = 1e-4, time = 0.0;
+  double tol_mom = 1e-6, tol_p = 1e-8;  // values hard-coded at NavierStokes.cpp:500,635
+  int maxit_mom = 1000, maxit_p = 1000;
+  int n_corr = 1;
+  double relax_u = 1.0, relax_p = 1.0;
+  int outlet_type = kDirichlet;
+  double outlet_pressure = 0.0;
+  int reference_node = -1;
+  int pressure_solver = 0;  // 0 = BiCGSTAB (reference), 1 = CG
+  std::vector<V3> inlet;    // per P2-node inlet velocity (the reference: one mean vector)
+  std::vector<V3> u, ustar;
+  std::vector<double> p, pcorr, inv_lumped;
+  CSR M, K, Gx, Gy, Gz, L;
+  bool initialized = false;
+
+  // stats of the last step
+  int it_mom[3] = {0, 0, 0}, it_p = 0;
+  double res_mom[3] = {0, 0, 0}, res_p = 0;
+  double t_conv = 0, t_mom = 0, t_press = 0, t_corr = 0, t_assembly = 0;
+
+  // ---------------------------------------------------------------- mesh processing
+  void build_mesh(const double *xyz, const int *tv) {
+    for (size_t i = 0; i < nv; ++i) vertices[i] = V3(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    for (size_t t = 0; t < nt; ++t)
+      for (int k = 0; k < 4; ++k) tets[t].v[k] = tv[4 * t + k];
+    // buildConnectivity (Mesh.cpp:494-530)
+    std::map<std::array<int, 3>, OFace> face_map;
+    for (int t = 0; t < (int)nt; ++t) {
+      for (int f = 0; f < 4; ++f) {
+        std::array<int, 3> fv = {tets[t].v[kLocalFaces[f][0]], tets[t].v[kLocalFaces[f][1]],
+                                 tets[t].v[kLocalFaces[f][2]]};
+        std::array<int, 3> sv = fv;
+        std::sort(sv.begin(), sv.end());
+        auto it = face_map.find(sv);
+        if (it == face_map.end()) {
+          OFace face;
+          face.v[0] = fv[0];
+          face.v[1] = fv[1];
+          face.v[2] = fv[2];
+          face.tet_a = t;
+          face.fa = f;
+          face_map[sv] = face;
+        } else {
+          it->second.tet_b = t;
+          it->second.fb = f;
+        }
+      }
+    }
+    faces.clear();
+    for (auto &kv : face_map) faces.push_back(kv.second);
+    // computeGeometry (Mesh.cpp:448-471)
+    for (auto &tet : tets) {
+      const V3 &a = vertices[tet.v[0]], &b = vertices[tet.v[1]], &c = vertices[tet.v[2]],
+               &d = vertices[tet.v[3]];
+      tet.centroid = (((a + b) + c) + d) / 4.0;
+      tet.volume = std::fabs((b - a).cross(c - a).dot(d - a) / 6.0);
+    }
+    for (auto &face : faces) {
+      const V3 &a = vertices[face.v[0]], &b = vertices[face.v[1]], &c = vertices[face.v[2]];
+      const V3 ab = b - a, ac = c - a;
+      face.normal = ac.cross(ab).normalized();
+      face.area = 0.5 * ab.cross(ac).norm();
+      face.center = ((a + b) + c) / 3.0;
+    }
+    // ensureConsistentFaceNormals (Mesh.cpp:615-639)
+    for (auto &face : faces) {
+      if (face.tet_a >= 0 && face.tet_b >= 0) {
+        const V3 &ca = tets[face.tet_a].centroid, &cb = tets[face.tet_b].centroid;
+        const V3 desired = (cb - ca).normalized();
+        if (face.normal.dot(desired) <= 1e-12) {
+          face.normal = -face.normal;
+          std::swap(face.v[1], face.v[2]);
+        } else {
+          const V3 out = (face.center - ca).normalized();
+          if (face.normal.dot(out) <= 1e-12) {
+            face.normal = -face.normal;
+            std::swap(face.v[1], face.v[2]);
+          }
+        }
+      }
+    }
+    // computeShapeFunctionGradients (Mesh.cpp:590-614)
+    grads.resize(nt);
+    for (size_t t = 0; t < nt; ++t) {
+      const V3 &p0 = vertices[tets[t].v[0]], &p1 = vertices[tets[t].v[1]],
+               &p2 = vertices[tets[t].v[2]], &p3 = vertices[tets[t].v[3]];
+      const V3 e1 = p1 - p0, e2 = p2 - p0, e3 = p3 - p0;
+      const double inv6v = 1.0 / e1.dot(e2.cross(e3));
+      grads[t][0] = inv6v * (p3 - p1).cross(p2 - p1);
+      grads[t][1] = inv6v * (p2 - p0).cross(p3 - p0);
+      grads[t][2] = inv6v * (p3 - p0).cross(p1 - p0);
+      grads[t][3] = inv6v * (p1 - p0).cross(p2 - p0);
+    }
+    // buildP2EdgeNodes (Mesh.cpp:641-677)
+    edge_map.clear();
+    tet_edges.assign(nt, {});
+    edge_nodes.clear();
+    int id = 0;
+    for (size_t t = 0; t < nt; ++t) {
+      for (int e = 0; e < 6; ++e) {
+        int a = tets[t].v[kEdgeVerts[e][0]], b = tets[t].v[kEdgeVerts[e][1]];
+        if (a > b) std::swap(a, b);
+        auto key = std::make_pair(a, b);
+        auto it = edge_map.find(key);
+        if (it == edge_map.end()) {
+          edge_nodes.push_back(0.5 * (vertices[a] + vertices[b]));
+          edge_map[key] = id;
+          tet_edges[t][e] = id++;
+        } else {
+          tet_edges[t][e] = it->second;
+        }
+      }
+    }
+    ne = edge_nodes.size();
+    N2 = nv + ne;
+    p1bc.assign(nv, kUndefined);
+    p2bc.assign(ne, kUndefined);
+  }
+
+  // Mesh::setupBoundaryConditions (Mesh.cpp:325-417) + setP2BoundariesFromP1Boundaries
+  // (Mesh.hpp:198-215)
+  void setup_bc(const double dir[3], double coverage) {
+    V3 mn = vertices[0], mx = vertices[0];
+    for (const auto &v : vertices)
+      for (int k = 0; k < 3; ++k) {
+        mn[k] = std::min(mn[k], v[k]);
+        mx[k] = std::max(mx[k], v[k]);
+      }
+    const V3 size = mx - mn;
+    int ax = 0;
+    if (size.y > size.x && size.y > size.z)
+      ax = 1;
+    else if (size.z > size.x && size.z > size.y)
+      ax = 2;
+    const double tol = size[ax] * 0.01 * coverage;
+    const double inlet_pos = dir[ax] > 0 ? mn[ax] : mx[ax];
+    const double outlet_pos = dir[ax] > 0 ? mx[ax] : mn[ax];
+    p1bc.assign(nv, kInternal);
+    for (const auto &f : faces) {
+      if (f.tet_b != -1) continue;
+      for (int k = 0; k < 3; ++k) p1bc[f.v[k]] = kWall;
+      const double di = std::abs(f.center[ax] - inlet_pos);
+      const double dout = std::abs(f.center[ax] - outlet_pos);
+      if (di < tol) {
+        for (int k = 0; k < 3; ++k) p1bc[f.v[k]] = kInlet;
+      } else if (dout < tol) {
+        for (int k = 0; k < 3; ++k) p1bc[f.v[k]] = kOutlet;
+      }
+    }
+    set_p2_bc();
+  }
+  void set_p2_bc() {
+    for (const auto &kv : edge_map) {
+      const int a = p1bc[kv.first.first], b = p1bc[kv.first.second];
+      p2bc[kv.second] = (a == b && a != kInternal) ? a : kInternal;
+    }
+  }
+  int bc_of(size_t i) const { return i < nv ? p1bc[i] : p2bc[i - nv]; }
+
+  // ---------------------------------------------------------------- assembly
+  // buildGradientMatrices (NavierStokes.cpp:70-133)
+  void build_gradient() {
+    std::vector<Triplet> tx, ty, tz;
+    tx.reserve(nt * 16);
+    ty.reserve(nt * 16);
+    tz.reserve(nt * 16);
+    for (size_t t = 0; t < nt; ++t) {
+      const double vol = tets[t].volume;
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+          const double c = vol / 4.0;
+          const V3 &g = grads[t][j];
+          tx.push_back({tets[t].v[i], tets[t].v[j], c * g.x});
+          ty.push_back({tets[t].v[i], tets[t].v[j], c * g.y});
+          tz.push_back({tets[t].v[i], tets[t].v[j], c * g.z});
+        }
+    }
+    Gx = from_triplets(nv, tx);
+    Gy = from_triplets(nv, ty);
+    Gz = from_triplets(nv, tz);
+  }
+  // buildStiffnessMatrix (NavierStokes.cpp:135-225); note mu = 1/viscosity
+  void build_stiffness() {
+    std::vector<Triplet> tr;
+    tr.reserve(nt * 100);
+    const double mu = 1.0 / viscosity;
+    for (size_t t = 0; t < nt; ++t) {
+      const double vol = tets[t].volume;
+      const auto &g = grads[t];
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+          tr.push_back({tets[t].v[i], tets[t].v[j], mu * vol * g[i].dot(g[j])});
+      for (int e = 0; e < 6; ++e) {
+        const int ei = (int)nv + tet_edges[t][e];
+        const V3 ge = g[kEdgeVerts[e][0]] + g[kEdgeVerts[e][1]];
+        for (int j = 0; j < 4; ++j) {
+          const double kev = mu * vol * ge.dot(g[j]);
+          tr.push_back({ei, tets[t].v[j], kev});
+          tr.push_back({tets[t].v[j], ei, kev});
+        }
+        for (int f = 0; f < 6; ++f) {
+          const int ej = (int)nv + tet_edges[t][f];
+          const V3 gf = g[kEdgeVerts[f][0]] + g[kEdgeVerts[f][1]];
+          tr.push_back({ei, ej, mu * vol * ge.dot(gf)});
+        }
+      }
+    }
+    K = from_triplets(N2, tr);
+  }
+  // buildMassMatrix (NavierStokes.cpp:227-310)
+  void build_mass() {
+    std::vector<Triplet> tr;
+    tr.reserve(nt * 100);
+    for (size_t t = 0; t < nt; ++t) {
+      const double mass = density * tets[t].volume;
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+          tr.push_back({tets[t].v[i], tets[t].v[j], (i == j) ? mass / 10.0 : mass / 20.0});
+      for (int e = 0; e < 6; ++e) {
+        const int ei = (int)nv + tet_edges[t][e];
+        for (int i = 0; i < 4; ++i) {
+          tr.push_back({ei, tets[t].v[i], mass / 30.0});
+          tr.push_back({tets[t].v[i], ei, mass / 30.0});
+        }
+        for (int f = 0; f < 6; ++f) {
+          const int ej = (int)nv + tet_edges[t][f];
+          tr.push_back({ei, ej, (e == f) ? mass / 15.0 : mass / 60.0});
+        }
+      }
+    }
+    M = from_triplets(N2, tr);
+    std::vector<double> ones(N2, 1.0), rs(N2);
+    spmv(M, ones.data(), rs.data());
+    inv_lumped.assign(N2, 0.0);
+    for (size_t i = 0; i < N2; ++i) inv_lumped[i] = (std::abs(rs[i]) > 1e-14) ? 1.0 / rs[i] : 1.0;
+  }
+  // buildPoissonMatrix (NavierStokes.cpp:316-356)
+  void build_poisson() {
+    std::vector<Triplet> tr;
+    tr.reserve(nt * 16);
+    for (size_t t = 0; t < nt; ++t) {
+      const double vol = tets[t].volume;
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+          tr.push_back({tets[t].v[i], tets[t].v[j], vol * grads[t][i].dot(grads[t][j])});
+    }
+    L = from_triplets(nv, tr);
+  }
+
+  // initialize (NavierStokes.cpp:10-68): matrices, zero fields, inlet nodes set from the inlet
+  // value current at this call, reference node for Neumann outlets.
+  void initialize() {
+    const double t0 = now_s();
+    u.assign(N2, V3());
+    ustar.assign(N2, V3());
+    p.assign(nv, 0.0);
+    pcorr.assign(nv, 0.0);
+    if (inlet.size() != N2) inlet.assign(N2, V3());
+    build_mass();
+    build_stiffness();
+    build_gradient();
+    build_poisson();
+    for (size_t i = 0; i < N2; ++i)
+      if (bc_of(i) == kInlet) u[i] = inlet[i];
+    if (reference_node < 0 && outlet_type == kNeumann) {
+      for (size_t i = 0; i < nv; ++i)
+        if (p1bc[i] == kInternal) {
+          reference_node = (int)i;
+          break;
+        }
+      if (reference_node < 0 && nv > 0) reference_node = 0;
+    }
+    initialized = true;
+    t_assembly = now_s() - t0;
+  }
+
+  // ---------------------------------------------------------------- step phases
+  // computeAdvectionRHS (NavierStokes.cpp:526-584)
+  std::vector<V3> advection() const {
+    std::vector<V3> conv(N2, V3());
+    for (size_t t = 0; t < nt; ++t) {
+      const double vol = tets[t].volume;
+      V3 ue;
+      for (int i = 0; i < 4; ++i) ue = ue + 0.25 * u[tets[t].v[i]];
+      double gu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int j = 0; j < 4; ++j) {
+        const V3 &uj = u[tets[t].v[j]];
+        const V3 &gj = grads[t][j];
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) gu[a][b] += uj[a] * gj[b];
+      }
+      V3 c;
+      for (int a = 0; a < 3; ++a) c[a] = (gu[a][0] * ue.x + gu[a][1] * ue.y) + gu[a][2] * ue.z;
+      for (int i = 0; i < 4; ++i) {
+        V3 &o = conv[tets[t].v[i]];
+        const double w = vol / 4.0;
+        o = o - w * c;
+      }
+      for (int e = 0; e < 6; ++e) {
+        V3 &o = conv[nv + tet_edges[t][e]];
+        const double w = vol / 24.0;
+        o = o - w * c;
+      }
+    }
+    return conv;
+  }
+
+  // solveMomentumPredictor (NavierStokes.cpp:416-524)
+  bool momentum() {
+    const double t0 = now_s();
+    std::vector<V3> conv = advection();
+    t_conv = now_s() - t0;
+    std::vector<double> uc(N2), rhs(N2), mu(N2), gp(nv), x;
+    for (int comp = 0; comp < 3; ++comp) {
+      for (size_t i = 0; i < N2; ++i) uc[i] = u[i][comp];
+      spmv(M, uc.data(), mu.data());
+      for (size_t i = 0; i < N2; ++i) rhs[i] = 0.0 + mu[i] / dt;
+      const CSR &G = comp == 0 ? Gx : (comp == 1 ? Gy : Gz);
+      spmv(G, p.data(), gp.data());
+      for (size_t i = 0; i < nv; ++i) rhs[i] -= gp[i];
+      for (size_t i = 0; i < N2; ++i) rhs[i] += conv[i][comp];
+      CSR lhs = M;  // same pattern as K
+      for (int64_t k = 0; k < lhs.nnz(); ++k) lhs.val[k] = M.val[k] / dt + K.val[k];
+      const double penalty = 1e10;
+      for (size_t i = 0; i < N2; ++i) {
+        const int bc = bc_of(i);
+        if (bc == kInlet || bc == kWall) {
+          const double up = (bc == kInlet) ? inlet[i][comp] : 0.0;
+          for (int64_t k = lhs.rowptr[i]; k < lhs.rowptr[i + 1]; ++k)
+            if (lhs.col[k] == (int)i) lhs.val[k] += penalty;
+          rhs[i] += penalty * up;
+        }
+      }
+      SolveInfo si = bicgstab(lhs, rhs, x, tol_mom, maxit_mom);
+      it_mom[comp] = si.iters;
+      res_mom[comp] = si.rel_res;
+      if (!si.converged) {
+        t_mom = now_s() - t0;
+        return false;
+      }
+      for (size_t i = 0; i < N2; ++i) ustar[i][comp] = x[i];
+    }
+    t_mom = now_s() - t0;
+    return true;
+  }
+
+  // computeDivergence (NavierStokes.cpp:670-700)
+  void divergence(const std::vector<V3> &uu, std::vector<double> &div) const {
+    div.assign(nv, 0.0);
+    for (size_t t = 0; t < nt; ++t) {
+      const double vol = tets[t].volume;
+      double gu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int j = 0; j < 4; ++j) {
+        const V3 &uj = uu[tets[t].v[j]];
+        const V3 &gj = grads[t][j];
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) gu[a][b] += uj[a] * gj[b];
+      }
+      const double d = (gu[0][0] + gu[1][1]) + gu[2][2];
+      for (int i = 0; i < 4; ++i) div[tets[t].v[i]] += (vol / 4.0) * d;
+    }
+  }
+
+  void reinforce_pressure_bcs() {
+    if (outlet_type == kDirichlet)
+      for (size_t i = 0; i < nv; ++i)
+        if (p1bc[i] == kOutlet) p[i] = outlet_pressure;
+  }
+  void normalize_pressure() {
+    if (reference_node >= 0 && reference_node < (int)p.size()) {
+      const double ref = p[reference_node];
+      for (auto &v : p) v -= ref;
+    }
+  }
+
+  // solvePressurePoisson (NavierStokes.cpp:586-668)
+  bool pressure() {
+    const double t0 = now_s();
+    std::vector<double> div, rhs(nv), x;
+    divergence(ustar, div);
+    for (size_t i = 0; i < nv; ++i) rhs[i] = -div[i] / dt;
+    CSR Lbc = L;
+    const double penalty = 1e12;
+    auto add_diag = [&](size_t i, double v) {
+      for (int64_t k = Lbc.rowptr[i]; k < Lbc.rowptr[i + 1]; ++k)
+        if (Lbc.col[k] == (int)i) Lbc.val[k] += v;
+    };
+    if (outlet_type == kNeumann) {
+      if (reference_node >= 0 && reference_node < (int)nv) {
+        add_diag(reference_node, penalty);
+        rhs[reference_node] += penalty * 0.0;
+      }
+    } else if (outlet_type == kDirichlet) {
+      for (size_t i = 0; i < nv; ++i)
+        if (p1bc[i] == kOutlet) {
+          add_diag(i, penalty);
+          rhs[i] += penalty * outlet_pressure;
+        }
+    }
+    SolveInfo si = (pressure_solver == 1) ? cg(Lbc, rhs, x, tol_p, maxit_p)
+                                          : bicgstab(Lbc, rhs, x, tol_p, maxit_p);
+    it_p = si.iters;
+    res_p = si.rel_res;
+    if (!si.converged) {
+      t_press += now_s() - t0;
+      return false;
+    }
+    for (size_t i = 0; i < nv; ++i) pcorr[i] = x[i];
+    for (size_t i = 0; i < nv; ++i) p[i] += relax_p * pcorr[i];
+    reinforce_pressure_bcs();
+    normalize_pressure();
+    t_press += now_s() - t0;
+    return true;
+  }
+
+  // correctVelocity (NavierStokes.cpp:702-771)
+  bool correct() {
+    const double t0 = now_s();
+    std::vector<double> gx(nv), gy(nv), gz(nv);
+    spmv(Gx, pcorr.data(), gx.data());
+    spmv(Gy, pcorr.data(), gy.data());
+    spmv(Gz, pcorr.data(), gz.data());
+    for (size_t i = 0; i < nv; ++i) {
+      const int bc = p1bc[i];
+      if (bc == kInlet) {
+        u[i] = inlet[i];
+        continue;
+      } else if (bc == kWall) {
+        u[i] = V3();
+        continue;
+      }
+      if (inv_lumped[i] > 1e-14) {
+        const double f = -dt * inv_lumped[i];
+        const V3 corr(f * gx[i], f * gy[i], f * gz[i]);
+        u[i] = ustar[i] + relax_u * corr;
+      } else {
+        u[i] = ustar[i];
+      }
+    }
+    for (size_t k = 0; k < ne; ++k) {
+      const int bc = p2bc[k];
+      const size_t idx = nv + k;
+      if (bc == kInlet) {
+        u[idx] = inlet[idx];
+        continue;
+      } else if (bc == kWall) {
+        u[idx] = V3();
+        continue;
+      }
+      u[idx] = ustar[idx];
+    }
+    t_corr += now_s() - t0;
+    return true;
+  }
+
+  // reenforceVelocityBCs (NavierStokes.cpp:815-839)
+  void reenforce_velocity_bcs() {
+    for (size_t i = 0; i < N2; ++i) {
+      const int bc = bc_of(i);
+      if (bc == kInlet)
+        u[i] = inlet[i];
+      else if (bc == kWall)
+        u[i] = V3();
+    }
+  }
+
+  bool has_nans() const {
+    for (const auto &v : u)
+      if (std::isnan(v.x) || std::isnan(v.y) || std::isnan(v.z)) return true;
+    for (const auto &v : ustar)
+      if (std::isnan(v.x) || std::isnan(v.y) || std::isnan(v.z)) return true;
+    for (double v : p)
+      if (std::isnan(v)) return true;
+    for (double v : pcorr)
+      if (std::isnan(v)) return true;
+    return false;
+  }
+
+  // pisoStep (NavierStokes.cpp:374-414)
+  int piso_step() {
+    if (!initialized) return 6;
+    t_press = t_corr = 0;
+    if (!momentum()) return 1;
+    for (int c = 0; c < n_corr; ++c) {
+      if (!pressure()) return 1;
+      if (!correct()) return 1;
+    }
+    reenforce_velocity_bcs();
+    time += dt;
+    return has_nans() ? 3 : 0;
+  }
+  // simpleStep (NavierStokes.cpp:968-1009)
+  int simple_step() {
+    if (!initialized) return 6;
+    t_press = t_corr = 0;
+    if (!momentum()) return 1;
+    if (!pressure()) return 1;
+    reinforce_pressure_bcs();
+    if (!correct()) return 1;
+    reenforce_velocity_bcs();
+    time += dt;
+    return has_nans() ? 3 : 0;
+  }
+
+  // computePressureForces / computeShearStress (NavierStokes.cpp:841-944)
+  void pressure_forces(double *out) const {
+    std::fill(out, out + 3 * nv, 0.0);
+    for (const auto &f : faces) {
+      if (f.tet_b != -1) continue;
+      double fp = 0.0;
+      for (int k = 0; k < 3; ++k) fp += p[f.v[k]];
+      fp /= 3.0;
+      const V3 ff = -fp * f.normal * f.area;
+      for (int k = 0; k < 3; ++k) {
+        const V3 c = ff * (1.0 / 3.0);
+        out[3 * f.v[k]] += c.x;
+        out[3 * f.v[k] + 1] += c.y;
+        out[3 * f.v[k] + 2] += c.z;
+      }
+    }
+  }
+  void shear_stress(double *out) const {
+    std::fill(out, out + 3 * nv, 0.0);
+    const double mu = viscosity;
+    for (const auto &f : faces) {
+      if (f.tet_b != -1) continue;
+      const int t = f.tet_a;
+      double gu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int i = 0; i < 4; ++i) {
+        const V3 &uu = u[tets[t].v[i]];
+        const V3 &g = grads[t][i];
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) gu[a][b] += uu[a] * g[b];
+      }
+      double tau[3][3];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) tau[a][b] = 2.0 * mu * (0.5 * (gu[a][b] + gu[b][a]));
+      V3 tr;
+      for (int a = 0; a < 3; ++a)
+        tr[a] = (tau[a][0] * f.normal.x + tau[a][1] * f.normal.y) + tau[a][2] * f.normal.z;
+      const V3 ff = tr * f.area;
+      for (int k = 0; k < 3; ++k) {
+        const V3 c = ff * (1.0 / 3.0);
+        out[3 * f.v[k]] += c.x;
+        out[3 * f.v[k] + 1] += c.y;
+        out[3 * f.v[k] + 2] += c.z;
+      }
+    }
+  }
+};
+
+const CSR *matrix_of(const Oracle *o, int which) {
+  switch (which) {
+    case 0: return &o->M;
+    case 1: return &o->K;
+    case 2: return &o->Gx;
+    case 3: return &o->Gy;
+    case 4: return &o->Gz;
+    case 5: return &o->L;
+    default: return nullptr;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Builds the oracle mesh from raw vertices [nv][3] and tets [nt][4] (0-based) and, when
+// apply_bc != 0, tags boundaries with Mesh::setupBoundaryConditions(dir, coverage).
+void *orc_create(int64_t nv, const double *xyz, int64_t nt, const int *tets, int apply_bc,
+                 const double *dir, double coverage) {
+  Oracle *o = new Oracle();
+  o->nv = (size_t)nv;
+  o->nt = (size_t)nt;
+  o->vertices.resize(o->nv);
+  o->tets.resize(o->nt);
+  o->build_mesh(xyz, tets);
+  if (apply_bc) o->setup_bc(dir, coverage);
+  return o;
+}
+void orc_destroy(void *h) { delete static_cast<Oracle *>(h); }
+
+// sizes: nv, nt, ne, nfaces, n boundary faces
+void orc_sizes(void *h, int64_t *out) {
+  Oracle *o = static_cast<Oracle *>(h);
+  int64_t nb = 0;
+  for (const auto &f : o->faces) nb += (f.tet_b == -1);
+  out[0] = (int64_t)o->nv;
+  out[1] = (int64_t)o->nt;
+  out[2] = (int64_t)o->ne;
+  out[3] = (int64_t)o->faces.size();
+  out[4] = nb;
+}
+void orc_get_mesh(void *h, int *tet_edges, int *p1bc, int *p2bc, int *face_verts, int *face_tets,
+                  double *face_geom, double *vol, double *grads, double *edge_xyz) {
+  Oracle *o = static_cast<Oracle *>(h);
+  for (size_t t = 0; t < o->nt; ++t) {
+    for (int e = 0; e < 6; ++e) tet_edges[6 * t + e] = o->tet_edges[t][e];
+    vol[t] = o->tets[t].volume;
+    for (int a = 0; a < 4; ++a)
+      for (int c = 0; c < 3; ++c) grads[12 * t + 3 * a + c] = o->grads[t][a][c];
+  }
+  for (size_t i = 0; i < o->nv; ++i) p1bc[i] = o->p1bc[i];
+  for (size_t k = 0; k < o->ne; ++k) {
+    p2bc[k] = o->p2bc[k];
+    for (int c = 0; c < 3; ++c) edge_xyz[3 * k + c] = o->edge_nodes[k][c];
+  }
+  for (size_t f = 0; f < o->faces.size(); ++f) {
+    const auto &F = o->faces[f];
+    for (int k = 0; k < 3; ++k) face_verts[3 * f + k] = F.v[k];
+    face_tets[2 * f] = F.tet_a;
+    face_tets[2 * f + 1] = F.tet_b;
+    double *g = face_geom + 7 * f;
+    g[0] = F.normal.x;
+    g[1] = F.normal.y;
+    g[2] = F.normal.z;
+    g[3] = F.area;
+    g[4] = F.center.x;
+    g[5] = F.center.y;
+    g[6] = F.center.z;
+  }
+}
+// Overrides the boundary tags (FluidBCType integers) before initialize.
+void orc_set_bc(void *h, const int *p1bc, const int *p2bc) {
+  Oracle *o = static_cast<Oracle *>(h);
+  for (size_t i = 0; i < o->nv; ++i) o->p1bc[i] = p1bc[i];
+  for (size_t k = 0; k < o->ne; ++k) o->p2bc[k] = p2bc[k];
+}
+
+void orc_set_fluid(void *h, double density, double viscosity) {
+  Oracle *o = static_cast<Oracle *>(h);
+  o->density = density;
+  o->viscosity = viscosity;
+}
+// Parameters: dt, momentum tol, pressure tol, momentum maxit, pressure maxit, corrections,
+// relax_u, relax_p, outlet type, outlet pressure, reference node, pressure solver (0 BiCGSTAB,
+// 1 CG).
+void orc_set_params(void *h, double dt, double tol_mom, double tol_p, int maxit_mom, int maxit_p,
+                    int n_corr, double relax_u, double relax_p, int outlet_type,
+                    double outlet_pressure, int reference_node, int pressure_solver) {
+  Oracle *o = static_cast<Oracle *>(h);
+  o->dt = dt;
+  o->tol_mom = tol_mom;
+  o->tol_p = tol_p;
+  o->maxit_mom = maxit_mom;
+  o->maxit_p = maxit_p;
+  o->n_corr = n_corr;
+  o->relax_u = relax_u;
+  o->relax_p = relax_p;
+  o->outlet_type = outlet_type;
+  o->outlet_pressure = outlet_pressure;
+  o->reference_node = reference_node;
+  o->pressure_solver = pressure_solver;
+}
+// Per-node inlet velocity [N2][3] (P1 nodes first, then P2 edge nodes).
+void orc_set_inlet(void *h, const double *vals) {
+  Oracle *o = static_cast<Oracle *>(h);
+  o->inlet.resize(o->N2);
+  for (size_t i = 0; i < o->N2; ++i) o->inlet[i] = V3(vals[3 * i], vals[3 * i + 1], vals[3 * i + 2]);
+}
+void orc_initialize(void *h) { static_cast<Oracle *>(h)->initialize(); }
+int orc_reference_node(void *h) { return static_cast<Oracle *>(h)->reference_node; }
+int orc_piso_step(void *h) { return static_cast<Oracle *>(h)->piso_step(); }
+int orc_simple_step(void *h) { return static_cast<Oracle *>(h)->simple_step(); }
+int orc_momentum(void *h) { return static_cast<Oracle *>(h)->momentum() ? 0 : 1; }
+int orc_pressure(void *h) { return static_cast<Oracle *>(h)->pressure() ? 0 : 1; }
+int orc_correct(void *h) { return static_cast<Oracle *>(h)->correct() ? 0 : 1; }
+
+void orc_get_state(void *h, double *u, double *ustar, double *p, double *pcorr, double *time) {
+  Oracle *o = static_cast<Oracle *>(h);
+  for (size_t i = 0; i < o->N2; ++i)
+    for (int c = 0; c < 3; ++c) {
+      u[3 * i + c] = o->u[i][c];
+      ustar[3 * i + c] = o->ustar[i][c];
+    }
+  for (size_t i = 0; i < o->nv; ++i) {
+    p[i] = o->p[i];
+    pcorr[i] = o->pcorr[i];
+  }
+  *time = o->time;
+}
+void orc_set_state(void *h, const double *u, const double *p) {
+  Oracle *o = static_cast<Oracle *>(h);
+  for (size_t i = 0; i < o->N2; ++i) o->u[i] = V3(u[3 * i], u[3 * i + 1], u[3 * i + 2]);
+  for (size_t i = 0; i < o->nv; ++i) o->p[i] = p[i];
+}
+// which: 0 M, 1 K, 2 Gx, 3 Gy, 4 Gz, 5 L. Returns nnz (rows in *nrows).
+int64_t orc_matrix_nnz(void *h, int which, int64_t *nrows) {
+  const CSR *A = matrix_of(static_cast<Oracle *>(h), which);
+  if (!A) return -1;
+  *nrows = A->n;
+  return A->nnz();
+}
+void orc_get_matrix(void *h, int which, int64_t *rowptr, int *cols, double *vals) {
+  const CSR *A = matrix_of(static_cast<Oracle *>(h), which);
+  std::copy(A->rowptr.begin(), A->rowptr.end(), rowptr);
+  std::copy(A->col.begin(), A->col.end(), cols);
+  std::copy(A->val.begin(), A->val.end(), vals);
+}
+void orc_get_inv_lumped_mass(void *h, double *out) {
+  Oracle *o = static_cast<Oracle *>(h);
+  std::copy(o->inv_lumped.begin(), o->inv_lumped.end(), out);
+}
+void orc_advection(void *h, double *out) {
+  Oracle *o = static_cast<Oracle *>(h);
+  std::vector<V3> c = o->advection();
+  for (size_t i = 0; i < o->N2; ++i)
+    for (int k = 0; k < 3; ++k) out[3 * i + k] = c[i][k];
+}
+void orc_divergence(void *h, const double *u, double *out) {
+  Oracle *o = static_cast<Oracle *>(h);
+  std::vector<V3> uu(o->N2);
+  for (size_t i = 0; i < o->N2; ++i) uu[i] = V3(u[3 * i], u[3 * i + 1], u[3 * i + 2]);
+  std::vector<double> d;
+  o->divergence(uu, d);
+  std::copy(d.begin(), d.end(), out);
+}
+void orc_pressure_forces(void *h, double *out) { static_cast<Oracle *>(h)->pressure_forces(out); }
+void orc_shear_stress(void *h, double *out) { static_cast<Oracle *>(h)->shear_stress(out); }
+// stats: it_mom[3], it_p, res_mom[3], res_p, t_assembly, t_conv, t_mom, t_press, t_corr
+void orc_stats(void *h, int *iters, double *res, double *times) {
+  Oracle *o = static_cast<Oracle *>(h);
+  for (int c = 0; c < 3; ++c) {
+    iters[c] = o->it_mom[c];
+    res[c] = o->res_mom[c];
+  }
+  iters[3] = o->it_p;
+  res[3] = o->res_p;
+  times[0] = o->t_assembly;
+  times[1] = o->t_conv;
+  times[2] = o->t_mom;
+  times[3] = o->t_press;
+  times[4] = o->t_corr;
+}
+int orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,312 @@
+"""GPU solver (libcfsa.so, sm_100a) against the CPU oracle on identical meshes and inputs.
+
+Bars: assembly, element operators and forces are bit-exact (same arithmetic order, no FMA);
+PISO states agree to relative L2 <= 1e-8 in FP64 (Krylov dot products are reduced in a
+different order on the device, everything else is identical).
+"""
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+RHO, NU = 1060.0, 0.004  # config-0 fluid
+
+
+def make_mesh(cf, rings=3, layers=12, length=30.0, radius=2.0):
+    m = cf.Mesh.cylinder(length, radius, rings, layers)
+    m.setupBoundaryConditions((1.0, 0.0, 0.0), 1.0)
+    return m
+
+
+def make_pair(cf, po, m, *, tol=1e-12, krylov=0, dt=0.01, inlet=0.5, profile=None, ncorr=1,
+              relax=(1.0, 1.0), outlet=0, outlet_p=0.0, maxit=(5000, 20000)):
+    """GPU solver and oracle configured identically (the reference's CLI order: initialize with
+    a zero inlet, then set the inlet)."""
+    s = cf.NavierStokesSolver()
+    s.setKrylovTolerances(tol, tol)
+    s.setMaxIterations(*maxit)
+    s.setPressureSolver(krylov)
+    s.setDt(dt)
+    s.setNumberOfCorrections(ncorr)
+    s.setRelaxU(relax[0])
+    s.setRelaxP(relax[1])
+    s.setOutletType(outlet)
+    s.initialize(m, cf.Fluid(RHO, NU))
+    s.setOutletPressure(outlet_p)
+    o = po.Oracle(m.vertices(), m.tets())
+    o.set_fluid(RHO, NU)
+    o.set_params(dt=dt, tol_mom=tol, tol_p=tol, maxit_mom=maxit[0], maxit_p=maxit[1],
+                 n_corr=ncorr, relax_u=relax[0], relax_p=relax[1], outlet_type=outlet,
+                 outlet_pressure=outlet_p, reference_node=s.reference_node,
+                 pressure_solver=1 if krylov == cf.KRYLOV_CG else 0)
+    o.initialize()
+    if profile is not None:
+        s.setInletVelocityProfile(profile)
+        o.set_inlet(profile)
+    else:
+        s.setMeanInletVelocity([inlet, 0.0, 0.0])
+        v = np.zeros((o.N2, 3))
+        v[:, 0] = inlet
+        o.set_inlet(v)
+    return s, o
+
+
+def csr_equal(a, b):
+    return (np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]))
+
+
+@pytest.fixture(scope="module")
+def small(cf, po):
+    m = make_mesh(cf, 3, 12)
+    s, o = make_pair(cf, po, m)
+    return m, s, o
+
+
+@pytest.mark.parametrize("which,name", [(0, "M"), (1, "K"), (2, "Gx"), (3, "Gy"), (4, "Gz"), (5, "L")])
+def test_assembly_bit_exact(small, which, name):
+    m, s, o = small
+    g = s.matrix(which)
+    r = o.matrix(name)
+    assert csr_equal(g, r), name
+
+
+def test_assembly_bit_exact_structured_prism(cf, po):
+    m = cf.Mesh.structuredRectangularPrism(3.0, 1.0, 1.0, 6, 2, 2)
+    m.setupBoundaryConditions()
+    s, o = make_pair(cf, po, m)
+    for which, name in [(0, "M"), (1, "K"), (2, "Gx"), (5, "L")]:
+        assert csr_equal(s.matrix(which), o.matrix(name)), name
+    assert np.array_equal(s.invLumpedMass(), o.inv_lumped_mass())
+
+
+def test_lumped_mass_bit_exact(small):
+    m, s, o = small
+    assert np.array_equal(s.invLumpedMass(), o.inv_lumped_mass())
+
+
+def test_operators_bit_exact(small, cf):
+    m, s, o = small
+    rng = np.random.default_rng(1)
+    u = rng.standard_normal((s.N2, 3))
+    p = rng.standard_normal(s.nv)
+    s.setFields(u, p)
+    o.set_state(u, p)
+    assert np.array_equal(s.computeAdvectionRHS(), o.advection())
+    assert np.array_equal(s.computeDivergence(u), o.divergence(u))
+
+
+def test_forces_bit_exact(small):
+    m, s, o = small
+    rng = np.random.default_rng(2)
+    u = rng.standard_normal((s.N2, 3))
+    p = rng.standard_normal(s.nv)
+    s.setFields(u, p)
+    o.set_state(u, p)
+    assert np.array_equal(s.computePressureForces(), o.pressure_forces())
+    assert np.array_equal(s.computeShearStress(), o.shear_stress())
+    tot = s.computeTotalFluidForces()
+    np.testing.assert_allclose(tot, o.pressure_forces() + o.shear_stress(), rtol=0, atol=0)
+
+
+def run_both(s, o, steps):
+    states = []
+    for _ in range(steps):
+        assert s.pisoStep()
+        assert o.piso_step() == 0
+        states.append((s.getVelocity(), s.getPressure(), o.state()))
+    return states
+
+
+@pytest.mark.parametrize("krylov", [0, 1], ids=["cg", "bicgstab"])
+def test_piso_parity_tight(cf, po, krylov):
+    m = make_mesh(cf, 3, 12)
+    s, o = make_pair(cf, po, m, tol=1e-13, krylov=krylov)
+    for u, p, st in run_both(s, o, 5):
+        assert rel_l2(u, st["u"]) < 1e-8
+        assert rel_l2(p, st["p"]) < 1e-8
+    assert abs(s.getTime() - st["time"]) == 0.0
+
+
+def test_piso_matches_golden_fixture(cf):
+    g = np.load(GOLD / "cyl_piso.npz")
+    m = cf.Mesh.cylinder(30.0, 2.0, 2, 4)
+    m.setupBoundaryConditions()
+    s = cf.NavierStokesSolver()
+    s.setKrylovTolerances(1e-14, 1e-14)
+    s.setMaxIterations(5000, 5000)
+    s.setDt(0.01)
+    s.initialize(m, cf.Fluid(RHO, NU))
+    s.setMeanInletVelocity([0.5, 0.0, 0.0])
+    for k in range(3):
+        assert s.pisoStep()
+        assert rel_l2(s.getVelocity(), g["u"][k]) < 1e-8
+        assert rel_l2(s.getPressure(), g["p"][k]) < 1e-8
+        assert rel_l2(s.getPressureCorrection(), g["pcorr"][k]) < 1e-8
+
+
+def test_config0_parity_100_steps(cf, po):
+    """Config 0: cylinder L=30 R=2 (~30k tets), rho 1060, nu 0.004, plug inlet 0.5, p=0 outlet,
+    dt 0.01, 100 steps from rest, Krylov tolerance 1e-10 (CG pressure on both sides)."""
+    m = make_mesh(cf, 5, 68)
+    assert 29000 < m.nTets() < 32000
+    s, o = make_pair(cf, po, m, tol=1e-10, krylov=cf.KRYLOV_CG)
+    for k in range(100):
+        assert s.pisoStep(), k
+        assert o.piso_step() == 0, k
+    st = o.state()
+    eu, ep = rel_l2(s.getVelocity(), st["u"]), rel_l2(s.getPressure(), st["p"])
+    print(f"config0 100 steps: rel L2 u {eu:.3e} p {ep:.3e}")
+    assert eu < 1e-8 and ep < 1e-8
+
+
+def test_reference_default_tolerances(cf, po):
+    """The reference's own solver settings: BiCGSTAB pressure, tolerances 1e-6 / 1e-8, 1000
+    iterations. Same iteration counts as the oracle and states within 1e-8."""
+    m = make_mesh(cf, 3, 12)
+    s = cf.NavierStokesSolver()
+    s.setPressureSolver(cf.KRYLOV_BICGSTAB)
+    s.setDt(0.01)
+    s.initialize(m, cf.Fluid(RHO, NU))
+    s.setMeanInletVelocity([0.5, 0.0, 0.0])
+    o = po.Oracle(m.vertices(), m.tets())
+    o.set_fluid(RHO, NU)
+    o.set_params(dt=0.01)
+    o.initialize()
+    v = np.zeros((o.N2, 3))
+    v[:, 0] = 0.5
+    o.set_inlet(v)
+    for _ in range(4):
+        assert s.pisoStep() and o.piso_step() == 0
+        gs, os_ = s.stats(), o.stats()
+        assert gs["momentum_iters"] == os_["momentum_iters"]
+        assert gs["pressure_iters"] == os_["pressure_iters"]
+    assert rel_l2(s.getVelocity(), o.state()["u"]) < 1e-8
+    assert rel_l2(s.getPressure(), o.state()["p"]) < 1e-8
+
+
+@pytest.mark.parametrize("case", ["neumann", "two_correctors", "relaxed", "parabolic", "outlet_p"])
+def test_variants_parity(cf, po, case):
+    m = make_mesh(cf, 3, 12)
+    kw = dict(tol=1e-13)
+    if case == "neumann":
+        kw.update(outlet=1)
+    elif case == "two_correctors":
+        kw.update(ncorr=2)
+    elif case == "relaxed":
+        kw.update(relax=(0.5, 0.5))
+    elif case == "parabolic":
+        kw.update(profile=cf.parabolic_inlet(m.nodePositions(), 1.0, 2.0))
+    elif case == "outlet_p":
+        kw.update(outlet_p=10.0)
+    s, o = make_pair(cf, po, m, **kw)
+    if case == "neumann":
+        assert s.reference_node >= 0 and o.reference_node() == s.reference_node
+    for u, p, st in run_both(s, o, 3):
+        assert rel_l2(u, st["u"]) < 1e-8, case
+        assert rel_l2(p, st["p"]) < 1e-8, case
+
+
+def test_simple_step_parity(cf, po):
+    m = make_mesh(cf, 3, 12)
+    s, o = make_pair(cf, po, m, tol=1e-13)
+    for _ in range(3):
+        assert s.simpleStep()
+        assert o.simple_step() == 0
+    st = o.state()
+    assert rel_l2(s.getVelocity(), st["u"]) < 1e-8
+    assert rel_l2(s.getPressure(), st["p"]) < 1e-8
+
+
+def test_phase_api_equals_step(cf, po):
+    """solveMomentumPredictor + solvePressurePoisson + correctVelocity == pisoStep (bit-exact)."""
+    m = make_mesh(cf, 3, 12)
+    a, _ = make_pair(cf, po, m, tol=1e-12)
+    b, _ = make_pair(cf, po, m, tol=1e-12)
+    for _ in range(2):
+        assert a.pisoStep()
+        assert b.solveMomentumPredictor() and b.solvePressurePoisson() and b.correctVelocity()
+    assert np.array_equal(a.getVelocity(), b.getVelocity())
+    assert np.array_equal(a.getPressure(), b.getPressure())
+
+
+def test_graph_and_eager_identical_and_deterministic(cf, po):
+    m = make_mesh(cf, 3, 12)
+    runs = []
+    for no_graph in ("0", "1", "0"):
+        os.environ["CFSA_NO_GRAPH"] = no_graph
+        try:
+            s, _ = make_pair(cf, po, m, tol=1e-12)
+        finally:
+            os.environ.pop("CFSA_NO_GRAPH", None)
+        ok, done = s.pisoSteps(4)
+        assert ok and done == 4
+        runs.append((s.getVelocity(), s.getPressure()))
+    for u, p in runs[1:]:
+        assert np.array_equal(u, runs[0][0]) and np.array_equal(p, runs[0][1])
+
+
+def test_batched_steps_equal_single_steps(cf, po):
+    m = make_mesh(cf, 3, 12)
+    a, _ = make_pair(cf, po, m, tol=1e-12)
+    b, _ = make_pair(cf, po, m, tol=1e-12)
+    ok, done = a.pisoSteps(5)
+    assert ok and done == 5
+    for _ in range(5):
+        assert b.pisoStep()
+    assert np.array_equal(a.getVelocity(), b.getVelocity())
+    assert a.getTime() == b.getTime()
+
+
+def test_not_converged_is_reported(cf, po):
+    """maxit = 1 with a tight tolerance: pisoStep returns false, time does not advance (the
+    reference returns before time_ += dt, NavierStokes.cpp:387-390)."""
+    m = make_mesh(cf, 3, 12)
+    s, _ = make_pair(cf, po, m, tol=1e-14, maxit=(1, 1))
+    assert not s.pisoStep()
+    assert s.getTime() == 0.0
+    ok, done = s.pisoSteps(3)
+    assert not ok and done == 0
+
+
+def test_nan_is_reported(cf, po):
+    """A NaN relaxation factor poisons u in the corrector: the step completes (time advances, as
+    in the reference) and pisoStep returns false through the hasNans() check."""
+    m = make_mesh(cf, 3, 12)
+    s, _ = make_pair(cf, po, m, tol=1e-12, relax=(float("nan"), 1.0))
+    assert not s.pisoStep()
+    assert s.getTime() == pytest.approx(0.01)
+    assert np.isnan(s.getVelocity()).any()
+
+
+def test_nan_input_fails_fast(cf, po):
+    m = make_mesh(cf, 3, 12)
+    s, _ = make_pair(cf, po, m, tol=1e-12)
+    p = np.zeros(s.nv)
+    p[5] = np.nan
+    s.setFields(None, p)
+    assert not s.pisoStep()
+    st = s.stats()
+    assert max(st["momentum_iters"]) <= 1
+
+
+def test_reassembly_after_vertex_motion(cf, po):
+    """build_sparse_matrices after the mesh moved (coupled path): device re-assembly equals the
+    oracle built on the moved mesh."""
+    m = make_mesh(cf, 3, 12)
+    s, _ = make_pair(cf, po, m)
+    xyz = m.vertices().copy()
+    xyz[:, 1] *= 1.0 + 0.05 * np.sin(xyz[:, 0] / 5.0)
+    s.updateVertices(xyz)
+    o2 = po.Oracle(xyz, m.tets())
+    o2.set_fluid(RHO, NU)
+    o2.initialize()
+    for which, name in [(0, "M"), (1, "K"), (2, "Gx"), (5, "L")]:
+        assert csr_equal(s.matrix(which), o2.matrix(name)), name
