@@ -527,7 +527,8 @@ __global__ void k_momentum_rhs(MomentumRhsArgs A) {
       s->r0norm2[c] = tot[c];
       s->rnorm2[c] = tot[c];
       s->tol2[c] = A.tol * A.tol * tot[c];
-      s->rho[c] = s->alpha[c] = s->omega[c] = 1.0;
+      s->rho[c] = tot[c];  // r0 . r with r = r0 = b
+      s->alpha[c] = s->omega[c] = 1.0;
       s->beta[c] = 0.0;
       s->iters[c] = 0;
       if (isnan(tot[c])) {
@@ -870,7 +871,8 @@ __global__ void k_pressure_rhs(PressureRhsArgs A) {
       s->restart = 0;
       s->bnorm2[0] = s->r0norm2[0] = s->rnorm2[0] = tot[0];
       s->tol2[0] = tol2;
-      s->rho[0] = s->alpha[0] = s->omega[0] = 1.0;
+      s->rho[0] = tot[0];  // r0 . r with r = r0 = b
+      s->alpha[0] = s->omega[0] = 1.0;
       s->beta[0] = 0.0;
       s->iters[0] = 0;
       s->status[0] = done ? final_status : KS_RUNNING;

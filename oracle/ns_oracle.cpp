@@ -146,22 +146,89 @@ void spmv(const CSR &A, const double *x, double *y) {
   }
 }
 
-// Deterministic dot product: fixed 4096-element chunks summed sequentially, chunk partials
-// summed in order. The result does not depend on the number of threads.
-double dot(const double *a, const double *b, int64_t n) {
-  const int64_t C = 4096;
-  const int64_t nch = (n + C - 1) / C;
-  std::vector<double> part(nch > 0 ? nch : 1, 0.0);
-#pragma omp parallel for schedule(static)
-  for (int64_t c = 0; c < nch; ++c) {
-    double s = 0.0;
-    const int64_t e = std::min(n, (c + 1) * C);
-    for (int64_t i = c * C; i < e; ++i) s += a[i] * b[i];
-    part[c] = s;
+// ---------------------------------------------------------------------------------------------
+// Reductions. Krylov dot products are summed in one fixed tree, the one the CUDA solver uses, so
+// that the two FP64 trajectories can be compared bit for bit (the reference's Eigen order depends
+// on its SIMD build and cannot be reproduced here in any case). Tree: the products are laid out
+// by "position"; positions are cut into blocks of 256 = 8 warps of 32; a warp sums its 32 values
+// by a butterfly (v_l + v_{l^o} for o = 16, 8, 4, 2, 1); a block adds its 8 warp sums in order;
+// 256 accumulators then take block b into accumulator b mod 256 in increasing b, and these 256
+// accumulators are combined by the same warp butterflies and in-order warp sum.
+// A position is either a row index ("natural" order) or a slot of the SELL-32 layout of the
+// operator (rows sorted by decreasing length inside windows of 256 rows, stable), for the
+// reductions that the device fuses into its sparse products.
+struct RedOrder {
+  std::vector<int> pos2row;  // row of each position, -1 for padding
+  int64_t nblocks = 0;
+};
+
+RedOrder natural_order(int64_t n) {
+  RedOrder o;
+  o.nblocks = (n + 255) / 256;
+  o.pos2row.resize(o.nblocks * 256);
+  for (int64_t r = 0; r < (int64_t)o.pos2row.size(); ++r) o.pos2row[r] = r < n ? (int)r : -1;
+  return o;
+}
+
+RedOrder sell_order(const CSR &A) {
+  const int64_t n = A.n;
+  const int64_t npad = (n + 31) / 32 * 32;
+  RedOrder o;
+  o.nblocks = (npad + 255) / 256;
+  o.pos2row.assign(o.nblocks * 256, -1);
+  std::vector<int> idx;
+  for (int64_t w0 = 0; w0 < n; w0 += 256) {
+    const int64_t w1 = std::min(n, w0 + 256);
+    idx.resize(w1 - w0);
+    std::iota(idx.begin(), idx.end(), (int)w0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+      return (A.rowptr[a + 1] - A.rowptr[a]) > (A.rowptr[b + 1] - A.rowptr[b]);
+    });
+    for (int64_t k = 0; k < w1 - w0; ++k) o.pos2row[w0 + k] = idx[k];
   }
+  return o;
+}
+
+inline double warp_butterfly(double *x) {
+  double y[32];
+  for (int off = 16; off > 0; off >>= 1) {
+    for (int l = 0; l < 32; ++l) y[l] = x[l] + x[l ^ off];
+    for (int l = 0; l < 32; ++l) x[l] = y[l];
+  }
+  return x[0];
+}
+
+inline double block_sum(double *v /*256 values*/) {
   double s = 0.0;
-  for (int64_t c = 0; c < nch; ++c) s += part[c];
+  for (int w = 0; w < 8; ++w) s += warp_butterfly(v + 32 * w);
   return s;
+}
+
+// sum over positions of f(row) (0 for padding) in the device tree
+template <class F>
+double tree_sum(const RedOrder &o, F f) {
+  const int64_t G = o.nblocks;
+  std::vector<double> part(G);
+#pragma omp parallel for schedule(static)
+  for (int64_t b = 0; b < G; ++b) {
+    double v[256];
+    for (int k = 0; k < 256; ++k) {
+      const int row = o.pos2row[b * 256 + k];
+      v[k] = row >= 0 ? f(row) : 0.0;
+    }
+    part[b] = block_sum(v);
+  }
+  double acc[256];
+  for (int t = 0; t < 256; ++t) {
+    double a = 0.0;
+    for (int64_t b = t; b < G; b += 256) a += part[b];
+    acc[t] = a;
+  }
+  return block_sum(acc);
+}
+
+double odot(const RedOrder &o, const double *a, const double *b) {
+  return tree_sum(o, [&](int i) { return a[i] * b[i]; });
 }
 
 struct SolveInfo {
@@ -170,70 +237,93 @@ struct SolveInfo {
   bool converged = false;
 };
 
-// Right-Jacobi-preconditioned BiCGSTAB, zero initial guess, stop when ||r||^2 <= tol^2 ||b||^2.
-// On near-breakdown (|rho| < eps^2 ||r0||^2) it restarts from the true residual with p = r.
+std::vector<double> inverse_diagonal(const CSR &A, std::vector<double> *diag = nullptr) {
+  std::vector<double> inv(A.n, 1.0);
+  if (diag) diag->assign(A.n, 0.0);
+  for (int64_t i = 0; i < A.n; ++i)
+    for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k)
+      if (A.col[k] == i) {
+        inv[i] = (A.val[k] != 0.0) ? 1.0 / A.val[k] : 1.0;
+        if (diag) (*diag)[i] = A.val[k];
+      }
+  return inv;
+}
+
+// Right-Jacobi-preconditioned BiCGSTAB (van der Vorst 1992), zero initial guess, stop when
+// ||r||^2 <= tol^2 ||b||^2 or after maxit iterations. The preconditioned operator is applied as
+// the column-scaled matrix At = A diag(1/a_jj); x is kept in original variables
+// (x += alpha D^-1 p + omega D^-1 s). A zero denominator (r0.v or, when unconverged, omega) or a
+// NaN residual ends the solve unconverged. Near-breakdown (|rho| < eps^2 ||r0||^2) restarts from
+// the true residual with r0 = r, p = r. `init` orders the ||b||^2 reduction, `sell` the products
+// fused into the sparse products, `nat` the rest.
 SolveInfo bicgstab(const CSR &A, const std::vector<double> &b, std::vector<double> &x, double tol,
-                   int maxit) {
+                   int maxit, const RedOrder &init, const RedOrder &sell, const RedOrder &nat) {
   const int64_t n = A.n;
   SolveInfo info;
-  std::vector<double> invdiag(n, 1.0);
+  std::vector<double> diag;
+  const std::vector<double> invdiag = inverse_diagonal(A, &diag);
+  CSR At = A;
   for (int64_t i = 0; i < n; ++i)
-    for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k)
-      if (A.col[k] == i) invdiag[i] = (A.val[k] != 0.0) ? 1.0 / A.val[k] : 1.0;
+    for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) At.val[k] = A.val[k] * invdiag[A.col[k]];
   x.assign(n, 0.0);
-  const double bnorm2 = dot(b.data(), b.data(), n);
-  if (std::isnan(bnorm2)) return info;  // NaN right-hand side: not converged
-  if (bnorm2 == 0.0) {
+  const double bnorm2 = odot(init, b.data(), b.data());
+  const double tol2 = tol * tol * bnorm2;
+  if (std::isnan(bnorm2)) return info;
+  if (bnorm2 == 0.0 || bnorm2 <= tol2) {
     info.converged = true;
     return info;
   }
-  std::vector<double> r(b), r0(b), p(n, 0.0), v(n, 0.0), y(n), s(n), z(n), t(n);
-  double r0norm2 = bnorm2;
-  double rho = 1.0, alpha = 1.0, w = 1.0;
-  const double tol2 = tol * tol * bnorm2;
+  std::vector<double> r(b), r0(b), p(n, 0.0), v(n, 0.0), s(n), t(n), dx(n);
+  double r0norm2 = bnorm2, rho = bnorm2, alpha = 1.0, w = 1.0, beta = 0.0;
   const double eps = std::numeric_limits<double>::epsilon();
+  bool restart = false;
   double rn2 = bnorm2;
   int i = 0;
-  while (rn2 > tol2 && i < maxit) {
-    const double rho_old = rho;
-    rho = dot(r0.data(), r.data(), n);
-    bool restart = std::fabs(rho) < eps * eps * r0norm2;
-    double beta;
+  while (true) {
     if (restart) {
-      spmv(A, x.data(), t.data());
-      for (int64_t k = 0; k < n; ++k) r[k] = b[k] - t[k];
-      r0 = r;
-      rho = r0norm2 = dot(r.data(), r.data(), n);
-      beta = 0.0;
+      for (int64_t k = 0; k < n; ++k) dx[k] = diag[k] * x[k];
+      spmv(At, dx.data(), t.data());
+      for (int64_t k = 0; k < n; ++k) {
+        r[k] = b[k] - t[k];
+        r0[k] = r[k];
+        p[k] = r[k];
+      }
+      rho = r0norm2 = odot(sell, r.data(), r.data());
+      restart = false;
     } else {
-      beta = (rho / rho_old) * (alpha / w);
-    }
 #pragma omp parallel for schedule(static)
-    for (int64_t k = 0; k < n; ++k) {
-      p[k] = r[k] + beta * (p[k] - w * v[k]);
-      y[k] = invdiag[k] * p[k];
+      for (int64_t k = 0; k < n; ++k) p[k] = r[k] + beta * (p[k] - w * v[k]);
     }
-    spmv(A, y.data(), v.data());
-    const double r0v = dot(r0.data(), v.data(), n);
-    if (r0v == 0.0) break;  // breakdown: reported as not converged
+    spmv(At, p.data(), v.data());
+    const double r0v = odot(sell, r0.data(), v.data());
+    if (r0v == 0.0) break;
     alpha = rho / r0v;
 #pragma omp parallel for schedule(static)
-    for (int64_t k = 0; k < n; ++k) {
-      s[k] = r[k] - alpha * v[k];
-      z[k] = invdiag[k] * s[k];
-    }
-    spmv(A, z.data(), t.data());
-    const double tt = dot(t.data(), t.data(), n);
-    w = (tt > 0.0) ? dot(t.data(), s.data(), n) / tt : 0.0;
+    for (int64_t k = 0; k < n; ++k) s[k] = r[k] - alpha * v[k];
+    spmv(At, s.data(), t.data());
+    const double tt = odot(sell, t.data(), t.data());
+    const double ts = odot(sell, t.data(), s.data());
+    w = (tt > 0.0) ? ts / tt : 0.0;
 #pragma omp parallel for schedule(static)
     for (int64_t k = 0; k < n; ++k) {
-      x[k] += alpha * y[k] + w * z[k];
+      const double y = invdiag[k] * p[k];
+      const double z = invdiag[k] * s[k];
+      x[k] += alpha * y + w * z;
       r[k] = s[k] - w * t[k];
     }
-    rn2 = dot(r.data(), r.data(), n);
+    rn2 = odot(nat, r.data(), r.data());
+    const double rho_new = odot(nat, r0.data(), r.data());
     ++i;
-    if (std::isnan(rn2)) break;         // NaN residual: reported as not converged
-    if (w == 0.0 && rn2 > tol2) break;  // breakdown: reported as not converged
+    if (std::isnan(rn2) || std::isnan(rho_new)) break;
+    if (rn2 <= tol2) break;
+    if (i >= maxit) break;
+    if (w == 0.0) break;
+    if (std::fabs(rho_new) < eps * eps * r0norm2) {
+      restart = true;
+    } else {
+      beta = (rho_new / rho) * (alpha / w);
+      rho = rho_new;
+    }
   }
   info.iters = i;
   info.rel_res = std::sqrt(rn2 / bnorm2);
@@ -241,48 +331,43 @@ SolveInfo bicgstab(const CSR &A, const std::vector<double> &b, std::vector<doubl
   return info;
 }
 
-// Jacobi-preconditioned CG, zero initial guess, same stopping rule.
+// Jacobi-preconditioned CG (Hestenes-Stiefel), zero initial guess, same stopping rule; p.q is
+// fused into the sparse product (`sell` order), the other reductions use `nat`.
 SolveInfo cg(const CSR &A, const std::vector<double> &b, std::vector<double> &x, double tol,
-             int maxit) {
+             int maxit, const RedOrder &sell, const RedOrder &nat) {
   const int64_t n = A.n;
   SolveInfo info;
-  std::vector<double> invdiag(n, 1.0);
-  for (int64_t i = 0; i < n; ++i)
-    for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k)
-      if (A.col[k] == i) invdiag[i] = (A.val[k] != 0.0) ? 1.0 / A.val[k] : 1.0;
+  const std::vector<double> invdiag = inverse_diagonal(A);
   x.assign(n, 0.0);
-  const double bnorm2 = dot(b.data(), b.data(), n);
-  if (bnorm2 == 0.0) {
-    info.converged = true;
-    return info;
-  }
-  if (std::isnan(bnorm2)) return info;  // NaN right-hand side: not converged
-  const double thr = tol * tol * bnorm2;
   std::vector<double> r(b), z(n), p(n), q(n);
+  for (int64_t k = 0; k < n; ++k) z[k] = invdiag[k] * r[k];
+  const double bnorm2 = odot(nat, b.data(), b.data());
+  double absnew = odot(nat, b.data(), z.data());
+  const double thr = tol * tol * bnorm2;
+  if (std::isnan(bnorm2)) return info;
   double rn2 = bnorm2;
   int i = 0;
-  if (rn2 > thr) {
-    for (int64_t k = 0; k < n; ++k) z[k] = invdiag[k] * r[k];
+  if (!(bnorm2 == 0.0 || bnorm2 <= thr)) {
     p = z;
-    double absnew = dot(r.data(), z.data(), n);
-    while (i < maxit) {
+    while (true) {
       spmv(A, p.data(), q.data());
-      const double pq = dot(p.data(), q.data(), n);
-      if (pq == 0.0) break;  // breakdown: reported as not converged
+      const double pq = odot(sell, p.data(), q.data());
+      if (pq == 0.0) break;
       const double alpha = absnew / pq;
 #pragma omp parallel for schedule(static)
       for (int64_t k = 0; k < n; ++k) {
         x[k] += alpha * p[k];
-        r[k] -= alpha * q[k];
+        r[k] = r[k] - alpha * q[k];
+        z[k] = invdiag[k] * r[k];
       }
-      rn2 = dot(r.data(), r.data(), n);
+      rn2 = odot(nat, r.data(), r.data());
+      const double rz = odot(nat, r.data(), z.data());
       ++i;
-      if (rn2 <= thr || std::isnan(rn2)) break;
-#pragma omp parallel for schedule(static)
-      for (int64_t k = 0; k < n; ++k) z[k] = invdiag[k] * r[k];
-      const double absold = absnew;
-      absnew = dot(r.data(), z.data(), n);
-      const double beta = absnew / absold;
+      if (std::isnan(rn2) || std::isnan(rz)) break;
+      if (rn2 <= thr) break;
+      if (i >= maxit) break;
+      const double beta = rz / absnew;
+      absnew = rz;
 #pragma omp parallel for schedule(static)
       for (int64_t k = 0; k < n; ++k) p[k] = z[k] + beta * p[k];
     }
@@ -323,6 +408,7 @@ struct Oracle {
   std::vector<V3> u, ustar;
   std::vector<double> p, pcorr, inv_lumped;
   CSR M, K, Gx, Gy, Gz, L;
+  RedOrder order_p2, order_p1, order_n2, order_nv;  // reduction orders (see tree_sum)
   bool initialized = false;
 
   // stats of the last step
@@ -572,6 +658,10 @@ struct Oracle {
     build_stiffness();
     build_gradient();
     build_poisson();
+    order_p2 = sell_order(M);
+    order_p1 = sell_order(L);
+    order_n2 = natural_order((int64_t)N2);
+    order_nv = natural_order((int64_t)nv);
     for (size_t i = 0; i < N2; ++i)
       if (bc_of(i) == kInlet) u[i] = inlet[i];
     if (reference_node < 0 && outlet_type == kNeumann) {
@@ -643,7 +733,7 @@ struct Oracle {
           rhs[i] += penalty * up;
         }
       }
-      SolveInfo si = bicgstab(lhs, rhs, x, tol_mom, maxit_mom);
+      SolveInfo si = bicgstab(lhs, rhs, x, tol_mom, maxit_mom, order_p2, order_p2, order_n2);
       it_mom[comp] = si.iters;
       res_mom[comp] = si.rel_res;
       if (!si.converged) {
@@ -709,8 +799,9 @@ struct Oracle {
           rhs[i] += penalty * outlet_pressure;
         }
     }
-    SolveInfo si = (pressure_solver == 1) ? cg(Lbc, rhs, x, tol_p, maxit_p)
-                                          : bicgstab(Lbc, rhs, x, tol_p, maxit_p);
+    SolveInfo si = (pressure_solver == 1)
+                       ? cg(Lbc, rhs, x, tol_p, maxit_p, order_p1, order_nv)
+                       : bicgstab(Lbc, rhs, x, tol_p, maxit_p, order_nv, order_p1, order_nv);
     it_p = si.iters;
     res_p = si.rel_res;
     if (!si.converged) {

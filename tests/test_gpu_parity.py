@@ -1,8 +1,9 @@
 """GPU solver (libcfsa.so, sm_100a) against the CPU oracle on identical meshes and inputs.
 
-Bars: assembly, element operators and forces are bit-exact (same arithmetic order, no FMA);
-PISO states agree to relative L2 <= 1e-8 in FP64 (Krylov dot products are reduced in a
-different order on the device, everything else is identical).
+Bars: assembly, element operators and forces are bit-exact (same arithmetic order, no FMA).
+PISO states must agree to relative L2 <= 1e-8 in FP64 (the stated tolerance); because the oracle
+reduces its Krylov dot products in the device's fixed tree, FP64 trajectories are in fact
+bit-identical, which test_trajectory_bit_exact and the config-0 run check explicitly.
 """
 import os
 import sys
@@ -165,6 +166,7 @@ def test_config0_parity_100_steps(cf, po):
     eu, ep = rel_l2(s.getVelocity(), st["u"]), rel_l2(s.getPressure(), st["p"])
     print(f"config0 100 steps: rel L2 u {eu:.3e} p {ep:.3e}")
     assert eu < 1e-8 and ep < 1e-8
+    assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"])
 
 
 def test_reference_default_tolerances(cf, po):
@@ -310,3 +312,21 @@ def test_reassembly_after_vertex_motion(cf, po):
     o2.initialize()
     for which, name in [(0, "M"), (1, "K"), (2, "Gx"), (5, "L")]:
         assert csr_equal(s.matrix(which), o2.matrix(name)), name
+
+
+@pytest.mark.parametrize("krylov", [0, 1], ids=["cg", "bicgstab"])
+def test_trajectory_bit_exact(cf, po, krylov):
+    """The oracle reduces its Krylov dot products in the device's fixed tree and applies the
+    same column-scaled operator, so FP64 trajectories agree bit for bit, iteration counts too."""
+    m = make_mesh(cf, 3, 12)
+    s, o = make_pair(cf, po, m, tol=1e-10, krylov=krylov)
+    for k in range(6):
+        assert s.pisoStep() and o.piso_step() == 0
+        gs, os_ = s.stats(), o.stats()
+        assert gs["momentum_iters"] == os_["momentum_iters"], k
+        assert gs["pressure_iters"] == os_["pressure_iters"], k
+        st = o.state()
+        assert np.array_equal(s.getVelocityStar(), st["ustar"]), k
+        assert np.array_equal(s.getPressureCorrection(), st["pcorr"]), k
+        assert np.array_equal(s.getVelocity(), st["u"]), k
+        assert np.array_equal(s.getPressure(), st["p"]), k
