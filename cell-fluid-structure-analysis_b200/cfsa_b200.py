@@ -180,6 +180,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "cfsa_ns_get_matrix": (i32, [vp, i32, vp, vp, vp]),
         "cfsa_ns_get_inv_lumped_mass": (i32, [vp, vp]),
         "cfsa_ns_profile_kernel": (i32, [vp, i32, i32, vp, vp]),
+        "cfsa_ns_compute_divergence_noalloc": (i32, [vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -454,6 +455,11 @@ class NavierStokesSolver:
         out = np.empty(self.nv)
         self._check(self._lib.cfsa_ns_compute_divergence(self._h, _ptr(u), _ptr(out)))
         return out
+
+    def computeDivergenceNoAlloc(self, u_dev_ptr: int, div_dev_ptr: int) -> int:
+        """Divergence on caller-owned device arrays (u [3][N2] component-major, div [nv]) with
+        no device allocation; returns the C status code."""
+        return self._lib.cfsa_ns_compute_divergence_noalloc(self._h, C.c_void_p(u_dev_ptr), C.c_void_p(div_dev_ptr))
 
     def computeAdvectionRHS(self) -> np.ndarray:
         out = np.empty((self.N2, 3))

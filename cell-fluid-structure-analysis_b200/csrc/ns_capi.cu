@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <exception>
+#include <mutex>
 #include <new>
 #include <numeric>
 #include <string>
@@ -1329,6 +1330,61 @@ extern "C" int cfsa_ns_profile_kernel(cfsa_ns *h, int which, int iters, double *
   if (!h || !avg_ms || !alg_bytes || iters < 1) return CFSA_BAD_ARG;
   return guarded(h, [&] {
     h->profile_kernel(which, iters, avg_ms, alg_bytes);
+    return CFSA_OK;
+  });
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free divergence. Its per-tet scratch is a static device array instead of handle
+// memory; callers pass device inputs and outputs.
+namespace {
+constexpr int64_t kNoAllocMaxTets = int64_t(1) << 20;  // 8 MiB per GPU that loads the library
+__device__ __align__(256) double g_noalloc_divt[kNoAllocMaxTets];
+
+std::mutex g_noalloc_mutex;
+constexpr int kNoAllocMaxDevices = 256;
+double *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_divt for the current device (host code cannot use the symbol
+// itself as a device address). Looked up once per device, under a lock.
+int noalloc_scratch(cfsa_ns *h, double **out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(h, CFSA_CUDA_ERROR, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(h, CFSA_BAD_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void *ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_noalloc_divt);
+    if (e != cudaSuccess || !ptr)
+      return fail(h, CFSA_CUDA_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<double *>(ptr);
+  }
+  *out = g_noalloc_ptr[dev];
+  return CFSA_OK;
+}
+}  // namespace
+
+extern "C" int cfsa_ns_compute_divergence_noalloc(cfsa_ns *h, const double *u_dev, double *div_dev) {
+  if (!h || !u_dev || !div_dev) return CFSA_BAD_ARG;
+  if (h->nt > kNoAllocMaxTets)
+    return fail(h, CFSA_BAD_ARG,
+                "cfsa_ns_compute_divergence_noalloc: mesh has " + std::to_string(h->nt) +
+                    " tets, the static scratch holds at most " + std::to_string(kNoAllocMaxTets));
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess || cur != h->device) {
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, CFSA_CUDA_ERROR, "cannot select the handle's device");
+  }
+  double *scratch = nullptr;
+  const int code = noalloc_scratch(h, &scratch);
+  if (code != CFSA_OK) return code;
+  return guarded(h, [&] {
+    k_tet_div<<<blocks_for(h->nt), kBlock, 0, h->stream>>>((int)h->nt, h->N2, h->tnode, h->grad, u_dev,
+                                                           scratch, nullptr);
+    k_gather_div<<<blocks_for(h->nv), kBlock, 0, h->stream>>>((int)h->nv, h->adj_ptr, h->adj, h->vol,
+                                                              scratch, div_dev);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
     return CFSA_OK;
   });
 }

@@ -185,6 +185,21 @@ int cfsa_ns_get_inv_lumped_mass(cfsa_ns *h, double *out /*[N2]*/);
  * row metadata, each vector element read or written once). */
 int cfsa_ns_profile_kernel(cfsa_ns *h, int which, int iters, double *avg_ms, double *alg_bytes);
 
+/* ---- allocation-free operator (no counterpart in the reference) ---- */
+/* Divergence (the computeDivergence operator above) for callers that cannot allocate device
+ * memory at call time: code running while a CUDA graph is being captured (cudaMalloc is not
+ * allowed then), hosts whose memory pool has reserved the whole device, and tight coupling loops
+ * that must not pay allocation latency. Inputs and outputs are the caller's device arrays:
+ * u_dev [3][N2] component-major doubles (all x, then all y, then all z), div_dev [nv] doubles.
+ * The per-tet intermediate lives in a file-scope static device array of 1,048,576 doubles (8 MiB),
+ * held by every GPU that loads this library until the process exits; meshes with more tets are
+ * rejected with CFSA_BAD_ARG. The first call on a device looks that array's address up, so make
+ * the first call before any stream capture. Every call shares the one array and every entry a
+ * call reads is written by the same call first, so nothing needs clearing; calls that overlap on
+ * the GPU (other threads or other handles) race on it. Runs on the handle's stream and returns
+ * once div_dev is written. */
+int cfsa_ns_compute_divergence_noalloc(cfsa_ns *h, const double *u_dev, double *div_dev);
+
 #ifdef __cplusplus
 }
 #endif
