@@ -313,6 +313,8 @@ def main():
             "dof_updates_per_s": value * (3 * N2 + nv),
             "krylov_iters_per_step": [st["krylov_iters"][0] / args.steps, st["krylov_iters"][1] / args.steps],
             "gpu_launches": int(st["kernel_launches"]),
+            "phase_ms_last_step": {"momentum": st["phase_ms"][0], "pressure_solve": st["phase_ms"][1],
+                                   "other": st["phase_ms"][2]},
             "roofline": roofline, "kernels": kernels,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(profile.nbytes),
                     "d2h_bytes_per_step": int(u.nbytes + p.nbytes)},

@@ -86,6 +86,7 @@ class Stats(C.Structure):
         ("steps", C.c_int64), ("time", C.c_double), ("last_step_ms", C.c_double),
         ("nnz_p2", C.c_int64), ("nnz_p1", C.c_int64),
         ("kernel_launches", C.c_int64), ("krylov_iters", C.c_int64 * 2),
+        ("phase_ms", C.c_double * 3),
     ]
 
     def as_dict(self) -> dict:
@@ -101,6 +102,7 @@ class Stats(C.Structure):
             "nnz_p2": int(self.nnz_p2), "nnz_p1": int(self.nnz_p1),
             "kernel_launches": int(self.kernel_launches),
             "krylov_iters": [int(x) for x in self.krylov_iters],
+            "phase_ms": [float(x) for x in self.phase_ms],
         }
 
 

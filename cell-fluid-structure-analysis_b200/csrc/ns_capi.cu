@@ -107,6 +107,12 @@ struct cfsa_ns {
   double *h_stage = nullptr;  // pinned [3][N2] staging for host transfers
   BicgState *bs_prof = nullptr;
   CgState *cs_prof = nullptr;
+  // persistent CG
+  bool cg_persistent = true;
+  int cg_grid = 0;
+  unsigned int *bar_count = nullptr, *bar_gen = nullptr;
+  int *bar_err = nullptr;
+  double *cg_part_a = nullptr, *cg_part_b = nullptr;
   int64_t batch_launches = 0;
   int64_t batch_iters[2] = {0, 0};
   int launches_per_step = 0;  // kernels of one step outside the Krylov loop bodies
@@ -116,6 +122,7 @@ struct cfsa_ns {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ph[4] = {nullptr, nullptr, nullptr, nullptr};  // step phase boundaries
 
   template <class T>
   T *dalloc(size_t count) {
@@ -142,6 +149,8 @@ struct cfsa_ns {
     if (h_stage) cudaFreeHost(h_stage);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    for (cudaEvent_t e : ph)
+      if (e) cudaEventDestroy(e);
     if (body_stream) cudaStreamDestroy(body_stream);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -226,6 +235,7 @@ struct cfsa_ns {
     CK(cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
+    for (cudaEvent_t &e : ph) CK(cudaEventCreate(&e));
     nv = m->nv;
     nt = m->nt;
     ne = m->ne;
@@ -364,6 +374,24 @@ struct cfsa_ns {
       fpress = dalloc<double>((size_t)nbf * 3);
     }
     fout = dalloc<double>((size_t)nv * 3);
+    // persistent CG: co-resident grid, barrier words, partial buffers
+    {
+      int nsm = 0, per_sm = 0;
+      CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent, kBlock, 0));
+      const int nblk_sell = (int)blocks_for(s1.nrows_pad), nblk_nat = (int)blocks_for(nv);
+      cg_grid = std::min(nsm * per_sm, std::max(nblk_sell, nblk_nat));
+      bar_count = dalloc<unsigned int>(1);
+      bar_gen = dalloc<unsigned int>(1);
+      bar_err = dalloc<int>(1);
+      CK(cudaMemsetAsync(bar_count, 0, sizeof(unsigned int), stream));
+      CK(cudaMemsetAsync(bar_gen, 0, sizeof(unsigned int), stream));
+      CK(cudaMemsetAsync(bar_err, 0, sizeof(int), stream));
+      cg_part_a = dalloc<double>((size_t)nblk_sell * kMaxRed);
+      cg_part_b = dalloc<double>((size_t)nblk_nat * kMaxRed);
+      if (cg_grid < 1) cg_persistent = false;
+    }
+    if (const char *e = std::getenv("CFSA_CG_LOOP")) cg_persistent = cg_persistent && (std::atoi(e) == 0);
     assemble();
     if (const char *e = std::getenv("CFSA_NO_GRAPH")) use_graph = (std::atoi(e) == 0);
     CK(cudaStreamSynchronize(stream));
@@ -590,6 +618,38 @@ struct cfsa_ns {
       else
         eager_while(body, [&] { return poll_bicg(bs_p); }, maxit_p);
       k_check_bicg<<<1, 1, 0, stream>>>(bs_p, 1, 1, st);
+    } else if (cg_persistent) {
+      CgPersistentArgs c{};
+      c.S = s1.view();
+      c.Ls = Ls;
+      c.invL = invL;
+      c.x = pc;
+      c.r = pr;
+      c.z = pz;
+      c.q = pq;
+      c.p[0] = pp;
+      c.p[1] = ps;
+      c.n = (int)nv;
+      c.nblk_sell = (int)blocks_for(s1.nrows_pad);
+      c.nblk_nat = (int)blocks_for(nv);
+      c.part_a = cg_part_a;
+      c.part_b = cg_part_b;
+      c.cs = cs;
+      c.st = st;
+      c.bar = GridBarrier{bar_count, bar_gen, bar_err};
+      CK(cudaMemsetAsync(bar_count, 0, sizeof(unsigned int), stream));
+      CK(cudaMemsetAsync(bar_err, 0, sizeof(int), stream));
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned int)cg_grid);
+      cfg.blockDim = dim3(kBlock);
+      cfg.stream = stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      CK(cudaLaunchKernelEx(&cfg, k_cg_persistent, c));
+      k_check_cg<<<1, 1, 0, stream>>>(cs, st, bar_err);
     } else {
       CgArgs c{};
       c.S = s1.view();
@@ -616,7 +676,7 @@ struct cfsa_ns {
         capture_while(body);
       else
         eager_while(body, [&] { return poll_cg(); }, maxit_p);
-      k_check_cg<<<1, 1, 0, stream>>>(cs, st);
+      k_check_cg<<<1, 1, 0, stream>>>(cs, st, nullptr);
     }
     CK(cudaGetLastError());
   }
@@ -670,16 +730,31 @@ struct cfsa_ns {
   // pisoStep (ncorr correctors) or simpleStep (one corrector). The 2nd and later correctors of
   // the reference solve the identical system again (the divergence is always that of u*), so
   // their pressure correction is the first one's; only the p update and u correction repeat.
+  // Phase boundary; inside stream capture it must become an event-record node of the graph.
+  void mark_phase(int k, bool capture) {
+    if (capture)
+      CK(cudaEventRecordWithFlags(ph[k], stream, cudaEventRecordExternal));
+    else
+      CK(cudaEventRecord(ph[k], stream));
+  }
+
   void enqueue_step(bool capture, bool simple) {
+    mark_phase(0, capture);
     enqueue_momentum(capture);
+    mark_phase(1, capture);
     const int nc = simple ? 1 : ncorr;
     const bool normalize = (ref_node >= 0 && ref_node < nv);
     for (int c = 0; c < nc; ++c) {
-      if (c == 0) enqueue_pressure_solve(capture);
+      if (c == 0) {
+        enqueue_pressure_solve(capture);
+        mark_phase(2, capture);
+      }
       enqueue_pressure_update();
       enqueue_correct();
     }
+    if (nc == 0) mark_phase(2, capture);
     enqueue_finish();
+    mark_phase(3, capture);
     // tet_conv, momentum_rhs, check, [tet_div, pressure_rhs, check], per corrector
     // update (+ stash + normalize) and correct, finish
     launches_per_step = 3 + (nc > 0 ? 3 : 0) + nc * (2 + (normalize ? 2 : 0)) + 1;
@@ -716,7 +791,7 @@ struct cfsa_ns {
     CK(cudaEventSynchronize(ev1));
     CK(cudaStreamSynchronize(stream));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
-    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : 3;
+    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : (cg_persistent ? 1 : 3);
     batch_launches = (int64_t)launched_steps * launches_per_step + 5 * (int64_t)h_st->body_runs[0] +
                      pressure_body * (int64_t)h_st->body_runs[1];
     batch_iters[0] = (int64_t)h_st->iters[0];
@@ -837,8 +912,11 @@ int fail(cfsa_ns *h, int code, const std::string &msg) {
   return code;
 }
 
+// Runs one C-ABI operation. The thread's CUDA last-error state is cleared first, so that the
+// launch checks inside report this operation's own failures only.
 template <class F>
 int guarded(cfsa_ns *h, F &&f) {
+  (void)cudaGetLastError();
   try {
     return f();
   } catch (const CudaError &e) {
@@ -1194,6 +1272,18 @@ int cfsa_ns_get_stats(const cfsa_ns *hc, cfsa_ns_stats *s) {
     s->nnz_p2 = h->nnz2;
     s->nnz_p1 = h->nnz1;
     s->kernel_launches = h->batch_launches;
+    if (h->steps > 0) {
+      float a = 0.f, b = 0.f, c = 0.f;
+      if (cudaEventElapsedTime(&a, h->ph[0], h->ph[1]) == cudaSuccess &&
+          cudaEventElapsedTime(&b, h->ph[1], h->ph[2]) == cudaSuccess &&
+          cudaEventElapsedTime(&c, h->ph[2], h->ph[3]) == cudaSuccess) {
+        s->phase_ms[0] = a;
+        s->phase_ms[1] = b;
+        s->phase_ms[2] = c;
+      } else {
+        (void)cudaGetLastError();  // phases not recorded (no full step yet): leave zeros
+      }
+    }
     s->krylov_iters[0] = h->batch_iters[0];
     s->krylov_iters[1] = h->batch_iters[1];
     return CFSA_OK;

@@ -438,6 +438,47 @@ __global__ void k_gather_div(int nv, const int *__restrict__ adj_ptr, const int 
   out[i] = gather_div(i, adj_ptr, adj, vol, divt);
 }
 
+// One SELL row, NC right-hand sides sharing the matrix. Entries are fetched in chunks of U
+// (all column indices and values of a chunk first, then the U*NC gathers) so that many loads are
+// in flight per thread; the products are still accumulated in ascending column order, so the
+// result is bit-identical to the sequential CSR row sum. Matrix entries are streamed once per
+// product (evict-first), the gathered vector stays cacheable.
+template <int NC, int U = 8>
+__device__ __forceinline__ void sell_spmv_row(const SellView &S, const double *__restrict__ val,
+                                              const double *__restrict__ x, int64_t n, int r,
+                                              double acc[NC]) {
+  const int base = S.sptr[r >> 5] + (r & 31), len = S.len[r];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+  int k = 0;
+  for (; k + U <= len; k += U) {
+    int j[U];
+    double a[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int pos = base + (k + u) * kSellC;
+      j[u] = __ldcs(S.col + pos);
+      a[u] = __ldcs(val + pos);
+    }
+    double xv[U][NC];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) xv[u][c] = __ldg(x + c * n + j[u]);
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[c] += a[u] * xv[u][c];
+  }
+  for (; k < len; ++k) {
+    const int pos = base + k * kSellC;
+    const int j = __ldcs(S.col + pos);
+    const double a = __ldcs(val + pos);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] += a * __ldg(x + c * n + j);
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Momentum right-hand side (NavierStokes.cpp:429-495) for the three components, fused with the
 // initialisation of the batched BiCGSTAB (x0 = 0, r = r0 = b, p = v = 0).
@@ -467,16 +508,8 @@ __global__ void k_momentum_rhs(MomentumRhsArgs A) {
   const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
   if (i >= 0) {
     const int64_t n = A.n;
-    const int base = A.S.sptr[r >> 5] + (r & 31), len = A.S.len[r];
-    double mu[3] = {0.0, 0.0, 0.0};
-    for (int k = 0; k < len; ++k) {
-      const int pos = base + k * kSellC;
-      const int c = A.S.col[pos];
-      const double m = A.Ms[pos];
-      mu[0] += m * A.u[c];
-      mu[1] += m * A.u[n + c];
-      mu[2] += m * A.u[2 * n + c];
-    }
+    double mu[3];
+    sell_spmv_row<3>(A.S, A.Ms, A.u, n, r, mu);
     double b[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) b[c] = 0.0 + mu[c] / A.dt;
@@ -561,22 +594,6 @@ struct BicgArgs {
   DevStatus *st;  // launch counters
   int slot;       // 0 momentum, 1 pressure
 };
-
-template <int NC>
-__device__ __forceinline__ void sell_spmv_row(const SellView &S, const double *__restrict__ val,
-                                              const double *__restrict__ x, int64_t n, int r,
-                                              double acc[NC]) {
-  const int base = S.sptr[r >> 5] + (r & 31), len = S.len[r];
-#pragma unroll
-  for (int c = 0; c < NC; ++c) acc[c] = 0.0;
-  for (int k = 0; k < len; ++k) {
-    const int pos = base + k * kSellC;
-    const int j = S.col[pos];
-    const double a = val[pos];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) acc[c] += a * x[c * n + j];
-  }
-}
 
 // K1: p = r + beta (p - omega v); on restart: r = b - A x, r0 = r, p = r, rho = |r|^2.
 template <int NC>
@@ -792,12 +809,13 @@ __global__ void k_check_bicg(const BicgState *__restrict__ bs, int ncomp, int sl
   }
 }
 
-__global__ void k_check_cg(const CgState *__restrict__ cs, DevStatus *st) {
+__global__ void k_check_cg(const CgState *__restrict__ cs, DevStatus *st, const int *__restrict__ barrier_err) {
   if (st->halt) return;
   st->iters[1] += (unsigned long long)cs->iters;
   int code = 0;
   if (cs->status == KS_MAXIT) code = 1;
   if (cs->status == KS_BREAKDOWN) code = 2;
+  if (barrier_err && *barrier_err) code = 4;  // persistent solve gave up waiting at a grid barrier
   if (code) {
     st->code = code;
     st->halt = 1;
@@ -965,6 +983,212 @@ __global__ void k_cg_p(CgArgs A) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   A.pk[i] = A.z[i] + A.cs->beta * A.pk[i];
+}
+
+// ------------------------------------------------------------------------------------------
+// Persistent CG: the whole pressure solve in one cooperative launch. Per iteration:
+//   A  (SELL blocks)    p_new = z + beta p (on the fly, double-buffered), q = L p_new, p.q partials
+//   -- grid barrier --
+//   B  (natural blocks) alpha = absnew / (p.q); x += alpha p; r -= alpha q; z = D^-1 r; r.r, r.z
+//   -- grid barrier --
+//   C  (every CTA)      totals, convergence test, beta
+// Every CTA recomputes the totals from the block partials with the same tree as grid_reduce, so
+// all CTAs take the same decisions and the iterates equal those of k_cg_q / k_cg_xr / k_cg_p bit
+// for bit. Data written by other CTAs inside the launch is read with L1-bypassing loads.
+// Barriers spin with a bound; on expiry the kernel records an error and every CTA returns.
+constexpr long long kBarrierSpinLimit = 1LL << 25;
+
+struct GridBarrier {
+  unsigned int *count;
+  unsigned int *gen;
+  int *err;
+};
+
+__device__ __forceinline__ bool grid_sync(const GridBarrier &B) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int *vgen = B.gen;
+    volatile int *verr = B.err;
+    const unsigned int g = *vgen;
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(B.count, 1u) == gridDim.x - 1) {
+      *B.count = 0u;
+      __threadfence();
+      atomicAdd(B.gen, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == g) {
+        if (*verr) {
+          ok = 0;
+          break;
+        }
+        if (++spins > kBarrierSpinLimit) {
+          atomicExch(B.err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    s_ok = ok && (*verr == 0);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Same tree as the last block of grid_reduce: thread t sums partials t, t+256, ... in order,
+// then warp butterflies and an in-order sum over the 8 warps. All threads get the totals.
+template <int NV>
+__device__ __forceinline__ void tree_total(const double *__restrict__ partials, int nblk,
+                                           double (&out)[NV]) {
+  __shared__ double sm[NV][kBlock / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += __ldcg(&partials[(size_t)b * kMaxRed + j]);
+    s = warp_sum(s);
+    if (lane == 0) sm[j][warp] = s;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sm[j][w];
+    out[j] = s;
+  }
+  __syncthreads();
+}
+
+// First stage of grid_reduce for one block of 256 positions: the block partial.
+template <int NV>
+__device__ __forceinline__ void block_partial(double (&v)[NV], double *__restrict__ partials, int b) {
+  __shared__ double sm[NV][kBlock / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    const double w = warp_sum(v[j]);
+    if (lane == 0) sm[j][warp] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sm[j][w];
+      partials[(size_t)b * kMaxRed + j] = s;
+    }
+  }
+  __syncthreads();
+}
+
+struct CgPersistentArgs {
+  SellView S;
+  const double *Ls, *invL;
+  double *x, *r, *z, *q;
+  double *p[2];  // search direction, double-buffered
+  int n;
+  int nblk_sell, nblk_nat;
+  double *part_a, *part_b;  // block partials of phases A and B
+  CgState *cs;
+  DevStatus *st;
+  GridBarrier bar;
+};
+
+__global__ void __launch_bounds__(kBlock) k_cg_persistent(CgPersistentArgs A) {
+  if (A.st && A.st->halt) return;
+  if (!A.cs->active) return;
+  const double tol2 = A.cs->tol2;
+  const int maxit = A.cs->maxit;
+  double absnew = A.cs->absnew, beta = 0.0, alpha = 0.0, rr = 0.0;
+  int it = 0, status = KS_RUNNING, cur = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[1] += 1;
+  while (true) {
+    const bool first = (it == 0);
+    const double *pold = A.p[cur];
+    double *pnew = A.p[cur ^ 1];
+    // phase A: q = L p_new on SELL blocks
+    for (int b = blockIdx.x; b < A.nblk_sell; b += gridDim.x) {
+      const int r = b * kBlock + threadIdx.x;
+      const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+      double v[1] = {0.0};
+      if (i >= 0) {
+        const int base = A.S.sptr[r >> 5] + (r & 31), len = A.S.len[r];
+        double acc = 0.0;
+        for (int k = 0; k < len; ++k) {
+          const int pos = base + k * kSellC;
+          const int jj = __ldg(A.S.col + pos);
+          const double a = __ldg(A.Ls + pos);
+          const double pj = first ? __ldcg(pold + jj) : __ldcg(A.z + jj) + beta * __ldcg(pold + jj);
+          acc += a * pj;
+        }
+        const double pi = first ? __ldcg(pold + i) : __ldcg(A.z + i) + beta * __ldcg(pold + i);
+        __stcg(pnew + i, pi);
+        __stcg(A.q + i, acc);
+        v[0] = pi * acc;
+      }
+      block_partial<1>(v, A.part_a, b);
+    }
+    if (!grid_sync(A.bar)) return;
+    double pq[1];
+    tree_total<1>(A.part_a, A.nblk_sell, pq);
+    if (pq[0] == 0.0) {
+      status = KS_BREAKDOWN;
+      break;
+    }
+    alpha = absnew / pq[0];
+    // phase B: vector updates on natural blocks
+    for (int b = blockIdx.x; b < A.nblk_nat; b += gridDim.x) {
+      const int i = b * kBlock + threadIdx.x;
+      double v[2] = {0.0, 0.0};
+      if (i < A.n) {
+        const double xi = __ldcg(A.x + i) + alpha * __ldcg(pnew + i);
+        const double ri = __ldcg(A.r + i) - alpha * __ldcg(A.q + i);
+        const double zi = __ldg(A.invL + i) * ri;
+        __stcg(A.x + i, xi);
+        __stcg(A.r + i, ri);
+        __stcg(A.z + i, zi);
+        v[0] = ri * ri;
+        v[1] = ri * zi;
+      }
+      block_partial<2>(v, A.part_b, b);
+    }
+    if (!grid_sync(A.bar)) return;
+    double tb[2];
+    tree_total<2>(A.part_b, A.nblk_nat, tb);
+    ++it;
+    rr = tb[0];
+    if (isnan(tb[0]) || isnan(tb[1])) {
+      status = KS_BREAKDOWN;
+      break;
+    }
+    if (tb[0] <= tol2) {
+      status = KS_CONVERGED;
+      break;
+    }
+    if (it >= maxit) {
+      status = KS_MAXIT;
+      break;
+    }
+    beta = tb[1] / absnew;
+    absnew = tb[1];
+    cur ^= 1;
+    // the next phase A reads z and p_old written in phase B / the previous phase A: both are
+    // behind the barrier above
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    CgState *c = A.cs;
+    c->iters = it;
+    c->rnorm2 = rr;
+    c->alpha = alpha;
+    c->beta = beta;
+    c->absnew = absnew;
+    c->status = status;
+    c->active = 0;
+  }
 }
 
 // ------------------------------------------------------------------------------------------

@@ -98,6 +98,8 @@ typedef struct {
   int64_t nnz_p2, nnz_p1;     /* matrix sizes */
   int64_t kernel_launches;    /* device kernels launched by the last stepping call */
   int64_t krylov_iters[2];    /* Krylov iterations in the last stepping call: momentum, pressure */
+  double phase_ms[3];         /* last PISO step on the device: momentum predictor, pressure solve,
+                                 everything else (CUDA events inside the step) */
 } cfsa_ns_stats;
 
 /* kernel ids for cfsa_ns_profile_kernel */

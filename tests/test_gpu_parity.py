@@ -330,3 +330,20 @@ def test_trajectory_bit_exact(cf, po, krylov):
         assert np.array_equal(s.getPressureCorrection(), st["pcorr"]), k
         assert np.array_equal(s.getVelocity(), st["u"]), k
         assert np.array_equal(s.getPressure(), st["p"]), k
+
+
+def test_persistent_cg_equals_loop_cg(cf, po):
+    """The single-launch cooperative CG equals the three-kernel loop body bit for bit."""
+    m = make_mesh(cf, 4, 20)
+    out = []
+    for loop in ("1", "0"):
+        os.environ["CFSA_CG_LOOP"] = loop
+        try:
+            s, _ = make_pair(cf, po, m, tol=1e-10)
+        finally:
+            os.environ.pop("CFSA_CG_LOOP", None)
+        ok, done = s.pisoSteps(3)
+        assert ok and done == 3
+        out.append((s.getVelocity(), s.getPressure(), s.stats()["pressure_iters"]))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
