@@ -6,6 +6,7 @@
 // loop continues, so a step (or a batch of steps) runs with no host round trip.
 #include "cfsa_ns.h"
 #include "ns_kernels.cuh"
+#include "ns_mixed.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -46,7 +47,7 @@ inline unsigned int blocks_for(int64_t n) { return (unsigned int)((n + kBlock - 
 
 struct cfsa_ns {
   int device = 0;
-  cudaStream_t stream = nullptr, body_stream = nullptr;
+  cudaStream_t stream = nullptr, body_stream = nullptr, body_stream2 = nullptr;
   std::string err;
   std::vector<void *> allocs;
 
@@ -113,6 +114,14 @@ struct cfsa_ns {
   unsigned int *bar_count = nullptr, *bar_gen = nullptr;
   int *bar_err = nullptr;
   double *cg_part_a = nullptr, *cg_part_b = nullptr;
+  // mixed precision (FP32 inner Krylov in FP64 defect correction)
+  float *At32 = nullptr, *invA32 = nullptr;
+  float *fr = nullptr, *fr0 = nullptr, *fp = nullptr, *fv = nullptr, *fs = nullptr, *ft = nullptr,
+        *fdx = nullptr;  // [3][N2]
+  MixedState *ms = nullptr;
+  MixedState *h_ms = nullptr;
+  double mixed_inner_tol = 1e-4;
+  int mixed_inner_maxit = 300, mixed_max_outer = 30;
   int64_t batch_launches = 0;
   int64_t batch_iters[2] = {0, 0};
   int launches_per_step = 0;  // kernels of one step outside the Krylov loop bodies
@@ -147,11 +156,13 @@ struct cfsa_ns {
     if (h_bs) cudaFreeHost(h_bs);
     if (h_cs) cudaFreeHost(h_cs);
     if (h_stage) cudaFreeHost(h_stage);
+    if (h_ms) cudaFreeHost(h_ms);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     for (cudaEvent_t e : ph)
       if (e) cudaEventDestroy(e);
     if (body_stream) cudaStreamDestroy(body_stream);
+    if (body_stream2) cudaStreamDestroy(body_stream2);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -233,6 +244,7 @@ struct cfsa_ns {
     CK(cudaGetDevice(&device));
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&body_stream2, cudaStreamNonBlocking));
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
     for (cudaEvent_t &e : ph) CK(cudaEventCreate(&e));
@@ -347,6 +359,15 @@ struct cfsa_ns {
     CK(cudaMallocHost(&h_bs, 2 * sizeof(BicgState)));
     CK(cudaMallocHost(&h_cs, sizeof(CgState)));
     CK(cudaMallocHost(&h_stage, n3 * sizeof(double)));
+    CK(cudaMallocHost(&h_ms, sizeof(MixedState)));
+    At32 = dalloc<float>((size_t)s2.nentries);
+    invA32 = dalloc<float>((size_t)N2);
+    CK(cudaMemsetAsync(At32, 0, (size_t)s2.nentries * sizeof(float), stream));
+    for (float **w : {&fr, &fr0, &fp, &fv, &fs, &ft, &fdx}) *w = dalloc<float>(n3);
+    ms = dalloc<MixedState>(1);
+    CK(cudaMemsetAsync(ms, 0, sizeof(MixedState), stream));
+    if (const char *e = std::getenv("CFSA_MIXED_INNER_TOL")) mixed_inner_tol = std::atof(e);
+    if (const char *e = std::getenv("CFSA_MIXED_INNER_MAXIT")) mixed_inner_maxit = std::atoi(e);
     bs_prof = dalloc<BicgState>(1);
     cs_prof = dalloc<CgState>(1);
     // boundary faces
@@ -414,6 +435,8 @@ struct cfsa_ns {
       k_momentum_diag<<<blocks_for(N2), kBlock, 0, stream>>>((int)N2, dt, dpos2, Mv, Kv, bc, diagA, invA);
       k_momentum_sell<<<blocks_for(nnz2), kBlock, 0, stream>>>(nnz2, dt, s2.posmap, rows2, ci2, Mv, Kv,
                                                                bc, invA, At, Ms);
+      k_to_f32<<<blocks_for(s2.nentries), kBlock, 0, stream>>>(s2.nentries, At, At32);
+      k_to_f32<<<blocks_for(N2), kBlock, 0, stream>>>(N2, invA, invA32);
       CK(cudaGetLastError());
       mom_dirty = false;
     }
@@ -432,27 +455,48 @@ struct cfsa_ns {
   // Krylov iteration) is captured from `body` on body_stream. Returns the handle.
   template <class Body>
   void capture_while(Body body) {
+    capture_while_on(stream, body_stream, body);
+  }
+
+  // WHILE node appended to the graph being captured on `cap`; the body is captured on `sub`.
+  template <class Body>
+  void capture_while_on(cudaStream_t cap, cudaStream_t sub, Body body) {
+    capture_while_with(cap, sub, new_cond_handle(cap), body);
+  }
+
+  // Handle of a conditional node of the graph being captured on `cap`. Its default (1) is
+  // applied when the top-level graph is launched; a loop nested in another loop's body must be
+  // re-armed by a kernel upstream of it in the same body (k_mp_inner_init does this).
+  cudaGraphConditionalHandle new_cond_handle(cudaStream_t cap) {
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamGetCaptureInfo(cap, &cst, nullptr, &g, nullptr, nullptr));
+    if (cst != cudaStreamCaptureStatusActive) throw CudaError{"stream is not capturing"};
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    return h;
+  }
+
+  template <class Body>
+  void capture_while_with(cudaStream_t cap, cudaStream_t sub, cudaGraphConditionalHandle h, Body body) {
     cudaStreamCaptureStatus cst;
     cudaGraph_t g = nullptr;
     const cudaGraphNode_t *deps = nullptr;
     size_t ndeps = 0;
-    CK(cudaStreamGetCaptureInfo(stream, &cst, nullptr, &g, &deps, &ndeps));
+    CK(cudaStreamGetCaptureInfo(cap, &cst, nullptr, &g, &deps, &ndeps));
     if (cst != cudaStreamCaptureStatusActive) throw CudaError{"stream is not capturing"};
-    cudaGraphConditionalHandle h;
-    CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
     cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
     cp.conditional.handle = h;
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
     cudaGraphNode_t node;
     CK(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
-    CK(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+    CK(cudaStreamUpdateCaptureDependencies(cap, &node, 1, cudaStreamSetCaptureDependencies));
     cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
-    CK(cudaStreamBeginCaptureToGraph(body_stream, bodyg, nullptr, nullptr, 0,
-                                     cudaStreamCaptureModeRelaxed));
-    body(body_stream, h, 1);
+    CK(cudaStreamBeginCaptureToGraph(sub, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    body(sub, h, 1);
     cudaGraph_t out = nullptr;
-    CK(cudaStreamEndCapture(body_stream, &out));
+    CK(cudaStreamEndCapture(sub, &out));
   }
 
   // Eager loop: enqueue iterations in growing chunks and poll the active flag in between.
@@ -544,6 +588,10 @@ struct cfsa_ns {
     m.red = red;
     k_momentum_rhs<<<blocks_for(s2.nrows_pad), kBlock, 0, stream>>>(m);
     CK(cudaGetLastError());
+    if (precision == CFSA_PRECISION_MIXED) {
+      enqueue_momentum_mixed(capture);
+      return;
+    }
     BicgArgs a = momentum_args();
     auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
       BicgArgs b = a;
@@ -557,6 +605,80 @@ struct cfsa_ns {
       eager_while(body, [&] { return poll_bicg(bs_mom); }, maxit_mom);
     k_check_bicg<<<1, 1, 0, stream>>>(bs_mom, 3, 0, st);
     CK(cudaGetLastError());
+  }
+
+  MixedArgs mixed_args() {
+    MixedArgs a{};
+    a.S = s2.view();
+    a.At32 = At32;
+    a.At64 = At;
+    a.diagA = diagA;
+    a.invA = invA;
+    a.invA32 = invA32;
+    a.b = wb;
+    a.x = ustar;
+    a.r64 = wr;
+    a.xs = wv;
+    a.r = fr;
+    a.r0 = fr0;
+    a.p = fp;
+    a.v = fv;
+    a.s = fs;
+    a.t = ft;
+    a.dx = fdx;
+    a.n = (int)N2;
+    a.ms = ms;
+    a.st = st;
+    a.red = red;
+    return a;
+  }
+
+  // FP32 inner BiCGSTAB sweeps inside FP64 defect correction (ns_mixed.cuh); outer and inner
+  // loops are nested WHILE nodes when captured.
+  void enqueue_momentum_mixed(bool capture) {
+    const MixedArgs a = mixed_args();
+    const unsigned int gp = blocks_for(N2), gs = blocks_for(s2.nrows_pad);
+    k_mp_outer_init<<<gp, kBlock, 0, stream>>>(a, tol_mom, mixed_max_outer, mixed_inner_tol, mixed_inner_maxit);
+    CK(cudaGetLastError());
+    auto inner_body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
+      MixedArgs b = a;
+      b.cond = h;
+      b.use_cond = use;
+      k_mp_p<<<gp, kBlock, 0, s>>>(b);
+      k_mp_v<<<gs, kBlock, 0, s>>>(b);
+      k_mp_s<<<gp, kBlock, 0, s>>>(b);
+      k_mp_t<<<gs, kBlock, 0, s>>>(b);
+      k_mp_xr<<<gp, kBlock, 0, s>>>(b);
+    };
+    auto outer_body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
+      MixedArgs b = a;
+      if (use) {
+        const cudaGraphConditionalHandle hin = new_cond_handle(s);
+        b.cond = hin;
+        b.use_cond = 1;
+        k_mp_inner_init<<<gp, kBlock, 0, s>>>(b);  // re-arms the inner loop every sweep
+        capture_while_with(s, body_stream2, hin, inner_body);
+      } else {
+        k_mp_inner_init<<<gp, kBlock, 0, s>>>(b);
+        eager_while(inner_body, [&] { return poll_mixed(true); }, mixed_inner_maxit);
+      }
+      b.cond = h;
+      b.use_cond = use;
+      k_mp_xupdate<<<gp, kBlock, 0, s>>>(b);
+      k_mp_residual<<<gs, kBlock, 0, s>>>(b);
+    };
+    if (capture)
+      capture_while(outer_body);
+    else
+      eager_while(outer_body, [&] { return poll_mixed(false); }, mixed_max_outer);
+    k_mp_check<<<1, 1, 0, stream>>>(ms, st);
+    CK(cudaGetLastError());
+  }
+
+  bool poll_mixed(bool inner) {
+    CK(cudaMemcpyAsync(h_ms, ms, sizeof(MixedState), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    return inner ? h_ms->in_active != 0 : h_ms->active != 0;
   }
 
   void enqueue_pressure_solve(bool capture) {
@@ -792,8 +914,11 @@ struct cfsa_ns {
     CK(cudaStreamSynchronize(stream));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
     const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : (cg_persistent ? 1 : 3);
-    batch_launches = (int64_t)launched_steps * launches_per_step + 5 * (int64_t)h_st->body_runs[0] +
-                     pressure_body * (int64_t)h_st->body_runs[1];
+    // mixed momentum: 5 kernels per inner body, 3 per outer sweep (inner init, x update,
+    // residual) plus the outer init kernel per step
+    batch_launches = (int64_t)launched_steps * (launches_per_step + (precision == CFSA_PRECISION_MIXED ? 1 : 0)) +
+                     5 * (int64_t)h_st->body_runs[0] + pressure_body * (int64_t)h_st->body_runs[1] +
+                     3 * (int64_t)h_st->body_runs[2];
     batch_iters[0] = (int64_t)h_st->iters[0];
     batch_iters[1] = (int64_t)h_st->iters[1];
     for (int64_t k = 0; k < h_st->steps_done; ++k) time += dt;
@@ -1066,8 +1191,9 @@ int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov) {
 
 int cfsa_ns_set_precision(cfsa_ns *h, int precision) {
   if (!h) return CFSA_BAD_ARG;
-  if (precision != CFSA_PRECISION_FP64)
-    return fail(h, CFSA_UNSUPPORTED, "only CFSA_PRECISION_FP64 is available in this build");
+  if (precision != CFSA_PRECISION_FP64 && precision != CFSA_PRECISION_MIXED)
+    return fail(h, CFSA_BAD_ARG, "unknown precision");
+  if (precision != h->precision) h->graph_dirty = true;
   h->precision = precision;
   return CFSA_OK;
 }
@@ -1252,10 +1378,21 @@ int cfsa_ns_get_stats(const cfsa_ns *hc, cfsa_ns_stats *s) {
     CK(cudaMemcpyAsync(h->h_cs, h->cs, sizeof(CgState), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     std::memset(s, 0, sizeof(*s));
-    for (int c = 0; c < 3; ++c) {
-      s->momentum_iters[c] = h->h_bs[0].iters[c];
-      const double b2 = h->h_bs[0].bnorm2[c];
-      s->momentum_residual[c] = b2 > 0 ? std::sqrt(h->h_bs[0].rnorm2[c] / b2) : 0.0;
+    if (h->precision == CFSA_PRECISION_MIXED) {
+      CK(cudaMemcpyAsync(h->h_ms, h->ms, sizeof(MixedState), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      for (int c = 0; c < 3; ++c) {
+        s->momentum_iters[c] = h->h_ms->total_iters[c];
+        s->momentum_outer[c] = h->h_ms->outer[c];
+        const double b2 = h->h_ms->bnorm2[c];
+        s->momentum_residual[c] = b2 > 0 ? std::sqrt(h->h_ms->rnorm2[c] / b2) : 0.0;
+      }
+    } else {
+      for (int c = 0; c < 3; ++c) {
+        s->momentum_iters[c] = h->h_bs[0].iters[c];
+        const double b2 = h->h_bs[0].bnorm2[c];
+        s->momentum_residual[c] = b2 > 0 ? std::sqrt(h->h_bs[0].rnorm2[c] / b2) : 0.0;
+      }
     }
     if (h->krylov == CFSA_KRYLOV_BICGSTAB) {
       s->pressure_iters = h->h_bs[1].iters[0];

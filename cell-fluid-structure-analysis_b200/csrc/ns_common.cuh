@@ -63,7 +63,8 @@ struct DevStatus {
   int code;        // first failure (CFSA_* code), 0 if none
   int steps_done;  // completed steps in this batch
   int nan;         // NaN flag of the current step
-  unsigned long long body_runs[2];  // Krylov loop bodies executed: [0] momentum, [1] pressure
+  unsigned long long body_runs[3];  // loop bodies executed: [0] momentum Krylov, [1] pressure,
+                                    // [2] mixed-precision outer sweeps
   unsigned long long iters[2];      // Krylov iterations completed: [0] momentum (max over rhs), [1] pressure
 };
 
