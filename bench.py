@@ -35,7 +35,6 @@ FLUID = (1060.0, 0.004)
 DT = 0.01
 TOL = 1e-10
 MAXIT = (5000, 50000)
-MIXED_TOL = 1e-12  # outer (true-residual) tolerance at which mixed meets 1e-6 vs converged FP64
 INLET_PEAK = 2 * 0.5
 
 
@@ -72,9 +71,10 @@ def make_mesh(cf, rings, layers):
     return m
 
 
-def make_solver(cf, m, tol=TOL):
+def make_solver(cf, m, tol=TOL, norm=0):
     s = cf.NavierStokesSolver()
     s.setKrylovTolerances(tol, tol)
+    s.setConvergenceNorm(norm)
     s.setMaxIterations(*MAXIT)
     s.setPressureSolver(cf.KRYLOV_CG)
     s.setDt(DT)
@@ -257,7 +257,6 @@ def main():
     clk = clocks.stop(set(range(world))) if rank == 0 else None
     if not ok:
         raise SystemExit(f"timed steps failed after {done} steps: {st}")
-    ref_u, ref_p = s.getVelocity(), s.getPressure()  # FP64 state after the timed steps
     ms_total = st["last_step_ms"]
     t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
     if dist is not None:
@@ -302,46 +301,54 @@ def main():
                 "unit": "GB/s", "frac": dom["achieved_gbs"] / peak, "peak_kind": peak_kind,
                 "traffic": dom["traffic"]}
 
-    # mixed precision on the same mesh (config 2): throughput and error against the FP64 run
+    # Config 2 (mixed precision) on the same mesh and inputs. The reference's criterion
+    # ||r|| <= tol ||b|| is dominated by the 1e10 penalty rows and pins the interior only loosely,
+    # so FP64 and mixed are compared under the Jacobi-scaled norm (||D^-1/2 r|| <= tol ||D^-1/2 b||),
+    # both timed over the same steps, both measured against a converged FP64 run (tol 1e-14).
     mixed = None
     if not args.no_mixed:
-        # converged FP64 reference (tol 1e-14) at the same step, untimed: at the configs' 1e-10 the
-        # penalty-dominated ||b|| leaves the FP64 interior itself loose (~1e-2 after 10 steps)
-        sr, _ = make_solver(cf, m, tol=1e-14)
-        sr.pisoSteps(max(args.warmup, 3) + args.steps)
-        conv_u, conv_p = sr.getVelocity(), sr.getPressure()
-        del sr
-        sm, _ = make_solver(cf, m, tol=MIXED_TOL)
-        sm.setPrecision(cf.PRECISION_MIXED)
-        ok, _ = sm.pisoSteps(max(args.warmup, 3))  # same step range as the FP64 timed region
-        barrier()
-        ok2, _ = sm.pisoSteps(args.steps)
-        stm = sm.stats()
-        barrier()
-        tm = torch.tensor([stm["last_step_ms"]], dtype=torch.float64, device="cuda")
-        if dist is not None:
-            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        mv = world * args.steps / (float(tm.item()) / 1e3)
-        from numpy.linalg import norm
+        nwarm = max(args.warmup, 3)
+
+        def timed_run(precision, tol):
+            sx, _ = make_solver(cf, m, tol=tol, norm=cf.NORM_JACOBI)
+            sx.setPrecision(precision)
+            ok_a, _ = sx.pisoSteps(nwarm)
+            barrier()
+            ok_b, _ = sx.pisoSteps(args.steps)
+            stx = sx.stats()
+            barrier()
+            t = torch.tensor([stx["last_step_ms"]], dtype=torch.float64, device="cuda")
+            if dist is not None:
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            out = (sx.getVelocity(), sx.getPressure(), stx, float(t.item()), bool(ok_a and ok_b))
+            del sx
+            return out
+
+        from numpy.linalg import norm as l2
 
         def rel(a, b):
-            return float(norm(a - b) / norm(b))
+            return float(l2(a - b) / l2(b))
 
-        mu_, mp_ = sm.getVelocity(), sm.getPressure()
-        mixed = {"value": mv, "unit": UNIT, "ok": bool(ok and ok2), "speedup_vs_fp64": mv / value,
-                 "ms_per_step": float(tm.item()) / args.steps, "outer_tol": MIXED_TOL,
-                 "rel_l2_vs_converged_fp64": {"u": rel(mu_, conv_u), "p": rel(mp_, conv_p),
-                                              "after_steps": int(sm.stats()["steps"]),
-                                              "reference": "FP64 GPU, Krylov tol 1e-14"},
-                 "rel_l2_vs_fp64_at_1e-10": {"u": rel(mu_, ref_u), "p": rel(mp_, ref_p)},
-                 "fp64_1e-10_vs_converged": {"u": rel(ref_u, conv_u), "p": rel(ref_p, conv_p)},
-                 "krylov_iters_per_step": [stm["krylov_iters"][0] / args.steps, stm["krylov_iters"][1] / args.steps],
-                 "outer_sweeps_last_step": stm["momentum_outer"],
-                 "phase_ms_last_step": {"momentum": stm["phase_ms"][0], "pressure_solve": stm["phase_ms"][1],
-                                        "other": stm["phase_ms"][2]},
-                 "workload": "config 2: same mesh and inputs, FP32 inner BiCGSTAB momentum in FP64 defect "
-                             f"correction to {MIXED_TOL:g} (true FP64 residual); pressure CG FP64 to {MIXED_TOL:g}"}
-        del sm
+        cu, cp_, _, _, _ = timed_run(cf.PRECISION_FP64, 1e-14)
+        fu, fp_, fst, fms, fok = timed_run(cf.PRECISION_FP64, TOL)
+        mu_, mp_, mst, mms, mok = timed_run(cf.PRECISION_MIXED, TOL)
+        fv_, mv_ = world * args.steps / (fms / 1e3), world * args.steps / (mms / 1e3)
+        mixed = {
+            "value": mv_, "unit": UNIT, "ok": mok and fok, "norm": "jacobi ||D^-1/2 r|| <= 1e-10 ||D^-1/2 b||",
+            "fp64_value": fv_, "speedup_vs_fp64": mv_ / fv_,
+            "ms_per_step": mms / args.steps, "fp64_ms_per_step": fms / args.steps,
+            "rel_l2_vs_converged": {"mixed": {"u": rel(mu_, cu), "p": rel(mp_, cp_)},
+                                    "fp64": {"u": rel(fu, cu), "p": rel(fp_, cp_)},
+                                    "after_steps": nwarm + args.steps,
+                                    "reference": "FP64 GPU, Krylov tol 1e-14, same norm"},
+            "rel_l2_mixed_vs_fp64": {"u": rel(mu_, fu), "p": rel(mp_, fp_)},
+            "krylov_iters_per_step": {"mixed": [mst["krylov_iters"][0] / args.steps, mst["krylov_iters"][1] / args.steps],
+                                      "fp64": [fst["krylov_iters"][0] / args.steps, fst["krylov_iters"][1] / args.steps]},
+            "outer_sweeps_last_step": mst["momentum_outer"],
+            "phase_ms_last_step": {"mixed": mst["phase_ms"], "fp64": fst["phase_ms"]},
+            "workload": "config 2: same mesh and inputs; momentum FP32 inner BiCGSTAB in FP64 defect "
+                        "correction (true FP64 residual) vs FP64 BiCGSTAB; pressure FP64 CG in both",
+        }
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -27,6 +27,7 @@ MAT_MASS, MAT_STIFFNESS, MAT_GRAD_X, MAT_GRAD_Y, MAT_GRAD_Z, MAT_POISSON, MAT_MO
 KERNEL_MOMENTUM_SPMV, KERNEL_PRESSURE_SPMV = 0, 1
 KRYLOV_CG, KRYLOV_BICGSTAB = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+NORM_REFERENCE, NORM_JACOBI = 0, 1
 
 
 class FluidBCType(enum.IntEnum):
@@ -155,6 +156,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "cfsa_ns_set_inlet_profile": (i32, [vp, vp]),
         "cfsa_ns_set_pressure_solver": (i32, [vp, i32]),
         "cfsa_ns_set_precision": (i32, [vp, i32]),
+        "cfsa_ns_set_convergence_norm": (i32, [vp, i32]),
         "cfsa_ns_set_viscosity": (i32, [vp, dbl]),
         "cfsa_ns_initialize_fields": (i32, [vp]),
         "cfsa_ns_assemble": (i32, [vp]),
@@ -354,6 +356,7 @@ class NavierStokesSolver:
         self.inlet_profile = None
         self.krylov = KRYLOV_CG
         self.precision = PRECISION_FP64
+        self.conv_norm = NORM_REFERENCE
         self.N2 = self.nv = self.ne = self.nt = 0
 
     def __del__(self):
@@ -383,6 +386,7 @@ class NavierStokesSolver:
         self._check(L.cfsa_ns_set_reference_node(h, int(self.reference_node)))
         self._check(L.cfsa_ns_set_pressure_solver(h, int(self.krylov)))
         self._check(L.cfsa_ns_set_precision(h, int(self.precision)))
+        self._check(L.cfsa_ns_set_convergence_norm(h, int(self.conv_norm)))
         self._push_inlet()
 
     def _push_inlet(self):
@@ -636,6 +640,12 @@ class NavierStokesSolver:
         self.precision = int(precision)
         if self._h is not None:
             self._check(self._lib.cfsa_ns_set_precision(self._h, self.precision))
+
+    def setConvergenceNorm(self, norm: int):
+        """NORM_REFERENCE (||r||/||b||, the reference's) or NORM_JACOBI (||D^-1/2 r||/||D^-1/2 b||)."""
+        self.conv_norm = int(norm)
+        if self._h is not None:
+            self._check(self._lib.cfsa_ns_set_convergence_norm(self._h, self.conv_norm))
 
     def setViscosity(self, nu: float):
         self.fluid.viscosity = float(nu)

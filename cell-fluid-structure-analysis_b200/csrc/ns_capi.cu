@@ -61,6 +61,7 @@ struct cfsa_ns {
   int ref_node = -1;
   int krylov = CFSA_KRYLOV_CG;
   int precision = CFSA_PRECISION_FP64;
+  int conv_norm = CFSA_NORM_REFERENCE;
   double time = 0.0;
   int64_t steps = 0;
   float last_ms = 0.f;
@@ -551,6 +552,7 @@ struct cfsa_ns {
     a.red = red;
     a.st = st;
     a.slot = 0;
+    a.cw = (conv_norm == CFSA_NORM_JACOBI) ? invA : nullptr;
     return a;
   }
 
@@ -586,6 +588,7 @@ struct cfsa_ns {
     m.bs = bs_mom;
     m.st = st;
     m.red = red;
+    m.cw = (conv_norm == CFSA_NORM_JACOBI) ? invA : nullptr;
     k_momentum_rhs<<<blocks_for(s2.nrows_pad), kBlock, 0, stream>>>(m);
     CK(cudaGetLastError());
     if (precision == CFSA_PRECISION_MIXED) {
@@ -630,6 +633,8 @@ struct cfsa_ns {
     a.ms = ms;
     a.st = st;
     a.red = red;
+    a.cw = (conv_norm == CFSA_NORM_JACOBI) ? invA : nullptr;
+    a.cw32 = (conv_norm == CFSA_NORM_JACOBI) ? invA32 : nullptr;
     return a;
   }
 
@@ -698,6 +703,7 @@ struct cfsa_ns {
     a.ref_node = ref_node;
     a.maxit = maxit_p;
     a.krylov = (krylov == CFSA_KRYLOV_BICGSTAB) ? 1 : 0;
+    a.scaled = (conv_norm == CFSA_NORM_JACOBI) ? 1 : 0;
     a.b = pb;
     a.x = pc;
     a.r = pr;
@@ -729,6 +735,7 @@ struct cfsa_ns {
       b.red = red;
       b.st = st;
       b.slot = 1;
+      b.cw = (conv_norm == CFSA_NORM_JACOBI) ? invL : nullptr;
       auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
         BicgArgs c = b;
         c.cond = h;
@@ -759,6 +766,7 @@ struct cfsa_ns {
       c.cs = cs;
       c.st = st;
       c.bar = GridBarrier{bar_count, bar_gen, bar_err};
+      c.scaled = (conv_norm == CFSA_NORM_JACOBI) ? 1 : 0;
       CK(cudaMemsetAsync(bar_count, 0, sizeof(unsigned int), stream));
       CK(cudaMemsetAsync(bar_err, 0, sizeof(int), stream));
       cudaLaunchConfig_t cfg = {};
@@ -786,6 +794,7 @@ struct cfsa_ns {
       c.cs = cs;
       c.red = red;
       c.st = st;
+      c.scaled = (conv_norm == CFSA_NORM_JACOBI) ? 1 : 0;
       auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
         CgArgs d = c;
         d.cond = h;
@@ -1195,6 +1204,15 @@ int cfsa_ns_set_precision(cfsa_ns *h, int precision) {
     return fail(h, CFSA_BAD_ARG, "unknown precision");
   if (precision != h->precision) h->graph_dirty = true;
   h->precision = precision;
+  return CFSA_OK;
+}
+
+int cfsa_ns_set_convergence_norm(cfsa_ns *h, int norm) {
+  if (!h) return CFSA_BAD_ARG;
+  if (norm != CFSA_NORM_REFERENCE && norm != CFSA_NORM_JACOBI)
+    return fail(h, CFSA_BAD_ARG, "unknown convergence norm");
+  if (norm != h->conv_norm) h->graph_dirty = true;
+  h->conv_norm = norm;
   return CFSA_OK;
 }
 

@@ -496,6 +496,7 @@ struct MomentumRhsArgs {
   double dt, tol;
   int n, nv, nt, maxit;
   double *b, *x, *r, *r0, *pk, *v;
+  const double *cw;  // convergence-norm weights (diag(A)^-1), nullptr: unscaled ||r||
   BicgState *bs;
   DevStatus *st;
   Reduce red;
@@ -504,10 +505,11 @@ struct MomentumRhsArgs {
 __global__ void k_momentum_rhs(MomentumRhsArgs A) {
   if (A.st->halt) return;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  double part[3] = {0.0, 0.0, 0.0};
+  double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
   if (i >= 0) {
     const int64_t n = A.n;
+    const double w = A.cw ? A.cw[i] : 1.0;
     double mu[3];
     sell_spmv_row<3>(A.S, A.Ms, A.u, n, r, mu);
     double b[3];
@@ -546,27 +548,28 @@ __global__ void k_momentum_rhs(MomentumRhsArgs A) {
       A.pk[o] = 0.0;
       A.v[o] = 0.0;
       part[c] = b[c] * b[c];
+      part[3 + c] = (b[c] * b[c]) * w;
     }
   }
-  double tot[3];
-  if (grid_reduce<3>(part, A.red, tot) && threadIdx.x == 0) {
+  double tot[6];
+  if (grid_reduce<6>(part, A.red, tot) && threadIdx.x == 0) {
     BicgState *s = A.bs;
     s->active = 0;
     s->restart = 0;
     s->maxit = A.maxit;
     s->ncomp = 3;
     for (int c = 0; c < 3; ++c) {
-      s->bnorm2[c] = tot[c];
-      s->r0norm2[c] = tot[c];
-      s->rnorm2[c] = tot[c];
-      s->tol2[c] = A.tol * A.tol * tot[c];
+      s->bnorm2[c] = tot[3 + c];  // convergence norm of b
+      s->r0norm2[c] = tot[c];     // r0 . r0 (restart threshold)
+      s->rnorm2[c] = tot[3 + c];
+      s->tol2[c] = A.tol * A.tol * tot[3 + c];
       s->rho[c] = tot[c];  // r0 . r with r = r0 = b
       s->alpha[c] = s->omega[c] = 1.0;
       s->beta[c] = 0.0;
       s->iters[c] = 0;
-      if (isnan(tot[c])) {
+      if (isnan(tot[c]) || isnan(tot[3 + c])) {
         s->status[c] = KS_BREAKDOWN;
-      } else if (tot[c] == 0.0 || tot[c] <= s->tol2[c]) {
+      } else if (tot[3 + c] == 0.0 || tot[3 + c] <= s->tol2[c]) {
         s->status[c] = KS_CONVERGED;
       } else {
         s->status[c] = KS_RUNNING;
@@ -593,6 +596,7 @@ struct BicgArgs {
   int use_cond;
   DevStatus *st;  // launch counters
   int slot;       // 0 momentum, 1 pressure
+  const double *cw;  // convergence-norm weights, nullptr: unscaled ||r||
 };
 
 // K1: p = r + beta (p - omega v); on restart: r = b - A x, r0 = r, p = r, rho = |r|^2.
@@ -744,6 +748,7 @@ __global__ void k_bicg_xr(BicgArgs A) {
   for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
   if (i < A.n) {
     const double dinv = A.invA[i];
+    const double w = A.cw ? A.cw[i] : 1.0;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       if (!((active >> c) & 1)) continue;
@@ -754,7 +759,7 @@ __global__ void k_bicg_xr(BicgArgs A) {
       A.x[o] += alpha * y + omega * z;
       const double ri = A.s[o] - omega * A.t[o];
       A.r[o] = ri;
-      part[c] = ri * ri;
+      part[c] = (ri * ri) * w;
       part[NC + c] = A.r0[o] * ri;
     }
   }
@@ -832,6 +837,7 @@ struct PressureRhsArgs {
   const double *invL;
   double dt, tol, outlet_pressure;
   int nv, outlet_type, ref_node, maxit, krylov;  // krylov: 0 CG, 1 BiCGSTAB
+  int scaled;  // convergence norm: 0 ||r||, 1 ||D^-1/2 r||
   double *b, *x, *r, *z_or_r0, *pk, *v;
   CgState *cs;
   BicgState *bs;
@@ -854,28 +860,30 @@ __global__ void k_pressure_rhs(PressureRhsArgs A) {
     A.b[i] = b;
     A.x[i] = 0.0;
     A.r[i] = b;
+    const double z = A.invL[i] * b;
     if (A.krylov == 0) {
-      const double z = A.invL[i] * b;
       A.z_or_r0[i] = z;
       A.pk[i] = z;
-      part[1] = b * z;
     } else {
       A.z_or_r0[i] = b;
       A.pk[i] = 0.0;
       A.v[i] = 0.0;
     }
     part[0] = b * b;
+    // scaled convergence norm of b in the form each method's iterations use: CG r.z, BiCGSTAB (r.r) w
+    part[1] = (A.krylov == 0) ? b * z : (b * b) * A.invL[i];
   }
   double tot[2];
   if (grid_reduce<2>(part, A.red, tot) && threadIdx.x == 0) {
-    const double tol2 = A.tol * A.tol * tot[0];
-    const bool bad = isnan(tot[0]);
-    const bool done = bad || (tot[0] == 0.0 || tot[0] <= tol2);
+    const double crit = A.scaled ? tot[1] : tot[0];  // convergence norm of b
+    const double tol2 = A.tol * A.tol * crit;
+    const bool bad = isnan(tot[0]) || isnan(tot[1]);
+    const bool done = bad || (crit == 0.0 || crit <= tol2);
     const int final_status = bad ? KS_BREAKDOWN : KS_CONVERGED;
     if (A.krylov == 0) {
       CgState *c = A.cs;
-      c->bnorm2 = tot[0];
-      c->rnorm2 = tot[0];
+      c->bnorm2 = crit;
+      c->rnorm2 = crit;
       c->tol2 = tol2;
       c->absnew = tot[1];
       c->iters = 0;
@@ -887,7 +895,8 @@ __global__ void k_pressure_rhs(PressureRhsArgs A) {
       s->ncomp = 1;
       s->maxit = A.maxit;
       s->restart = 0;
-      s->bnorm2[0] = s->r0norm2[0] = s->rnorm2[0] = tot[0];
+      s->bnorm2[0] = s->rnorm2[0] = crit;
+      s->r0norm2[0] = tot[0];
       s->tol2[0] = tol2;
       s->rho[0] = tot[0];  // r0 . r with r = r0 = b
       s->alpha[0] = s->omega[0] = 1.0;
@@ -911,6 +920,7 @@ struct CgArgs {
   cudaGraphConditionalHandle cond;
   int use_cond;
   DevStatus *st;  // launch counters
+  int scaled;     // convergence norm: 0 r.r, 1 r.z = ||D^-1/2 r||^2
 };
 
 // C1: q = L p, alpha = absnew / (p . q)
@@ -958,12 +968,13 @@ __global__ void k_cg_xr(CgArgs A) {
   double tot[2];
   if (grid_reduce<2>(part, A.red, tot) && threadIdx.x == 0) {
     CgState *c = A.cs;
+    const double crit = A.scaled ? tot[1] : tot[0];
     c->iters += 1;
-    c->rnorm2 = tot[0];
+    c->rnorm2 = crit;
     if (isnan(tot[0]) || isnan(tot[1])) {
       c->status = KS_BREAKDOWN;
       c->active = 0;
-    } else if (tot[0] <= c->tol2) {
+    } else if (crit <= c->tol2) {
       c->status = KS_CONVERGED;
       c->active = 0;
     } else if (c->iters >= c->maxit) {
@@ -1096,6 +1107,7 @@ struct CgPersistentArgs {
   CgState *cs;
   DevStatus *st;
   GridBarrier bar;
+  int scaled;  // convergence norm: 0 r.r, 1 r.z
 };
 
 __global__ void __launch_bounds__(kBlock) k_cg_persistent(CgPersistentArgs A) {
@@ -1160,12 +1172,12 @@ __global__ void __launch_bounds__(kBlock) k_cg_persistent(CgPersistentArgs A) {
     double tb[2];
     tree_total<2>(A.part_b, A.nblk_nat, tb);
     ++it;
-    rr = tb[0];
+    rr = A.scaled ? tb[1] : tb[0];
     if (isnan(tb[0]) || isnan(tb[1])) {
       status = KS_BREAKDOWN;
       break;
     }
-    if (tb[0] <= tol2) {
+    if (rr <= tol2) {
       status = KS_CONVERGED;
       break;
     }

@@ -45,6 +45,8 @@ struct MixedArgs {
   Reduce red;
   cudaGraphConditionalHandle cond;
   int use_cond;
+  const double *cw;   // convergence-norm weights (diag(A)^-1), nullptr: unscaled ||r||
+  const float *cw32;  // the same for the inner solve
 };
 
 template <int U = 8>
@@ -89,11 +91,12 @@ __global__ void k_mp_outer_init(MixedArgs A, double tol, int max_outer, double t
   const int64_t n = A.n;
   double part[3] = {0.0, 0.0, 0.0};
   if (i < A.n) {
+    const double w = A.cw ? A.cw[i] : 1.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const double bi = A.b[c * n + i];
       A.r64[c * n + i] = bi;
-      part[c] = bi * bi;
+      part[c] = (bi * bi) * w;
     }
   }
   double tot[3];
@@ -135,8 +138,9 @@ __global__ void k_mp_inner_init(MixedArgs A) {
   }
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n = A.n;
-  double part[3] = {0.0, 0.0, 0.0};
+  double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   if (i < A.n) {
+    const double w = A.cw32 ? (double)A.cw32[i] : 1.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t o = c * n + i;
@@ -146,11 +150,14 @@ __global__ void k_mp_inner_init(MixedArgs A) {
       A.p[o] = 0.f;
       A.v[o] = 0.f;
       A.dx[o] = 0.f;
-      if ((active >> c) & 1) part[c] = (double)ri * (double)ri;
+      if ((active >> c) & 1) {
+        part[c] = (double)ri * (double)ri;
+        part[3 + c] = ((double)ri * (double)ri) * w;
+      }
     }
   }
-  double tot[3];
-  if (grid_reduce<3>(part, A.red, tot) && threadIdx.x == 0) {
+  double tot[6];
+  if (grid_reduce<6>(part, A.red, tot) && threadIdx.x == 0) {
     MixedState *m = A.ms;
     m->in_active = 0;
     for (int c = 0; c < 3; ++c) {
@@ -158,8 +165,8 @@ __global__ void k_mp_inner_init(MixedArgs A) {
       if (!((active >> c) & 1)) continue;
       m->rho[c] = tot[c];
       m->r0norm2[c] = tot[c];
-      m->rin2[c] = tot[c];
-      m->tol_in2[c] = m->tol_in * m->tol_in * tot[c];
+      m->rin2[c] = tot[3 + c];
+      m->tol_in2[c] = m->tol_in * m->tol_in * tot[3 + c];
       m->alpha[c] = m->omega[c] = 1.0;
       m->beta[c] = 0.0;
       if (tot[c] > 0.0 && !isnan(tot[c])) m->in_active |= 1 << c;
@@ -270,6 +277,7 @@ __global__ void k_mp_xr(MixedArgs A) {
   double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   if (i < A.n) {
     const float dinv = A.invA32[i];
+    const double w = A.cw32 ? (double)A.cw32[i] : 1.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       if (!((act >> c) & 1)) continue;
@@ -278,7 +286,7 @@ __global__ void k_mp_xr(MixedArgs A) {
       A.dx[o] += alpha * (dinv * A.p[o]) + omega * (dinv * A.s[o]);
       const float ri = A.s[o] - omega * A.t[o];
       A.r[o] = ri;
-      part[c] = (double)ri * (double)ri;
+      part[c] = ((double)ri * (double)ri) * w;
       part[3 + c] = (double)A.r0[o] * (double)ri;
     }
   }
@@ -339,12 +347,13 @@ __global__ void k_mp_residual(MixedArgs A) {
   if (i >= 0) {
     double acc[3];
     sell_spmv_row<3>(A.S, A.At64, A.xs, n, r, acc);
+    const double w = A.cw ? A.cw[i] : 1.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       if (!((active >> c) & 1)) continue;
       const double ri = A.b[c * n + i] - acc[c];
       A.r64[c * n + i] = ri;
-      part[c] = ri * ri;
+      part[c] = (ri * ri) * w;
     }
   }
   double tot[3];

@@ -54,6 +54,7 @@ void NavierStokesSolver::pushParameters() {
   status(cfsa_ns_set_reference_node(h_, reference_node_), "setReferencePressureNode");
   status(cfsa_ns_set_pressure_solver(h_, krylov_), "setPressureSolver");
   status(cfsa_ns_set_precision(h_, precision_), "setPrecision");
+  status(cfsa_ns_set_convergence_norm(h_, conv_norm_), "setConvergenceNorm");
   pushInlet();
 }
 
@@ -346,6 +347,11 @@ void NavierStokesSolver::setPressureSolver(int krylov) {
 void NavierStokesSolver::setPrecision(int precision) {
   precision_ = precision;
   if (h_) status(cfsa_ns_set_precision(h_, precision), "setPrecision");
+}
+
+void NavierStokesSolver::setConvergenceNorm(int norm) {
+  conv_norm_ = norm;
+  if (h_) status(cfsa_ns_set_convergence_norm(h_, norm), "setConvergenceNorm");
 }
 
 double NavierStokesSolver::getTime() const {

@@ -32,6 +32,7 @@ class NavierStokesSolver {
   double dt_ = 1e-4;
   int krylov_ = CFSA_KRYLOV_CG;
   int precision_ = CFSA_PRECISION_FP64;
+  int conv_norm_ = CFSA_NORM_REFERENCE;
 
   Fluid fluid_properties_;
 
@@ -139,6 +140,7 @@ class NavierStokesSolver {
   void setMaxIterations(int momentum, int pressure);
   void setPressureSolver(int krylov);  // CFSA_KRYLOV_CG or CFSA_KRYLOV_BICGSTAB
   void setPrecision(int precision);    // CFSA_PRECISION_FP64 or CFSA_PRECISION_MIXED
+  void setConvergenceNorm(int norm);   // CFSA_NORM_REFERENCE or CFSA_NORM_JACOBI
   void setInletVelocityProfile(const std::vector<Vec3> &per_node);
   bool pisoSteps(int n, int *n_done = nullptr);  // n steps, one host synchronisation
   cfsa_ns_stats getStats() const;

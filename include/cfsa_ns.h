@@ -53,6 +53,13 @@ extern "C" {
 #define CFSA_PRECISION_FP64 0
 #define CFSA_PRECISION_MIXED 1 /* FP32 inner Krylov inside FP64 defect correction */
 
+/* Krylov convergence norm. REFERENCE: ||r|| <= tol ||b|| (NavierStokes.cpp:500,635). With the
+ * 1e10 / 1e12 penalty rows in b this norm is dominated by the Dirichlet rows, so it constrains the
+ * interior only loosely. JACOBI: ||D^-1/2 r|| <= tol ||D^-1/2 b||, D = diag of the operator, which
+ * weighs the penalty rows down by their diagonal. */
+#define CFSA_NORM_REFERENCE 0
+#define CFSA_NORM_JACOBI 1
+
 /* matrix ids for cfsa_ns_get_matrix */
 #define CFSA_MAT_MASS 0       /* M  (buildMassMatrix, NavierStokes.cpp:227-310) */
 #define CFSA_MAT_STIFFNESS 1  /* K  (buildStiffnessMatrix, NavierStokes.cpp:135-225) */
@@ -130,6 +137,7 @@ int cfsa_ns_set_inlet_uniform(cfsa_ns *h, const double u[3]);             /* set
 int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u /*[N2][3]*/);   /* new: per-node inlet */
 int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov);                   /* new: CG or BiCGSTAB */
 int cfsa_ns_set_precision(cfsa_ns *h, int precision);                      /* new: FP64 or mixed */
+int cfsa_ns_set_convergence_norm(cfsa_ns *h, int norm);                     /* new: see CFSA_NORM_* */
 /* Fluid viscosity; stiffness (scaled by 1/viscosity, NavierStokes.cpp:153) is re-assembled. */
 int cfsa_ns_set_viscosity(cfsa_ns *h, double viscosity);
 

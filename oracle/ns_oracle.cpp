@@ -256,8 +256,10 @@ std::vector<double> inverse_diagonal(const CSR &A, std::vector<double> *diag = n
 // NaN residual ends the solve unconverged. Near-breakdown (|rho| < eps^2 ||r0||^2) restarts from
 // the true residual with r0 = r, p = r. `init` orders the ||b||^2 reduction, `sell` the products
 // fused into the sparse products, `nat` the rest.
+// `scaled`: convergence norm ||D^-1/2 r|| (sum of (r_i r_i) / a_ii) instead of ||r||.
 SolveInfo bicgstab(const CSR &A, const std::vector<double> &b, std::vector<double> &x, double tol,
-                   int maxit, const RedOrder &init, const RedOrder &sell, const RedOrder &nat) {
+                   int maxit, const RedOrder &init, const RedOrder &sell, const RedOrder &nat,
+                   bool scaled) {
   const int64_t n = A.n;
   SolveInfo info;
   std::vector<double> diag;
@@ -266,15 +268,20 @@ SolveInfo bicgstab(const CSR &A, const std::vector<double> &b, std::vector<doubl
   for (int64_t i = 0; i < n; ++i)
     for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) At.val[k] = A.val[k] * invdiag[A.col[k]];
   x.assign(n, 0.0);
-  const double bnorm2 = odot(init, b.data(), b.data());
+  auto crit_of = [&](const RedOrder &o, const std::vector<double> &v) {
+    return scaled ? tree_sum(o, [&](int i) { return (v[i] * v[i]) * invdiag[i]; })
+                  : odot(o, v.data(), v.data());
+  };
+  const double b2 = odot(init, b.data(), b.data());
+  const double bnorm2 = crit_of(init, b);
   const double tol2 = tol * tol * bnorm2;
-  if (std::isnan(bnorm2)) return info;
+  if (std::isnan(bnorm2) || std::isnan(b2)) return info;
   if (bnorm2 == 0.0 || bnorm2 <= tol2) {
     info.converged = true;
     return info;
   }
   std::vector<double> r(b), r0(b), p(n, 0.0), v(n, 0.0), s(n), t(n), dx(n);
-  double r0norm2 = bnorm2, rho = bnorm2, alpha = 1.0, w = 1.0, beta = 0.0;
+  double r0norm2 = b2, rho = b2, alpha = 1.0, w = 1.0, beta = 0.0;
   const double eps = std::numeric_limits<double>::epsilon();
   bool restart = false;
   double rn2 = bnorm2;
@@ -311,7 +318,7 @@ SolveInfo bicgstab(const CSR &A, const std::vector<double> &b, std::vector<doubl
       x[k] += alpha * y + w * z;
       r[k] = s[k] - w * t[k];
     }
-    rn2 = odot(nat, r.data(), r.data());
+    rn2 = crit_of(nat, r);
     const double rho_new = odot(nat, r0.data(), r.data());
     ++i;
     if (std::isnan(rn2) || std::isnan(rho_new)) break;
@@ -333,16 +340,18 @@ SolveInfo bicgstab(const CSR &A, const std::vector<double> &b, std::vector<doubl
 
 // Jacobi-preconditioned CG (Hestenes-Stiefel), zero initial guess, same stopping rule; p.q is
 // fused into the sparse product (`sell` order), the other reductions use `nat`.
+// `scaled`: convergence norm r.z = ||D^-1/2 r||^2 instead of r.r.
 SolveInfo cg(const CSR &A, const std::vector<double> &b, std::vector<double> &x, double tol,
-             int maxit, const RedOrder &sell, const RedOrder &nat) {
+             int maxit, const RedOrder &sell, const RedOrder &nat, bool scaled) {
   const int64_t n = A.n;
   SolveInfo info;
   const std::vector<double> invdiag = inverse_diagonal(A);
   x.assign(n, 0.0);
   std::vector<double> r(b), z(n), p(n), q(n);
   for (int64_t k = 0; k < n; ++k) z[k] = invdiag[k] * r[k];
-  const double bnorm2 = odot(nat, b.data(), b.data());
+  const double b2 = odot(nat, b.data(), b.data());
   double absnew = odot(nat, b.data(), z.data());
+  const double bnorm2 = scaled ? absnew : b2;
   const double thr = tol * tol * bnorm2;
   if (std::isnan(bnorm2)) return info;
   double rn2 = bnorm2;
@@ -360,10 +369,11 @@ SolveInfo cg(const CSR &A, const std::vector<double> &b, std::vector<double> &x,
         r[k] = r[k] - alpha * q[k];
         z[k] = invdiag[k] * r[k];
       }
-      rn2 = odot(nat, r.data(), r.data());
+      const double rr = odot(nat, r.data(), r.data());
       const double rz = odot(nat, r.data(), z.data());
+      rn2 = scaled ? rz : rr;
       ++i;
-      if (std::isnan(rn2) || std::isnan(rz)) break;
+      if (std::isnan(rr) || std::isnan(rz)) break;
       if (rn2 <= thr) break;
       if (i >= maxit) break;
       const double beta = rz / absnew;
@@ -404,6 +414,7 @@ struct Oracle {
   double outlet_pressure = 0.0;
   int reference_node = -1;
   int pressure_solver = 0;  // 0 = BiCGSTAB (reference), 1 = CG
+  int conv_norm = 0;        // 0 = ||r|| (reference), 1 = ||D^-1/2 r||
   std::vector<V3> inlet;    // per P2-node inlet velocity (the reference: one mean vector)
   std::vector<V3> u, ustar;
   std::vector<double> p, pcorr, inv_lumped;
@@ -733,7 +744,7 @@ struct Oracle {
           rhs[i] += penalty * up;
         }
       }
-      SolveInfo si = bicgstab(lhs, rhs, x, tol_mom, maxit_mom, order_p2, order_p2, order_n2);
+      SolveInfo si = bicgstab(lhs, rhs, x, tol_mom, maxit_mom, order_p2, order_p2, order_n2, conv_norm == 1);
       it_mom[comp] = si.iters;
       res_mom[comp] = si.rel_res;
       if (!si.converged) {
@@ -800,8 +811,9 @@ struct Oracle {
         }
     }
     SolveInfo si = (pressure_solver == 1)
-                       ? cg(Lbc, rhs, x, tol_p, maxit_p, order_p1, order_nv)
-                       : bicgstab(Lbc, rhs, x, tol_p, maxit_p, order_nv, order_p1, order_nv);
+                       ? cg(Lbc, rhs, x, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1)
+                       : bicgstab(Lbc, rhs, x, tol_p, maxit_p, order_nv, order_p1, order_nv,
+                                  conv_norm == 1);
     it_p = si.iters;
     res_p = si.rel_res;
     if (!si.converged) {
@@ -1037,11 +1049,12 @@ void orc_set_fluid(void *h, double density, double viscosity) {
 }
 // Parameters: dt, momentum tol, pressure tol, momentum maxit, pressure maxit, corrections,
 // relax_u, relax_p, outlet type, outlet pressure, reference node, pressure solver (0 BiCGSTAB,
-// 1 CG).
+// 1 CG), convergence norm (0 ||r||, 1 ||D^-1/2 r||).
 void orc_set_params(void *h, double dt, double tol_mom, double tol_p, int maxit_mom, int maxit_p,
                     int n_corr, double relax_u, double relax_p, int outlet_type,
-                    double outlet_pressure, int reference_node, int pressure_solver) {
+                    double outlet_pressure, int reference_node, int pressure_solver, int conv_norm) {
   Oracle *o = static_cast<Oracle *>(h);
+  o->conv_norm = conv_norm;
   o->dt = dt;
   o->tol_mom = tol_mom;
   o->tol_p = tol_p;

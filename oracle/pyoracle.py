@@ -38,7 +38,7 @@ def lib() -> C.CDLL:
         "orc_get_mesh": (None, [vp] + [vp] * 9),
         "orc_set_bc": (None, [vp, vp, vp]),
         "orc_set_fluid": (None, [vp, dbl, dbl]),
-        "orc_set_params": (None, [vp, dbl, dbl, dbl, i32, i32, i32, dbl, dbl, i32, dbl, i32, i32]),
+        "orc_set_params": (None, [vp, dbl, dbl, dbl, i32, i32, i32, dbl, dbl, i32, dbl, i32, i32, i32]),
         "orc_set_inlet": (None, [vp, vp]),
         "orc_initialize": (None, [vp]),
         "orc_reference_node": (i32, [vp]),
@@ -91,7 +91,7 @@ class Oracle:
         self.N2 = self.nv + self.ne
         self.params = dict(dt=1e-4, tol_mom=1e-6, tol_p=1e-8, maxit_mom=1000, maxit_p=1000,
                            n_corr=1, relax_u=1.0, relax_p=1.0, outlet_type=0,
-                           outlet_pressure=0.0, reference_node=-1, pressure_solver=0)
+                           outlet_pressure=0.0, reference_node=-1, pressure_solver=0, conv_norm=0)
 
     def __del__(self):
         if getattr(self, "h", None) is not None:
@@ -123,7 +123,7 @@ class Oracle:
                               int(p["maxit_mom"]), int(p["maxit_p"]), int(p["n_corr"]),
                               float(p["relax_u"]), float(p["relax_p"]), int(p["outlet_type"]),
                               float(p["outlet_pressure"]), int(p["reference_node"]),
-                              int(p["pressure_solver"]))
+                              int(p["pressure_solver"]), int(p["conv_norm"]))
 
     def set_inlet(self, per_node):
         v = np.ascontiguousarray(per_node, np.float64).reshape(self.N2, 3)

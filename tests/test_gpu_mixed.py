@@ -18,7 +18,8 @@ pytestmark = pytest.mark.gpu
 
 
 def run(cf, po, m, precision, steps, tol, **kw):
-    s, _ = make_pair(cf, po, m, tol=tol, maxit=(20000, 50000), **kw)
+    kw.setdefault("maxit", (20000, 50000))
+    s, _ = make_pair(cf, po, m, tol=tol, **kw)
     s.setPrecision(precision)
     out = []
     for _ in range(steps):
@@ -76,3 +77,20 @@ def test_mixed_reports_non_convergence(cf, po):
     s.setPrecision(cf.PRECISION_MIXED)
     assert not s.pisoStep()
     assert s.getTime() == 0.0
+
+
+def test_jacobi_norm_makes_1e10_meaningful(cf, po):
+    """Under the Jacobi-scaled norm the configs' 1e-10 constrains the interior: FP64 at 1e-10 is
+    close to the converged solution and mixed at 1e-10 meets the 1e-6 bar against it."""
+    m = make_mesh(cf, 5, 68)
+    J = cf.NORM_JACOBI
+    ref = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-14, norm=J)
+    f64 = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-10, norm=J)
+    mix = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-10, norm=J)
+    for k in (0, 4, 9):
+        e64 = (rel_l2(f64[k][0], ref[k][0]), rel_l2(f64[k][1], ref[k][1]))
+        emx = (rel_l2(mix[k][0], ref[k][0]), rel_l2(mix[k][1], ref[k][1]))
+        print(f"jacobi norm step {k + 1}: fp64(1e-10) u {e64[0]:.2e} p {e64[1]:.2e}; "
+              f"mixed(1e-10) u {emx[0]:.2e} p {emx[1]:.2e}; iters fp64 {f64[k][2]['momentum_iters']} "
+              f"mixed {mix[k][2]['momentum_iters']} sweeps {mix[k][2]['momentum_outer']}")
+        assert max(emx) <= 1e-6, (k, emx)

@@ -28,7 +28,7 @@ def make_mesh(cf, rings=3, layers=12, length=30.0, radius=2.0):
 
 
 def make_pair(cf, po, m, *, tol=1e-12, krylov=0, dt=0.01, inlet=0.5, profile=None, ncorr=1,
-              relax=(1.0, 1.0), outlet=0, outlet_p=0.0, maxit=(5000, 20000)):
+              relax=(1.0, 1.0), outlet=0, outlet_p=0.0, maxit=(5000, 20000), norm=0):
     """GPU solver and oracle configured identically (the reference's CLI order: initialize with
     a zero inlet, then set the inlet)."""
     s = cf.NavierStokesSolver()
@@ -40,6 +40,7 @@ def make_pair(cf, po, m, *, tol=1e-12, krylov=0, dt=0.01, inlet=0.5, profile=Non
     s.setRelaxU(relax[0])
     s.setRelaxP(relax[1])
     s.setOutletType(outlet)
+    s.setConvergenceNorm(norm)
     s.initialize(m, cf.Fluid(RHO, NU))
     s.setOutletPressure(outlet_p)
     o = po.Oracle(m.vertices(), m.tets())
@@ -47,7 +48,7 @@ def make_pair(cf, po, m, *, tol=1e-12, krylov=0, dt=0.01, inlet=0.5, profile=Non
     o.set_params(dt=dt, tol_mom=tol, tol_p=tol, maxit_mom=maxit[0], maxit_p=maxit[1],
                  n_corr=ncorr, relax_u=relax[0], relax_p=relax[1], outlet_type=outlet,
                  outlet_pressure=outlet_p, reference_node=s.reference_node,
-                 pressure_solver=1 if krylov == cf.KRYLOV_CG else 0)
+                 pressure_solver=1 if krylov == cf.KRYLOV_CG else 0, conv_norm=norm)
     o.initialize()
     if profile is not None:
         s.setInletVelocityProfile(profile)
@@ -347,3 +348,16 @@ def test_persistent_cg_equals_loop_cg(cf, po):
         out.append((s.getVelocity(), s.getPressure(), s.stats()["pressure_iters"]))
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
     assert out[0][2] == out[1][2]
+
+
+@pytest.mark.parametrize("krylov", [0, 1], ids=["cg", "bicgstab"])
+def test_jacobi_norm_trajectory_bit_exact(cf, po, krylov):
+    """The Jacobi-scaled convergence norm, oracle and device in the same reduction tree."""
+    m = make_mesh(cf, 3, 12)
+    s, o = make_pair(cf, po, m, tol=1e-10, krylov=krylov, norm=cf.NORM_JACOBI, outlet_p=5.0)
+    for k in range(4):
+        assert s.pisoStep() and o.piso_step() == 0
+        assert s.stats()["momentum_iters"] == o.stats()["momentum_iters"], k
+        assert s.stats()["pressure_iters"] == o.stats()["pressure_iters"], k
+        st = o.state()
+        assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"]), k
