@@ -403,10 +403,11 @@ struct cfsa_ns {
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent, kBlock, 0));
       const int nblk_sell = (int)blocks_for(s1.nrows_pad), nblk_nat = (int)blocks_for(nv);
       cg_grid = std::min(nsm * per_sm, std::max(nblk_sell, nblk_nat));
-      bar_count = dalloc<unsigned int>(1);
+      cg_grid = std::min(cg_grid, kBarrierGroupSize * kBarrierGroups);
+      bar_count = dalloc<unsigned int>(1 + kBarrierGroups);
       bar_gen = dalloc<unsigned int>(1);
       bar_err = dalloc<int>(1);
-      CK(cudaMemsetAsync(bar_count, 0, sizeof(unsigned int), stream));
+      CK(cudaMemsetAsync(bar_count, 0, (1 + kBarrierGroups) * sizeof(unsigned int), stream));
       CK(cudaMemsetAsync(bar_gen, 0, sizeof(unsigned int), stream));
       CK(cudaMemsetAsync(bar_err, 0, sizeof(int), stream));
       cg_part_a = dalloc<double>((size_t)nblk_sell * kMaxRed);
@@ -767,7 +768,7 @@ struct cfsa_ns {
       c.st = st;
       c.bar = GridBarrier{bar_count, bar_gen, bar_err};
       c.scaled = (conv_norm == CFSA_NORM_JACOBI) ? 1 : 0;
-      CK(cudaMemsetAsync(bar_count, 0, sizeof(unsigned int), stream));
+      CK(cudaMemsetAsync(bar_count, 0, (1 + kBarrierGroups) * sizeof(unsigned int), stream));
       CK(cudaMemsetAsync(bar_err, 0, sizeof(int), stream));
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3((unsigned int)cg_grid);
