@@ -28,6 +28,7 @@ KERNEL_MOMENTUM_SPMV, KERNEL_PRESSURE_SPMV = 0, 1
 KRYLOV_CG, KRYLOV_BICGSTAB = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 NORM_REFERENCE, NORM_JACOBI = 0, 1
+OBJECTIVE_WALL_SHEAR, OBJECTIVE_PRESSURE_DROP = 0, 1
 
 
 class FluidBCType(enum.IntEnum):
@@ -105,6 +106,25 @@ class Stats(C.Structure):
             "krylov_iters": [int(x) for x in self.krylov_iters],
             "phase_ms": [float(x) for x in self.phase_ms],
         }
+
+
+class Objective(C.Structure):
+    """cfsa_objective: kind (OBJECTIVE_*), axis and [lo, hi] of a wall-shear patch."""
+
+    _fields_ = [("kind", C.c_int32), ("axis", C.c_int32), ("lo", C.c_double), ("hi", C.c_double)]
+
+
+class AdjointStats(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int64), ("checkpoint_every", C.c_int32), ("checkpoints", C.c_int32),
+        ("recomputed_steps", C.c_int64), ("momentum_iters", C.c_int64), ("pressure_iters", C.c_int64),
+        ("forward_ms", C.c_double), ("backward_ms", C.c_double), ("record_bytes", C.c_int64),
+        ("kernel_launches", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: (float(getattr(self, k)) if t is C.c_double else int(getattr(self, k)))
+                for k, t in self._fields_}
 
 
 _LIB = None
@@ -185,6 +205,11 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "cfsa_ns_get_inv_lumped_mass": (i32, [vp, vp]),
         "cfsa_ns_profile_kernel": (i32, [vp, i32, i32, vp, vp]),
         "cfsa_ns_compute_divergence_noalloc": (i32, [vp, vp, vp]),
+        "cfsa_ns_objective": (i32, [vp, vp, vp]),
+        "cfsa_ns_adjoint_forward": (i32, [vp, i32, i32, vp]),
+        "cfsa_ns_adjoint_backward": (i32, [vp, vp, vp, vp, vp, vp, vp]),
+        "cfsa_ns_adjoint_backward_seed": (i32, [vp, vp, vp, C.c_double, vp, vp, vp, vp]),
+        "cfsa_ns_get_adjoint_stats": (i32, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -554,6 +579,50 @@ class NavierStokesSolver:
         va = np.empty(nnz.value)
         self._check(self._lib.cfsa_ns_get_matrix(self._h, int(which), _ptr(rp), _ptr(ci), _ptr(va)))
         return rp, ci, va
+
+    # ---- discrete adjoint (forward / backward operator pair)
+    def objective(self, kind: int = OBJECTIVE_WALL_SHEAR, axis: int = 0, lo: float = 0.0,
+                  hi: float = 0.0) -> float:
+        o = Objective(int(kind), int(axis), float(lo), float(hi))
+        J = C.c_double()
+        self._check(self._lib.cfsa_ns_objective(self._h, C.byref(o), C.byref(J)))
+        return J.value
+
+    def adjointForward(self, nsteps: int, checkpoint_every: int = 0) -> bool:
+        """nsteps PISO steps recorded for the backward pass (checkpoint_every <= 0: automatic)."""
+        done = C.c_int()
+        return self._status(self._lib.cfsa_ns_adjoint_forward(self._h, int(nsteps), int(checkpoint_every),
+                                                              C.byref(done)))
+
+    def adjointBackward(self, kind: int = OBJECTIVE_WALL_SHEAR, axis: int = 0, lo: float = 0.0,
+                        hi: float = 0.0) -> dict:
+        """J and its gradients: grad_inlet [N2, 3], grad_viscosity, grad_u0 [N2, 3], grad_p0 [nv]."""
+        o = Objective(int(kind), int(axis), float(lo), float(hi))
+        J, gnu = C.c_double(), C.c_double()
+        gin = np.empty((self.N2, 3))
+        gu0 = np.empty((self.N2, 3))
+        gp0 = np.empty(self.nv)
+        self._check(self._lib.cfsa_ns_adjoint_backward(self._h, C.byref(o), C.byref(J), _ptr(gin),
+                                                       C.byref(gnu), _ptr(gu0), _ptr(gp0)))
+        return dict(J=J.value, grad_inlet=gin, grad_viscosity=gnu.value, grad_u0=gu0, grad_p0=gp0)
+
+    def adjointBackwardSeed(self, dJ_du=None, dJ_dp=None, dJ_dviscosity: float = 0.0) -> dict:
+        """Backward pass from a caller seed (dJ/du^N [N2, 3], dJ/dp^N [nv], explicit dJ/dnu)."""
+        du = None if dJ_du is None else _c(dJ_du, np.float64).reshape(self.N2, 3)
+        dp = None if dJ_dp is None else _c(dJ_dp, np.float64).reshape(self.nv)
+        gnu = C.c_double()
+        gin = np.empty((self.N2, 3))
+        gu0 = np.empty((self.N2, 3))
+        gp0 = np.empty(self.nv)
+        self._check(self._lib.cfsa_ns_adjoint_backward_seed(
+            self._h, None if du is None else _ptr(du), None if dp is None else _ptr(dp),
+            float(dJ_dviscosity), _ptr(gin), C.byref(gnu), _ptr(gu0), _ptr(gp0)))
+        return dict(grad_inlet=gin, grad_viscosity=gnu.value, grad_u0=gu0, grad_p0=gp0)
+
+    def adjointStats(self) -> dict:
+        s = AdjointStats()
+        self._check(self._lib.cfsa_ns_get_adjoint_stats(self._h, C.byref(s)))
+        return s.as_dict()
 
     def profileKernel(self, which: int, iters: int = 50) -> tuple[float, float]:
         """(mean launch ms, algorithmic bytes per launch) of one step kernel on live data."""

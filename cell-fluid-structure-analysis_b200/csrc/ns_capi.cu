@@ -5,6 +5,7 @@
 // WHILE nodes: the last reduction kernel of each iteration decides on the device whether the
 // loop continues, so a step (or a batch of steps) runs with no host round trip.
 #include "cfsa_ns.h"
+#include "ns_adjoint.cuh"
 #include "ns_kernels.cuh"
 #include "ns_mixed.cuh"
 
@@ -12,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <cstdint>
 #include <exception>
 #include <mutex>
 #include <new>
@@ -123,6 +125,28 @@ struct cfsa_ns {
   MixedState *h_ms = nullptr;
   double mixed_inner_tol = 1e-4;
   int mixed_inner_maxit = 300, mixed_max_outer = 30;
+  // discrete adjoint (ns_adjoint.cuh): transposed P1 slots, vertex -> (boundary face, local
+  // index in the face's tet) incidence, host vertex coordinates for objective patches
+  int *tpos1 = nullptr, *vbf_ptr = nullptr, *vbf = nullptr;
+  std::vector<double> h_xyz;
+  int64_t geom_gen = 0;
+  bool adj_work = false;
+  double *a_lu = nullptr, *a_lp = nullptr, *a_x = nullptr, *a_px = nullptr, *a_q = nullptr,
+         *a_lpp = nullptr, *a_tsc = nullptr, *a_gin = nullptr, *a_scal = nullptr, *a_un = nullptr,
+         *a_us = nullptr, *a_w = nullptr, *a_W = nullptr;  // a_scal: dJ/dnu, J, chain sum
+  signed char *a_mask = nullptr;
+  DevStatus *st_adj = nullptr;
+  std::vector<void *> rec_allocs;  // checkpoints and step records (re-planned per forward pass)
+  double *a_rec = nullptr, *a_ck = nullptr, *a_fin = nullptr;
+  int64_t a_rec_slots = 0, a_ck_slots = 0;
+  int adj_steps = 0, adj_C = 0, adj_nseg = 0;
+  bool adj_valid = false, adj_last_valid = false;
+  double adj_time_end = 0.0;
+  int64_t adj_steps_end = 0;
+  uint64_t adj_fp = 0;
+  cfsa_adjoint_stats adj_stats{};
+  cudaGraphExec_t adj_exec = nullptr;
+  int64_t adj_launches_fixed = 0;
   int64_t batch_launches = 0;
   int64_t batch_iters[2] = {0, 0};
   int launches_per_step = 0;  // kernels of one step outside the Krylov loop bodies
@@ -150,6 +174,8 @@ struct cfsa_ns {
   }
 
   ~cfsa_ns() {
+    if (adj_exec) cudaGraphExecDestroy(adj_exec);
+    for (void *ptr : rec_allocs) cudaFree(ptr);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     for (void *ptr : allocs) cudaFree(ptr);
@@ -283,7 +309,7 @@ struct cfsa_ns {
       for (int64_t t = 0; t < nt; ++t)
         for (int l = 0; l < 10; ++l) h_adj[fill[h_tnode[(size_t)l * nt + t]]++] = (int)(t * 16 + l);
     }
-    std::vector<double> h_xyz(m->vertices, m->vertices + 3 * nv);
+    h_xyz.assign(m->vertices, m->vertices + 3 * nv);
     xyz = dupload(h_xyz);
     tnode = dupload(h_tnode);
     bc = dupload(h_bc);
@@ -308,6 +334,15 @@ struct cfsa_ns {
     CK(cudaGetLastError());
     build_sell((int)N2, h_rp2, s2, rp2, ci2);
     build_sell((int)nv, h_rp1, s1, rp1, ci1);
+    tpos1 = dalloc<int>((size_t)nnz1);
+    k_transpose_slots<<<blocks_for(nnz1), kBlock, 0, stream>>>(nnz1, rows1, rp1, ci1, tpos1, d_err);
+    CK(cudaGetLastError());
+    {
+      int herr = 0;
+      CK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      if (herr) throw CudaError{"P1 sparsity pattern is not structurally symmetric"};
+    }
     Mv = dalloc<double>((size_t)nnz2);
     Kv = dalloc<double>((size_t)nnz2);
     Ms = dalloc<double>((size_t)s2.nentries);
@@ -394,6 +429,18 @@ struct cfsa_ns {
       vf = dupload(hvf);
       fshear = dalloc<double>((size_t)nbf * 3);
       fpress = dalloc<double>((size_t)nbf * 3);
+      // vertex -> (face, local index of the vertex in the face's tet), ascending face order
+      std::vector<int> hbp((size_t)nv + 1, 0), hb((size_t)nbf * 4);
+      for (int64_t fi = 0; fi < nbf; ++fi) {
+        if (ht[fi] < 0 || ht[fi] >= nt) throw CudaError{"boundary face tet out of range"};
+        for (int l = 0; l < 4; ++l) hbp[h_tnode[(size_t)l * nt + ht[fi]] + 1]++;
+      }
+      for (int64_t i = 0; i < nv; ++i) hbp[i + 1] += hbp[i];
+      std::vector<int> fb(hbp.begin(), hbp.end() - 1);
+      for (int64_t fi = 0; fi < nbf; ++fi)
+        for (int l = 0; l < 4; ++l) hb[fb[h_tnode[(size_t)l * nt + ht[fi]]]++] = (int)(fi * 4 + l);
+      vbf_ptr = dupload(hbp);
+      vbf = dupload(hb);
     }
     fout = dalloc<double>((size_t)nv * 3);
     // persistent CG: co-resident grid, barrier words, partial buffers
@@ -422,6 +469,7 @@ struct cfsa_ns {
 
   // buildMassMatrix + buildStiffnessMatrix + buildGradientMatrices + buildPoissonMatrix
   void assemble() {
+    ++geom_gen;
     k_geometry<<<blocks_for(nt), kBlock, 0, stream>>>((int)nt, xyz, tnode, vol, grad);
     k_assemble_p2<<<blocks_for(N2), kBlock, 0, stream>>>((int)N2, (int)nt, density, 1.0 / viscosity,
                                                          adj_ptr, adj, tnode, vol, grad, rp2, ci2, Mv, Kv);
@@ -534,14 +582,14 @@ struct cfsa_ns {
     return h_cs->active != 0;
   }
 
-  BicgArgs momentum_args() {
+  BicgArgs momentum_args(double *x_out = nullptr, DevStatus *s_out = nullptr) {
     BicgArgs a{};
     a.S = s2.view();
     a.At = At;
     a.diagA = diagA;
     a.invA = invA;
     a.b = wb;
-    a.x = ustar;
+    a.x = x_out ? x_out : ustar;
     a.r = wr;
     a.r0 = wr0;
     a.pk = wp;
@@ -551,7 +599,7 @@ struct cfsa_ns {
     a.n = (int)N2;
     a.bs = bs_mom;
     a.red = red;
-    a.st = st;
+    a.st = s_out ? s_out : st;
     a.slot = 0;
     a.cw = (conv_norm == CFSA_NORM_JACOBI) ? invA : nullptr;
     return a;
@@ -592,11 +640,17 @@ struct cfsa_ns {
     m.cw = (conv_norm == CFSA_NORM_JACOBI) ? invA : nullptr;
     k_momentum_rhs<<<blocks_for(s2.nrows_pad), kBlock, 0, stream>>>(m);
     CK(cudaGetLastError());
+    enqueue_momentum_krylov(capture, ustar, st);
+  }
+
+  // Batched momentum Krylov solve (x = 0, r = b in wb set up by k_momentum_rhs) into x; the
+  // check kernel records failures and iteration counts in `s`.
+  void enqueue_momentum_krylov(bool capture, double *x, DevStatus *s_out) {
     if (precision == CFSA_PRECISION_MIXED) {
-      enqueue_momentum_mixed(capture);
+      enqueue_momentum_mixed(capture, x, s_out);
       return;
     }
-    BicgArgs a = momentum_args();
+    BicgArgs a = momentum_args(x, s_out);
     auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
       BicgArgs b = a;
       b.cond = h;
@@ -607,11 +661,11 @@ struct cfsa_ns {
       capture_while(body);
     else
       eager_while(body, [&] { return poll_bicg(bs_mom); }, maxit_mom);
-    k_check_bicg<<<1, 1, 0, stream>>>(bs_mom, 3, 0, st);
+    k_check_bicg<<<1, 1, 0, stream>>>(bs_mom, 3, 0, s_out);
     CK(cudaGetLastError());
   }
 
-  MixedArgs mixed_args() {
+  MixedArgs mixed_args(double *x_out, DevStatus *s_out) {
     MixedArgs a{};
     a.S = s2.view();
     a.At32 = At32;
@@ -620,7 +674,7 @@ struct cfsa_ns {
     a.invA = invA;
     a.invA32 = invA32;
     a.b = wb;
-    a.x = ustar;
+    a.x = x_out;
     a.r64 = wr;
     a.xs = wv;
     a.r = fr;
@@ -632,7 +686,7 @@ struct cfsa_ns {
     a.dx = fdx;
     a.n = (int)N2;
     a.ms = ms;
-    a.st = st;
+    a.st = s_out;
     a.red = red;
     a.cw = (conv_norm == CFSA_NORM_JACOBI) ? invA : nullptr;
     a.cw32 = (conv_norm == CFSA_NORM_JACOBI) ? invA32 : nullptr;
@@ -641,8 +695,8 @@ struct cfsa_ns {
 
   // FP32 inner BiCGSTAB sweeps inside FP64 defect correction (ns_mixed.cuh); outer and inner
   // loops are nested WHILE nodes when captured.
-  void enqueue_momentum_mixed(bool capture) {
-    const MixedArgs a = mixed_args();
+  void enqueue_momentum_mixed(bool capture, double *x, DevStatus *s_out) {
+    const MixedArgs a = mixed_args(x, s_out);
     const unsigned int gp = blocks_for(N2), gs = blocks_for(s2.nrows_pad);
     k_mp_outer_init<<<gp, kBlock, 0, stream>>>(a, tol_mom, mixed_max_outer, mixed_inner_tol, mixed_inner_maxit);
     CK(cudaGetLastError());
@@ -677,7 +731,7 @@ struct cfsa_ns {
       capture_while(outer_body);
     else
       eager_while(outer_body, [&] { return poll_mixed(false); }, mixed_max_outer);
-    k_mp_check<<<1, 1, 0, stream>>>(ms, st);
+    k_mp_check<<<1, 1, 0, stream>>>(ms, s_out);
     CK(cudaGetLastError());
   }
 
@@ -689,6 +743,13 @@ struct cfsa_ns {
 
   void enqueue_pressure_solve(bool capture) {
     k_tet_div<<<blocks_for(nt), kBlock, 0, stream>>>((int)nt, N2, tnode, grad, ustar, divt, st);
+    const PressureRhsArgs a = pressure_rhs_args(pc, st);
+    k_pressure_rhs<<<blocks_for(nv), kBlock, 0, stream>>>(a);
+    CK(cudaGetLastError());
+    enqueue_pressure_krylov(capture, pc, st);
+  }
+
+  PressureRhsArgs pressure_rhs_args(double *x, DevStatus *s_out) {
     PressureRhsArgs a{};
     a.adj_ptr = adj_ptr;
     a.adj = adj;
@@ -706,17 +767,21 @@ struct cfsa_ns {
     a.krylov = (krylov == CFSA_KRYLOV_BICGSTAB) ? 1 : 0;
     a.scaled = (conv_norm == CFSA_NORM_JACOBI) ? 1 : 0;
     a.b = pb;
-    a.x = pc;
+    a.x = x;
     a.r = pr;
     a.z_or_r0 = pz;
     a.pk = pp;
     a.v = pv;
     a.cs = cs;
     a.bs = bs_p;
-    a.st = st;
+    a.st = s_out;
     a.red = red;
-    k_pressure_rhs<<<blocks_for(nv), kBlock, 0, stream>>>(a);
-    CK(cudaGetLastError());
+    return a;
+  }
+
+  // Pressure Krylov solve (state set up by k_pressure_rhs) into x; failures and iteration
+  // counts go to `s_out`.
+  void enqueue_pressure_krylov(bool capture, double *x, DevStatus *s_out) {
     if (krylov == CFSA_KRYLOV_BICGSTAB) {
       BicgArgs b{};
       b.S = s1.view();
@@ -724,7 +789,7 @@ struct cfsa_ns {
       b.diagA = diagL;
       b.invA = invL;
       b.b = pb;
-      b.x = pc;
+      b.x = x;
       b.r = pr;
       b.r0 = pz;
       b.pk = pp;
@@ -734,7 +799,7 @@ struct cfsa_ns {
       b.n = (int)nv;
       b.bs = bs_p;
       b.red = red;
-      b.st = st;
+      b.st = s_out;
       b.slot = 1;
       b.cw = (conv_norm == CFSA_NORM_JACOBI) ? invL : nullptr;
       auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
@@ -747,13 +812,13 @@ struct cfsa_ns {
         capture_while(body);
       else
         eager_while(body, [&] { return poll_bicg(bs_p); }, maxit_p);
-      k_check_bicg<<<1, 1, 0, stream>>>(bs_p, 1, 1, st);
+      k_check_bicg<<<1, 1, 0, stream>>>(bs_p, 1, 1, s_out);
     } else if (cg_persistent) {
       CgPersistentArgs c{};
       c.S = s1.view();
       c.Ls = Ls;
       c.invL = invL;
-      c.x = pc;
+      c.x = x;
       c.r = pr;
       c.z = pz;
       c.q = pq;
@@ -765,7 +830,7 @@ struct cfsa_ns {
       c.part_a = cg_part_a;
       c.part_b = cg_part_b;
       c.cs = cs;
-      c.st = st;
+      c.st = s_out;
       c.bar = GridBarrier{bar_count, bar_gen, bar_err};
       c.scaled = (conv_norm == CFSA_NORM_JACOBI) ? 1 : 0;
       CK(cudaMemsetAsync(bar_count, 0, (1 + kBarrierGroups) * sizeof(unsigned int), stream));
@@ -780,13 +845,13 @@ struct cfsa_ns {
       cfg.attrs = attr;
       cfg.numAttrs = 1;
       CK(cudaLaunchKernelEx(&cfg, k_cg_persistent, c));
-      k_check_cg<<<1, 1, 0, stream>>>(cs, st, bar_err);
+      k_check_cg<<<1, 1, 0, stream>>>(cs, s_out, bar_err);
     } else {
       CgArgs c{};
       c.S = s1.view();
       c.Ls = Ls;
       c.invL = invL;
-      c.x = pc;
+      c.x = x;
       c.r = pr;
       c.z = pz;
       c.pk = pp;
@@ -794,7 +859,7 @@ struct cfsa_ns {
       c.n = (int)nv;
       c.cs = cs;
       c.red = red;
-      c.st = st;
+      c.st = s_out;
       c.scaled = (conv_norm == CFSA_NORM_JACOBI) ? 1 : 0;
       auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
         CgArgs d = c;
@@ -808,7 +873,7 @@ struct cfsa_ns {
         capture_while(body);
       else
         eager_while(body, [&] { return poll_cg(); }, maxit_p);
-      k_check_cg<<<1, 1, 0, stream>>>(cs, st, nullptr);
+      k_check_cg<<<1, 1, 0, stream>>>(cs, s_out, nullptr);
     }
     CK(cudaGetLastError());
   }
@@ -983,6 +1048,432 @@ struct cfsa_ns {
     }
     CK(cudaMemcpyAsync(d, h_stage, (size_t)3 * N2 * sizeof(double), cudaMemcpyHostToDevice, stream));
     CK(cudaStreamSynchronize(stream));
+  }
+
+  // ------------------------------------------------------------------ discrete adjoint
+  // Everything the recorded forward pass depends on besides the state: parameters, inlet
+  // values, boundary tags and the geometry generation. The backward pass refuses to run when
+  // it differs from the value taken at recording time.
+  uint64_t adjoint_fingerprint() const {
+    uint64_t hsh = 1469598103934665603ull;
+    auto mix = [&](const void *ptr, size_t nb) {
+      const unsigned char *b = static_cast<const unsigned char *>(ptr);
+      for (size_t k = 0; k < nb; ++k) hsh = (hsh ^ b[k]) * 1099511628211ull;
+    };
+    const double d[] = {dt, tol_mom, tol_p, relax_u, relax_p, outlet_pressure, viscosity, density,
+                        mixed_inner_tol};
+    const int64_t k[] = {maxit_mom, maxit_p, ncorr, outlet_type, ref_node, krylov, precision,
+                         conv_norm, geom_gen, mixed_inner_maxit, (int64_t)cg_persistent};
+    mix(d, sizeof(d));
+    mix(k, sizeof(k));
+    mix(h_inlet.data(), h_inlet.size() * sizeof(double));
+    mix(h_bc.data(), h_bc.size());
+    return hsh;
+  }
+
+  void ensure_adjoint_work() {
+    if (adj_work) return;
+    const size_t n3 = (size_t)3 * N2;
+    a_lu = dalloc<double>(n3);
+    a_x = dalloc<double>(n3);
+    a_gin = dalloc<double>(n3);
+    a_us = dalloc<double>(n3);
+    a_lp = dalloc<double>(nv);
+    a_px = dalloc<double>(nv);
+    a_lpp = dalloc<double>(nv);
+    a_q = dalloc<double>((size_t)3 * nv);
+    a_un = dalloc<double>((size_t)3 * nv);
+    a_w = dalloc<double>((size_t)3 * nv);
+    a_W = dalloc<double>((size_t)3 * std::max<int64_t>(nbf, 1));
+    a_tsc = dalloc<double>((size_t)9 * nt);
+    a_scal = dalloc<double>(4);
+    a_mask = dalloc<signed char>(nv);
+    st_adj = dalloc<DevStatus>(1);
+    CK(cudaMemsetAsync(a_scal, 0, 4 * sizeof(double), stream));
+    adj_work = true;
+  }
+
+  int64_t rec_slot_doubles() const { return 3 * nv + 3 * N2; }
+  int64_t ck_slot_doubles() const { return 3 * N2 + nv; }
+
+  // Checkpoint and record storage for nsteps steps in segments of C (C <= 0: automatic).
+  void plan_records(int nsteps, int C) {
+    for (void *ptr : rec_allocs) CK(cudaFree(ptr));
+    rec_allocs.clear();
+    a_rec = a_ck = a_fin = nullptr;
+    const int64_t slot_b = rec_slot_doubles() * (int64_t)sizeof(double);
+    if (C <= 0) {
+      size_t freeb = 0, totb = 0;
+      CK(cudaMemGetInfo(&freeb, &totb));
+      const int64_t fit = (int64_t)(freeb / 2) / std::max<int64_t>(slot_b, 1);
+      C = (int)std::max<int64_t>(1, std::min<int64_t>(fit, nsteps));
+    }
+    C = std::max(1, std::min(C, std::max(nsteps, 1)));
+    adj_C = C;
+    adj_nseg = (nsteps + C - 1) / C;
+    a_rec_slots = C;
+    a_ck_slots = std::max(adj_nseg, 1);
+    auto alloc = [&](int64_t count) {
+      void *ptr = nullptr;
+      CK(cudaMalloc(&ptr, (size_t)std::max<int64_t>(count, 1) * sizeof(double)));
+      rec_allocs.push_back(ptr);
+      return static_cast<double *>(ptr);
+    };
+    a_rec = alloc(a_rec_slots * rec_slot_doubles());
+    a_ck = alloc(a_ck_slots * ck_slot_doubles());
+    a_fin = alloc((int64_t)6 * N2 + 2 * nv);
+  }
+
+  double *rec_u1(int slot) const { return a_rec + (int64_t)slot * rec_slot_doubles(); }
+  double *rec_us(int slot) const { return rec_u1(slot) + 3 * nv; }
+
+  void save_state(double *dst_u, double *dst_p) {
+    CK(cudaMemcpyAsync(dst_u, u, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(dst_p, p, (size_t)nv * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  }
+  void load_state(const double *src_u, const double *src_p) {
+    CK(cudaMemcpyAsync(u, src_u, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(p, src_p, (size_t)nv * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  }
+
+  // Steps n0..n1-1 of the recording: before each step u on the P1 vertices, after it u*, into
+  // the record slot n - n0. Eager stepping polls the status between steps.
+  void enqueue_recorded_steps(int n0, int n1) {
+    for (int n = n0; n < n1; ++n) {
+      const int slot = n - n0;
+      CK(cudaMemcpy2DAsync(rec_u1(slot), (size_t)nv * sizeof(double), u, (size_t)N2 * sizeof(double),
+                           (size_t)nv * sizeof(double), 3, cudaMemcpyDeviceToDevice, stream));
+      if (use_graph) {
+        CK(cudaGraphLaunch(graph_exec, stream));
+      } else {
+        enqueue_step(false, false);
+      }
+      CK(cudaMemcpyAsync(rec_us(slot), ustar, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                         stream));
+      if (!use_graph) {
+        CK(cudaMemcpyAsync(h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        if (h_st->halt) break;
+      }
+    }
+  }
+
+  int adjoint_forward(int nsteps, int C, int *n_done) {
+    if (ncorr < 1) throw CudaError{"the adjoint needs at least one pressure corrector"};
+    ensure_operators();
+    ensure_adjoint_work();
+    adj_valid = false;
+    plan_records(nsteps, C);
+    if (use_graph) ensure_graph();
+    reset_status();
+    CK(cudaEventRecord(ev0, stream));
+    for (int seg = 0; seg < adj_nseg; ++seg) {
+      const int n0 = seg * adj_C, n1 = std::min(nsteps, n0 + adj_C);
+      double *ck = a_ck + (int64_t)seg * ck_slot_doubles();
+      save_state(ck, ck + 3 * N2);
+      enqueue_recorded_steps(n0, n1);
+    }
+    if (adj_nseg == 0) save_state(a_ck, a_ck + 3 * N2);
+    CK(cudaEventRecord(ev1, stream));
+    const int code = finish_batch(nsteps);
+    if (n_done) *n_done = h_st->steps_done;
+    // final snapshot: u, u*, p, p'
+    CK(cudaMemcpyAsync(a_fin, u, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(a_fin + 3 * N2, ustar, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                       stream));
+    CK(cudaMemcpyAsync(a_fin + 6 * N2, p, (size_t)nv * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(a_fin + 6 * N2 + nv, pc, (size_t)nv * sizeof(double), cudaMemcpyDeviceToDevice,
+                       stream));
+    CK(cudaStreamSynchronize(stream));
+    adj_stats = cfsa_adjoint_stats{};
+    adj_stats.steps = nsteps;
+    adj_stats.checkpoint_every = adj_C;
+    adj_stats.checkpoints = adj_nseg;
+    adj_stats.forward_ms = last_ms;
+    adj_stats.record_bytes =
+        (int64_t)sizeof(double) * (a_rec_slots * rec_slot_doubles() + a_ck_slots * ck_slot_doubles() +
+                                   6 * N2 + 2 * nv);
+    if (code != CFSA_OK) return code;
+    adj_steps = nsteps;
+    adj_last_valid = true;  // the last segment's records are the ones just written
+    adj_time_end = time;
+    adj_steps_end = steps;
+    adj_fp = adjoint_fingerprint();
+    adj_valid = true;
+    return CFSA_OK;
+  }
+
+  void restore_final_state() {
+    CK(cudaMemcpyAsync(u, a_fin, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(ustar, a_fin + 3 * N2, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                       stream));
+    CK(cudaMemcpyAsync(p, a_fin + 6 * N2, (size_t)nv * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(pc, a_fin + 6 * N2 + nv, (size_t)nv * sizeof(double), cudaMemcpyDeviceToDevice,
+                       stream));
+  }
+
+  // Objective on the current fields: J -> a_scal[1]; with seed, dJ/du -> a_lu, dJ/dp -> a_lp,
+  // explicit dJ/dnu -> a_scal[0]. Returns false when the objective's vertex set is empty.
+  bool enqueue_objective(const cfsa_objective &o, bool seed) {
+    ensure_adjoint_work();
+    const size_t n3 = (size_t)3 * N2;
+    if (o.kind == CFSA_OBJECTIVE_WALL_SHEAR) {
+      if (nbf <= 0) throw CudaError{"wall-shear objective needs boundary faces"};
+      if (o.axis < 0 || o.axis > 2) throw CudaError{"objective axis must be 0, 1 or 2"};
+      std::vector<signed char> mask((size_t)nv, 0);
+      int64_t np = 0;
+      for (int64_t v = 0; v < nv; ++v) {
+        const double x = h_xyz[3 * v + o.axis];
+        if (h_bc[v] == BC_WALL && x >= o.lo && x <= o.hi) {
+          mask[v] = 1;
+          ++np;
+        }
+      }
+      if (np == 0) return false;
+      CK(cudaMemcpyAsync(a_mask, mask.data(), (size_t)nv, cudaMemcpyHostToDevice, stream));
+      k_face_forces<<<blocks_for(nbf), kBlock, 0, stream>>>((int)nbf, (int)nt, N2, viscosity, fverts, ftet,
+                                                           fnormal, farea, tnode, grad, u, p, fshear, fpress);
+      k_face_gather<<<blocks_for(nv), kBlock, 0, stream>>>((int)nv, vf_ptr, vf, fshear, fout);
+      k_obj_wss_value<<<blocks_for(nv), kBlock, 0, stream>>>((int)nv, fout, a_mask, 1.0 / (double)np,
+                                                             viscosity, a_w, a_scal + 1, a_scal, red);
+      if (seed) {
+        k_obj_wss_face<<<blocks_for(nbf), kBlock, 0, stream>>>((int)nbf, fverts, farea, a_w, a_W);
+        k_obj_wss_seed<<<blocks_for(N2), kBlock, 0, stream>>>((int)nv, N2, (int)nt, vbf_ptr, vbf, ftet,
+                                                              fnormal, grad, a_W, viscosity, a_lu);
+        CK(cudaMemsetAsync(a_lp, 0, (size_t)nv * sizeof(double), stream));
+      }
+      CK(cudaGetLastError());
+      // the mask upload reads host memory that goes out of scope
+      CK(cudaStreamSynchronize(stream));
+      return true;
+    }
+    if (o.kind == CFSA_OBJECTIVE_PRESSURE_DROP) {
+      int64_t nin = 0, nout = 0;
+      for (int64_t v = 0; v < nv; ++v) {
+        nin += h_bc[v] == BC_INLET;
+        nout += h_bc[v] == BC_OUTLET;
+      }
+      if (nin == 0 || nout == 0) return false;
+      k_obj_pdrop<<<blocks_for(nv), kBlock, 0, stream>>>((int)nv, p, bc, 1.0 / (double)nin,
+                                                         1.0 / (double)nout, a_lp, a_scal + 1, red);
+      if (seed) {
+        CK(cudaMemsetAsync(a_lu, 0, n3 * sizeof(double), stream));
+        CK(cudaMemsetAsync(a_scal, 0, sizeof(double), stream));
+      }
+      CK(cudaGetLastError());
+      return true;
+    }
+    throw CudaError{"unknown objective kind"};
+  }
+
+  // One reverse step on (a_lu, a_lp) with the step's records in a_un (u^n on P1) and a_us (u*).
+  void enqueue_adj_step(bool capture) {
+    const unsigned int gN2 = blocks_for(N2), gnv = blocks_for(nv);
+    AdjCorrectArgs c{};
+    c.lu = a_lu;
+    c.bc = bc;
+    c.invm = invm;
+    c.dt = dt;
+    c.relax_u = relax_u;
+    c.n = (int)N2;
+    c.nv = (int)nv;
+    c.lus = wb;
+    c.gin = a_gin;
+    c.q = a_q;
+    c.st = st_adj;
+    k_adj_correct<<<gN2, kBlock, 0, stream>>>(c);
+    const bool normalize = (ref_node >= 0 && ref_node < nv);
+    for (int k = ncorr - 1; k >= 0; --k) {
+      if (normalize) k_adj_sum<<<gnv, kBlock, 0, stream>>>((int)nv, a_lp, a_scal + 2, red, st_adj);
+      AdjChainArgs ch{};
+      ch.chain = a_lp;
+      ch.lpp = a_lpp;
+      ch.S = normalize ? a_scal + 2 : nullptr;
+      ch.bc = bc;
+      ch.relax_p = relax_p;
+      ch.nv = (int)nv;
+      ch.ref_node = ref_node;
+      ch.dirichlet = (outlet_type == CFSA_OUTLET_DIRICHLET) ? 1 : 0;
+      ch.first = (k == ncorr - 1) ? 1 : 0;
+      ch.st = st_adj;
+      k_adj_pchain<<<gnv, kBlock, 0, stream>>>(ch);
+    }
+    PressureRhsArgs pa = pressure_rhs_args(a_px, st_adj);
+    pa.adj_q = a_q;
+    pa.adj_lpp = a_lpp;
+    pa.G = CsrView{rp1, ci1};
+    pa.tpos = tpos1;
+    pa.Gv = Gv;
+    pa.nnz1 = nnz1;
+    k_pressure_rhs<<<gnv, kBlock, 0, stream>>>(pa);
+    CK(cudaGetLastError());
+    enqueue_pressure_krylov(capture, a_px, st_adj);
+    MomentumRhsArgs m{};
+    m.S = s2.view();
+    m.G = CsrView{rp1, ci1};
+    m.Gv = Gv;
+    m.nnz1 = nnz1;
+    m.bc = bc;
+    m.dt = dt;
+    m.tol = tol_mom;
+    m.n = (int)N2;
+    m.nv = (int)nv;
+    m.nt = (int)nt;
+    m.maxit = maxit_mom;
+    m.b = wb;
+    m.x = a_x;
+    m.r = wr;
+    m.r0 = wr0;
+    m.pk = wp;
+    m.v = wv;
+    m.bs = bs_mom;
+    m.st = st_adj;
+    m.red = red;
+    m.cw = (conv_norm == CFSA_NORM_JACOBI) ? invA : nullptr;
+    m.adj_mu = a_px;
+    m.tpos = tpos1;
+    k_momentum_rhs<<<blocks_for(s2.nrows_pad), kBlock, 0, stream>>>(m);
+    CK(cudaGetLastError());
+    enqueue_momentum_krylov(capture, a_x, st_adj);
+    k_adj_conv_tet<<<blocks_for(nt), kBlock, 0, stream>>>((int)nt, N2, nv, tnode, grad, vol, a_x, a_un,
+                                                          a_tsc, st_adj);
+    AdjMomOutArgs o{};
+    o.S = s2.view();
+    o.Ms = Ms;
+    o.K = CsrView{rp2, ci2};
+    o.Kv = Kv;
+    o.G = CsrView{rp1, ci1};
+    o.tpos = tpos1;
+    o.Gv = Gv;
+    o.nnz1 = nnz1;
+    o.adj_ptr = adj_ptr;
+    o.adj = adj;
+    o.grad = grad;
+    o.tsc = a_tsc;
+    o.bc = bc;
+    o.nu = a_x;
+    o.us = a_us;
+    o.dt = dt;
+    o.viscosity = viscosity;
+    o.n = (int)N2;
+    o.nv = (int)nv;
+    o.nt = (int)nt;
+    o.lu = a_lu;
+    o.lp = a_lp;
+    o.gin = a_gin;
+    o.gnu = a_scal;
+    o.red = red;
+    o.st = st_adj;
+    k_adj_mom_out<<<blocks_for(s2.nrows_pad), kBlock, 0, stream>>>(o);
+    CK(cudaGetLastError());
+    // correct, [sum,] chain per corrector, pressure rhs + check, momentum rhs + check,
+    // conv_tet, mom_out (Krylov loop bodies counted from the status)
+    adj_launches_fixed = 1 + ncorr * (normalize ? 2 : 1) + 2 + 2 + 2 +
+                         (precision == CFSA_PRECISION_MIXED ? 1 : 0);
+  }
+
+  void ensure_adj_graph() {
+    if (adj_exec) {
+      CK(cudaGraphExecDestroy(adj_exec));
+      adj_exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+    try {
+      enqueue_adj_step(true);
+    } catch (...) {
+      cudaGraph_t gg = nullptr;
+      cudaStreamEndCapture(stream, &gg);
+      if (gg) cudaGraphDestroy(gg);
+      throw;
+    }
+    CK(cudaStreamEndCapture(stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&adj_exec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+  }
+
+  // Backward pass. The seed is already in a_lu / a_lp / a_scal[0].
+  int adjoint_backward_core(double *grad_inlet, double *grad_viscosity, double *grad_u0, double *grad_p0) {
+    const size_t n3 = (size_t)3 * N2;
+    CK(cudaMemsetAsync(a_gin, 0, n3 * sizeof(double), stream));
+    CK(cudaMemsetAsync(st_adj, 0, sizeof(DevStatus), stream));
+    reset_status();
+    if (use_graph) {
+      ensure_graph();
+      ensure_adj_graph();
+    }
+    const double time_save = time;
+    const int64_t steps_save = steps;
+    int64_t recomputed = 0;
+    CK(cudaEventRecord(ev0, stream));
+    for (int seg = adj_nseg - 1; seg >= 0; --seg) {
+      const int n0 = seg * adj_C, n1 = std::min(adj_steps, n0 + adj_C);
+      if (!(seg == adj_nseg - 1 && adj_last_valid)) {
+        const double *ck = a_ck + (int64_t)seg * ck_slot_doubles();
+        load_state(ck, ck + 3 * N2);
+        enqueue_recorded_steps(n0, n1);
+        recomputed += n1 - n0;
+      }
+      for (int n = n1 - 1; n >= n0; --n) {
+        const int slot = n - n0;
+        CK(cudaMemcpyAsync(a_un, rec_u1(slot), (size_t)3 * nv * sizeof(double), cudaMemcpyDeviceToDevice,
+                           stream));
+        CK(cudaMemcpyAsync(a_us, rec_us(slot), n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        if (use_graph) {
+          CK(cudaGraphLaunch(adj_exec, stream));
+        } else {
+          enqueue_adj_step(false);
+        }
+      }
+    }
+    CK(cudaEventRecord(ev1, stream));
+    restore_final_state();
+    // the last segment's records now hold its own steps again only if it was not recomputed
+    adj_last_valid = (adj_nseg <= 1);
+    DevStatus hs_adj{};
+    CK(cudaMemcpyAsync(h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(&hs_adj, st_adj, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    time = time_save;
+    steps = steps_save;
+    adj_stats.recomputed_steps = recomputed;
+    adj_stats.momentum_iters = (int64_t)hs_adj.iters[0];
+    adj_stats.pressure_iters = (int64_t)hs_adj.iters[1];
+    adj_stats.backward_ms = ms;
+    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : (cg_persistent ? 1 : 3);
+    adj_stats.kernel_launches = (int64_t)adj_steps * adj_launches_fixed + 5 * (int64_t)hs_adj.body_runs[0] +
+                                pressure_body * (int64_t)hs_adj.body_runs[1] +
+                                3 * (int64_t)hs_adj.body_runs[2];
+    if (h_st->code != CFSA_OK) {
+      err = "forward recomputation failed with status " + std::to_string(h_st->code);
+      return h_st->code;
+    }
+    if (hs_adj.code != CFSA_OK) {
+      err = "adjoint solve failed with status " + std::to_string(hs_adj.code);
+      return hs_adj.code;
+    }
+    std::vector<double> tmp(n3);
+    if (grad_inlet) download_vec3(a_gin, grad_inlet);
+    if (grad_u0) download_vec3(a_lu, grad_u0);
+    if (grad_p0) CK(cudaMemcpy(grad_p0, a_lp, (size_t)nv * sizeof(double), cudaMemcpyDeviceToHost));
+    if (grad_viscosity) CK(cudaMemcpy(grad_viscosity, a_scal, sizeof(double), cudaMemcpyDeviceToHost));
+    return CFSA_OK;
+  }
+
+  int check_adjoint_ready() {
+    if (!adj_valid) {
+      err = "no recorded forward pass (cfsa_ns_adjoint_forward) for the backward pass";
+      return CFSA_NOT_INITIALIZED;
+    }
+    if (mom_dirty || poisson_dirty || adjoint_fingerprint() != adj_fp) {
+      adj_valid = false;
+      err = "parameters, inlet values, tags or geometry changed since the recorded forward pass";
+      return CFSA_BAD_ARG;
+    }
+    return CFSA_OK;
   }
 
   // Kernel timing on the live data with private Krylov states (solver state untouched).
@@ -1260,6 +1751,7 @@ int cfsa_ns_update_vertices(cfsa_ns *h, const double *xyz) {
   if (!h || !xyz) return CFSA_BAD_ARG;
   return guarded(h, [&] {
     CK(cudaMemcpyAsync(h->xyz, xyz, (size_t)3 * h->nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    h->h_xyz.assign(xyz, xyz + 3 * h->nv);
     h->assemble();
     CK(cudaStreamSynchronize(h->stream));
     return CFSA_OK;
@@ -1567,6 +2059,73 @@ int cfsa_ns_get_inv_lumped_mass(cfsa_ns *h, double *out) {
     CK(cudaStreamSynchronize(h->stream));
     return CFSA_OK;
   });
+}
+
+// ---- discrete adjoint ----
+int cfsa_ns_objective(cfsa_ns *h, const cfsa_objective *obj, double *J) {
+  if (!h || !obj || !J) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    if (!h->enqueue_objective(*obj, false)) return fail(h, CFSA_BAD_ARG, "objective vertex set is empty");
+    CK(cudaMemcpyAsync(J, h->a_scal + 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_adjoint_forward(cfsa_ns *h, int nsteps, int checkpoint_every, int *n_done) {
+  if (!h) return CFSA_BAD_ARG;
+  if (nsteps < 1) return fail(h, CFSA_BAD_ARG, "the forward pass needs at least one step");
+  if (h->ncorr < 1) return fail(h, CFSA_UNSUPPORTED, "the adjoint needs at least one pressure corrector");
+  return guarded(h, [&] {
+    const int code = h->adjoint_forward(nsteps, checkpoint_every, n_done);
+    if (code != CFSA_OK) h->err = "forward pass failed with status " + std::to_string(code);
+    return code;
+  });
+}
+
+int cfsa_ns_adjoint_backward(cfsa_ns *h, const cfsa_objective *obj, double *J, double *grad_inlet,
+                             double *grad_viscosity, double *grad_u0, double *grad_p0) {
+  if (!h || !obj) return CFSA_BAD_ARG;
+  const int ready = h->check_adjoint_ready();
+  if (ready != CFSA_OK) return ready;
+  return guarded(h, [&] {
+    h->restore_final_state();
+    if (!h->enqueue_objective(*obj, true)) return fail(h, CFSA_BAD_ARG, "objective vertex set is empty");
+    if (J) {
+      CK(cudaMemcpyAsync(J, h->a_scal + 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+    }
+    return h->adjoint_backward_core(grad_inlet, grad_viscosity, grad_u0, grad_p0);
+  });
+}
+
+int cfsa_ns_adjoint_backward_seed(cfsa_ns *h, const double *dJ_du, const double *dJ_dp,
+                                  double dJ_dviscosity, double *grad_inlet, double *grad_viscosity,
+                                  double *grad_u0, double *grad_p0) {
+  if (!h) return CFSA_BAD_ARG;
+  const int ready = h->check_adjoint_ready();
+  if (ready != CFSA_OK) return ready;
+  return guarded(h, [&] {
+    h->ensure_adjoint_work();
+    h->restore_final_state();
+    if (dJ_du)
+      h->upload_vec3(dJ_du, h->a_lu);
+    else
+      CK(cudaMemsetAsync(h->a_lu, 0, (size_t)3 * h->N2 * sizeof(double), h->stream));
+    if (dJ_dp)
+      CK(cudaMemcpyAsync(h->a_lp, dJ_dp, (size_t)h->nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    else
+      CK(cudaMemsetAsync(h->a_lp, 0, (size_t)h->nv * sizeof(double), h->stream));
+    CK(cudaMemcpyAsync(h->a_scal, &dJ_dviscosity, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return h->adjoint_backward_core(grad_inlet, grad_viscosity, grad_u0, grad_p0);
+  });
+}
+
+int cfsa_ns_get_adjoint_stats(cfsa_ns *h, cfsa_adjoint_stats *out) {
+  if (!h || !out) return CFSA_BAD_ARG;
+  *out = h->adj_stats;
+  return CFSA_OK;
 }
 
 }  // extern "C"

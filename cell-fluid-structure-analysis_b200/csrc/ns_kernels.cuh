@@ -479,6 +479,26 @@ __device__ __forceinline__ void sell_spmv_row(const SellView &S, const double *_
   }
 }
 
+// Row i of the transposed P1 operators G_a^T (a = 0..2) applied to x_a. The P1 pattern is
+// structurally symmetric: the entry (i, j) of G_a^T is G_a(j, i), stored at the transposed slot
+// tpos[k] of the entry k = (i, j); entries are summed in ascending column order.
+__device__ __forceinline__ void gt_row3(int i, const int *__restrict__ rp, const int *__restrict__ ci,
+                                        const int *__restrict__ tpos, const double *__restrict__ Gv,
+                                        int64_t nnz1, const double *__restrict__ x0,
+                                        const double *__restrict__ x1,
+                                        const double *__restrict__ x2, double out[3]) {
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const int j = ci[k], t = tpos[k];
+    s0 += Gv[t] * x0[j];
+    s1 += Gv[nnz1 + t] * x1[j];
+    s2 += Gv[2 * nnz1 + t] * x2[j];
+  }
+  out[0] = s0;
+  out[1] = s1;
+  out[2] = s2;
+}
+
 // ------------------------------------------------------------------------------------------
 // Momentum right-hand side (NavierStokes.cpp:429-495) for the three components, fused with the
 // initialisation of the batched BiCGSTAB (x0 = 0, r = r0 = b, p = v = 0).
@@ -500,6 +520,10 @@ struct MomentumRhsArgs {
   BicgState *bs;
   DevStatus *st;
   Reduce red;
+  // Adjoint mode (adj_mu != nullptr): b holds the adjoint right-hand side on entry and its P1
+  // rows receive -G_a^T mu / dt (transposed slots tpos); the forward terms are not formed.
+  const double *adj_mu;
+  const int *tpos;
 };
 
 __global__ void k_momentum_rhs(MomentumRhsArgs A) {
@@ -510,9 +534,19 @@ __global__ void k_momentum_rhs(MomentumRhsArgs A) {
   if (i >= 0) {
     const int64_t n = A.n;
     const double w = A.cw ? A.cw[i] : 1.0;
+    double b[3];
+    if (A.adj_mu) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) b[c] = A.b[c * n + i];
+      if (i < A.nv) {
+        double g[3];
+        gt_row3(i, A.G.rp, A.G.ci, A.tpos, A.Gv, A.nnz1, A.adj_mu, A.adj_mu, A.adj_mu, g);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) b[c] = b[c] - g[c] / A.dt;
+      }
+    } else {
     double mu[3];
     sell_spmv_row<3>(A.S, A.Ms, A.u, n, r, mu);
-    double b[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) b[c] = 0.0 + mu[c] / A.dt;
     if (i < A.nv) {
@@ -537,6 +571,7 @@ __global__ void k_momentum_rhs(MomentumRhsArgs A) {
         const double up = (bcv == BC_INLET) ? A.inlet[c * n + i] : 0.0;
         b[c] += kMomentumPenalty * up;
       }
+    }
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -843,6 +878,12 @@ struct PressureRhsArgs {
   BicgState *bs;
   DevStatus *st;
   Reduce red;
+  // Adjoint mode (adj_q != nullptr): b = sum_a G_a^T q_a + adj_lpp (q_a = adj_q + a*nv).
+  const double *adj_q, *adj_lpp;
+  CsrView G;
+  const int *tpos;
+  const double *Gv;
+  int64_t nnz1;
 };
 
 __global__ void k_pressure_rhs(PressureRhsArgs A) {
@@ -850,12 +891,20 @@ __global__ void k_pressure_rhs(PressureRhsArgs A) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double part[2] = {0.0, 0.0};
   if (i < A.nv) {
-    const double d = gather_div(i, A.adj_ptr, A.adj, A.vol, A.divt);
-    double b = -d / A.dt;
-    if (A.outlet_type == 1) {
-      if (i == A.ref_node) b += kPoissonPenalty * 0.0;
-    } else if (A.outlet_type == 0) {
-      if (A.bc[i] == BC_OUTLET) b += kPoissonPenalty * A.outlet_pressure;
+    double b;
+    if (A.adj_q) {
+      double g[3];
+      gt_row3(i, A.G.rp, A.G.ci, A.tpos, A.Gv, A.nnz1, A.adj_q, A.adj_q + A.nv,
+              A.adj_q + 2 * (int64_t)A.nv, g);
+      b = ((g[0] + g[1]) + g[2]) + A.adj_lpp[i];
+    } else {
+      const double d = gather_div(i, A.adj_ptr, A.adj, A.vol, A.divt);
+      b = -d / A.dt;
+      if (A.outlet_type == 1) {
+        if (i == A.ref_node) b += kPoissonPenalty * 0.0;
+      } else if (A.outlet_type == 0) {
+        if (A.bc[i] == BC_OUTLET) b += kPoissonPenalty * A.outlet_pressure;
+      }
     }
     A.b[i] = b;
     A.x[i] = 0.0;

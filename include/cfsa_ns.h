@@ -210,6 +210,58 @@ int cfsa_ns_profile_kernel(cfsa_ns *h, int which, int iters, double *avg_ms, dou
  * once div_dev is written. */
 int cfsa_ns_compute_divergence_noalloc(cfsa_ns *h, const double *u_dev, double *div_dev);
 
+/* ---- discrete adjoint (no counterpart in the reference) ----
+ * Reverse mode through the PISO steps exactly as the forward kernels compute them (every Krylov
+ * solve taken as the exact linear solve it converges to). The differentiated map is
+ *   (inlet values g [N2][3], viscosity) -> J(u^N, p^N),
+ * N PISO steps from the state (u^0, p^0) held when cfsa_ns_adjoint_forward starts, which is held
+ * fixed (its adjoint is returned as dJ/du0, dJ/dp0 so that callers can chain). The pair
+ * forward/backward is used like a torch.autograd.Function: forward runs and records, backward
+ * takes the objective (or a caller seed dJ/du^N, dJ/dp^N) and returns the gradients.
+ * Objectives read the fields computeShearStress / getPressure expose (NavierStokes.cpp:874-944). */
+#define CFSA_OBJECTIVE_WALL_SHEAR 0    /* mean over wall vertices with lo <= x[axis] <= hi of |s_v|^2,
+                                          s = computeShearStress (traction per vertex) */
+#define CFSA_OBJECTIVE_PRESSURE_DROP 1 /* mean p over inlet vertices - mean p over outlet vertices */
+
+typedef struct {
+  int32_t kind; /* CFSA_OBJECTIVE_* */
+  int32_t axis; /* wall-shear patch: coordinate axis 0..2 */
+  double lo, hi;
+} cfsa_objective;
+
+typedef struct {
+  int64_t steps;             /* recorded forward steps N */
+  int32_t checkpoint_every;  /* steps per checkpoint segment */
+  int32_t checkpoints;       /* stored (u, p) checkpoints */
+  int64_t recomputed_steps;  /* forward steps re-run by the last backward pass */
+  int64_t momentum_iters;    /* adjoint Krylov iterations of the last backward pass */
+  int64_t pressure_iters;
+  double forward_ms;         /* device time of the forward pass (CUDA events) */
+  double backward_ms;        /* device time of the last backward pass, recomputation included */
+  int64_t record_bytes;      /* device memory held by checkpoints and step records */
+  int64_t kernel_launches;   /* device kernels launched by the last backward pass */
+} cfsa_adjoint_stats;
+
+/* Objective value on the current fields. */
+int cfsa_ns_objective(cfsa_ns *h, const cfsa_objective *obj, double *J);
+/* Forward half: runs nsteps PISO steps (same kernels and results as cfsa_ns_piso_steps) and keeps
+ * a checkpoint of (u, p) every checkpoint_every steps plus the per-step data of the last segment
+ * (u^n on P1 vertices and u* of each step). checkpoint_every <= 0 chooses the largest segment
+ * whose step records fit in half of the free device memory (no recomputation when all steps
+ * fit). The backward pass re-runs each earlier segment from its checkpoint. Any later change of
+ * parameters, inlet values, tags or geometry invalidates the recording. */
+int cfsa_ns_adjoint_forward(cfsa_ns *h, int nsteps, int checkpoint_every, int *n_done);
+/* Backward half for a built-in objective, evaluated on the recorded final state. Outputs may be
+ * NULL: J; grad_inlet [N2][3] = dJ/dg (zero off inlet nodes); grad_viscosity = dJ/dnu;
+ * grad_u0 [N2][3], grad_p0 [nv]. The solver's fields are left at the recorded final state. */
+int cfsa_ns_adjoint_backward(cfsa_ns *h, const cfsa_objective *obj, double *J, double *grad_inlet,
+                             double *grad_viscosity, double *grad_u0, double *grad_p0);
+/* Backward half from a caller seed dJ/du^N [N2][3], dJ/dp^N [nv] and the explicit dJ/dnu. */
+int cfsa_ns_adjoint_backward_seed(cfsa_ns *h, const double *dJ_du, const double *dJ_dp,
+                                  double dJ_dviscosity, double *grad_inlet, double *grad_viscosity,
+                                  double *grad_u0, double *grad_p0);
+int cfsa_ns_get_adjoint_stats(cfsa_ns *h, cfsa_adjoint_stats *out);
+
 #ifdef __cplusplus
 }
 #endif

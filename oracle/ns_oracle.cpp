@@ -962,6 +962,287 @@ struct Oracle {
       }
     }
   }
+
+  // ---------------------------------------------------------------- discrete adjoint
+  // Reverse mode through the PISO steps exactly as implemented above (each Krylov solve taken
+  // as the exact linear solve it converges to). The differentiated map is
+  //   (inlet values g, viscosity) -> J(u^N, p^N)
+  // with the state (u^0, p^0) at the start of recording held fixed. Operators: M, K, L are
+  // symmetric, so the adjoint solves reuse the forward operators; G needs its transpose.
+  struct AdjRecord {
+    std::vector<V3> u, us;  // u^n (step input) and u* of step n
+  };
+  std::vector<AdjRecord> adj_rec;
+  std::vector<V3> adj_u0;
+  std::vector<double> adj_p0;
+  int adj_it_mom = 0, adj_it_p = 0;
+
+  // Forward half: nsteps PISO steps from the current state, recording step inputs and u*.
+  int adjoint_forward(int nsteps) {
+    adj_rec.clear();
+    adj_u0 = u;
+    adj_p0 = p;
+    for (int n = 0; n < nsteps; ++n) {
+      adj_rec.push_back({u, {}});
+      const int rc = piso_step();
+      adj_rec.back().us = ustar;
+      if (rc) return rc;
+    }
+    return 0;
+  }
+
+  static CSR transpose(const CSR &A, int64_t ncols) {
+    CSR T;
+    T.n = ncols;
+    T.rowptr.assign(ncols + 1, 0);
+    for (int c : A.col) T.rowptr[c + 1]++;
+    for (int64_t i = 0; i < ncols; ++i) T.rowptr[i + 1] += T.rowptr[i];
+    T.col.resize(A.col.size());
+    T.val.resize(A.val.size());
+    std::vector<int64_t> fill(T.rowptr.begin(), T.rowptr.end() - 1);
+    for (int64_t i = 0; i < A.n; ++i)
+      for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) {
+        const int64_t q = fill[A.col[k]]++;
+        T.col[q] = (int)i;
+        T.val[q] = A.val[k];
+      }
+    return T;
+  }
+
+  CSR momentum_lhs() const {
+    CSR lhs = M;
+    for (int64_t k = 0; k < lhs.nnz(); ++k) lhs.val[k] = M.val[k] / dt + K.val[k];
+    for (size_t i = 0; i < N2; ++i) {
+      const int bc = bc_of(i);
+      if (bc == kInlet || bc == kWall)
+        for (int64_t k = lhs.rowptr[i]; k < lhs.rowptr[i + 1]; ++k)
+          if (lhs.col[k] == (int)i) lhs.val[k] += 1e10;
+    }
+    return lhs;
+  }
+  CSR poisson_lhs() const {
+    CSR Lbc = L;
+    auto add_diag = [&](size_t i, double v) {
+      for (int64_t k = Lbc.rowptr[i]; k < Lbc.rowptr[i + 1]; ++k)
+        if (Lbc.col[k] == (int)i) Lbc.val[k] += v;
+    };
+    if (outlet_type == kNeumann) {
+      if (reference_node >= 0 && reference_node < (int)nv) add_diag(reference_node, 1e12);
+    } else if (outlet_type == kDirichlet) {
+      for (size_t i = 0; i < nv; ++i)
+        if (p1bc[i] == kOutlet) add_diag(i, 1e12);
+    }
+    return Lbc;
+  }
+
+  // Objectives on the current state. kind 0: mean over wall vertices with
+  // lo <= x[axis] <= hi of |s_v|^2, s = computeShearStress (NavierStokes.cpp:874-944);
+  // kind 1: mean p over inlet vertices minus mean p over outlet vertices. Returns J and the
+  // seeds dJ/du [N2], dJ/dp [nv] and the explicit dJ/dviscosity; -1 if the vertex set is empty.
+  int objective(int kind, int axis, double lo, double hi, double *J, std::vector<V3> &su,
+                std::vector<double> &sp, double *dnu) const {
+    su.assign(N2, V3());
+    sp.assign(nv, 0.0);
+    *dnu = 0.0;
+    if (kind == 0) {
+      std::vector<double> s(3 * nv);
+      shear_stress(s.data());
+      std::vector<char> in(nv, 0);
+      int64_t np = 0;
+      for (size_t v = 0; v < nv; ++v)
+        if (p1bc[v] == kWall && vertices[v][axis] >= lo && vertices[v][axis] <= hi) {
+          in[v] = 1;
+          ++np;
+        }
+      if (np == 0) return -1;
+      const double inv = 1.0 / (double)np;
+      const double acc = tree_sum(order_nv, [&](int v) {
+        return in[v] ? (s[3 * v] * s[3 * v] + s[3 * v + 1] * s[3 * v + 1]) + s[3 * v + 2] * s[3 * v + 2]
+                     : 0.0;
+      });
+      *J = acc * inv;
+      const double c = 2.0 * inv;
+      std::vector<V3> w(nv);
+      for (size_t v = 0; v < nv; ++v)
+        if (in[v]) w[v] = V3(c * s[3 * v], c * s[3 * v + 1], c * s[3 * v + 2]);
+      const double mu = viscosity;
+      for (const auto &f : faces) {
+        if (f.tet_b != -1) continue;
+        const V3 ws = (w[f.v[0]] + w[f.v[1]]) + w[f.v[2]];
+        const V3 W = ws * (f.area * (1.0 / 3.0));
+        const int t = f.tet_a;
+        for (int l = 0; l < 4; ++l) {
+          const V3 &g = grads[t][l];
+          const double ng = f.normal.dot(g), wg = W.dot(g);
+          V3 &o = su[tets[t].v[l]];
+          for (int a = 0; a < 3; ++a) o[a] = o[a] + mu * (W[a] * ng + f.normal[a] * wg);
+        }
+      }
+      *dnu = 2.0 * (*J) / viscosity;
+      return 0;
+    }
+    int64_t nin = 0, nout = 0;
+    for (size_t v = 0; v < nv; ++v) {
+      nin += p1bc[v] == kInlet;
+      nout += p1bc[v] == kOutlet;
+    }
+    if (nin == 0 || nout == 0) return -1;
+    const double ii = 1.0 / (double)nin, io = 1.0 / (double)nout;
+    const double si = tree_sum(order_nv, [&](int v) { return p1bc[v] == kInlet ? p[v] : 0.0; });
+    const double so = tree_sum(order_nv, [&](int v) { return p1bc[v] == kOutlet ? p[v] : 0.0; });
+    *J = si * ii - so * io;
+    for (size_t v = 0; v < nv; ++v) {
+      if (p1bc[v] == kInlet) sp[v] = ii;
+      if (p1bc[v] == kOutlet) sp[v] = -io;
+    }
+    return 0;
+  }
+
+  // Backward half. lu/lp: dJ/du^N, dJ/dp^N on entry, dJ/du^0, dJ/dp^0 on exit. gin: dJ/dg per
+  // node [N2] (zero off inlet nodes); gnu: dJ/dviscosity (dnu_explicit included).
+  int adjoint_backward(std::vector<V3> &lu, std::vector<double> &lp, double dnu_explicit,
+                       std::vector<V3> &gin, double *gnu) {
+    const CSR A = momentum_lhs();
+    const CSR Lbc = poisson_lhs();
+    const CSR GT[3] = {transpose(Gx, nv), transpose(Gy, nv), transpose(Gz, nv)};
+    gin.assign(N2, V3());
+    double gn = dnu_explicit;
+    adj_it_mom = adj_it_p = 0;
+    const bool normalize = reference_node >= 0 && reference_node < (int)nv;
+    const int ncorr = std::max(n_corr, 0);
+    std::vector<double> q[3], lam(N2), x, lpp(nv), chain(nv), rhs(nv), mu_p, t0(nv), t1(nv), t2(nv);
+    std::vector<V3> lus(N2), nu(N2), cadj(N2);
+    for (int a = 0; a < 3; ++a) q[a].assign(nv, 0.0);
+    for (int n = (int)adj_rec.size() - 1; n >= 0; --n) {
+      const AdjRecord &R = adj_rec[n];
+      // correctVelocity + reenforceVelocityBCs (NavierStokes.cpp:702-771, 815-839)
+      for (size_t i = 0; i < N2; ++i) {
+        const int bc = bc_of(i);
+        lus[i] = V3();
+        if (i < nv)
+          for (int a = 0; a < 3; ++a) q[a][i] = 0.0;
+        if (bc == kInlet) {
+          gin[i] = gin[i] + lu[i];
+          continue;
+        }
+        if (bc == kWall) continue;
+        lus[i] = lu[i];
+        if (i < nv && inv_lumped[i] > 1e-14) {
+          const double f = -dt * inv_lumped[i];
+          for (int a = 0; a < 3; ++a) q[a][i] = relax_u * (f * lu[i][a]);
+        }
+      }
+      // p += relax_p p', reinforcePressureBCs, normalizePressire, once per corrector
+      chain = lp;
+      std::fill(lpp.begin(), lpp.end(), 0.0);
+      for (int c = ncorr - 1; c >= 0; --c) {
+        double S = 0.0;
+        if (normalize) S = tree_sum(order_nv, [&](int i) { return chain[i]; });
+        for (size_t i = 0; i < nv; ++i) {
+          double w = chain[i];
+          if (normalize && (int)i == reference_node) w = w - S;
+          if (outlet_type == kDirichlet && p1bc[i] == kOutlet) w = 0.0;
+          lpp[i] = lpp[i] + relax_p * w;
+          chain[i] = w;
+        }
+      }
+      // velocity correction u -= relax_u dt m^-1 G p'
+      spmv(GT[0], q[0].data(), t0.data());
+      spmv(GT[1], q[1].data(), t1.data());
+      spmv(GT[2], q[2].data(), t2.data());
+      for (size_t i = 0; i < nv; ++i) rhs[i] = ((t0[i] + t1[i]) + t2[i]) + lpp[i];
+      // pressure Poisson solve (L symmetric)
+      {
+        SolveInfo si = (pressure_solver == 1)
+                           ? cg(Lbc, rhs, mu_p, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1)
+                           : bicgstab(Lbc, rhs, mu_p, tol_p, maxit_p, order_nv, order_p1, order_nv,
+                                      conv_norm == 1);
+        adj_it_p += si.iters;
+        if (!si.converged) return 1;
+      }
+      // b = -div(u*)/dt = -(1/dt) sum_a G_a u*_a|P1
+      spmv(GT[0], mu_p.data(), t0.data());
+      spmv(GT[1], mu_p.data(), t1.data());
+      spmv(GT[2], mu_p.data(), t2.data());
+      for (size_t i = 0; i < nv; ++i) {
+        lus[i].x = lus[i].x - t0[i] / dt;
+        lus[i].y = lus[i].y - t1[i] / dt;
+        lus[i].z = lus[i].z - t2[i] / dt;
+      }
+      // momentum solves (A symmetric)
+      for (int a = 0; a < 3; ++a) {
+        for (size_t i = 0; i < N2; ++i) lam[i] = lus[i][a];
+        SolveInfo si = bicgstab(A, lam, x, tol_mom, maxit_mom, order_p2, order_p2, order_n2,
+                                conv_norm == 1);
+        adj_it_mom = std::max(adj_it_mom, si.iters);
+        if (!si.converged) return 1;
+        for (size_t i = 0; i < N2; ++i) nu[i][a] = x[i];
+      }
+      // viscosity: dA/dnu = -K/nu  ->  dJ/dnu += sum_a nu_a . K u*_a / nu
+      {
+        std::vector<double> ku[3], na[3], usa(N2);
+        for (int a = 0; a < 3; ++a) {
+          for (size_t i = 0; i < N2; ++i) usa[i] = R.us[i][a];
+          ku[a].resize(N2);
+          spmv(K, usa.data(), ku[a].data());
+        }
+        const double tot = tree_sum(order_p2, [&](int i) {
+          return (nu[i].x * ku[0][i] + nu[i].y * ku[1][i]) + nu[i].z * ku[2][i];
+        });
+        gn += tot / viscosity;
+      }
+      // convection adjoint (computeAdvectionRHS, NavierStokes.cpp:550-580) over u^n
+      std::fill(cadj.begin(), cadj.end(), V3());
+      for (size_t t = 0; t < nt; ++t) {
+        const double vol = tets[t].volume;
+        V3 s1, s2;
+        for (int l = 0; l < 4; ++l) s1 = s1 + nu[tets[t].v[l]];
+        for (int e = 0; e < 6; ++e) s2 = s2 + nu[nv + tet_edges[t][e]];
+        double ch[3];
+        for (int a = 0; a < 3; ++a) ch[a] = -((vol / 4.0) * s1[a] + (vol / 24.0) * s2[a]);
+        V3 ue;
+        for (int l = 0; l < 4; ++l) ue = ue + 0.25 * R.u[tets[t].v[l]];
+        double gu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int j = 0; j < 4; ++j) {
+          const V3 &uj = R.u[tets[t].v[j]];
+          const V3 &gj = grads[t][j];
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) gu[a][b] += uj[a] * gj[b];
+        }
+        double h[3];
+        for (int b = 0; b < 3; ++b) h[b] = 0.25 * ((gu[0][b] * ch[0] + gu[1][b] * ch[1]) + gu[2][b] * ch[2]);
+        for (int l = 0; l < 4; ++l) {
+          const double d = grads[t][l].dot(ue);
+          V3 &o = cadj[tets[t].v[l]];
+          for (int a = 0; a < 3; ++a) o[a] = o[a] + (ch[a] * d + h[a]);
+        }
+      }
+      // momentum right-hand side: M u^n / dt - G p^n + conv(u^n) + penalty g
+      std::vector<double> mv[3], na(N2);
+      for (int a = 0; a < 3; ++a) {
+        for (size_t i = 0; i < N2; ++i) na[i] = nu[i][a];
+        mv[a].resize(N2);
+        spmv(M, na.data(), mv[a].data());
+      }
+      for (int a = 0; a < 3; ++a) {
+        std::vector<double> nP(nv);
+        for (size_t i = 0; i < nv; ++i) nP[i] = nu[i][a];
+        spmv(GT[a], nP.data(), a == 0 ? t0.data() : (a == 1 ? t1.data() : t2.data()));
+      }
+      for (size_t i = 0; i < N2; ++i) {
+        for (int a = 0; a < 3; ++a) {
+          double v = mv[a][i] / dt;
+          if (i < nv) v = v + cadj[i][a];
+          lu[i][a] = v;
+        }
+        if (bc_of(i) == kInlet)
+          for (int a = 0; a < 3; ++a) gin[i][a] = gin[i][a] + 1e10 * nu[i][a];
+      }
+      for (size_t i = 0; i < nv; ++i) lp[i] = chain[i] - ((t0[i] + t1[i]) + t2[i]);
+    }
+    *gnu = gn;
+    return 0;
+  }
 };
 
 const CSR *matrix_of(const Oracle *o, int which) {
@@ -1147,6 +1428,43 @@ void orc_stats(void *h, int *iters, double *res, double *times) {
   times[2] = o->t_mom;
   times[3] = o->t_press;
   times[4] = o->t_corr;
+}
+// ---- discrete adjoint ----
+// Runs nsteps PISO steps from the current state, recording what the backward pass needs.
+int orc_adjoint_forward(void *h, int nsteps) { return static_cast<Oracle *>(h)->adjoint_forward(nsteps); }
+// Objective on the current state (kind 0: wall-shear patch over [lo,hi] along axis; 1: pressure
+// drop inlet-outlet); seeds returned as dJ/du [N2][3], dJ/dp [nv] and explicit dJ/dviscosity.
+int orc_objective(void *h, int kind, int axis, double lo, double hi, double *J, double *su,
+                  double *sp, double *dnu) {
+  Oracle *o = static_cast<Oracle *>(h);
+  std::vector<V3> u_s;
+  std::vector<double> p_s;
+  const int rc = o->objective(kind, axis, lo, hi, J, u_s, p_s, dnu);
+  if (rc) return rc;
+  for (size_t i = 0; i < o->N2; ++i)
+    for (int c = 0; c < 3; ++c) su[3 * i + c] = u_s[i][c];
+  std::copy(p_s.begin(), p_s.end(), sp);
+  return 0;
+}
+// Backward pass from seeds (lu [N2][3], lp [nv] are overwritten by dJ/du^0, dJ/dp^0);
+// gin [N2][3] = dJ/d(inlet values), *gnu = dJ/dviscosity (dnu_explicit included).
+int orc_adjoint_backward(void *h, double *lu, double *lp, double dnu_explicit, double *gin,
+                         double *gnu, int *iters) {
+  Oracle *o = static_cast<Oracle *>(h);
+  std::vector<V3> L(o->N2), G;
+  for (size_t i = 0; i < o->N2; ++i) L[i] = V3(lu[3 * i], lu[3 * i + 1], lu[3 * i + 2]);
+  std::vector<double> P(lp, lp + o->nv);
+  const int rc = o->adjoint_backward(L, P, dnu_explicit, G, gnu);
+  iters[0] = o->adj_it_mom;
+  iters[1] = o->adj_it_p;
+  if (rc) return rc;
+  for (size_t i = 0; i < o->N2; ++i)
+    for (int c = 0; c < 3; ++c) {
+      lu[3 * i + c] = L[i][c];
+      gin[3 * i + c] = G[i][c];
+    }
+  std::copy(P.begin(), P.end(), lp);
+  return 0;
 }
 int orc_set_threads(int n) {
 #ifdef _OPENMP

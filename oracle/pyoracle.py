@@ -58,6 +58,9 @@ def lib() -> C.CDLL:
         "orc_shear_stress": (None, [vp, vp]),
         "orc_stats": (None, [vp, vp, vp, vp]),
         "orc_set_threads": (i32, [i32]),
+        "orc_adjoint_forward": (i32, [vp, i32]),
+        "orc_objective": (i32, [vp, i32, i32, dbl, dbl, vp, vp, vp, vp]),
+        "orc_adjoint_backward": (i32, [vp, vp, vp, dbl, vp, vp, vp]),
     }
     for k, (r, a) in sig.items():
         f = getattr(L, k)
@@ -199,6 +202,33 @@ class Oracle:
         out = np.empty((self.nv, 3))
         self.L.orc_shear_stress(self.h, _p(out))
         return out
+
+    # ---- discrete adjoint
+    def adjoint_forward(self, nsteps: int) -> int:
+        return self.L.orc_adjoint_forward(self.h, int(nsteps))
+
+    def objective(self, kind=0, axis=0, lo=0.0, hi=0.0):
+        """(J, dJ/du [N2,3], dJ/dp [nv], explicit dJ/dviscosity) on the current state."""
+        J = C.c_double()
+        dnu = C.c_double()
+        su = np.zeros((self.N2, 3))
+        sp = np.zeros(self.nv)
+        rc = self.L.orc_objective(self.h, int(kind), int(axis), float(lo), float(hi),
+                                  C.addressof(J), _p(su), _p(sp), C.addressof(dnu))
+        if rc:
+            raise ValueError("objective vertex set is empty")
+        return J.value, su, sp, dnu.value
+
+    def adjoint_backward(self, seed_u, seed_p, dnu_explicit=0.0) -> dict:
+        lu = np.ascontiguousarray(seed_u, np.float64).reshape(self.N2, 3).copy()
+        lp = np.ascontiguousarray(seed_p, np.float64).reshape(self.nv).copy()
+        gin = np.zeros((self.N2, 3))
+        gnu = C.c_double()
+        it = np.zeros(2, np.int32)
+        rc = self.L.orc_adjoint_backward(self.h, _p(lu), _p(lp), float(dnu_explicit), _p(gin),
+                                         C.addressof(gnu), _p(it))
+        return dict(rc=rc, grad_inlet=gin, grad_viscosity=gnu.value, grad_u0=lu, grad_p0=lp,
+                    iters=it.tolist())
 
     def stats(self) -> dict:
         it = np.zeros(4, np.int32)
