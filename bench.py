@@ -38,6 +38,53 @@ MAXIT = (5000, 50000)
 INLET_PEAK = 2 * 0.5
 
 
+ADJ_GEOM = dict(rings=8, layers=217)  # 249,984 tets: the 1M mesh coarsened 2x in the cross-section
+ADJ_STEPS, ADJ_CHECKPOINT, ADJ_SEED, ADJ_NODES = 50, 10, 20261203, 20
+ADJ_TOL = 1e-18  # Jacobi-scaled; see adjoint_section
+ADJ_PATCH = dict(kind=0, axis=0, lo=14.0, hi=16.0)  # wall patch at mid-length of the x-axis tube
+
+
+class MT19937_64:
+    """64-bit Mersenne Twister (Nishimura, ACM TOMACS 10(4), 2000), the generator behind C++
+    std::mt19937_64; used to pick the seeded inlet nodes."""
+
+    def __init__(self, seed: int):
+        self.mt = [0] * 312
+        self.mt[0] = seed & 0xFFFFFFFFFFFFFFFF
+        for i in range(1, 312):
+            self.mt[i] = (6364136223846793005 * (self.mt[i - 1] ^ (self.mt[i - 1] >> 62)) + i) & 0xFFFFFFFFFFFFFFFF
+        self.idx = 312
+
+    def __call__(self) -> int:
+        if self.idx >= 312:
+            for i in range(312):
+                x = (self.mt[i] & 0xFFFFFFFF80000000) | (self.mt[(i + 1) % 312] & 0x7FFFFFFF)
+                xa = x >> 1
+                if x & 1:
+                    xa ^= 0xB5026F5AA96619E9
+                self.mt[i] = self.mt[(i + 156) % 312] ^ xa
+            self.idx = 0
+        y = self.mt[self.idx]
+        self.idx += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        return y
+
+
+def seeded_nodes(candidates, count, seed):
+    """`count` distinct entries of `candidates`: raw mt19937_64(seed) draws modulo the candidate
+    count, repeats skipped."""
+    g = MT19937_64(seed)
+    out = []
+    while len(out) < min(count, len(candidates)):
+        c = int(candidates[g() % len(candidates)])
+        if c not in out:
+            out.append(c)
+    return out
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -48,6 +95,9 @@ def parse():
     ap.add_argument("--layers", type=int, default=GEOM["layers"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint run")
+    ap.add_argument("--adjoint-fd-nodes", type=int, default=ADJ_NODES,
+                    help="seeded inlet nodes checked against central finite differences")
     ap.add_argument("--reference-budget-s", type=float, default=120.0,
                     help="cap on the timed CPU work of --impl reference")
     return ap.parse_args()
@@ -146,6 +196,90 @@ def measured_peak():
 def traffic_table():
     p = ROOT / "profiles" / "dram_traffic.json"
     return json.loads(p.read_text()) if p.exists() else {}
+
+
+def adjoint_section(cf, args, barrier):
+    """Discrete adjoint on the 250k-tet cylinder: 50 FP64 PISO steps from rest, objective
+    J = mean |WSS|^2 over the wall vertices with 14 <= x <= 16, checkpoint every 10 steps with
+    recomputation; gradients with respect to every inlet nodal axial velocity and the viscosity,
+    checked against central finite differences (h = 1e-6; relative h for the viscosity) on seeded
+    inlet nodes. The 1e10 inlet penalty rows dominate ||b|| of the momentum solve even in the
+    Jacobi-scaled norm, so the relative tolerance pins the interior only loosely; the FD
+    quotients need the Krylov solves at 1e-18 (Jacobi-scaled) to get their solver noise below
+    the 1e-5 bar, and the adjoint run uses the same setting."""
+    m = make_mesh(cf, ADJ_GEOM["rings"], ADJ_GEOM["layers"])
+    nv, nt, ne, _, _ = m.sizes
+    prof = cf.parabolic_inlet(m.nodePositions(), INLET_PEAK, GEOM["radius"])
+    s = cf.NavierStokesSolver()
+    s.setKrylovTolerances(ADJ_TOL, ADJ_TOL)
+    s.setConvergenceNorm(cf.NORM_JACOBI)
+    s.setMaxIterations(50000, 200000)
+    s.setPressureSolver(cf.KRYLOV_CG)
+    s.setDt(DT)
+    s.initialize(m, cf.Fluid(*FLUID))
+    s.setInletVelocityProfile(prof)
+    u0, p0 = s.getVelocity().copy(), s.getPressure().copy()
+    barrier()
+    ok = s.adjointForward(ADJ_STEPS, ADJ_CHECKPOINT)
+    g = s.adjointBackward(**ADJ_PATCH) if ok else None
+    barrier()
+    if g is None:
+        return {"ok": False, "error": "forward pass failed"}
+    st = s.adjointStats()
+    p1, p2 = m.fluidBC()
+    inlet = np.nonzero(np.concatenate([p1, p2]) == 1)[0]
+    res = {
+        "workload": f"config 3: cylinder L=30 R=2, {nt} tets ({ADJ_GEOM['rings']} rings x "
+                    f"{ADJ_GEOM['layers']} layers), N2={nv + ne}; {ADJ_STEPS} FP64 PISO steps from rest, "
+                    f"parabolic inlet peak 1.0, J = mean |WSS|^2 over wall vertices with 14<=x<=16, "
+                    f"checkpoint every {ADJ_CHECKPOINT} steps; Krylov tol {ADJ_TOL:g} (Jacobi-scaled)",
+        "J": g["J"], "grad_viscosity": g["grad_viscosity"], "inlet_nodes": int(len(inlet)),
+        "forward_ms": st["forward_ms"], "backward_ms": st["backward_ms"],
+        "recomputed_steps": st["recomputed_steps"], "checkpoints": st["checkpoints"],
+        "record_mb": st["record_bytes"] / 2**20,
+        "adjoint_krylov_iters": [st["momentum_iters"], st["pressure_iters"]],
+        "gpu_launches_backward": st["kernel_launches"],
+        "steps_per_s_forward_plus_backward": ADJ_STEPS / ((st["forward_ms"] + st["backward_ms"]) / 1e3),
+        "backward_over_forward": st["backward_ms"] / st["forward_ms"],
+    }
+    nodes = seeded_nodes(inlet, args.adjoint_fd_nodes, ADJ_SEED)
+    if nodes:
+        h = 1e-6
+
+        def J_of(pr, nu=FLUID[1]):
+            s.setViscosity(nu)
+            s.setInletVelocityProfile(pr)
+            s.setFields(u0, p0)
+            ok_, done = s.pisoSteps(ADJ_STEPS)
+            if not ok_:
+                raise SystemExit(f"FD forward run failed after {done} steps")
+            return s.objective(**ADJ_PATCH)
+
+        t0 = time.perf_counter()
+        adj, fd = [], []
+        for i in nodes:
+            pp, pm = prof.copy(), prof.copy()
+            pp[i, 0] += h
+            pm[i, 0] -= h
+            fd.append((J_of(pp) - J_of(pm)) / (2 * h))
+            adj.append(float(g["grad_inlet"][i, 0]))
+        hn = h * FLUID[1]
+        fdn = (J_of(prof, FLUID[1] + hn) - J_of(prof, FLUID[1] - hn)) / (2 * hn)
+        adj_a, fd_a = np.array(adj), np.array(fd)
+        big = np.abs(fd_a) >= 1e-3 * np.abs(fd_a).max()
+        res["fd_check"] = {
+            "nodes": nodes, "p1_nodes": int(sum(1 for i in nodes if i < nv)), "h": h,
+            "seed": f"std::mt19937_64({ADJ_SEED}) draws modulo the inlet-node count",
+            "rel_err_vector": float(np.linalg.norm(adj_a - fd_a) / np.linalg.norm(fd_a)),
+            "rel_err_max_significant": float(np.max(np.abs(adj_a[big] - fd_a[big]) / np.abs(fd_a[big]))),
+            "rel_err_viscosity": abs(g["grad_viscosity"] - fdn) / abs(fdn),
+            "adjoint": adj, "fd": fd, "fd_viscosity": fdn, "fd_seconds": time.perf_counter() - t0,
+        }
+        res["ok"] = bool(res["fd_check"]["rel_err_vector"] <= 1e-5 and res["fd_check"]["rel_err_viscosity"] <= 1e-5)
+    else:
+        res["ok"] = True
+    del s
+    return res
 
 
 def cpu_baseline(xyz, tets, profile, n_threads):
@@ -350,6 +484,10 @@ def main():
                         "correction (true FP64 residual) vs FP64 BiCGSTAB; pressure FP64 CG in both",
         }
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_section(cf, args, barrier)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(m.vertices(), m.tets(), profile, os.cpu_count() or 1)
@@ -369,7 +507,7 @@ def main():
             "roofline": roofline, "kernels": kernels,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(profile.nbytes),
                     "d2h_bytes_per_step": int(u.nbytes + p.nbytes)},
-            "cpu_baseline": cpu, "clocks": clk, "mixed": mixed,
+            "cpu_baseline": cpu, "clocks": clk, "mixed": mixed, "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

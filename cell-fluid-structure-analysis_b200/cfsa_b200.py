@@ -147,6 +147,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "cfsa_mesh_from_arrays": (i32, [i64, vp, i64, vp, pp]),
         "cfsa_mesh_structured_prism": (i32, [dbl, dbl, dbl, i32, i32, i32, pp]),
         "cfsa_mesh_cylinder": (i32, [dbl, dbl, i32, i32, pp]),
+        "cfsa_mesh_y_bifurcation": (i32, [vp, pp]),
         "cfsa_mesh_setup_boundary_conditions": (i32, [vp, vp, dbl]),
         "cfsa_mesh_set_fluid_bc": (i32, [vp, vp, vp]),
         "cfsa_mesh_write_msh": (i32, [vp, C.c_char_p]),
@@ -257,6 +258,15 @@ class Mesh:
     @classmethod
     def cylinder(cls, length: float, radius: float, rings: int, layers: int) -> "Mesh":
         return cls._make("cfsa_mesh_cylinder", float(length), float(radius), int(rings), int(layers))
+
+    @classmethod
+    def yBifurcation(cls, parent_radius=2.0, parent_length=15.0, daughter_radius=1.5,
+                     daughter_length=12.0, angle_deg=35.0, blend=0.5, cell=0.0813) -> "Mesh":
+        """Y-bifurcation meshed on a Kuhn lattice of edge `cell`, tagged by the generator
+        (inlet at x = 0, both daughter caps outlet, wall elsewhere)."""
+        spec = np.array([parent_radius, parent_length, daughter_radius, daughter_length, angle_deg,
+                         blend, cell], np.float64)
+        return cls._make("cfsa_mesh_y_bifurcation", _ptr(spec))
 
     @classmethod
     def fromMshFile(cls, path) -> "Mesh":

@@ -281,6 +281,218 @@ void Mesh::generateCylinder(double length, double radius, int rings, int layers)
   finalizeFromArrays(true);
 }
 
+namespace {
+
+struct YGeom {
+  Vec3 a[3], b[3], d[3];
+  double r[3];
+  double k;
+  // signed distance to the capsule union (smooth, quadratic polynomial min), cut by the inlet
+  // plane x = 0 and the two daughter end planes
+  double sdf(const Vec3 &p) const {
+    double f = 0.0;
+    for (int s = 0; s < 3; ++s) {
+      const Vec3 ab = b[s] - a[s];
+      double t = (p - a[s]).dot(ab) / ab.dot(ab);
+      t = std::min(1.0, std::max(0.0, t));
+      const double di = (p - (a[s] + ab * t)).norm() - r[s];
+      if (s == 0) {
+        f = di;
+      } else {
+        const double h = std::max(k - std::fabs(f - di), 0.0) / k;
+        f = std::min(f, di) - h * h * k * 0.25;
+      }
+    }
+    f = std::max(f, -p.x());
+    for (int s = 1; s < 3; ++s) f = std::max(f, (p - b[s]).dot(d[s]));
+    return f;
+  }
+  Vec3 grad(const Vec3 &p, double h) const {
+    Vec3 g;
+    for (int c = 0; c < 3; ++c) {
+      Vec3 e(0, 0, 0);
+      e[c] = h;
+      g[c] = (sdf(p + e) - sdf(p - e)) / (2.0 * h);
+    }
+    return g;
+  }
+};
+
+double signed_volume(const Vec3 &a, const Vec3 &b, const Vec3 &c, const Vec3 &d) {
+  return (b - a).cross(c - a).dot(d - a) / 6.0;
+}
+
+}  // namespace
+
+void Mesh::generateYBifurcation(const YBifurcation &sp) {
+  if (!(sp.cell > 0.0) || !(sp.parent_radius > 0.0) || !(sp.daughter_radius > 0.0) ||
+      !(sp.parent_length > 0.0) || !(sp.daughter_length > 0.0) || !(sp.blend > 0.0))
+    throw std::invalid_argument("yBifurcation: positive sizes required");
+  YGeom G;
+  const double ang = sp.angle_deg * M_PI / 180.0;
+  G.a[0] = Vec3(0, 0, 0);
+  G.b[0] = Vec3(sp.parent_length, 0, 0);
+  G.r[0] = sp.parent_radius;
+  for (int s = 1; s < 3; ++s) {
+    const double sg = (s == 1) ? 1.0 : -1.0;
+    G.d[s] = Vec3(std::cos(ang), sg * std::sin(ang), 0.0);
+    G.a[s] = G.b[0];
+    G.b[s] = G.a[s] + G.d[s] * sp.daughter_length;
+    G.r[s] = sp.daughter_radius;
+  }
+  G.k = sp.blend;
+  const double a = sp.cell;
+  // lattice: x from 0 (the inlet plane is a lattice plane), y and z symmetric about 0
+  double xmax = sp.parent_length + sp.parent_radius, ymax = sp.parent_radius;
+  for (int s = 1; s < 3; ++s) {
+    xmax = std::max(xmax, G.b[s].x() + sp.daughter_radius);
+    ymax = std::max(ymax, std::fabs(G.b[s].y()) + sp.daughter_radius);
+  }
+  const double zmax = std::max(sp.parent_radius, sp.daughter_radius) + sp.blend;
+  const int nx = (int)std::ceil(xmax / a) + 1;
+  const int ny = 2 * ((int)std::ceil(ymax / a) + 1), nz = 2 * ((int)std::ceil(zmax / a) + 1);
+  const double y0 = -0.5 * ny * a, z0 = -0.5 * nz * a;
+  if ((double)nx * ny * nz > 2.0e9) throw std::invalid_argument("yBifurcation: lattice too large");
+  auto node_id = [&](int i, int j, int k) -> int64_t { return ((int64_t)k * (ny + 1) + j) * (nx + 1) + i; };
+  auto node_pos = [&](int i, int j, int k) { return Vec3(i * a, y0 + j * a, z0 + k * a); };
+  // Kuhn subdivision: the 6 monotone lattice paths from corner 000 to 111
+  static const int paths[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  std::vector<int64_t> used_nodes;
+  std::vector<std::array<int64_t, 4>> ltets;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const Vec3 cc = node_pos(i, j, k) + Vec3(0.5 * a, 0.5 * a, 0.5 * a);
+        if (G.sdf(cc) > 1.0 * a) continue;  // no tet of this cube can be inside
+        for (const auto &pth : paths) {
+          int c[3] = {0, 0, 0};
+          std::array<int64_t, 4> t;
+          Vec3 cen(0, 0, 0);
+          t[0] = node_id(i, j, k);
+          cen = cen + node_pos(i, j, k);
+          for (int q = 0; q < 3; ++q) {
+            c[pth[q]] = 1;
+            t[q + 1] = node_id(i + c[0], j + c[1], k + c[2]);
+            cen = cen + node_pos(i + c[0], j + c[1], k + c[2]);
+          }
+          if (G.sdf(cen * 0.25) < 0.0) ltets.push_back(t);
+        }
+      }
+  if (ltets.empty()) throw std::invalid_argument("yBifurcation: empty mesh");
+  // compact numbering in lattice order
+  for (const auto &t : ltets)
+    for (int q = 0; q < 4; ++q) used_nodes.push_back(t[q]);
+  std::sort(used_nodes.begin(), used_nodes.end());
+  used_nodes.erase(std::unique(used_nodes.begin(), used_nodes.end()), used_nodes.end());
+  std::vector<Vec3> verts(used_nodes.size());
+  for (size_t v = 0; v < used_nodes.size(); ++v) {
+    const int64_t id = used_nodes[v];
+    const int i = (int)(id % (nx + 1)), j = (int)((id / (nx + 1)) % (ny + 1)), k = (int)(id / ((int64_t)(nx + 1) * (ny + 1)));
+    verts[v] = node_pos(i, j, k);
+  }
+  std::vector<std::array<int, 4>> tets(ltets.size());
+  for (size_t t = 0; t < ltets.size(); ++t) {
+    for (int q = 0; q < 4; ++q)
+      tets[t][q] = (int)(std::lower_bound(used_nodes.begin(), used_nodes.end(), ltets[t][q]) - used_nodes.begin());
+    if (signed_volume(verts[tets[t][0]], verts[tets[t][1]], verts[tets[t][2]], verts[tets[t][3]]) < 0.0)
+      std::swap(tets[t][2], tets[t][3]);
+  }
+  ltets.clear();
+  // classify the lattice boundary faces: inlet (on x = 0), outlet s (outward normal along the
+  // daughter axis, within 1.5 cells of its end plane), wall (the rest)
+  Mesh lat;
+  lat.generateFromArrays(verts, tets);
+  const size_t nv = verts.size();
+  std::vector<unsigned char> is_wall(nv, 0), is_in(nv, 0), out_of(nv, 0);
+  std::vector<int> face_kind(lat.faces_.size(), -1);  // 0 wall, 1 inlet, 2/3 outlet
+  for (size_t fi = 0; fi < lat.faces_.size(); ++fi) {
+    const Face &f = lat.faces_[fi];
+    if (f.tet_b != -1) continue;
+    const auto &fv = f.vertids;
+    Vec3 n = f.normal;
+    const Vec3 tc = lat.tets_[f.tet_a].centroid;
+    if (n.dot(f.center - tc) < 0.0) n = -n;
+    int kind = 0;
+    if (verts[fv[0]].x() == 0.0 && verts[fv[1]].x() == 0.0 && verts[fv[2]].x() == 0.0) {
+      kind = 1;
+    } else {
+      for (int s = 1; s < 3; ++s) {
+        bool near = n.dot(G.d[s]) > 0.3;
+        for (int q = 0; q < 3 && near; ++q) near = (verts[fv[q]] - G.b[s]).dot(G.d[s]) > -1.5 * a;
+        if (near) kind = 1 + s;
+      }
+    }
+    face_kind[fi] = kind;
+    for (int q = 0; q < 3; ++q) {
+      if (kind == 0) is_wall[fv[q]] = 1;
+      if (kind == 1) is_in[fv[q]] = 1;
+      if (kind >= 2) out_of[fv[q]] = (unsigned char)kind;
+    }
+  }
+  // vertex -> tets
+  std::vector<int> vt_ptr(nv + 1, 0), vt(tets.size() * 4);
+  for (const auto &t : tets)
+    for (int q = 0; q < 4; ++q) vt_ptr[t[q] + 1]++;
+  for (size_t v = 0; v < nv; ++v) vt_ptr[v + 1] += vt_ptr[v];
+  {
+    std::vector<int> fill(vt_ptr.begin(), vt_ptr.end() - 1);
+    for (size_t t = 0; t < tets.size(); ++t)
+      for (int q = 0; q < 4; ++q) vt[fill[tets[t][q]]++] = (int)t;
+  }
+  const double vmin = 0.1 * a * a * a / 6.0;
+  auto try_move = [&](size_t v, const Vec3 &target, double max_step) {
+    const Vec3 orig = verts[v];
+    Vec3 step = target - orig;
+    if (step.norm() > max_step) step = step * (max_step / step.norm());
+    for (int attempt = 0; attempt < 4; ++attempt) {
+      verts[v] = orig + step;
+      bool ok = true;
+      for (int q = vt_ptr[v]; q < vt_ptr[v + 1] && ok; ++q) {
+        const auto &t = tets[vt[q]];
+        ok = signed_volume(verts[t[0]], verts[t[1]], verts[t[2]], verts[t[3]]) > vmin;
+      }
+      if (ok) return;
+      step = step * 0.5;
+    }
+    verts[v] = orig;
+  };
+  for (size_t v = 0; v < nv; ++v) {
+    if (!is_wall[v]) continue;
+    Vec3 p = verts[v];
+    for (int it = 0; it < 3; ++it) {
+      const Vec3 g = G.grad(p, 1e-4 * a);
+      const double g2 = g.dot(g);
+      if (g2 < 1e-12) break;
+      p = p - g * (G.sdf(p) / g2);
+    }
+    if (is_in[v]) p[0] = 0.0;  // inlet rim vertices stay on the inlet plane
+    try_move(v, p, 0.5 * a);
+  }
+  for (size_t v = 0; v < nv; ++v) {
+    if (!out_of[v]) continue;
+    const int s = out_of[v] - 1;
+    const Vec3 p = verts[v] - G.d[s] * (verts[v] - G.b[s]).dot(G.d[s]);
+    try_move(v, p, 1.6 * a);
+  }
+  generateFromArrays(verts, tets);
+  // tags: boundary faces in their sorted order tag their vertices Wall, inlet/outlet faces then
+  // overwrite with Inlet/Outlet (the write order of setupBoundaryConditions)
+  for (size_t v = 0; v < vertices_.size(); ++v) setFluidVertexBC(v, FluidBCType::Internal);
+  for (size_t fi = 0; fi < faces_.size(); ++fi) {
+    const Face &f = faces_[fi];
+    if (f.tet_b != -1) continue;
+    const auto &fv = f.vertids;
+    for (const int vi : fv) setFluidVertexBC(vi, FluidBCType::Wall);
+    if (is_in[fv[0]] && is_in[fv[1]] && is_in[fv[2]] && vertices_[fv[0]].x() == 0.0 &&
+        vertices_[fv[1]].x() == 0.0 && vertices_[fv[2]].x() == 0.0) {
+      for (const int vi : fv) setFluidVertexBC(vi, FluidBCType::Inlet);
+    } else if (out_of[fv[0]] && out_of[fv[0]] == out_of[fv[1]] && out_of[fv[0]] == out_of[fv[2]]) {
+      for (const int vi : fv) setFluidVertexBC(vi, FluidBCType::Outlet);
+    }
+  }
+  setP2BoundariesFromP1Boundaries();
+}
+
 void Mesh::writeMshFile(const std::string &filename) const {
   FILE *f = std::fopen(filename.c_str(), "w");
   if (!f) throw std::runtime_error("[Mesh] Could not write msh file: " + filename);

@@ -35,6 +35,21 @@ struct Tet {
   Vec3 centroid = Vec3(0, 0, 0);
 };
 
+// Y-bifurcation: a parent tube of radius parent_radius along +x from x = 0 to parent_length
+// splits into two daughter tubes (radius daughter_radius, length daughter_length) at angles
+// +-angle_deg in the x-y plane, joined by a smooth union of blend radius `blend`. Meshed on a
+// Kuhn-subdivided cubic lattice of edge `cell` (6 tets per cube, conforming), tets kept where
+// the signed distance at their centroid is negative, wall vertices moved onto the surface and
+// outlet vertices onto the cut planes when no tet around them degenerates. Tags: inlet on the
+// x = 0 cap, outlet on both daughter caps, wall elsewhere (tilted outlets cannot be tagged by the
+// axis-extreme rule of setupBoundaryConditions).
+struct YBifurcation {
+  double parent_radius = 2.0, parent_length = 15.0;
+  double daughter_radius = 1.5, daughter_length = 12.0, angle_deg = 35.0;
+  double blend = 0.5;
+  double cell = 0.0813;  // lattice edge; about 4M tets at the defaults
+};
+
 struct Face {
   bool is_ecm = false;
   int tet_a = -1;
@@ -83,6 +98,8 @@ class Mesh {
   // cross-section has `rings` concentric rings (ring k has 6k points) and the axis is cut
   // into `layers` prism layers; each prism is split into 3 tets conformingly.
   void generateCylinder(double length, double radius, int rings, int layers);
+  // Procedural Y-bifurcation with generator-assigned fluid tags (see YBifurcation).
+  void generateYBifurcation(const struct YBifurcation &spec);
   void computeGeometry();
 
   static Mesh fromMshFile(const std::string &filename) {
@@ -105,6 +122,11 @@ class Mesh {
   static Mesh cylinder(double length, double radius, int rings, int layers) {
     Mesh m;
     m.generateCylinder(length, radius, rings, layers);
+    return m;
+  }
+  static Mesh yBifurcation(const YBifurcation &spec) {
+    Mesh m;
+    m.generateYBifurcation(spec);
     return m;
   }
   static void setupBoundaryConditions(const Vec3 &inlet_to_outlet_direction,

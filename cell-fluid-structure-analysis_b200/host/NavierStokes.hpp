@@ -145,6 +145,9 @@ class NavierStokesSolver {
   bool pisoSteps(int n, int *n_done = nullptr);  // n steps, one host synchronisation
   cfsa_ns_stats getStats() const;
   cfsa_ns *handle() const { return h_; }
+  // Host mirrors are re-read on the next getter call (for callers that change the device
+  // fields through the C ABI directly, such as the adjoint forward/backward pair).
+  void invalidateMirrors() const { mirrors_stale_ = true; }
 };
 
 // include/FEM/NavierStokes.hpp:201-251

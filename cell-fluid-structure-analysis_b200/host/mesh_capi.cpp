@@ -100,6 +100,29 @@ int cfsa_mesh_cylinder(double length, double radius, int rings, int layers, cfsa
   });
 }
 
+int cfsa_mesh_y_bifurcation(const double spec[7], cfsa_mesh **out) {
+  if (!out || !spec) return fail(CFSA_BAD_ARG, "null argument");
+  return guarded([&] {
+    YBifurcation y;
+    y.parent_radius = spec[0];
+    y.parent_length = spec[1];
+    y.daughter_radius = spec[2];
+    y.daughter_length = spec[3];
+    y.angle_deg = spec[4];
+    y.blend = spec[5];
+    y.cell = spec[6];
+    auto *m = new cfsa_mesh();
+    try {
+      m->mesh.generateYBifurcation(y);
+    } catch (...) {
+      delete m;
+      throw;
+    }
+    *out = m;
+    return CFSA_OK;
+  });
+}
+
 int cfsa_mesh_setup_boundary_conditions(cfsa_mesh *m, const double dir[3], double coverage) {
   if (!m || !dir) return fail(CFSA_BAD_ARG, "null argument");
   return guarded([&] {

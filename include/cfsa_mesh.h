@@ -35,6 +35,12 @@ int cfsa_mesh_structured_prism(double length, double width, double height, int n
  * Mesh::fromPolyhedron(Polyhedron::cylendar(...)) (src/Mesh/Mesh.cpp:227-323), whose TetGen
  * dependency is not available; see Mesh::generateCylinder for the construction. */
 int cfsa_mesh_cylinder(double length, double radius, int rings, int layers, cfsa_mesh **out);
+/* Procedural Y-bifurcation with generator-assigned fluid tags (inlet cap at x = 0, both daughter
+ * caps outlet, wall elsewhere; P2 tags derived as in Mesh.hpp:198-215). spec[7] = parent radius,
+ * parent length, daughter radius, daughter length, daughter angle (degrees, +-, x-y plane),
+ * blend radius of the smooth junction, lattice cell edge. Replaces the TetGen meshing of a
+ * bifurcation surface for synthetic inputs. */
+int cfsa_mesh_y_bifurcation(const double spec[7], cfsa_mesh **out);
 
 /* Mesh::setupBoundaryConditions (src/Mesh/Mesh.cpp:325-417), which ends with
  * setP2BoundariesFromP1Boundaries (include/Mesh/Mesh.hpp:198-215). dir[3] = inlet->outlet. */

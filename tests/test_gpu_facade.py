@@ -45,3 +45,33 @@ def test_cpp_example_matches_oracle(cf, po, tmp_path):
     st = o.state()
     assert np.array_equal(u, st["u"])
     assert np.array_equal(p, st["p"])
+
+
+def test_cpp_adjoint_pair_matches_python_api(cf, tmp_path):
+    """examples/ns_adjoint.cpp (NavierStokesAdjoint forward/backward through the C++ facade)
+    against the same run through the Python binding: identical bits."""
+    exe = PKG / "examples" / "ns_adjoint"
+    assert exe.exists(), "build the package (make) first"
+    out = tmp_path / "grad.bin"
+    r = subprocess.run([str(exe), "3", "12", "5", "2", str(out)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "recomputed steps 4" in r.stdout, r.stdout
+    raw = open(out, "rb").read()
+    n2 = int(np.frombuffer(raw[:8], np.int64)[0])
+    J, gnu = np.frombuffer(raw[8:24], np.float64)
+    gin = np.frombuffer(raw[24:], np.float64).reshape(n2, 3)
+
+    m = cf.Mesh.cylinder(30.0, 2.0, 3, 12)
+    m.setupBoundaryConditions((1.0, 0.0, 0.0), 1.0)
+    s = cf.NavierStokesSolver()
+    s.setKrylovTolerances(1e-13, 1e-13)
+    s.setMaxIterations(20000, 50000)
+    s.setConvergenceNorm(cf.NORM_JACOBI)
+    s.setDt(0.01)
+    s.initialize(m, cf.Fluid(1060.0, 0.004))
+    s.setInletVelocityProfile(cf.parabolic_inlet(m.nodePositions(), 1.0, 2.0))
+    assert s.adjointForward(5, 2)
+    g = s.adjointBackward(kind=cf.OBJECTIVE_WALL_SHEAR, axis=0, lo=14.0, hi=16.0)
+    assert J == g["J"]
+    assert gnu == g["grad_viscosity"]
+    assert np.array_equal(gin, g["grad_inlet"])

@@ -113,3 +113,29 @@ def test_errors_are_reported(cf, tmp_path):
     bad.write_text("$Nodes\n1 1 1 1\n3 1 0 1\n1\n0 0 0\n$EndNodes\n$Elements\n1 1 1 1\n3 1 4 1\n1 1 2 3 4\n$EndElements\n")
     with pytest.raises(cf.CfsaError):
         cf.Mesh.fromMshFile(bad)
+
+
+def test_y_bifurcation_mesher(cf):
+    """Procedural Y-bifurcation: positive tets, inlet tags on the x = 0 cap only, outlet tags at
+    both daughter ends, wall elsewhere, P2 tags derived from P1 (Mesh.hpp:198-215 rule)."""
+    import numpy as np
+
+    m = cf.Mesh.yBifurcation(cell=0.3)
+    nv, nt, ne, nf, nb = m.sizes
+    assert nt > 50000 and nb > 0
+    vol, _ = m.tetGeometry()
+    assert vol.min() > 0.0
+    x = m.vertices()
+    p1, p2 = m.fluidBC()
+    assert set(np.unique(p1)) == {0, 1, 2, 3}
+    assert np.all(x[p1 == 1, 0] == 0.0)
+    ang = np.deg2rad(35.0)
+    for sg in (1.0, -1.0):
+        end = np.array([15.0 + 12.0 * np.cos(ang), sg * 12.0 * np.sin(ang), 0.0])
+        d = np.array([np.cos(ang), sg * np.sin(ang), 0.0])
+        o = x[(p1 == 2) & (sg * x[:, 1] > 0)]
+        assert len(o) > 20
+        assert np.all(np.abs((o - end) @ d) <= 1.5 * 0.3 + 1e-12)
+    # P2 rule: an edge node gets its endpoints' tag when both share the same non-internal tag
+    edges_ok = np.isin(p2, [0, 1, 2, 3])
+    assert edges_ok.all() and (p2 == 1).sum() > 0 and (p2 == 2).sum() > 0
