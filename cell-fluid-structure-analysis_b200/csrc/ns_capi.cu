@@ -29,6 +29,7 @@ struct Sell {
   int *sptr = nullptr, *col = nullptr, *len = nullptr, *perm = nullptr, *posmap = nullptr;
   int nrows = 0, nrows_pad = 0, nslices = 0;
   int64_t nentries = 0;
+  std::vector<int> h_sptr;  // host copy of sptr
   SellView view() const { return SellView{sptr, col, len, perm, nrows_pad}; }
 };
 
@@ -114,6 +115,10 @@ struct cfsa_ns {
   // persistent CG
   bool cg_persistent = true;
   int cg_grid = 0;
+  // SMEM-resident variant of the persistent CG (k_cg_resident): one 1024-thread CTA per SM
+  bool cg_resident = false;
+  int cg_res_grid = 0, cg_res_bpc_sell = 0, cg_res_bpc_nat = 0, cg_res_col_cap = 0;
+  size_t cg_res_smem = 0;
   unsigned int *bar_count = nullptr, *bar_gen = nullptr;
   int *bar_err = nullptr;
   double *cg_part_a = nullptr, *cg_part_b = nullptr;
@@ -219,6 +224,7 @@ struct cfsa_ns {
       sptr[s + 1] = sptr[s] + w * kSellC;
     }
     S.nentries = sptr[S.nslices];
+    S.h_sptr = sptr;
     S.perm = dupload(perm);
     S.len = dupload(len);
     S.sptr = dupload(sptr);
@@ -460,8 +466,40 @@ struct cfsa_ns {
       cg_part_a = dalloc<double>((size_t)nblk_sell * kMaxRed);
       cg_part_b = dalloc<double>((size_t)nblk_nat * kMaxRed);
       if (cg_grid < 1) cg_persistent = false;
+      // resident variant: blocks split into contiguous runs, one run per SM
+      int optin = 0;
+      CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+      const int grid = std::max(1, std::min(nsm, std::max(nblk_sell, nblk_nat)));
+      const int bpc_s = (nblk_sell + grid - 1) / grid, bpc_n = (nblk_nat + grid - 1) / grid;
+      int max_entries = 0;
+      for (int c = 0; c < grid; ++c) {
+        const int b0 = std::min(nblk_sell, c * bpc_s), b1 = std::min(nblk_sell, b0 + bpc_s);
+        if (b1 > b0)
+          max_entries = std::max(max_entries, s1.h_sptr[std::min(8 * b1, s1.nslices)] - s1.h_sptr[8 * b0]);
+      }
+      const int64_t row_bytes = (int64_t)3 * bpc_s * kBlock * (int64_t)sizeof(int);
+      const int64_t avail = (int64_t)optin - 2048 - row_bytes;  // 2 KiB for static shared memory
+      if (avail > 0) {
+        cg_res_col_cap = (int)std::min<int64_t>(max_entries, avail / (int64_t)sizeof(int));
+        cg_res_smem = (size_t)(row_bytes + (int64_t)cg_res_col_cap * (int64_t)sizeof(int));
+        int per_sm_res = 0;
+        if (cudaFuncSetAttribute(k_cg_resident, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cg_res_smem) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_res, k_cg_resident, kCgResThreads,
+                                                          cg_res_smem) == cudaSuccess &&
+            per_sm_res >= 1) {
+          cg_resident = true;
+          cg_res_grid = grid;
+          cg_res_bpc_sell = bpc_s;
+          cg_res_bpc_nat = bpc_n;
+        }
+        cudaGetLastError();
+      }
     }
     if (const char *e = std::getenv("CFSA_CG_LOOP")) cg_persistent = cg_persistent && (std::atoi(e) == 0);
+    // CFSA_CG_KERNEL=persistent selects the 256-thread persistent kernel over the resident one
+    if (const char *e = std::getenv("CFSA_CG_KERNEL"))
+      if (std::string(e) == "persistent") cg_resident = false;
     assemble();
     if (const char *e = std::getenv("CFSA_NO_GRAPH")) use_graph = (std::atoi(e) == 0);
     CK(cudaStreamSynchronize(stream));
@@ -844,7 +882,20 @@ struct cfsa_ns {
       attr[0].val.cooperative = 1;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
-      CK(cudaLaunchKernelEx(&cfg, k_cg_persistent, c));
+      if (cg_resident) {
+        CgResidentArgs rz{};
+        rz.P = c;
+        rz.nslices = s1.nslices;
+        rz.bpc_sell = cg_res_bpc_sell;
+        rz.bpc_nat = cg_res_bpc_nat;
+        rz.col_cap = cg_res_col_cap;
+        cfg.gridDim = dim3((unsigned int)cg_res_grid);
+        cfg.blockDim = dim3(kCgResThreads);
+        cfg.dynamicSmemBytes = cg_res_smem;
+        CK(cudaLaunchKernelEx(&cfg, k_cg_resident, rz));
+      } else {
+        CK(cudaLaunchKernelEx(&cfg, k_cg_persistent, c));
+      }
       k_check_cg<<<1, 1, 0, stream>>>(cs, s_out, bar_err);
     } else {
       CgArgs c{};

@@ -1298,6 +1298,223 @@ __global__ void __launch_bounds__(kBlock, 5) k_cg_persistent(CgPersistentArgs A)
 }
 
 // ------------------------------------------------------------------------------------------
+// SMEM-resident persistent CG: one CTA of 1024 threads per SM for the whole solve. Each CTA owns
+// a contiguous run of 256-position blocks (SELL blocks for the product, natural blocks for the
+// vector updates) and keeps, in shared memory for the whole solve, the row id, length and entry
+// base of each of its SELL positions and the column indices of as many of its slices as fit
+// (the rest are read from global memory). Inside an iteration the column indices then cost a
+// shared-memory read instead of an L2 round trip before the gathers can be issued. The
+// arithmetic, the per-block partial sums and the 256-accumulator tree are those of
+// k_cg_persistent, so both kernels produce the same bits.
+constexpr int kCgResThreads = 1024;
+constexpr int kCgResGroups = kCgResThreads / kBlock;  // 256-thread groups per CTA
+
+struct CgResidentArgs {
+  CgPersistentArgs P;
+  int nslices;
+  int bpc_sell, bpc_nat;  // blocks per CTA
+  int col_cap;            // column indices that fit in shared memory per CTA
+};
+
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kBlock) : "memory");
+}
+
+// block_partial for one 256-thread group of a larger CTA (named barrier 1 + g).
+template <int NV>
+__device__ __forceinline__ void group_partial(double (&v)[NV], double *__restrict__ partials, int b,
+                                              int g, double (*sm)[2][kBlock / 32]) {
+  const int lt = threadIdx.x & (kBlock - 1), warp = lt >> 5, lane = lt & 31;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    const double w = warp_sum(v[j]);
+    if (lane == 0) sm[g][j][warp] = w;
+  }
+  group_sync(g);
+  if (lt == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double s = 0.0;
+      for (int w = 0; w < kBlock / 32; ++w) s += sm[g][j][w];
+      partials[(size_t)b * kMaxRed + j] = s;
+    }
+  }
+  group_sync(g);
+}
+
+// tree_total for a 1024-thread CTA: the first 256 threads form the 256 accumulators.
+template <int NV>
+__device__ __forceinline__ void tree_total_cta(const double *__restrict__ partials, int nblk,
+                                               double (&out)[NV], double (*sm)[kBlock / 32]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x < kBlock) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double s = 0.0;
+      int b = threadIdx.x;
+      for (; b + 3 * kBlock < nblk; b += 4 * kBlock) {
+        const double v0 = __ldcg(&partials[(size_t)b * kMaxRed + j]);
+        const double v1 = __ldcg(&partials[(size_t)(b + kBlock) * kMaxRed + j]);
+        const double v2 = __ldcg(&partials[(size_t)(b + 2 * kBlock) * kMaxRed + j]);
+        const double v3 = __ldcg(&partials[(size_t)(b + 3 * kBlock) * kMaxRed + j]);
+        s += v0;
+        s += v1;
+        s += v2;
+        s += v3;
+      }
+      for (; b < nblk; b += kBlock) s += __ldcg(&partials[(size_t)b * kMaxRed + j]);
+      s = warp_sum(s);
+      if (lane == 0) sm[j][warp] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double s = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) s += sm[j][w];
+    out[j] = s;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kCgResThreads, 1) k_cg_resident(CgResidentArgs R) {
+  extern __shared__ int s_dyn[];
+  __shared__ double s_grp[kCgResGroups][2][kBlock / 32];
+  __shared__ double s_tree[2][kBlock / 32];
+  const CgPersistentArgs &A = R.P;
+  if (A.st && A.st->halt) return;
+  if (!A.cs->active) return;
+  const int g = threadIdx.x / kBlock, lt = threadIdx.x & (kBlock - 1);
+  // owned blocks
+  const int b0 = min(A.nblk_sell, (int)blockIdx.x * R.bpc_sell);
+  const int b1 = min(A.nblk_sell, b0 + R.bpc_sell);
+  const int c0 = min(A.nblk_nat, (int)blockIdx.x * R.bpc_nat);
+  const int c1 = min(A.nblk_nat, c0 + R.bpc_nat);
+  int *s_row = s_dyn;                          // [bpc_sell * 256]
+  int *s_len = s_row + R.bpc_sell * kBlock;    // [bpc_sell * 256]
+  int *s_base = s_len + R.bpc_sell * kBlock;   // [bpc_sell * 256]
+  int *s_col = s_base + R.bpc_sell * kBlock;   // [col_cap]
+  const int e0 = (b0 < b1) ? A.S.sptr[8 * b0] : 0;
+  int bs = b0;  // blocks [b0, bs) have their column indices in shared memory
+  while (bs < b1 && A.S.sptr[min(8 * (bs + 1), R.nslices)] - e0 <= R.col_cap) ++bs;
+  const int e1 = (bs > b0) ? A.S.sptr[min(8 * bs, R.nslices)] : e0;
+  for (int e = e0 + (int)threadIdx.x; e < e1; e += kCgResThreads) s_col[e - e0] = A.S.col[e];
+  for (int q = threadIdx.x; q < (b1 - b0) * kBlock; q += kCgResThreads) {
+    const int r = b0 * kBlock + q;
+    const bool in = r < A.S.nrows_pad;
+    s_row[q] = in ? A.S.perm[r] : -1;
+    s_len[q] = in ? A.S.len[r] : 0;
+    s_base[q] = in ? A.S.sptr[r >> 5] + (r & 31) : 0;
+  }
+  __syncthreads();
+  const double tol2 = A.cs->tol2;
+  const int maxit = A.cs->maxit;
+  double absnew = A.cs->absnew, beta = 0.0, alpha = 0.0, rr = 0.0;
+  int it = 0, status = KS_RUNNING, cur = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[1] += 1;
+  while (true) {
+    const bool fly = it > 0;
+    const double *pold = A.p[cur];
+    double *pnew = A.p[cur ^ 1];
+    // phase A: q = L p on the owned SELL blocks, one group per block
+    for (int b = b0 + g; b < b1; b += kCgResGroups) {
+      const int lp = (b - b0) * kBlock + lt;
+      const int i = s_row[lp];
+      double v[1] = {0.0};
+      if (i >= 0) {
+        const int base = s_base[lp], len = s_len[lp];
+        const bool staged = b < bs;
+        double acc = 0.0;
+        int k = 0;
+        for (; k + kCgChunk <= len; k += kCgChunk) {
+          int jj[kCgChunk];
+          double a[kCgChunk], po[kCgChunk], zz[kCgChunk];
+#pragma unroll
+          for (int u = 0; u < kCgChunk; ++u) {
+            const int pos = base + (k + u) * kSellC;
+            jj[u] = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+            a[u] = __ldg(A.Ls + pos);
+          }
+#pragma unroll
+          for (int u = 0; u < kCgChunk; ++u) {
+            po[u] = __ldcg(pold + jj[u]);
+            zz[u] = fly ? __ldcg(A.z + jj[u]) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kCgChunk; ++u) acc += a[u] * (fly ? zz[u] + beta * po[u] : po[u]);
+        }
+        for (; k < len; ++k) {
+          const int pos = base + k * kSellC;
+          const int jj = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+          const double a = __ldg(A.Ls + pos);
+          const double pj = fly ? __ldcg(A.z + jj) + beta * __ldcg(pold + jj) : __ldcg(pold + jj);
+          acc += a * pj;
+        }
+        const double pi = fly ? __ldcg(A.z + i) + beta * __ldcg(pold + i) : __ldcg(pold + i);
+        __stcg(pnew + i, pi);
+        __stcg(A.q + i, acc);
+        v[0] = pi * acc;
+      }
+      group_partial<1>(v, A.part_a, b, g, s_grp);
+    }
+    if (!grid_sync(A.bar)) return;
+    double pq[1];
+    tree_total_cta<1>(A.part_a, A.nblk_sell, pq, s_tree);
+    if (pq[0] == 0.0) {
+      status = KS_BREAKDOWN;
+      break;
+    }
+    alpha = absnew / pq[0];
+    // phase B: vector updates on the owned natural blocks
+    for (int b = c0 + g; b < c1; b += kCgResGroups) {
+      const int i = b * kBlock + lt;
+      double v[2] = {0.0, 0.0};
+      if (i < A.n) {
+        const double xi = __ldcg(A.x + i) + alpha * __ldcg(pnew + i);
+        const double ri = __ldcg(A.r + i) - alpha * __ldcg(A.q + i);
+        const double zi = __ldg(A.invL + i) * ri;
+        __stcg(A.x + i, xi);
+        __stcg(A.r + i, ri);
+        __stcg(A.z + i, zi);
+        v[0] = ri * ri;
+        v[1] = ri * zi;
+      }
+      group_partial<2>(v, A.part_b, b, g, s_grp);
+    }
+    if (!grid_sync(A.bar)) return;
+    double tb[2];
+    tree_total_cta<2>(A.part_b, A.nblk_nat, tb, s_tree);
+    ++it;
+    rr = A.scaled ? tb[1] : tb[0];
+    if (isnan(tb[0]) || isnan(tb[1])) {
+      status = KS_BREAKDOWN;
+      break;
+    }
+    if (rr <= tol2) {
+      status = KS_CONVERGED;
+      break;
+    }
+    if (it >= maxit) {
+      status = KS_MAXIT;
+      break;
+    }
+    beta = tb[1] / absnew;
+    absnew = tb[1];
+    cur ^= 1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    CgState *c = A.cs;
+    c->iters = it;
+    c->rnorm2 = rr;
+    c->alpha = alpha;
+    c->beta = beta;
+    c->absnew = absnew;
+    c->status = status;
+    c->active = 0;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
 // p += relax_p p'; Dirichlet outlet reset (NavierStokes.cpp:652-662, reinforcePressureBCs
 // :1011-1024). The pressure correction p' is the Krylov solution.
 __global__ void k_pressure_update(int nv, double relax_p, int outlet_type, double outlet_pressure,

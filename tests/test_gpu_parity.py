@@ -350,6 +350,27 @@ def test_persistent_cg_equals_loop_cg(cf, po):
     assert out[0][2] == out[1][2]
 
 
+@pytest.mark.parametrize("layers", [20, 300], ids=["small", "many_blocks"])
+def test_resident_cg_equals_persistent_cg(cf, po, layers):
+    """The shared-memory-resident CG (one 1024-thread CTA per SM) equals the 256-thread persistent
+    kernel and the three-kernel loop bit for bit; the larger mesh gives each CTA several blocks."""
+    m = make_mesh(cf, 6, layers)
+    out = []
+    for env in ({"CFSA_CG_LOOP": "1"}, {"CFSA_CG_KERNEL": "persistent"}, {}):
+        os.environ.update(env)
+        try:
+            s, _ = make_pair(cf, po, m, tol=1e-10)
+        finally:
+            for k in env:
+                os.environ.pop(k, None)
+        ok, done = s.pisoSteps(2)
+        assert ok and done == 2
+        out.append((s.getVelocity(), s.getPressure(), s.stats()["pressure_iters"]))
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
+        assert out[0][2] == o[2]
+
+
 @pytest.mark.parametrize("krylov", [0, 1], ids=["cg", "bicgstab"])
 def test_jacobi_norm_trajectory_bit_exact(cf, po, krylov):
     """The Jacobi-scaled convergence norm, oracle and device in the same reduction tree."""
