@@ -96,6 +96,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint run")
+    ap.add_argument("--y-bifurcation", action="store_true",
+                    help="also run config 4 (Y-bifurcation, ~4M tets, mixed precision + adjoint)")
+    ap.add_argument("--y-cell", type=float, default=0.081, help="lattice edge of the Y-bifurcation mesh")
     ap.add_argument("--adjoint-fd-nodes", type=int, default=ADJ_NODES,
                     help="seeded inlet nodes checked against central finite differences")
     ap.add_argument("--reference-budget-s", type=float, default=120.0,
@@ -280,6 +283,86 @@ def adjoint_section(cf, args, barrier):
         res["ok"] = True
     del s
     return res
+
+
+Y_CELL = 0.081  # Kuhn lattice edge of the Y-bifurcation: ~4M tets (mean volume ~1e-4)
+Y_STEPS, Y_CHECKPOINT = 100, 20
+
+
+def ybif_section(cf, args, barrier):
+    """Config 4: Y-bifurcation (parent R=2 L=15, daughters R=1.5 L=12 at +-35 deg, blend 0.5),
+    ~4M tets, parabolic inlet peak 1.0, both outlets p=0, 100 steps from rest. FP64 and mixed
+    precision forward runs (Jacobi-scaled criterion, tol 1e-10), then the mixed-precision
+    forward/backward pair with checkpoints every 20 steps for the pressure-drop objective
+    differentiated with respect to the inlet profile."""
+    import torch
+
+    t0 = time.perf_counter()
+    m = cf.Mesh.yBifurcation(cell=args.y_cell)
+    mesh_s = time.perf_counter() - t0
+    nv, nt, ne, _, _ = m.sizes
+    prof = cf.parabolic_inlet(m.nodePositions(), INLET_PEAK, 2.0)
+    p1, p2 = m.fluidBC()
+
+    def solver(precision):
+        s = cf.NavierStokesSolver()
+        s.setKrylovTolerances(TOL, TOL)
+        s.setConvergenceNorm(cf.NORM_JACOBI)
+        s.setMaxIterations(*MAXIT)
+        s.setPressureSolver(cf.KRYLOV_CG)
+        s.setPrecision(precision)
+        s.setDt(DT)
+        s.initialize(m, cf.Fluid(*FLUID))
+        s.setInletVelocityProfile(prof)
+        return s
+
+    out = {"workload": f"config 4: Y-bifurcation, {nt} tets, N2={nv + ne}, nv={nv} (Kuhn lattice cell "
+                       f"{args.y_cell}); {Y_STEPS} steps from rest, parabolic inlet peak 1.0, both outlets "
+                       f"p=0, Krylov tol {TOL:g} Jacobi-scaled",
+           "tets": nt, "p2_nodes": nv + ne, "inlet_vertices": int((p1 == 1).sum()),
+           "outlet_vertices": int((p1 == 2).sum()), "mesh_seconds": mesh_s}
+    res = {}
+    for name, prec in (("fp64", cf.PRECISION_FP64), ("mixed", cf.PRECISION_MIXED)):
+        s = solver(prec)
+        barrier()
+        ok, done = s.pisoSteps(Y_STEPS)
+        st = s.stats()
+        barrier()
+        res[name] = dict(ok=bool(ok), steps=done, ms=st["last_step_ms"], u=s.getVelocity(), p=s.getPressure(),
+                         iters=[st["krylov_iters"][0] / max(done, 1), st["krylov_iters"][1] / max(done, 1)],
+                         phase_ms=st["phase_ms"])
+        del s
+        torch.cuda.empty_cache()
+    from numpy.linalg import norm as l2
+    for name in ("fp64", "mixed"):
+        r = res[name]
+        out[name] = {"ok": r["ok"], "steps_per_s": r["steps"] / (r["ms"] / 1e3), "ms_per_step": r["ms"] / max(r["steps"], 1),
+                     "krylov_iters_per_step": r["iters"], "phase_ms_last_step": r["phase_ms"],
+                     "dof_updates_per_s": (3 * (nv + ne) + nv) * r["steps"] / (r["ms"] / 1e3)}
+    out["mixed_speedup_vs_fp64"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
+    out["rel_l2_mixed_vs_fp64"] = {"u": float(l2(res["mixed"]["u"] - res["fp64"]["u"]) / l2(res["fp64"]["u"])),
+                                   "p": float(l2(res["mixed"]["p"] - res["fp64"]["p"]) / l2(res["fp64"]["p"]))}
+    # adjoint (mixed precision forward and adjoint solves)
+    s = solver(cf.PRECISION_MIXED)
+    barrier()
+    ok = s.adjointForward(Y_STEPS, Y_CHECKPOINT)
+    g = s.adjointBackward(kind=cf.OBJECTIVE_PRESSURE_DROP) if ok else None
+    barrier()
+    if g is not None:
+        ast = s.adjointStats()
+        inl = np.concatenate([p1, p2]) == 1
+        out["adjoint"] = {"ok": True, "J_pressure_drop": g["J"], "forward_ms": ast["forward_ms"],
+                          "backward_ms": ast["backward_ms"], "recomputed_steps": ast["recomputed_steps"],
+                          "checkpoints": ast["checkpoints"], "record_gb": ast["record_bytes"] / 2**30,
+                          "adjoint_krylov_iters": [ast["momentum_iters"], ast["pressure_iters"]],
+                          "grad_inlet_axial_l2": float(l2(g["grad_inlet"][inl, 0])),
+                          "grad_viscosity": g["grad_viscosity"],
+                          "steps_per_s_forward_plus_backward": Y_STEPS / ((ast["forward_ms"] + ast["backward_ms"]) / 1e3)}
+    else:
+        out["adjoint"] = {"ok": False}
+    del s
+    torch.cuda.empty_cache()
+    return out
 
 
 def cpu_baseline(xyz, tets, profile, n_threads):
@@ -488,6 +571,10 @@ def main():
     if not args.no_adjoint:
         adjoint = adjoint_section(cf, args, barrier)
 
+    ybif = None
+    if args.y_bifurcation:
+        ybif = ybif_section(cf, args, barrier)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(m.vertices(), m.tets(), profile, os.cpu_count() or 1)
@@ -508,6 +595,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(profile.nbytes),
                     "d2h_bytes_per_step": int(u.nbytes + p.nbytes)},
             "cpu_baseline": cpu, "clocks": clk, "mixed": mixed, "adjoint": adjoint,
+            "y_bifurcation": ybif,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

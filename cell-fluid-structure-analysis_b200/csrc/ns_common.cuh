@@ -108,12 +108,30 @@ __device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&out)[NV
   __syncthreads();
   if (!last) return false;
   __threadfence();
+  // Thread t adds partials t, t+blockDim, ... in increasing order. The loads of four blocks (all
+  // NV values) are issued before their additions so that the L2 latency is paid once per four
+  // blocks instead of once per load; the order of the additions is unchanged.
+  double acc[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+  unsigned int b = threadIdx.x;
+  for (; b + 3 * blockDim.x < gridDim.x; b += 4 * blockDim.x) {
+    double v[4][NV];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int j = 0; j < NV; ++j) v[q][j] = __ldcg(&red.partials[(size_t)(b + q * blockDim.x) * kMaxRed + j]);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int j = 0; j < NV; ++j) acc[j] += v[q][j];
+  }
+  for (; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int j = 0; j < NV; ++j) acc[j] += __ldcg(&red.partials[(size_t)b * kMaxRed + j]);
 #pragma unroll
   for (int j = 0; j < NV; ++j) {
-    double s = 0.0;
-    for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
-      s += __ldcg(&red.partials[(size_t)b * kMaxRed + j]);
-    s = warp_sum(s);
+    const double s = warp_sum(acc[j]);
     if (lane == 0) sm[j][warp] = s;
   }
   __syncthreads();
