@@ -4,7 +4,8 @@
 Workload (one "step" = one pisoStep): cylinder L=30, R=2 along x, ~1M tets (16 disk rings x 217
 axial prism layers -> 999,936 tets, N2 = 1,378,515 P2 nodes, nv = 178,106 pressure DOFs),
 rho = 1060, nu = 0.004, dt = 0.01, parabolic inlet u_x = 2*0.5*(1 - r^2/4), no-slip wall, p = 0
-outlet, FP64, CG pressure and batched BiCGSTAB momentum to 1e-10 relative residual, from rest.
+outlet, FP64, single-reduction CG pressure and batched BiCGSTAB momentum to 1e-10 relative residual,
+from rest. The CPU baseline is the oracle port of the reference algorithm (BiCGSTAB pressure).
 The mesh is synthetic (the reference meshes with TetGen, which is not available here).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cfsa|reference]
@@ -110,7 +111,7 @@ def workload_desc(m, rings, layers):
     nv, nt, ne, _, _ = m.sizes
     return {
         "workload": f"cylinder L=30 R=2, {nt} tets ({rings} rings x {layers} layers), "
-                    f"N2={nv + ne} P2 nodes, nv={nv}; FP64 PISO, CG pressure + batched BiCGSTAB "
+                    f"N2={nv + ne} P2 nodes, nv={nv}; FP64 PISO, single-reduction CG pressure + batched BiCGSTAB "
                     f"momentum to 1e-10, parabolic inlet peak 1.0, rho 1060, nu 0.004, dt 0.01",
         "tets": nt, "p2_nodes": nv + ne, "pressure_dofs": nv,
         "velocity_dofs": 3 * (nv + ne),
@@ -129,7 +130,7 @@ def make_solver(cf, m, tol=TOL, norm=0):
     s.setKrylovTolerances(tol, tol)
     s.setConvergenceNorm(norm)
     s.setMaxIterations(*MAXIT)
-    s.setPressureSolver(cf.KRYLOV_CG)
+    s.setPressureSolver(cf.KRYLOV_CG1)
     s.setDt(DT)
     s.initialize(m, cf.Fluid(*FLUID))  # from rest; inlet set after initialize (CLI order)
     profile = cf.parabolic_inlet(m.nodePositions(), INLET_PEAK, GEOM["radius"])
@@ -217,7 +218,7 @@ def adjoint_section(cf, args, barrier):
     s.setKrylovTolerances(ADJ_TOL, ADJ_TOL)
     s.setConvergenceNorm(cf.NORM_JACOBI)
     s.setMaxIterations(50000, 200000)
-    s.setPressureSolver(cf.KRYLOV_CG)
+    s.setPressureSolver(cf.KRYLOV_CG1)
     s.setDt(DT)
     s.initialize(m, cf.Fluid(*FLUID))
     s.setInletVelocityProfile(prof)
@@ -309,7 +310,7 @@ def ybif_section(cf, args, barrier):
         s.setKrylovTolerances(TOL, TOL)
         s.setConvergenceNorm(cf.NORM_JACOBI)
         s.setMaxIterations(*MAXIT)
-        s.setPressureSolver(cf.KRYLOV_CG)
+        s.setPressureSolver(cf.KRYLOV_CG1)
         s.setPrecision(precision)
         s.setDt(DT)
         s.initialize(m, cf.Fluid(*FLUID))
@@ -374,7 +375,7 @@ def cpu_baseline(xyz, tets, profile, n_threads):
     cores = po.set_threads(n_threads)
     o = po.Oracle(xyz, tets)
     o.set_fluid(*FLUID)
-    o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=1)
+    o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=0)
     o.initialize()
     o.set_inlet(profile)
     if o.piso_step() != 0:
@@ -384,7 +385,7 @@ def cpu_baseline(xyz, tets, profile, n_threads):
     dt = time.perf_counter() - t
     return {"value": (1.0 / dt) if code == 0 else 0.0, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"1 PISO step (2nd from rest) of the {len(tets)}-tet workload, {dt:.2f} s, "
-                      f"FP64 oracle with OpenMP on {cores} threads"}
+                      f"FP64 oracle port of the reference algorithm (BiCGSTAB pressure) with OpenMP on {cores} threads"}
 
 
 def run_reference(args):
@@ -402,7 +403,7 @@ def run_reference(args):
     profile = cf.parabolic_inlet(m.nodePositions(), INLET_PEAK, GEOM["radius"])
     o = po.Oracle(xyz, tets)
     o.set_fluid(*FLUID)
-    o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=1)
+    o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=0)
     o.initialize()
     o.set_inlet(profile)
     for _ in range(max(1, min(args.warmup, 3))):
@@ -417,7 +418,7 @@ def run_reference(args):
     el = time.perf_counter() - t0
     value = done / el if el > 0 else 0.0
     sample = (f"{done} of {args.steps} requested PISO steps after {max(1, min(args.warmup, 3))} warm-up "
-              f"steps, FP64 oracle port with OpenMP on {cores} threads, capped at "
+              f"steps, FP64 oracle port of the reference algorithm (BiCGSTAB pressure) with OpenMP on {cores} threads, capped at "
               f"{args.reference_budget_s:.0f} s of timed work")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
             "steps": done, "warmup": max(1, min(args.warmup, 3)),

@@ -25,7 +25,7 @@ OK, NOT_CONVERGED, BREAKDOWN, NAN, CUDA_ERROR, BAD_ARG, NOT_INITIALIZED, UNSUPPO
 
 MAT_MASS, MAT_STIFFNESS, MAT_GRAD_X, MAT_GRAD_Y, MAT_GRAD_Z, MAT_POISSON, MAT_MOMENTUM, MAT_POISSON_BC = range(8)
 KERNEL_MOMENTUM_SPMV, KERNEL_PRESSURE_SPMV = 0, 1
-KRYLOV_CG, KRYLOV_BICGSTAB = 0, 1
+KRYLOV_CG, KRYLOV_BICGSTAB, KRYLOV_CG1 = 0, 1, 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 NORM_REFERENCE, NORM_JACOBI = 0, 1
 OBJECTIVE_WALL_SHEAR, OBJECTIVE_PRESSURE_DROP = 0, 1

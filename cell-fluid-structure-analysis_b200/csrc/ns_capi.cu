@@ -117,6 +117,7 @@ struct cfsa_ns {
   int cg_grid = 0;
   // SMEM-resident variant of the persistent CG (k_cg_resident): one 1024-thread CTA per SM
   bool cg_resident = false;
+  double *cg1_vec[3] = {nullptr, nullptr, nullptr};  // second r, w, s buffers of k_cg1_resident
   int cg_res_grid = 0, cg_res_bpc_sell = 0, cg_res_bpc_nat = 0, cg_res_col_cap = 0;
   size_t cg_res_smem = 0;
   unsigned int *bar_count = nullptr, *bar_gen = nullptr;
@@ -463,8 +464,9 @@ struct cfsa_ns {
       CK(cudaMemsetAsync(bar_count, 0, (1 + kBarrierGroups) * sizeof(unsigned int), stream));
       CK(cudaMemsetAsync(bar_gen, 0, sizeof(unsigned int), stream));
       CK(cudaMemsetAsync(bar_err, 0, sizeof(int), stream));
-      cg_part_a = dalloc<double>((size_t)nblk_sell * kMaxRed);
-      cg_part_b = dalloc<double>((size_t)nblk_nat * kMaxRed);
+      cg_part_a = dalloc<double>((size_t)std::max(nblk_sell, nblk_nat) * kMaxRed);
+      cg_part_b = dalloc<double>((size_t)std::max(nblk_sell, nblk_nat) * kMaxRed);
+      for (double *&v : cg1_vec) v = dalloc<double>((size_t)nv);
       if (cg_grid < 1) cg_persistent = false;
       // resident variant: blocks split into contiguous runs, one run per SM
       int optin = 0;
@@ -483,11 +485,16 @@ struct cfsa_ns {
         cg_res_col_cap = (int)std::min<int64_t>(max_entries, avail / (int64_t)sizeof(int));
         cg_res_smem = (size_t)(row_bytes + (int64_t)cg_res_col_cap * (int64_t)sizeof(int));
         int per_sm_res = 0;
+        int per_sm_res1 = 0;
         if (cudaFuncSetAttribute(k_cg_resident, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cg_res_smem) == cudaSuccess &&
+            cudaFuncSetAttribute(k_cg1_resident, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cg_res_smem) == cudaSuccess &&
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_res, k_cg_resident, kCgResThreads,
                                                           cg_res_smem) == cudaSuccess &&
-            per_sm_res >= 1) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_res1, k_cg1_resident, kCgResThreads,
+                                                          cg_res_smem) == cudaSuccess &&
+            per_sm_res >= 1 && per_sm_res1 >= 1) {
           cg_resident = true;
           cg_res_grid = grid;
           cg_res_bpc_sell = bpc_s;
@@ -851,7 +858,7 @@ struct cfsa_ns {
       else
         eager_while(body, [&] { return poll_bicg(bs_p); }, maxit_p);
       k_check_bicg<<<1, 1, 0, stream>>>(bs_p, 1, 1, s_out);
-    } else if (cg_persistent) {
+    } else if (cg_persistent || krylov == CFSA_KRYLOV_CG1) {
       CgPersistentArgs c{};
       c.S = s1.view();
       c.Ls = Ls;
@@ -882,7 +889,30 @@ struct cfsa_ns {
       attr[0].val.cooperative = 1;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
-      if (cg_resident) {
+      if (krylov == CFSA_KRYLOV_CG1) {
+        CgResidentArgs rz{};
+        rz.P = c;
+        rz.nslices = s1.nslices;
+        rz.bpc_sell = cg_res_bpc_sell;
+        rz.bpc_nat = cg_res_bpc_nat;
+        rz.col_cap = cg_res_col_cap;
+        Cg1Args c1{};
+        c1.R = rz;
+        c1.r[0] = pr;
+        c1.r[1] = cg1_vec[0];
+        c1.w[0] = pq;
+        c1.w[1] = cg1_vec[1];
+        c1.s[0] = ps;
+        c1.s[1] = cg1_vec[2];
+        c1.u0 = pz;
+        c1.p = pp;
+        CK(cudaMemsetAsync(pp, 0, (size_t)nv * sizeof(double), stream));
+        CK(cudaMemsetAsync(ps, 0, (size_t)nv * sizeof(double), stream));
+        cfg.gridDim = dim3((unsigned int)cg_res_grid);
+        cfg.blockDim = dim3(kCgResThreads);
+        cfg.dynamicSmemBytes = cg_res_smem;
+        CK(cudaLaunchKernelEx(&cfg, k_cg1_resident, c1));
+      } else if (cg_resident) {
         CgResidentArgs rz{};
         rz.P = c;
         rz.nslices = s1.nslices;
@@ -1039,7 +1069,7 @@ struct cfsa_ns {
     CK(cudaEventSynchronize(ev1));
     CK(cudaStreamSynchronize(stream));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
-    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : (cg_persistent ? 1 : 3);
+    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : ((cg_persistent || krylov == CFSA_KRYLOV_CG1) ? 1 : 3);
     // mixed momentum: 5 kernels per inner body, 3 per outer sweep (inner init, x update,
     // residual) plus the outer init kernel per step
     batch_launches = (int64_t)launched_steps * (launches_per_step + (precision == CFSA_PRECISION_MIXED ? 1 : 0)) +
@@ -1494,7 +1524,7 @@ struct cfsa_ns {
     adj_stats.momentum_iters = (int64_t)hs_adj.iters[0];
     adj_stats.pressure_iters = (int64_t)hs_adj.iters[1];
     adj_stats.backward_ms = ms;
-    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : (cg_persistent ? 1 : 3);
+    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : ((cg_persistent || krylov == CFSA_KRYLOV_CG1) ? 1 : 3);
     adj_stats.kernel_launches = (int64_t)adj_steps * adj_launches_fixed + 5 * (int64_t)hs_adj.body_runs[0] +
                                 pressure_body * (int64_t)hs_adj.body_runs[1] +
                                 3 * (int64_t)hs_adj.body_runs[2];
@@ -1734,8 +1764,10 @@ int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u) {
 
 int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov) {
   if (!h) return CFSA_BAD_ARG;
-  if (krylov != CFSA_KRYLOV_CG && krylov != CFSA_KRYLOV_BICGSTAB)
+  if (krylov != CFSA_KRYLOV_CG && krylov != CFSA_KRYLOV_BICGSTAB && krylov != CFSA_KRYLOV_CG1)
     return fail(h, CFSA_BAD_ARG, "unknown Krylov method");
+  if (krylov == CFSA_KRYLOV_CG1 && !h->cg_resident)
+    return fail(h, CFSA_UNSUPPORTED, "single-reduction CG needs the shared-memory-resident grid on this device");
   h->krylov = krylov;
   h->graph_dirty = true;
   return CFSA_OK;

@@ -13,6 +13,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda/atomic>
 #include <cuda_runtime.h>
 
 namespace cfsa {
@@ -101,34 +102,56 @@ __device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&out)[NV
       for (int w = 0; w < nwarps; ++w) s += sm[j][w];
       red.partials[(size_t)blockIdx.x * kMaxRed + j] = s;
     }
-    __threadfence();
-    const unsigned int ticket = atomicAdd(red.counter, 1u);
+    // release: this block's partials are visible to the block that takes the last ticket
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> ctr(*red.counter);
+    const unsigned int ticket = ctr.fetch_add(1u, cuda::memory_order_acq_rel);
     last = (ticket == gridDim.x - 1);
   }
   __syncthreads();
   if (!last) return false;
   __threadfence();
-  // Thread t adds partials t, t+blockDim, ... in increasing order. The loads of four blocks (all
-  // NV values) are issued before their additions so that the L2 latency is paid once per four
-  // blocks instead of once per load; the order of the additions is unchanged.
+  // Thread t adds partials t, t+blockDim, ... in increasing order. Loads are issued in batches
+  // before their additions so that the L2 latency is paid once per batch instead of once per
+  // load; the order of the additions is unchanged. Few values: four blocks x all values per
+  // batch; many values: one value at a time, eight blocks per batch (measured faster for 6).
   double acc[NV];
 #pragma unroll
   for (int j = 0; j < NV; ++j) acc[j] = 0.0;
-  unsigned int b = threadIdx.x;
-  for (; b + 3 * blockDim.x < gridDim.x; b += 4 * blockDim.x) {
-    double v[4][NV];
+  const unsigned int G = gridDim.x, T = blockDim.x;
+  if (NV <= 3) {
+    unsigned int b = threadIdx.x;
+    for (; b + 3 * T < G; b += 4 * T) {
+      double v[4][NV];
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < 4; ++q)
 #pragma unroll
-      for (int j = 0; j < NV; ++j) v[q][j] = __ldcg(&red.partials[(size_t)(b + q * blockDim.x) * kMaxRed + j]);
+        for (int j = 0; j < NV; ++j) v[q][j] = __ldcg(&red.partials[(size_t)(b + q * T) * kMaxRed + j]);
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < 4; ++q)
 #pragma unroll
-      for (int j = 0; j < NV; ++j) acc[j] += v[q][j];
+        for (int j = 0; j < NV; ++j) acc[j] += v[q][j];
+    }
+    for (; b < G; b += T)
+#pragma unroll
+      for (int j = 0; j < NV; ++j) acc[j] += __ldcg(&red.partials[(size_t)b * kMaxRed + j]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double s = 0.0;
+      for (unsigned int b0 = threadIdx.x; b0 < G; b0 += 8 * T) {
+        double x[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const unsigned int b = b0 + q * T;
+          x[q] = (b < G) ? __ldcg(&red.partials[(size_t)b * kMaxRed + j]) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (b0 + q * T < G) s += x[q];
+      }
+      acc[j] = s;
+    }
   }
-  for (; b < gridDim.x; b += blockDim.x)
-#pragma unroll
-    for (int j = 0; j < NV; ++j) acc[j] += __ldcg(&red.partials[(size_t)b * kMaxRed + j]);
 #pragma unroll
   for (int j = 0; j < NV; ++j) {
     const double s = warp_sum(acc[j]);

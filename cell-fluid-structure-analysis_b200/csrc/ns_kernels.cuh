@@ -1323,7 +1323,7 @@ __device__ __forceinline__ void group_sync(int g) {
 // block_partial for one 256-thread group of a larger CTA (named barrier 1 + g).
 template <int NV>
 __device__ __forceinline__ void group_partial(double (&v)[NV], double *__restrict__ partials, int b,
-                                              int g, double (*sm)[2][kBlock / 32]) {
+                                              int g, double (*sm)[3][kBlock / 32]) {
   const int lt = threadIdx.x & (kBlock - 1), warp = lt >> 5, lane = lt & 31;
 #pragma unroll
   for (int j = 0; j < NV; ++j) {
@@ -1379,8 +1379,8 @@ __device__ __forceinline__ void tree_total_cta(const double *__restrict__ partia
 
 __global__ void __launch_bounds__(kCgResThreads, 1) k_cg_resident(CgResidentArgs R) {
   extern __shared__ int s_dyn[];
-  __shared__ double s_grp[kCgResGroups][2][kBlock / 32];
-  __shared__ double s_tree[2][kBlock / 32];
+  __shared__ double s_grp[kCgResGroups][3][kBlock / 32];
+  __shared__ double s_tree[3][kBlock / 32];
   const CgPersistentArgs &A = R.P;
   if (A.st && A.st->halt) return;
   if (!A.cs->active) return;
@@ -1509,6 +1509,188 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg_resident(CgResidentArgs
     c->alpha = alpha;
     c->beta = beta;
     c->absnew = absnew;
+    c->status = status;
+    c->active = 0;
+  }
+}
+
+// Jacobi-preconditioned CG with one reduction per iteration (Chronopoulos & Gear 1989), the same
+// iterates as CG in exact arithmetic: s = A p is carried by a recurrence, so an iteration is ONE
+// fused pass (vector updates, product, three dot products) and ONE grid barrier instead of two:
+//   p = u + b p;  s = w + b s;  x += a p;  r -= a s;  u = M r;  w = A u;
+//   gamma = r.u, delta = w.u, rr = r.r;   b' = gamma'/gamma,  a' = gamma' / (delta' - b' gamma' / a).
+// The product needs the new u of neighbouring rows: each gathering thread forms it from that row's
+// previous r, w and s (the expression its owner evaluates, so the same bits). r, w and s are
+// double-buffered; p and x are only read by their own row. Layout, staging and reduction tree
+// are those of k_cg_resident.
+struct Cg1Args {
+  CgResidentArgs R;
+  double *r[2], *w[2], *s[2];  // r[0] = b on entry; s[0] zero on entry
+  const double *u0;            // M b (from the right-hand-side kernel)
+  double *p;                   // zero on entry
+};
+
+__global__ void __launch_bounds__(kCgResThreads, 1) k_cg1_resident(Cg1Args C) {
+  extern __shared__ int s_dyn[];
+  __shared__ double s_grp[kCgResGroups][3][kBlock / 32];
+  __shared__ double s_tree[3][kBlock / 32];
+  const CgResidentArgs &R = C.R;
+  const CgPersistentArgs &A = R.P;
+  if (A.st && A.st->halt) return;
+  if (!A.cs->active) return;
+  const int g = threadIdx.x / kBlock, lt = threadIdx.x & (kBlock - 1);
+  const int b0 = min(A.nblk_sell, (int)blockIdx.x * R.bpc_sell);
+  const int b1 = min(A.nblk_sell, b0 + R.bpc_sell);
+  int *s_row = s_dyn;
+  int *s_len = s_row + R.bpc_sell * kBlock;
+  int *s_base = s_len + R.bpc_sell * kBlock;
+  int *s_col = s_base + R.bpc_sell * kBlock;
+  const int e0 = (b0 < b1) ? A.S.sptr[8 * b0] : 0;
+  int bs = b0;
+  while (bs < b1 && A.S.sptr[min(8 * (bs + 1), R.nslices)] - e0 <= R.col_cap) ++bs;
+  const int e1 = (bs > b0) ? A.S.sptr[min(8 * bs, R.nslices)] : e0;
+  for (int e = e0 + (int)threadIdx.x; e < e1; e += kCgResThreads) s_col[e - e0] = A.S.col[e];
+  for (int q = threadIdx.x; q < (b1 - b0) * kBlock; q += kCgResThreads) {
+    const int r = b0 * kBlock + q;
+    const bool in = r < A.S.nrows_pad;
+    s_row[q] = in ? A.S.perm[r] : -1;
+    s_len[q] = in ? A.S.len[r] : 0;
+    s_base[q] = in ? A.S.sptr[r >> 5] + (r & 31) : 0;
+  }
+  __syncthreads();
+  const double tol2 = A.cs->tol2;
+  const int maxit = A.cs->maxit;
+  double gamma = A.cs->absnew, alpha = 0.0, beta = 0.0, rn2 = A.cs->bnorm2;
+  int it = 0, status = KS_RUNNING, cur = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[1] += 1;
+  // start: w = A u0, delta = w.u0
+  for (int b = b0 + g; b < b1; b += kCgResGroups) {
+    const int lp = (b - b0) * kBlock + lt;
+    const int i = s_row[lp];
+    double v[1] = {0.0};
+    if (i >= 0) {
+      const int base = s_base[lp], len = s_len[lp];
+      const bool staged = b < bs;
+      double acc = 0.0;
+      for (int k = 0; k < len; ++k) {
+        const int pos = base + k * kSellC;
+        const int jj = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+        acc += __ldg(A.Ls + pos) * __ldcg(C.u0 + jj);
+      }
+      __stcg(C.w[0] + i, acc);
+      v[0] = acc * __ldcg(C.u0 + i);
+    }
+    group_partial<1>(v, A.part_a, b, g, s_grp);
+  }
+  if (!grid_sync(A.bar)) return;
+  {
+    double d0[1];
+    tree_total_cta<1>(A.part_a, A.nblk_sell, d0, s_tree);
+    if (d0[0] == 0.0)
+      status = KS_BREAKDOWN;
+    else
+      alpha = gamma / d0[0];
+  }
+  while (status == KS_RUNNING) {
+    // partials alternate between the two buffers: with one barrier per iteration a CTA may write
+    // this iteration's partials while another still reads the previous iteration's
+    double *part = (it & 1) ? A.part_a : A.part_b;
+    const double *ro = C.r[cur], *wo = C.w[cur], *so = C.s[cur];
+    double *rn = C.r[cur ^ 1], *wn = C.w[cur ^ 1], *sn = C.s[cur ^ 1];
+    for (int b = b0 + g; b < b1; b += kCgResGroups) {
+      const int lp = (b - b0) * kBlock + lt;
+      const int i = s_row[lp];
+      double v[3] = {0.0, 0.0, 0.0};
+      if (i >= 0) {
+        const int base = s_base[lp], len = s_len[lp];
+        const bool staged = b < bs;
+        double acc = 0.0;
+        int k = 0;
+        for (; k + kCgChunk <= len; k += kCgChunk) {
+          int jj[kCgChunk];
+          double a[kCgChunk], rr_[kCgChunk], ww[kCgChunk], ss[kCgChunk], mm[kCgChunk];
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            const int pos = base + (k + q) * kSellC;
+            jj[q] = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+            a[q] = __ldg(A.Ls + pos);
+          }
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            rr_[q] = __ldcg(ro + jj[q]);
+            ww[q] = __ldcg(wo + jj[q]);
+            ss[q] = __ldcg(so + jj[q]);
+            mm[q] = __ldg(A.invL + jj[q]);
+          }
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            const double sj = ww[q] + beta * ss[q];
+            const double rj = rr_[q] - alpha * sj;
+            acc += a[q] * (mm[q] * rj);
+          }
+        }
+        for (; k < len; ++k) {
+          const int pos = base + k * kSellC;
+          const int jj = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+          const double sj = __ldcg(wo + jj) + beta * __ldcg(so + jj);
+          const double rj = __ldcg(ro + jj) - alpha * sj;
+          acc += __ldg(A.Ls + pos) * (__ldg(A.invL + jj) * rj);
+        }
+        // own row
+        const double mi = __ldg(A.invL + i);
+        const double roi = __ldcg(ro + i);
+        const double uoi = (it == 0) ? __ldcg(C.u0 + i) : mi * roi;
+        const double pi = uoi + beta * __ldcg(C.p + i);
+        const double si = __ldcg(wo + i) + beta * __ldcg(so + i);
+        const double xi = __ldcg(A.x + i) + alpha * pi;
+        const double ri = roi - alpha * si;
+        const double ui = mi * ri;
+        __stcg(C.p + i, pi);
+        __stcg(sn + i, si);
+        __stcg(A.x + i, xi);
+        __stcg(rn + i, ri);
+        __stcg(wn + i, acc);
+        v[0] = ri * ui;
+        v[1] = acc * ui;
+        v[2] = ri * ri;
+      }
+      group_partial<3>(v, part, b, g, s_grp);
+    }
+    if (!grid_sync(A.bar)) return;
+    double t[3];
+    tree_total_cta<3>(part, A.nblk_sell, t, s_tree);
+    ++it;
+    rn2 = A.scaled ? t[0] : t[2];
+    cur ^= 1;
+    if (isnan(t[0]) || isnan(t[1]) || isnan(t[2])) {
+      status = KS_BREAKDOWN;
+      break;
+    }
+    if (rn2 <= tol2) {
+      status = KS_CONVERGED;
+      break;
+    }
+    if (it >= maxit) {
+      status = KS_MAXIT;
+      break;
+    }
+    const double beta_new = t[0] / gamma;
+    const double den = t[1] - beta_new * t[0] / alpha;
+    if (den == 0.0) {
+      status = KS_BREAKDOWN;
+      break;
+    }
+    alpha = t[0] / den;
+    beta = beta_new;
+    gamma = t[0];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    CgState *c = A.cs;
+    c->iters = it;
+    c->rnorm2 = rn2;
+    c->alpha = alpha;
+    c->beta = beta;
+    c->absnew = gamma;
     c->status = status;
     c->active = 0;
   }

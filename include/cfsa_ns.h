@@ -48,6 +48,9 @@ extern "C" {
  * Poisson matrix with penalty rows is SPD, so CG is offered and is the default here. */
 #define CFSA_KRYLOV_CG 0
 #define CFSA_KRYLOV_BICGSTAB 1
+/* CG with one reduction per iteration (Chronopoulos & Gear 1989): CG's iterates in exact
+ * arithmetic, one fused product-and-reduction pass and one grid synchronisation per iteration */
+#define CFSA_KRYLOV_CG1 2
 
 /* arithmetic of the Krylov solves */
 #define CFSA_PRECISION_FP64 0

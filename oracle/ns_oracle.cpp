@@ -388,6 +388,69 @@ SolveInfo cg(const CSR &A, const std::vector<double> &b, std::vector<double> &x,
   return info;
 }
 
+// Jacobi-preconditioned CG with one reduction per iteration (Chronopoulos & Gear, J. Comput.
+// Appl. Math. 25 (1989)): the same iterates as cg() in exact arithmetic. s = A p is carried by a
+// recurrence, so one fused product-and-reduction pass per iteration suffices:
+//   p = u + beta p;  s = w + beta s;  x += alpha p;  r -= alpha s;  u = M r;  w = A u;
+//   gamma = r.u, delta = w.u, rr = r.r;
+//   beta' = gamma'/gamma, alpha' = gamma' / (delta' - beta' gamma' / alpha).
+// Start: u = M b, w = A u, gamma = b.u (natural order), delta = w.u (product order), alpha =
+// gamma/delta, beta = 0. The three dots of an iteration are summed in `sell` order (they are fused
+// into the product); the stopping rule is cg()'s.
+SolveInfo cg1(const CSR &A, const std::vector<double> &b, std::vector<double> &x, double tol,
+              int maxit, const RedOrder &sell, const RedOrder &nat, bool scaled) {
+  const int64_t n = A.n;
+  SolveInfo info;
+  const std::vector<double> invdiag = inverse_diagonal(A);
+  x.assign(n, 0.0);
+  std::vector<double> r(b), u(n), w(n), p(n, 0.0), s(n, 0.0);
+  for (int64_t k = 0; k < n; ++k) u[k] = invdiag[k] * r[k];
+  const double b2 = odot(nat, b.data(), b.data());
+  double gamma = odot(nat, b.data(), u.data());
+  const double bnorm2 = scaled ? gamma : b2;
+  const double thr = tol * tol * bnorm2;
+  if (std::isnan(bnorm2)) return info;
+  double rn2 = bnorm2;
+  int it = 0;
+  if (!(bnorm2 == 0.0 || bnorm2 <= thr)) {
+    spmv(A, u.data(), w.data());
+    const double delta0 = odot(sell, w.data(), u.data());
+    if (delta0 == 0.0) {
+      info.rel_res = 1.0;
+      return info;
+    }
+    double alpha = gamma / delta0, beta = 0.0;
+    while (true) {
+      for (int64_t k = 0; k < n; ++k) {
+        p[k] = u[k] + beta * p[k];
+        s[k] = w[k] + beta * s[k];
+        x[k] += alpha * p[k];
+        r[k] = r[k] - alpha * s[k];
+        u[k] = invdiag[k] * r[k];
+      }
+      spmv(A, u.data(), w.data());
+      const double g_new = odot(sell, r.data(), u.data());
+      const double delta = odot(sell, w.data(), u.data());
+      const double rr = odot(sell, r.data(), r.data());
+      rn2 = scaled ? g_new : rr;
+      ++it;
+      if (std::isnan(g_new) || std::isnan(delta) || std::isnan(rr)) break;
+      if (rn2 <= thr) break;
+      if (it >= maxit) break;
+      const double beta_new = g_new / gamma;
+      const double den = delta - beta_new * g_new / alpha;
+      if (den == 0.0) break;
+      alpha = g_new / den;
+      beta = beta_new;
+      gamma = g_new;
+    }
+  }
+  info.iters = it;
+  info.rel_res = std::sqrt(rn2 / bnorm2);
+  info.converged = rn2 <= thr;
+  return info;
+}
+
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -413,7 +476,7 @@ struct Oracle {
   int outlet_type = kDirichlet;
   double outlet_pressure = 0.0;
   int reference_node = -1;
-  int pressure_solver = 0;  // 0 = BiCGSTAB (reference), 1 = CG
+  int pressure_solver = 0;  // 0 = BiCGSTAB (reference), 1 = CG, 2 = CG with one reduction
   int conv_norm = 0;        // 0 = ||r|| (reference), 1 = ||D^-1/2 r||
   std::vector<V3> inlet;    // per P2-node inlet velocity (the reference: one mean vector)
   std::vector<V3> u, ustar;
@@ -812,6 +875,8 @@ struct Oracle {
     }
     SolveInfo si = (pressure_solver == 1)
                        ? cg(Lbc, rhs, x, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1)
+                   : (pressure_solver == 2)
+                       ? cg1(Lbc, rhs, x, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1)
                        : bicgstab(Lbc, rhs, x, tol_p, maxit_p, order_nv, order_p1, order_nv,
                                   conv_norm == 1);
     it_p = si.iters;
@@ -1155,6 +1220,8 @@ struct Oracle {
       {
         SolveInfo si = (pressure_solver == 1)
                            ? cg(Lbc, rhs, mu_p, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1)
+                       : (pressure_solver == 2)
+                           ? cg1(Lbc, rhs, mu_p, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1)
                            : bicgstab(Lbc, rhs, mu_p, tol_p, maxit_p, order_nv, order_p1, order_nv,
                                       conv_norm == 1);
         adj_it_p += si.iters;
@@ -1330,7 +1397,7 @@ void orc_set_fluid(void *h, double density, double viscosity) {
 }
 // Parameters: dt, momentum tol, pressure tol, momentum maxit, pressure maxit, corrections,
 // relax_u, relax_p, outlet type, outlet pressure, reference node, pressure solver (0 BiCGSTAB,
-// 1 CG), convergence norm (0 ||r||, 1 ||D^-1/2 r||).
+// 1 CG, 2 single-reduction CG), convergence norm (0 ||r||, 1 ||D^-1/2 r||).
 void orc_set_params(void *h, double dt, double tol_mom, double tol_p, int maxit_mom, int maxit_p,
                     int n_corr, double relax_u, double relax_p, int outlet_type,
                     double outlet_pressure, int reference_node, int pressure_solver, int conv_norm) {
