@@ -439,7 +439,7 @@ void Mesh::generateYBifurcation(const YBifurcation &sp) {
     for (size_t t = 0; t < tets.size(); ++t)
       for (int q = 0; q < 4; ++q) vt[fill[tets[t][q]]++] = (int)t;
   }
-  const double vmin = 0.1 * a * a * a / 6.0;
+  const double vmin = 0.3 * a * a * a / 6.0;  // keep moved tets at >= 30% of the lattice tet volume
   auto try_move = [&](size_t v, const Vec3 &target, double max_step) {
     const Vec3 orig = verts[v];
     Vec3 step = target - orig;
