@@ -29,6 +29,7 @@ KRYLOV_CG, KRYLOV_BICGSTAB, KRYLOV_CG1 = 0, 1, 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 NORM_REFERENCE, NORM_JACOBI = 0, 1
 OBJECTIVE_WALL_SHEAR, OBJECTIVE_PRESSURE_DROP = 0, 1
+VTK_SHEAR_STRESS, VTK_PRESSURE_FORCES = 1, 2
 
 
 class FluidBCType(enum.IntEnum):
@@ -207,6 +208,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "cfsa_ns_profile_kernel": (i32, [vp, i32, i32, vp, vp]),
         "cfsa_ns_compute_divergence_noalloc": (i32, [vp, vp, vp]),
         "cfsa_ns_objective": (i32, [vp, vp, vp]),
+        "cfsa_ns_write_vtk": (i32, [vp, C.c_char_p, C.c_double, i32]),
         "cfsa_ns_adjoint_forward": (i32, [vp, i32, i32, vp]),
         "cfsa_ns_adjoint_backward": (i32, [vp, vp, vp, vp, vp, vp, vp]),
         "cfsa_ns_adjoint_backward_seed": (i32, [vp, vp, vp, C.c_double, vp, vp, vp, vp]),
@@ -589,6 +591,11 @@ class NavierStokesSolver:
         va = np.empty(nnz.value)
         self._check(self._lib.cfsa_ns_get_matrix(self._h, int(which), _ptr(rp), _ptr(ci), _ptr(va)))
         return rp, ci, va
+
+    def exportToVtk(self, filename, scale: float = 1.0, fields: int = 0):
+        """io::exportToVtk(filename, solver, scale) (src/IO/VtkExport.cpp:238-268); `fields` adds
+        VTK_SHEAR_STRESS / VTK_PRESSURE_FORCES vectors."""
+        self._check(self._lib.cfsa_ns_write_vtk(self._h, str(filename).encode(), float(scale), int(fields)))
 
     # ---- discrete adjoint (forward / backward operator pair)
     def objective(self, kind: int = OBJECTIVE_WALL_SHEAR, axis: int = 0, lo: float = 0.0,

@@ -213,6 +213,16 @@ int cfsa_ns_profile_kernel(cfsa_ns *h, int which, int iters, double *avg_ms, dou
  * once div_dev is written. */
 int cfsa_ns_compute_divergence_noalloc(cfsa_ns *h, const double *u_dev, double *div_dev);
 
+/* ---- output ---- */
+/* io::exportToVtk(filename, const NavierStokesSolver&, scale) (src/IO/VtkExport.cpp:49-84,
+ * 238-268): legacy ASCII VTK unstructured grid of the P1 mesh (points scaled by `scale`), point
+ * data FluidBoundaryType, pressure and velocity (scaled) on the P1 vertices, formatted as the
+ * reference writes them. The fields are copied from the device asynchronously while the points
+ * and cells are formatted. `fields` adds (new) boundary-force vectors per vertex: */
+#define CFSA_VTK_SHEAR_STRESS 1    /* computeShearStress (NavierStokes.cpp:874-944) */
+#define CFSA_VTK_PRESSURE_FORCES 2 /* computePressureForces (NavierStokes.cpp:841-873) */
+int cfsa_ns_write_vtk(cfsa_ns *h, const char *path, double scale, int fields);
+
 /* ---- discrete adjoint (no counterpart in the reference) ----
  * Reverse mode through the PISO steps exactly as the forward kernels compute them (every Krylov
  * solve taken as the exact linear solve it converges to). The differentiated map is

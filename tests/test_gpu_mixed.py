@@ -30,9 +30,12 @@ def run(cf, po, m, precision, steps, tol, **kw):
 
 @pytest.mark.parametrize("rings,layers", [(3, 12), (5, 68)])
 def test_mixed_matches_converged_fp64(cf, po, rings, layers):
+    """Mixed at outer tolerance 1e-12 against FP64 at 1e-14, both under the Jacobi-scaled
+    criterion (under the reference criterion 1e-12 itself leaves ~1e-6 of interior slack, for FP64
+    as much as for mixed; that norm is covered by the next test)."""
     m = make_mesh(cf, rings, layers)
-    ref = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-14)
-    mix = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-12)
+    ref = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-14, norm=cf.NORM_JACOBI)
+    mix = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-12, norm=cf.NORM_JACOBI)
     for k in (0, 4, 9):
         eu, ep = rel_l2(mix[k][0], ref[k][0]), rel_l2(mix[k][1], ref[k][1])
         print(f"step {k + 1}: mixed(1e-12) vs fp64(1e-14) rel L2 u {eu:.2e} p {ep:.2e}; "

@@ -1,0 +1,60 @@
+"""VTK export from device buffers (cfsa_ns_write_vtk behind io::exportToVtk): the file must be
+the text the reference's writer (src/IO/VtkExport.cpp:49-84, 238-268) produces from the same
+mesh and fields, i.e. C++ default stream formatting (6 significant digits, %g style)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def g(x):
+    return format(float(x), "g")
+
+
+def expected_text(m, u, p, scale):
+    xyz = m.vertices()
+    tets = m.tets()
+    p1, _ = m.fluidBC()
+    out = ["# vtk DataFile Version 3.0", "Shape export", "ASCII", "DATASET UNSTRUCTURED_GRID",
+           f"POINTS {len(xyz)} double"]
+    out += [f"{g(a * scale)} {g(b * scale)} {g(c * scale)}" for a, b, c in xyz]
+    out.append(f"CELLS {len(tets)} {len(tets) * 5}")
+    out += [f"4 {a} {b} {c} {d}" for a, b, c, d in tets]
+    out.append(f"CELL_TYPES {len(tets)}")
+    out += ["10"] * len(tets)
+    out += ["", f"POINT_DATA {len(xyz)}", "SCALARS FluidBoundaryType int 1", "LOOKUP_TABLE default"]
+    out += [str(int(b)) for b in p1]
+    out += ["", "SCALARS pressure double 1", "LOOKUP_TABLE default"]
+    out += [g(v) for v in p]
+    out += ["", "VECTORS velocity double"]
+    nv = len(xyz)
+    out += [f"{g(a * scale)} {g(b * scale)} {g(c * scale)}" for a, b, c in u[:nv]]
+    return "\n".join(out) + "\n"
+
+
+def test_vtk_export_matches_reference_format(cf, tmp_path):
+    m = cf.Mesh.cylinder(30.0, 2.0, 3, 12)
+    m.setupBoundaryConditions((1.0, 0.0, 0.0), 1.0)
+    s = cf.NavierStokesSolver()
+    s.setTolerance(1e-10)
+    s.setDt(0.01)
+    s.initialize(m, cf.Fluid(1060.0, 0.004))
+    s.setMeanInletVelocity([0.5, 0.0, 0.0])
+    ok, _ = s.pisoSteps(3)
+    assert ok
+    path = tmp_path / "ns.vtk"
+    s.exportToVtk(path, 2.0)
+    assert path.read_text() == expected_text(m, s.getVelocity(), s.getPressure(), 2.0)
+    # the optional boundary-force vectors equal computeShearStress / computePressureForces
+    path2 = tmp_path / "ns_forces.vtk"
+    s.exportToVtk(path2, 1.0, cf.VTK_SHEAR_STRESS | cf.VTK_PRESSURE_FORCES)
+    text = path2.read_text()
+    assert text.startswith(expected_text(m, s.getVelocity(), s.getPressure(), 1.0))
+    tail = text[len(expected_text(m, s.getVelocity(), s.getPressure(), 1.0)):].split("\n")
+    nv = m.sizes[0]
+    assert tail[0] == "" and tail[1] == "VECTORS shear_stress double"
+    sh = np.array([[float(x) for x in l.split()] for l in tail[2:2 + nv]])
+    assert np.allclose(sh, s.computeShearStress(), rtol=1e-5, atol=1e-300)
+    assert tail[2 + nv] == "" and tail[3 + nv] == "VECTORS pressure_forces double"
+    pf = np.array([[float(x) for x in l.split()] for l in tail[4 + nv:4 + 2 * nv]])
+    assert np.allclose(pf, s.computePressureForces(), rtol=1e-5, atol=1e-300)
