@@ -58,3 +58,43 @@ def test_vtk_export_matches_reference_format(cf, tmp_path):
     assert tail[2 + nv] == "" and tail[3 + nv] == "VECTORS pressure_forces double"
     pf = np.array([[float(x) for x in l.split()] for l in tail[4 + nv:4 + 2 * nv]])
     assert np.allclose(pf, s.computePressureForces(), rtol=1e-5, atol=1e-300)
+
+
+def test_yaml_cli_run_matches_api(cf, tmp_path):
+    """`simulation config.yaml` (the reference CLI's fluid-only loop) writes the VTK files of the
+    same run through the API: identical text at the last output step."""
+    import subprocess
+
+    from conftest import PKG
+
+    exe = PKG / "examples" / "simulation"
+    cfg = tmp_path / "cfg.yaml"
+    cfg.write_text(
+        "mesh:\n  type: cylinder\n  length: 30.0\n  radius: 2.0\n  rings: 3\n  layers: 12\n"
+        "  flow_direction: [1.0, 0.0, 0.0]\n"
+        "navier_stokes:\n  enabled: true\n  density: 1060.0\n  viscosity: 0.004\n"
+        "  inlet_velocity: [0.5, 0.0, 0.0]\n  outlet_pressure: 0.0\n  dt: 0.01\n  relax_p: 0.5\n"
+        "  relax_u: 0.5\n  tolerance: 1e-10\n  max_iterations: [5000, 50000]\n  pressure_solver: cg\n"
+        f"output:\n  prefix: {tmp_path / 'run'}\n  total_steps: 5\n  output_frequency: 2\n  vtk_scale: 1.0\n")
+    r = subprocess.run([str(exe), str(cfg)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    files = sorted(p.name for p in tmp_path.glob("run_*.vtk"))
+    assert files == ["run_0.vtk", "run_1.vtk", "run_2.vtk"]
+    m = cf.Mesh.cylinder(30.0, 2.0, 3, 12)
+    m.setupBoundaryConditions((1.0, 0.0, 0.0), 1.0)
+    s = cf.NavierStokesSolver()
+    s.setTolerance(1e-10)
+    s.setMaxIterations(5000, 50000)
+    s.setPressureSolver(cf.KRYLOV_CG)
+    s.initialize(m, cf.Fluid(1060.0, 0.004))
+    s.setMeanInletVelocity([0.5, 0.0, 0.0])
+    s.setOutletType(cf.OutletType.DirichletPressure)
+    s.setOutletPressure(0.0)
+    s.setRelaxP(0.5)
+    s.setRelaxU(0.5)
+    s.setDt(0.01)
+    for _ in range(5):
+        assert s.pisoStep()
+    api = tmp_path / "api.vtk"
+    s.exportToVtk(api, 1.0)
+    assert (tmp_path / "run_2.vtk").read_text() == api.read_text()
