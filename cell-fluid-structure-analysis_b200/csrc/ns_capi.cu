@@ -16,6 +16,7 @@
 #include <cstdint>
 #include <exception>
 #include <fstream>
+#include <map>
 #include <mutex>
 #include <new>
 #include <numeric>
@@ -131,6 +132,7 @@ struct cfsa_ns {
   // persistent CG
   bool cg_persistent = true;
   int cg_grid = 0;
+  std::map<const void *, int> stride_ctas_of;  // one resident wave of each grid-stride kernel
   // SMEM-resident variant of the persistent CG (k_cg_resident): one 1024-thread CTA per SM
   bool cg_resident = false;
   double *cg1_vec[3] = {nullptr, nullptr, nullptr};  // second r, w, s buffers of k_cg1_resident
@@ -470,6 +472,18 @@ struct cfsa_ns {
     {
       int nsm = 0, per_sm = 0;
       CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+      {  // one resident wave per grid-stride reduction kernel
+        auto q = [&](const void *fn) {
+          int o = 0;
+          CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, kBlock, 0));
+          stride_ctas_of[fn] = std::max(o, 1) * nsm;
+        };
+        q((const void *)k_mp_v);
+        q((const void *)k_mp_t);
+        q((const void *)k_mp_xr);
+        q((const void *)k_mp_inner_init);
+        q((const void *)k_mp_residual);
+      }
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent, kBlock, 0));
       const int nblk_sell = (int)blocks_for(s1.nrows_pad), nblk_nat = (int)blocks_for(nv);
       cg_grid = std::min(nsm * per_sm, std::max(nblk_sell, nblk_nat));
@@ -622,14 +636,27 @@ struct cfsa_ns {
     }
   }
 
+  // Grid of a grid-stride reduction kernel over nblk blocks of 256 positions. The FP32 mixed-
+  // precision kernels run one resident wave of CTAs that each visit several blocks (fewer
+  // CTA-wide barriers and tickets: measured 325 vs 355 us per inner iteration at 1M tets); the
+  // FP64 products keep one CTA per block, whose dynamic scheduling measured faster for them
+  // (435 vs 459 us per iteration) than a resident wave.
+  template <class K>
+  unsigned int strided(K kernel, unsigned int nblk) const {
+    auto it = stride_ctas_of.find((const void *)kernel);
+    if (it == stride_ctas_of.end()) return nblk;
+    const unsigned int need = (nblk + kMaxStride - 1) / kMaxStride;
+    return std::min(nblk, std::max(need, (unsigned int)it->second));
+  }
+
   template <int NC>
   void bicg_body(BicgArgs a, cudaStream_t s, int nrows_pad, int n) {
     const unsigned int gs = blocks_for(nrows_pad), gp = blocks_for(n);
     k_bicg_p<NC><<<gs, kBlock, 0, s>>>(a);
-    k_bicg_v<NC><<<gs, kBlock, 0, s>>>(a);
+    k_bicg_v<NC><<<strided(k_bicg_v<NC>, gs), kBlock, 0, s>>>(a);
     k_bicg_s<NC><<<gp, kBlock, 0, s>>>(a);
-    k_bicg_t<NC><<<gs, kBlock, 0, s>>>(a);
-    k_bicg_xr<NC><<<gp, kBlock, 0, s>>>(a);
+    k_bicg_t<NC><<<strided(k_bicg_t<NC>, gs), kBlock, 0, s>>>(a);
+    k_bicg_xr<NC><<<strided(k_bicg_xr<NC>, gp), kBlock, 0, s>>>(a);
   }
 
   bool poll_bicg(const BicgState *d) {
@@ -766,10 +793,10 @@ struct cfsa_ns {
       b.cond = h;
       b.use_cond = use;
       k_mp_p<<<gp, kBlock, 0, s>>>(b);
-      k_mp_v<<<gs, kBlock, 0, s>>>(b);
+      k_mp_v<<<strided(k_mp_v, gs), kBlock, 0, s>>>(b);
       k_mp_s<<<gp, kBlock, 0, s>>>(b);
-      k_mp_t<<<gs, kBlock, 0, s>>>(b);
-      k_mp_xr<<<gp, kBlock, 0, s>>>(b);
+      k_mp_t<<<strided(k_mp_t, gs), kBlock, 0, s>>>(b);
+      k_mp_xr<<<strided(k_mp_xr, gp), kBlock, 0, s>>>(b);
     };
     auto outer_body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
       MixedArgs b = a;
@@ -777,16 +804,16 @@ struct cfsa_ns {
         const cudaGraphConditionalHandle hin = new_cond_handle(s);
         b.cond = hin;
         b.use_cond = 1;
-        k_mp_inner_init<<<gp, kBlock, 0, s>>>(b);  // re-arms the inner loop every sweep
+        k_mp_inner_init<<<strided(k_mp_inner_init, gp), kBlock, 0, s>>>(b);  // re-arms the inner loop every sweep
         capture_while_with(s, body_stream2, hin, inner_body);
       } else {
-        k_mp_inner_init<<<gp, kBlock, 0, s>>>(b);
+        k_mp_inner_init<<<strided(k_mp_inner_init, gp), kBlock, 0, s>>>(b);
         eager_while(inner_body, [&] { return poll_mixed(true); }, mixed_inner_maxit);
       }
       b.cond = h;
       b.use_cond = use;
       k_mp_xupdate<<<gp, kBlock, 0, s>>>(b);
-      k_mp_residual<<<gs, kBlock, 0, s>>>(b);
+      k_mp_residual<<<strided(k_mp_residual, gs), kBlock, 0, s>>>(b);
     };
     if (capture)
       capture_while(outer_body);
@@ -1588,9 +1615,9 @@ struct cfsa_ns {
       a.st = nullptr;
       a.v = ws;  // scratch output
       const unsigned int g = blocks_for(s2.nrows_pad);
-      k_bicg_v<3><<<g, kBlock, 0, stream>>>(a);  // warm-up
+      k_bicg_v<3><<<strided(k_bicg_v<3>, g), kBlock, 0, stream>>>(a);  // warm-up
       CK(cudaEventRecord(ev0, stream));
-      for (int k = 0; k < iters; ++k) k_bicg_v<3><<<g, kBlock, 0, stream>>>(a);
+      for (int k = 0; k < iters; ++k) k_bicg_v<3><<<strided(k_bicg_v<3>, g), kBlock, 0, stream>>>(a);
       CK(cudaEventRecord(ev1, stream));
       *alg_bytes = 12.0 * (double)nnz2 + 8.0 * s2.nrows_pad + 4.0 * (s2.nslices + 1) + 72.0 * (double)N2;
     } else if (which == CFSA_KERNEL_PRESSURE_SPMV) {

@@ -80,36 +80,14 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Deterministic grid reduction of NV doubles per thread. Every block writes its partial;
-// the last block to arrive (ticket counter) sums the partials in block order and returns true
-// with the totals in `out` (valid in all threads of that block). Other blocks return false.
+// Second stage of the reduction tree, run by one block of 256 threads: the 256 accumulators
+// (accumulator t sums block partials t, t+256, ... in order) are combined by warp butterflies and an
+// in-order sum over the 8 warps; every thread gets the totals.
 template <int NV>
-__device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&out)[NV]) {
+__device__ __forceinline__ void combine_partials(const Reduce &red, unsigned int G, double (&out)[NV]) {
   __shared__ double sm[NV][kBlock / 32];
-  __shared__ bool last;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
-#pragma unroll
-  for (int j = 0; j < NV; ++j) {
-    double w = warp_sum(v[j]);
-    if (lane == 0) sm[j][warp] = w;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int j = 0; j < NV; ++j) {
-      double s = 0.0;
-      for (int w = 0; w < nwarps; ++w) s += sm[j][w];
-      red.partials[(size_t)blockIdx.x * kMaxRed + j] = s;
-    }
-    // release: this block's partials are visible to the block that takes the last ticket
-    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> ctr(*red.counter);
-    const unsigned int ticket = ctr.fetch_add(1u, cuda::memory_order_acq_rel);
-    last = (ticket == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last) return false;
-  __threadfence();
   // Thread t adds partials t, t+blockDim, ... in increasing order. Loads are issued in batches
   // before their additions so that the L2 latency is paid once per batch instead of once per
   // load; the order of the additions is unchanged. Few values: four blocks x all values per
@@ -117,7 +95,7 @@ __device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&out)[NV
   double acc[NV];
 #pragma unroll
   for (int j = 0; j < NV; ++j) acc[j] = 0.0;
-  const unsigned int G = gridDim.x, T = blockDim.x;
+  const unsigned int T = blockDim.x;
   if (NV <= 3) {
     unsigned int b = threadIdx.x;
     for (; b + 3 * T < G; b += 4 * T) {
@@ -165,6 +143,89 @@ __device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&out)[NV
     out[j] = s;
   }
   __syncthreads();
+}
+
+// Deterministic grid reduction of NV doubles per thread. Every block writes its partial;
+// the last block to arrive (ticket counter) sums the partials in block order and returns true
+// with the totals in `out` (valid in all threads of that block). Other blocks return false.
+template <int NV>
+__device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&out)[NV]) {
+  __shared__ double sm[NV][kBlock / 32];
+  __shared__ bool last;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double w = warp_sum(v[j]);
+    if (lane == 0) sm[j][warp] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double s = 0.0;
+      for (int w = 0; w < nwarps; ++w) s += sm[j][w];
+      red.partials[(size_t)blockIdx.x * kMaxRed + j] = s;
+    }
+    // release: this block's partials are visible to the block that takes the last ticket
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> ctr(*red.counter);
+    const unsigned int ticket = ctr.fetch_add(1u, cuda::memory_order_acq_rel);
+    last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  combine_partials<NV>(red, gridDim.x, out);
+  if (threadIdx.x == 0) *red.counter = 0u;
+  return true;
+}
+
+// Grid-stride form of grid_reduce for kernels whose CTAs each visit up to kMaxStride blocks of
+// 256 positions (blocks blockIdx.x, blockIdx.x + gridDim.x, ...). Each visited block leaves its 8
+// warp sums in shared memory (no block-wide synchronisation per block); at the end the CTA forms
+// the block partials (warp sums added in warp order, as grid_reduce does), writes them at their
+// block index, and the last CTA to take a ticket combines all nblk partials in the same tree.
+// Same tree, same bits as grid_reduce over one block per position block; fewer CTA-wide barriers
+// and nblk / kMaxStride tickets instead of nblk.
+constexpr int kMaxStride = 16;
+
+template <int NV>
+struct WarpSums {
+  double v[kMaxStride][NV][kBlock / 32];
+};
+
+template <int NV>
+__device__ __forceinline__ void warp_partial(const double (&v)[NV], WarpSums<NV> &S, int slot) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    const double w = warp_sum(v[j]);
+    if (lane == 0) S.v[slot][j][warp] = w;
+  }
+}
+
+template <int NV>
+__device__ bool grid_reduce_strided(WarpSums<NV> &S, int nslots, unsigned int nblk, const Reduce &red,
+                                    double (&out)[NV]) {
+  __shared__ bool last;
+  __syncthreads();
+  if ((int)threadIdx.x < nslots * NV) {
+    const int slot = threadIdx.x / NV, j = threadIdx.x % NV;
+    double s = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) s += S.v[slot][j][w];
+    red.partials[(size_t)(blockIdx.x + slot * gridDim.x) * kMaxRed + j] = s;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> ctr(*red.counter);
+    const unsigned int ticket = ctr.fetch_add(1u, cuda::memory_order_acq_rel);
+    last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  combine_partials<NV>(red, nblk, out);
   if (threadIdx.x == 0) *red.counter = 0u;
   return true;
 }

@@ -688,25 +688,31 @@ template <int NC>
 __global__ void k_bicg_v(BicgArgs A) {
   const int active = A.bs->active;
   if (!active) return;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  __shared__ WarpSums<NC> S;
+  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
   const int64_t n = A.n;
-  double part[NC];
+  int slot = 0;
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
+    const int r = b * kBlock + threadIdx.x;
+    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+    double part[NC];
 #pragma unroll
-  for (int c = 0; c < NC; ++c) part[c] = 0.0;
-  if (i >= 0) {
-    double acc[NC];
-    sell_spmv_row<NC>(A.S, A.At, A.pk, n, r, acc);
+    for (int c = 0; c < NC; ++c) part[c] = 0.0;
+    if (i >= 0) {
+      double acc[NC];
+      sell_spmv_row<NC>(A.S, A.At, A.pk, n, r, acc);
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      if (!((active >> c) & 1)) continue;
-      const int64_t o = c * n + i;
-      A.v[o] = acc[c];
-      part[c] = A.r0[o] * acc[c];
+      for (int c = 0; c < NC; ++c) {
+        if (!((active >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        A.v[o] = acc[c];
+        part[c] = A.r0[o] * acc[c];
+      }
     }
+    warp_partial<NC>(part, S, slot);
   }
   double tot[NC];
-  if (grid_reduce<NC>(part, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_strided<NC>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < NC; ++c) {
       if (!((active >> c) & 1)) continue;
       if (tot[c] == 0.0) {
@@ -740,26 +746,32 @@ template <int NC>
 __global__ void k_bicg_t(BicgArgs A) {
   const int active = A.bs->active;
   if (!active) return;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  __shared__ WarpSums<2 * NC> S;
+  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
   const int64_t n = A.n;
-  double part[2 * NC];
+  int slot = 0;
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
+    const int r = b * kBlock + threadIdx.x;
+    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+    double part[2 * NC];
 #pragma unroll
-  for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
-  if (i >= 0) {
-    double acc[NC];
-    sell_spmv_row<NC>(A.S, A.At, A.s, n, r, acc);
+    for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
+    if (i >= 0) {
+      double acc[NC];
+      sell_spmv_row<NC>(A.S, A.At, A.s, n, r, acc);
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      if (!((active >> c) & 1)) continue;
-      const int64_t o = c * n + i;
-      A.t[o] = acc[c];
-      part[c] = acc[c] * acc[c];
-      part[NC + c] = acc[c] * A.s[o];
+      for (int c = 0; c < NC; ++c) {
+        if (!((active >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        A.t[o] = acc[c];
+        part[c] = acc[c] * acc[c];
+        part[NC + c] = acc[c] * A.s[o];
+      }
     }
+    warp_partial<2 * NC>(part, S, slot);
   }
   double tot[2 * NC];
-  if (grid_reduce<2 * NC>(part, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_strided<2 * NC>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < NC; ++c) {
       if (!((active >> c) & 1)) continue;
       A.bs->omega[c] = (tot[c] > 0.0) ? tot[NC + c] / tot[c] : 0.0;
@@ -776,30 +788,36 @@ __global__ void k_bicg_xr(BicgArgs A) {
     if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0);
     return;
   }
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ WarpSums<2 * NC> S;
+  const int nblk = (A.n + kBlock - 1) / kBlock;
   const int64_t n = A.n;
-  double part[2 * NC];
+  int slot = 0;
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
+    const int i = b * kBlock + threadIdx.x;
+    double part[2 * NC];
 #pragma unroll
-  for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
-  if (i < A.n) {
-    const double dinv = A.invA[i];
-    const double w = A.cw ? A.cw[i] : 1.0;
+    for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
+    if (i < A.n) {
+      const double dinv = A.invA[i];
+      const double w = A.cw ? A.cw[i] : 1.0;
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      if (!((active >> c) & 1)) continue;
-      const int64_t o = c * n + i;
-      const double alpha = A.bs->alpha[c], omega = A.bs->omega[c];
-      const double y = dinv * A.pk[o];
-      const double z = dinv * A.s[o];
-      A.x[o] += alpha * y + omega * z;
-      const double ri = A.s[o] - omega * A.t[o];
-      A.r[o] = ri;
-      part[c] = (ri * ri) * w;
-      part[NC + c] = A.r0[o] * ri;
+      for (int c = 0; c < NC; ++c) {
+        if (!((active >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        const double alpha = A.bs->alpha[c], omega = A.bs->omega[c];
+        const double y = dinv * A.pk[o];
+        const double z = dinv * A.s[o];
+        A.x[o] += alpha * y + omega * z;
+        const double ri = A.s[o] - omega * A.t[o];
+        A.r[o] = ri;
+        part[c] = (ri * ri) * w;
+        part[NC + c] = A.r0[o] * ri;
+      }
     }
+    warp_partial<2 * NC>(part, S, slot);
   }
   double tot[2 * NC];
-  if (grid_reduce<2 * NC>(part, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_strided<2 * NC>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     BicgState *s = A.bs;
     const double eps = 2.220446049250313e-16;
     for (int c = 0; c < NC; ++c) {

@@ -136,28 +136,34 @@ __global__ void k_mp_inner_init(MixedArgs A) {
     }
     return;
   }
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n = A.n;
-  double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  if (i < A.n) {
-    const double w = A.cw32 ? (double)A.cw32[i] : 1.0;
+  __shared__ WarpSums<6> S;
+  const int nblk = (A.n + kBlock - 1) / kBlock;
+  int slot = 0;
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
+    const int i = b * kBlock + threadIdx.x;
+    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (i < A.n) {
+      const double w = A.cw32 ? (double)A.cw32[i] : 1.0;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int64_t o = c * n + i;
-      const float ri = (float)A.r64[o];
-      A.r[o] = ri;
-      A.r0[o] = ri;
-      A.p[o] = 0.f;
-      A.v[o] = 0.f;
-      A.dx[o] = 0.f;
-      if ((active >> c) & 1) {
-        part[c] = (double)ri * (double)ri;
-        part[3 + c] = ((double)ri * (double)ri) * w;
+      for (int c = 0; c < 3; ++c) {
+        const int64_t o = c * n + i;
+        const float ri = (float)A.r64[o];
+        A.r[o] = ri;
+        A.r0[o] = ri;
+        A.p[o] = 0.f;
+        A.v[o] = 0.f;
+        A.dx[o] = 0.f;
+        if ((active >> c) & 1) {
+          part[c] = (double)ri * (double)ri;
+          part[3 + c] = ((double)ri * (double)ri) * w;
+        }
       }
     }
+    warp_partial<6>(part, S, slot);
   }
   double tot[6];
-  if (grid_reduce<6>(part, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     MixedState *m = A.ms;
     m->in_active = 0;
     for (int c = 0; c < 3; ++c) {
@@ -195,22 +201,28 @@ __global__ void k_mp_p(MixedArgs A) {
 __global__ void k_mp_v(MixedArgs A) {
   const int act = A.ms->in_active;
   if (!act) return;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
   const int64_t n = A.n;
-  double part[3] = {0.0, 0.0, 0.0};
-  if (i >= 0) {
-    float acc[3];
-    sell_spmv_row_f32x3(A.S, A.At32, A.p, n, r, acc);
+  __shared__ WarpSums<3> S;
+  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
+  int slot = 0;
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
+    const int r = b * kBlock + threadIdx.x;
+    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+    double part[3] = {0.0, 0.0, 0.0};
+    if (i >= 0) {
+      float acc[3];
+      sell_spmv_row_f32x3(A.S, A.At32, A.p, n, r, acc);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (!((act >> c) & 1)) continue;
-      A.v[c * n + i] = acc[c];
-      part[c] = (double)A.r0[c * n + i] * (double)acc[c];
+      for (int c = 0; c < 3; ++c) {
+        if (!((act >> c) & 1)) continue;
+        A.v[c * n + i] = acc[c];
+        part[c] = (double)A.r0[c * n + i] * (double)acc[c];
+      }
     }
+    warp_partial<3>(part, S, slot);
   }
   double tot[3];
-  if (grid_reduce<3>(part, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_strided<3>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < 3; ++c) {
       if (!((act >> c) & 1)) continue;
       if (tot[c] == 0.0 || isnan(tot[c]))
@@ -240,23 +252,29 @@ __global__ void k_mp_s(MixedArgs A) {
 __global__ void k_mp_t(MixedArgs A) {
   const int act = A.ms->in_active;
   if (!act) return;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
   const int64_t n = A.n;
-  double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  if (i >= 0) {
-    float acc[3];
-    sell_spmv_row_f32x3(A.S, A.At32, A.s, n, r, acc);
+  __shared__ WarpSums<6> S;
+  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
+  int slot = 0;
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
+    const int r = b * kBlock + threadIdx.x;
+    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (i >= 0) {
+      float acc[3];
+      sell_spmv_row_f32x3(A.S, A.At32, A.s, n, r, acc);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (!((act >> c) & 1)) continue;
-      A.t[c * n + i] = acc[c];
-      part[c] = (double)acc[c] * (double)acc[c];
-      part[3 + c] = (double)acc[c] * (double)A.s[c * n + i];
+      for (int c = 0; c < 3; ++c) {
+        if (!((act >> c) & 1)) continue;
+        A.t[c * n + i] = acc[c];
+        part[c] = (double)acc[c] * (double)acc[c];
+        part[3 + c] = (double)acc[c] * (double)A.s[c * n + i];
+      }
     }
+    warp_partial<6>(part, S, slot);
   }
   double tot[6];
-  if (grid_reduce<6>(part, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < 3; ++c) {
       if (!((act >> c) & 1)) continue;
       A.ms->omega[c] = (tot[c] > 0.0) ? tot[3 + c] / tot[c] : 0.0;
@@ -272,26 +290,32 @@ __global__ void k_mp_xr(MixedArgs A) {
     if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0);
     return;
   }
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n = A.n;
-  double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  if (i < A.n) {
-    const float dinv = A.invA32[i];
-    const double w = A.cw32 ? (double)A.cw32[i] : 1.0;
+  __shared__ WarpSums<6> S;
+  const int nblk = (A.n + kBlock - 1) / kBlock;
+  int slot = 0;
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
+    const int i = b * kBlock + threadIdx.x;
+    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (i < A.n) {
+      const float dinv = A.invA32[i];
+      const double w = A.cw32 ? (double)A.cw32[i] : 1.0;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (!((act >> c) & 1)) continue;
-      const int64_t o = c * n + i;
-      const float alpha = (float)A.ms->alpha[c], omega = (float)A.ms->omega[c];
-      A.dx[o] += alpha * (dinv * A.p[o]) + omega * (dinv * A.s[o]);
-      const float ri = A.s[o] - omega * A.t[o];
-      A.r[o] = ri;
-      part[c] = ((double)ri * (double)ri) * w;
-      part[3 + c] = (double)A.r0[o] * (double)ri;
+      for (int c = 0; c < 3; ++c) {
+        if (!((act >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        const float alpha = (float)A.ms->alpha[c], omega = (float)A.ms->omega[c];
+        A.dx[o] += alpha * (dinv * A.p[o]) + omega * (dinv * A.s[o]);
+        const float ri = A.s[o] - omega * A.t[o];
+        A.r[o] = ri;
+        part[c] = ((double)ri * (double)ri) * w;
+        part[3 + c] = (double)A.r0[o] * (double)ri;
+      }
     }
+    warp_partial<6>(part, S, slot);
   }
   double tot[6];
-  if (grid_reduce<6>(part, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     MixedState *m = A.ms;
     const double eps = 2.220446049250313e-16;
     for (int c = 0; c < 3; ++c) {
@@ -340,24 +364,30 @@ __global__ void k_mp_residual(MixedArgs A) {
     if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0);
     return;
   }
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
   const int64_t n = A.n;
-  double part[3] = {0.0, 0.0, 0.0};
-  if (i >= 0) {
-    double acc[3];
-    sell_spmv_row<3>(A.S, A.At64, A.xs, n, r, acc);
-    const double w = A.cw ? A.cw[i] : 1.0;
+  __shared__ WarpSums<3> S;
+  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
+  int slot = 0;
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
+    const int r = b * kBlock + threadIdx.x;
+    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+    double part[3] = {0.0, 0.0, 0.0};
+    if (i >= 0) {
+      double acc[3];
+      sell_spmv_row<3>(A.S, A.At64, A.xs, n, r, acc);
+      const double w = A.cw ? A.cw[i] : 1.0;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (!((active >> c) & 1)) continue;
-      const double ri = A.b[c * n + i] - acc[c];
-      A.r64[c * n + i] = ri;
-      part[c] = (ri * ri) * w;
+      for (int c = 0; c < 3; ++c) {
+        if (!((active >> c) & 1)) continue;
+        const double ri = A.b[c * n + i] - acc[c];
+        A.r64[c * n + i] = ri;
+        part[c] = (ri * ri) * w;
+      }
     }
+    warp_partial<3>(part, S, slot);
   }
   double tot[3];
-  if (grid_reduce<3>(part, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_strided<3>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     MixedState *m = A.ms;
     for (int c = 0; c < 3; ++c) {
       if (!((active >> c) & 1)) continue;
