@@ -478,6 +478,8 @@ struct cfsa_ns {
           CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, kBlock, 0));
           stride_ctas_of[fn] = std::max(o, 1) * nsm;
         };
+        q((const void *)k_bicg_xr<3>);
+        q((const void *)k_bicg_xr<1>);
         q((const void *)k_mp_v);
         q((const void *)k_mp_t);
         q((const void *)k_mp_xr);
@@ -637,10 +639,10 @@ struct cfsa_ns {
   }
 
   // Grid of a grid-stride reduction kernel over nblk blocks of 256 positions. The FP32 mixed-
-  // precision kernels run one resident wave of CTAs that each visit several blocks (fewer
-  // CTA-wide barriers and tickets: measured 325 vs 355 us per inner iteration at 1M tets); the
-  // FP64 products keep one CTA per block, whose dynamic scheduling measured faster for them
-  // (435 vs 459 us per iteration) than a resident wave.
+  // precision kernels and the FP64 x/r update run one resident wave of CTAs that each visit
+  // several blocks (fewer CTA-wide barriers and tickets: 325 vs 355 us per FP32 inner iteration,
+  // 438 vs 448 us per FP64 iteration at 1M tets); the FP64 products keep one CTA per block, whose
+  // dynamic scheduling measured faster for them (a resident wave cost 6-14 us per iteration).
   template <class K>
   unsigned int strided(K kernel, unsigned int nblk) const {
     auto it = stride_ctas_of.find((const void *)kernel);
