@@ -32,8 +32,28 @@ struct Sell {
   int nrows = 0, nrows_pad = 0, nslices = 0;
   int64_t nentries = 0;
   std::vector<int> h_sptr;  // host copy of sptr
-  SellView view() const { return SellView{sptr, col, len, perm, nrows_pad}; }
+  int *rfirst = nullptr;    // slice runs of the run-walking kernels (one per SM)
+  double *spart = nullptr;  // their per-slice warp sums
+  int nruns = 0;
+  SellView view() const { return SellView{sptr, col, len, perm, nrows_pad, rfirst, spart}; }
 };
+
+// Entry-balanced runs of slices, one per CTA of a run-walking kernel, split on 256-row block
+// boundaries: run c starts at the first block boundary at or after c/nruns of the entries.
+std::vector<int> slice_runs(const std::vector<int> &sptr, int nslices, int nruns) {
+  std::vector<int> f(nruns + 1, 0);
+  const int64_t ne = sptr[nslices];
+  for (int c = 1; c < nruns; ++c) {
+    const int64_t target = ne * c / nruns;
+    int sl = (int)(std::lower_bound(sptr.begin(), sptr.begin() + nslices + 1, target,
+                                    [](int a, int64_t t) { return (int64_t)a < t; }) -
+                   sptr.begin());
+    sl = (sl + kSlicesPerBlock - 1) / kSlicesPerBlock * kSlicesPerBlock;
+    f[c] = std::max(f[c - 1], std::min(sl, nslices));
+  }
+  f[nruns] = nslices;
+  return f;
+}
 
 struct CudaError {
   std::string msg;
@@ -244,6 +264,13 @@ struct cfsa_ns {
     }
     S.nentries = sptr[S.nslices];
     S.h_sptr = sptr;
+    {
+      int nsm = 0;
+      CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+      S.nruns = std::max(1, nsm);
+      S.rfirst = dupload(slice_runs(sptr, S.nslices, S.nruns));
+      S.spart = dalloc<double>((size_t)S.nslices * kMaxRed);
+    }
     S.perm = dupload(perm);
     S.len = dupload(len);
     S.sptr = dupload(sptr);
@@ -480,11 +507,8 @@ struct cfsa_ns {
         };
         q((const void *)k_bicg_xr<3>);
         q((const void *)k_bicg_xr<1>);
-        q((const void *)k_mp_v);
-        q((const void *)k_mp_t);
         q((const void *)k_mp_xr);
         q((const void *)k_mp_inner_init);
-        q((const void *)k_mp_residual);
       }
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent, kBlock, 0));
       const int nblk_sell = (int)blocks_for(s1.nrows_pad), nblk_nat = (int)blocks_for(nv);
@@ -639,10 +663,10 @@ struct cfsa_ns {
   }
 
   // Grid of a grid-stride reduction kernel over nblk blocks of 256 positions. The FP32 mixed-
-  // precision kernels and the FP64 x/r update run one resident wave of CTAs that each visit
+  // precision x/r update and the FP64 x/r update run one resident wave of CTAs that each visit
   // several blocks (fewer CTA-wide barriers and tickets: 325 vs 355 us per FP32 inner iteration,
-  // 438 vs 448 us per FP64 iteration at 1M tets); the FP64 products keep one CTA per block, whose
-  // dynamic scheduling measured faster for them (a resident wave cost 6-14 us per iteration).
+  // 438 vs 448 us per FP64 iteration at 1M tets). The SELL products of the Krylov loops are
+  // run-walking kernels instead (one kRunThreads CTA per SM over a contiguous run of slices).
   template <class K>
   unsigned int strided(K kernel, unsigned int nblk) const {
     auto it = stride_ctas_of.find((const void *)kernel);
@@ -652,12 +676,12 @@ struct cfsa_ns {
   }
 
   template <int NC>
-  void bicg_body(BicgArgs a, cudaStream_t s, int nrows_pad, int n) {
-    const unsigned int gs = blocks_for(nrows_pad), gp = blocks_for(n);
+  void bicg_body(BicgArgs a, cudaStream_t s, const Sell &S, int n) {
+    const unsigned int gs = blocks_for(S.nrows_pad), gp = blocks_for(n);
     k_bicg_p<NC><<<gs, kBlock, 0, s>>>(a);
-    k_bicg_v<NC><<<strided(k_bicg_v<NC>, gs), kBlock, 0, s>>>(a);
+    k_bicg_v<NC><<<S.nruns, kRunThreads, 0, s>>>(a);
     k_bicg_s<NC><<<gp, kBlock, 0, s>>>(a);
-    k_bicg_t<NC><<<strided(k_bicg_t<NC>, gs), kBlock, 0, s>>>(a);
+    k_bicg_t<NC><<<S.nruns, kRunThreads, 0, s>>>(a);
     k_bicg_xr<NC><<<strided(k_bicg_xr<NC>, gp), kBlock, 0, s>>>(a);
   }
 
@@ -745,7 +769,7 @@ struct cfsa_ns {
       BicgArgs b = a;
       b.cond = h;
       b.use_cond = use;
-      bicg_body<3>(b, s, s2.nrows_pad, (int)N2);
+      bicg_body<3>(b, s, s2, (int)N2);
     };
     if (capture)
       capture_while(body);
@@ -787,7 +811,7 @@ struct cfsa_ns {
   // loops are nested WHILE nodes when captured.
   void enqueue_momentum_mixed(bool capture, double *x, DevStatus *s_out) {
     const MixedArgs a = mixed_args(x, s_out);
-    const unsigned int gp = blocks_for(N2), gs = blocks_for(s2.nrows_pad);
+    const unsigned int gp = blocks_for(N2);
     k_mp_outer_init<<<gp, kBlock, 0, stream>>>(a, tol_mom, mixed_max_outer, mixed_inner_tol, mixed_inner_maxit);
     CK(cudaGetLastError());
     auto inner_body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
@@ -795,9 +819,9 @@ struct cfsa_ns {
       b.cond = h;
       b.use_cond = use;
       k_mp_p<<<gp, kBlock, 0, s>>>(b);
-      k_mp_v<<<strided(k_mp_v, gs), kBlock, 0, s>>>(b);
+      k_mp_v<<<s2.nruns, kRunThreads, 0, s>>>(b);
       k_mp_s<<<gp, kBlock, 0, s>>>(b);
-      k_mp_t<<<strided(k_mp_t, gs), kBlock, 0, s>>>(b);
+      k_mp_t<<<s2.nruns, kRunThreads, 0, s>>>(b);
       k_mp_xr<<<strided(k_mp_xr, gp), kBlock, 0, s>>>(b);
     };
     auto outer_body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
@@ -815,7 +839,7 @@ struct cfsa_ns {
       b.cond = h;
       b.use_cond = use;
       k_mp_xupdate<<<gp, kBlock, 0, s>>>(b);
-      k_mp_residual<<<strided(k_mp_residual, gs), kBlock, 0, s>>>(b);
+      k_mp_residual<<<s2.nruns, kRunThreads, 0, s>>>(b);
     };
     if (capture)
       capture_while(outer_body);
@@ -896,7 +920,7 @@ struct cfsa_ns {
         BicgArgs c = b;
         c.cond = h;
         c.use_cond = use;
-        bicg_body<1>(c, s, s1.nrows_pad, (int)nv);
+        bicg_body<1>(c, s, s1, (int)nv);
       };
       if (capture)
         capture_while(body);
@@ -1616,10 +1640,9 @@ struct cfsa_ns {
       a.bs = bs_prof;
       a.st = nullptr;
       a.v = ws;  // scratch output
-      const unsigned int g = blocks_for(s2.nrows_pad);
-      k_bicg_v<3><<<strided(k_bicg_v<3>, g), kBlock, 0, stream>>>(a);  // warm-up
+      k_bicg_v<3><<<s2.nruns, kRunThreads, 0, stream>>>(a);  // warm-up
       CK(cudaEventRecord(ev0, stream));
-      for (int k = 0; k < iters; ++k) k_bicg_v<3><<<strided(k_bicg_v<3>, g), kBlock, 0, stream>>>(a);
+      for (int k = 0; k < iters; ++k) k_bicg_v<3><<<s2.nruns, kRunThreads, 0, stream>>>(a);
       CK(cudaEventRecord(ev1, stream));
       *alg_bytes = 12.0 * (double)nnz2 + 8.0 * s2.nrows_pad + 4.0 * (s2.nslices + 1) + 72.0 * (double)N2;
     } else if (which == CFSA_KERNEL_PRESSURE_SPMV) {

@@ -685,16 +685,14 @@ __global__ void k_bicg_p(BicgArgs A) {
 
 // K2: v = At p, alpha = rho / (r0 . v)
 template <int NC>
-__global__ void k_bicg_v(BicgArgs A) {
+__global__ void __launch_bounds__(kRunThreads, 1) k_bicg_v(BicgArgs A) {
   const int active = A.bs->active;
   if (!active) return;
-  __shared__ WarpSums<NC> S;
-  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
   const int64_t n = A.n;
-  int slot = 0;
-  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
-    const int r = b * kBlock + threadIdx.x;
-    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  const int s1 = A.S.rfirst[blockIdx.x + 1];
+  for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+    const int r = sl * kSellC + (threadIdx.x & 31);
+    const int i = A.S.perm[r];
     double part[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) part[c] = 0.0;
@@ -709,10 +707,10 @@ __global__ void k_bicg_v(BicgArgs A) {
         part[c] = A.r0[o] * acc[c];
       }
     }
-    warp_partial<NC>(part, S, slot);
+    slice_partial<NC>(part, A.S, sl);
   }
   double tot[NC];
-  if (grid_reduce_strided<NC>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_runs<NC>(A.S, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < NC; ++c) {
       if (!((active >> c) & 1)) continue;
       if (tot[c] == 0.0) {
@@ -743,16 +741,14 @@ __global__ void k_bicg_s(BicgArgs A) {
 
 // K4: t = At s, omega = (t . s) / (t . t) (0 when t . t == 0)
 template <int NC>
-__global__ void k_bicg_t(BicgArgs A) {
+__global__ void __launch_bounds__(kRunThreads, 1) k_bicg_t(BicgArgs A) {
   const int active = A.bs->active;
   if (!active) return;
-  __shared__ WarpSums<2 * NC> S;
-  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
   const int64_t n = A.n;
-  int slot = 0;
-  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
-    const int r = b * kBlock + threadIdx.x;
-    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  const int s1 = A.S.rfirst[blockIdx.x + 1];
+  for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+    const int r = sl * kSellC + (threadIdx.x & 31);
+    const int i = A.S.perm[r];
     double part[2 * NC];
 #pragma unroll
     for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
@@ -768,10 +764,10 @@ __global__ void k_bicg_t(BicgArgs A) {
         part[NC + c] = acc[c] * A.s[o];
       }
     }
-    warp_partial<2 * NC>(part, S, slot);
+    slice_partial<2 * NC>(part, A.S, sl);
   }
   double tot[2 * NC];
-  if (grid_reduce_strided<2 * NC>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_runs<2 * NC>(A.S, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < NC; ++c) {
       if (!((active >> c) & 1)) continue;
       A.bs->omega[c] = (tot[c] > 0.0) ? tot[NC + c] / tot[c] : 0.0;

@@ -198,16 +198,14 @@ __global__ void k_mp_p(MixedArgs A) {
 }
 
 // K2: v = At32 p, alpha = rho / (r0 . v)
-__global__ void k_mp_v(MixedArgs A) {
+__global__ void __launch_bounds__(kRunThreads, 1) k_mp_v(MixedArgs A) {
   const int act = A.ms->in_active;
   if (!act) return;
   const int64_t n = A.n;
-  __shared__ WarpSums<3> S;
-  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
-  int slot = 0;
-  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
-    const int r = b * kBlock + threadIdx.x;
-    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  const int s1 = A.S.rfirst[blockIdx.x + 1];
+  for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+    const int r = sl * kSellC + (threadIdx.x & 31);
+    const int i = A.S.perm[r];
     double part[3] = {0.0, 0.0, 0.0};
     if (i >= 0) {
       float acc[3];
@@ -219,10 +217,10 @@ __global__ void k_mp_v(MixedArgs A) {
         part[c] = (double)A.r0[c * n + i] * (double)acc[c];
       }
     }
-    warp_partial<3>(part, S, slot);
+    slice_partial<3>(part, A.S, sl);
   }
   double tot[3];
-  if (grid_reduce_strided<3>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_runs<3>(A.S, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < 3; ++c) {
       if (!((act >> c) & 1)) continue;
       if (tot[c] == 0.0 || isnan(tot[c]))
@@ -249,16 +247,14 @@ __global__ void k_mp_s(MixedArgs A) {
 }
 
 // K4: t = At32 s, omega = (t . s) / (t . t)
-__global__ void k_mp_t(MixedArgs A) {
+__global__ void __launch_bounds__(kRunThreads, 1) k_mp_t(MixedArgs A) {
   const int act = A.ms->in_active;
   if (!act) return;
   const int64_t n = A.n;
-  __shared__ WarpSums<6> S;
-  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
-  int slot = 0;
-  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
-    const int r = b * kBlock + threadIdx.x;
-    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  const int s1 = A.S.rfirst[blockIdx.x + 1];
+  for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+    const int r = sl * kSellC + (threadIdx.x & 31);
+    const int i = A.S.perm[r];
     double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (i >= 0) {
       float acc[3];
@@ -271,10 +267,10 @@ __global__ void k_mp_t(MixedArgs A) {
         part[3 + c] = (double)acc[c] * (double)A.s[c * n + i];
       }
     }
-    warp_partial<6>(part, S, slot);
+    slice_partial<6>(part, A.S, sl);
   }
   double tot[6];
-  if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_runs<6>(A.S, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < 3; ++c) {
       if (!((act >> c) & 1)) continue;
       A.ms->omega[c] = (tot[c] > 0.0) ? tot[3 + c] / tot[c] : 0.0;
@@ -357,7 +353,7 @@ __global__ void k_mp_xupdate(MixedArgs A) {
 }
 
 // r64 = b - At64 (D x) (FP64 true residual); outer convergence and loop condition.
-__global__ void k_mp_residual(MixedArgs A) {
+__global__ void __launch_bounds__(kRunThreads, 1) k_mp_residual(MixedArgs A) {
   const int active = A.ms->active;
   if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[2] += 1;
   if (!active) {
@@ -365,12 +361,10 @@ __global__ void k_mp_residual(MixedArgs A) {
     return;
   }
   const int64_t n = A.n;
-  __shared__ WarpSums<3> S;
-  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
-  int slot = 0;
-  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
-    const int r = b * kBlock + threadIdx.x;
-    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  const int s1 = A.S.rfirst[blockIdx.x + 1];
+  for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+    const int r = sl * kSellC + (threadIdx.x & 31);
+    const int i = A.S.perm[r];
     double part[3] = {0.0, 0.0, 0.0};
     if (i >= 0) {
       double acc[3];
@@ -384,10 +378,10 @@ __global__ void k_mp_residual(MixedArgs A) {
         part[c] = (ri * ri) * w;
       }
     }
-    warp_partial<3>(part, S, slot);
+    slice_partial<3>(part, A.S, sl);
   }
   double tot[3];
-  if (grid_reduce_strided<3>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_runs<3>(A.S, A.red, tot) && threadIdx.x == 0) {
     MixedState *m = A.ms;
     for (int c = 0; c < 3; ++c) {
       if (!((active >> c) & 1)) continue;
