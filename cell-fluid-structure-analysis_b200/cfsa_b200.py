@@ -25,7 +25,7 @@ OK, NOT_CONVERGED, BREAKDOWN, NAN, CUDA_ERROR, BAD_ARG, NOT_INITIALIZED, UNSUPPO
 
 MAT_MASS, MAT_STIFFNESS, MAT_GRAD_X, MAT_GRAD_Y, MAT_GRAD_Z, MAT_POISSON, MAT_MOMENTUM, MAT_POISSON_BC = range(8)
 KERNEL_MOMENTUM_SPMV, KERNEL_PRESSURE_SPMV = 0, 1
-KRYLOV_CG, KRYLOV_BICGSTAB, KRYLOV_CG1 = 0, 1, 2
+KRYLOV_CG, KRYLOV_BICGSTAB, KRYLOV_CG1, KRYLOV_CG2L = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 NORM_REFERENCE, NORM_JACOBI = 0, 1
 OBJECTIVE_WALL_SHEAR, OBJECTIVE_PRESSURE_DROP = 0, 1
@@ -177,6 +177,8 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "cfsa_ns_set_inlet_uniform": (i32, [vp, vp]),
         "cfsa_ns_set_inlet_profile": (i32, [vp, vp]),
         "cfsa_ns_set_pressure_solver": (i32, [vp, i32]),
+        "cfsa_ns_set_coarse_target": (i32, [vp, i32]),
+        "cfsa_ns_get_coarse_size": (i32, [vp, vp]),
         "cfsa_ns_set_precision": (i32, [vp, i32]),
         "cfsa_ns_set_convergence_norm": (i32, [vp, i32]),
         "cfsa_ns_set_viscosity": (i32, [vp, dbl]),
@@ -392,6 +394,7 @@ class NavierStokesSolver:
         self.mean_inlet_velocity = np.zeros(3)
         self.inlet_profile = None
         self.krylov = KRYLOV_CG
+        self.coarse_target = 256
         self.precision = PRECISION_FP64
         self.conv_norm = NORM_REFERENCE
         self.N2 = self.nv = self.ne = self.nt = 0
@@ -422,6 +425,7 @@ class NavierStokesSolver:
         self._check(L.cfsa_ns_set_outlet(h, int(self.outlet_type), float(self.outlet_pressure)))
         self._check(L.cfsa_ns_set_reference_node(h, int(self.reference_node)))
         self._check(L.cfsa_ns_set_pressure_solver(h, int(self.krylov)))
+        self._check(L.cfsa_ns_set_coarse_target(h, int(self.coarse_target)))
         self._check(L.cfsa_ns_set_precision(h, int(self.precision)))
         self._check(L.cfsa_ns_set_convergence_norm(h, int(self.conv_norm)))
         self._push_inlet()
@@ -721,6 +725,18 @@ class NavierStokesSolver:
         self.krylov = int(krylov)
         if self._h is not None:
             self._check(self._lib.cfsa_ns_set_pressure_solver(self._h, self.krylov))
+
+    def setCoarseTarget(self, target: int):
+        """Aggregate count of the KRYLOV_CG2L coarse space (default 256)."""
+        self.coarse_target = int(target)
+        if self._h is not None:
+            self._check(self._lib.cfsa_ns_set_coarse_target(self._h, self.coarse_target))
+
+    def coarseSize(self) -> int:
+        """Aggregates of the current KRYLOV_CG2L coarse space (0 for the other methods)."""
+        nc = C.c_int()
+        self._check(self._lib.cfsa_ns_get_coarse_size(self._h, C.byref(nc)))
+        return nc.value
 
     def setPrecision(self, precision: int):
         self.precision = int(precision)

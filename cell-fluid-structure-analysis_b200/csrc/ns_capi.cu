@@ -160,6 +160,14 @@ struct cfsa_ns {
   size_t cg_res_smem = 0;
   unsigned int *bar_count = nullptr, *bar_gen = nullptr;
   int *bar_err = nullptr;
+  // two-level pressure preconditioner of k_cg2l_resident (rebuilt with the Poisson operator)
+  int coarse_target = 256;
+  bool coarse_dirty = true;
+  int coarse_nc = 0, coarse_np = 0;
+  std::vector<void *> coarse_allocs;
+  CoarseView coarse_view{};
+  int cg2l_col_cap = 0;
+  size_t cg2l_smem = 0;
   double *cg_part_a = nullptr, *cg_part_b = nullptr;
   // mixed precision (FP32 inner Krylov in FP64 defect correction)
   float *At32 = nullptr, *invA32 = nullptr;
@@ -220,6 +228,7 @@ struct cfsa_ns {
   ~cfsa_ns() {
     if (adj_exec) cudaGraphExecDestroy(adj_exec);
     for (void *ptr : rec_allocs) cudaFree(ptr);
+    for (void *ptr : coarse_allocs) cudaFree(ptr);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     for (void *ptr : allocs) cudaFree(ptr);
@@ -598,7 +607,245 @@ struct cfsa_ns {
                                                               rows1, ci1, Lv, bc, invL, Ls, Lt);
       CK(cudaGetLastError());
       poisson_dirty = false;
+      coarse_dirty = true;
     }
+    if (krylov == CFSA_KRYLOV_CG2L && coarse_dirty) build_coarse();
+  }
+
+  // ------------------------------------------------------------------ two-level preconditioner
+  // Coarse space of k_cg2l_resident: geometric aggregates over the vertices without a penalty
+  // row, Z = (P^T L P)^-1 by Cholesky, and the index lists of the aggregate sums. Every step of
+  // the construction is fixed in order (the oracle's build_coarse follows the same steps), so the
+  // device and oracle solves agree bit for bit.
+  //   box edge h_k = e c^k, e the largest extent of the bounding box of the unpenalised vertices,
+  //   c = 2^-1/4, k in [0, 64] the smallest exponent (bisection) with >= coarse_target occupied
+  //   boxes; boxes numbered by first vertex; an A_c that is not SPD disables the coarse part.
+  template <class T>
+  T *cupload(const std::vector<T> &h) {
+    void *ptr = nullptr;
+    CK(cudaMalloc(&ptr, std::max<size_t>(h.size(), 1) * sizeof(T)));
+    coarse_allocs.push_back(ptr);
+    if (!h.empty()) CK(cudaMemcpyAsync(ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    return static_cast<T *>(ptr);
+  }
+
+  static int count_boxes(const std::vector<double> &xyz, const std::vector<char> &pen, int64_t n,
+                         double h, const double lo[3], std::vector<int64_t> *keys_out) {
+    std::vector<int64_t> keys;
+    keys.reserve(n);
+    for (int64_t i = 0; i < n; ++i) {
+      if (pen[i]) continue;
+      const int64_t ix = (int64_t)std::floor((xyz[3 * i] - lo[0]) / h);
+      const int64_t iy = (int64_t)std::floor((xyz[3 * i + 1] - lo[1]) / h);
+      const int64_t iz = (int64_t)std::floor((xyz[3 * i + 2] - lo[2]) / h);
+      keys.push_back((ix * 2097152 + iy) * 2097152 + iz);
+    }
+    if (keys_out) *keys_out = keys;
+    std::sort(keys.begin(), keys.end());
+    return (int)(std::unique(keys.begin(), keys.end()) - keys.begin());
+  }
+
+  void build_coarse() {
+    CK(cudaStreamSynchronize(stream));
+    for (void *q : coarse_allocs) CK(cudaFree(q));
+    coarse_allocs.clear();
+    const int64_t n = nv;
+    std::vector<char> pen(n, 0);
+    if (outlet_type == CFSA_OUTLET_NEUMANN) {
+      if (ref_node >= 0 && ref_node < n) pen[ref_node] = 1;
+    } else if (outlet_type == CFSA_OUTLET_DIRICHLET) {
+      for (int64_t i = 0; i < n; ++i) pen[i] = h_bc[i] == BC_OUTLET;
+    }
+    std::vector<int> agg(n, 0);
+    int nc = 0;
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool any = false;
+    for (int64_t i = 0; i < n; ++i) {
+      if (pen[i]) continue;
+      for (int d = 0; d < 3; ++d) {
+        const double x = h_xyz[3 * i + d];
+        if (!any) lo[d] = hi[d] = x;
+        lo[d] = std::min(lo[d], x);
+        hi[d] = std::max(hi[d], x);
+      }
+      any = true;
+    }
+    const double e = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+    if (any && e > 0.0 && coarse_target >= 1) {
+      auto h_of = [&](int k) {
+        double h = e;
+        for (int q = 0; q < k; ++q) h = h * 0.8408964152537145;  // 2^-1/4
+        return h;
+      };
+      int klo = 0, khi = 64;
+      while (klo < khi) {
+        const int km = (klo + khi) / 2;
+        if (count_boxes(h_xyz, pen, n, h_of(km), lo, nullptr) >= coarse_target)
+          khi = km;
+        else
+          klo = km + 1;
+      }
+      std::vector<int64_t> keys;
+      count_boxes(h_xyz, pen, n, h_of(klo), lo, &keys);
+      // number the boxes by their first vertex
+      std::vector<std::pair<int64_t, int>> kv(keys.size());
+      for (size_t q = 0; q < keys.size(); ++q) kv[q] = {keys[q], (int)q};
+      std::stable_sort(kv.begin(), kv.end(), [](const std::pair<int64_t, int> &a, const std::pair<int64_t, int> &b) {
+        return a.first < b.first;
+      });
+      std::vector<std::pair<int, int>> firsts;  // (first vertex rank, start in kv)
+      for (size_t q = 0; q < kv.size();) {
+        size_t r = q;
+        while (r < kv.size() && kv[r].first == kv[q].first) ++r;
+        firsts.push_back({kv[q].second, (int)q});
+        q = r;
+      }
+      std::sort(firsts.begin(), firsts.end());
+      std::vector<int> id_sorted(kv.size()), id_of(keys.size());
+      for (size_t gq = 0; gq < firsts.size(); ++gq) {
+        size_t q = firsts[gq].second;
+        const int64_t key = kv[q].first;
+        while (q < kv.size() && kv[q].first == key) id_sorted[q++] = (int)gq;
+      }
+      for (size_t q = 0; q < kv.size(); ++q) id_of[kv[q].second] = id_sorted[q];
+      nc = (int)firsts.size();
+      size_t q = 0;
+      for (int64_t i = 0; i < n; ++i) agg[i] = pen[i] ? nc : id_of[q++];
+    }
+    std::vector<double> Z;
+    if (nc > 0) {
+      // A_c = P^T L P over the unpenalised rows (the penalties sit on penalised rows only)
+      std::vector<int> ci((size_t)nnz1);
+      std::vector<double> lv((size_t)nnz1);
+      CK(cudaMemcpyAsync(ci.data(), ci1, (size_t)nnz1 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      CK(cudaMemcpyAsync(lv.data(), Lv, (size_t)nnz1 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      std::vector<double> Ac((size_t)nc * nc, 0.0), G((size_t)nc * nc, 0.0), Gi((size_t)nc * nc, 0.0);
+      for (int64_t i = 0; i < n; ++i) {
+        if (agg[i] >= nc) continue;
+        for (int k = h_rp1[i]; k < h_rp1[i + 1]; ++k) {
+          const int j = ci[k];
+          if (agg[j] >= nc) continue;
+          double &a = Ac[(size_t)agg[i] * nc + agg[j]];
+          a = a + lv[k];
+        }
+      }
+      bool spd = true;
+      for (int i = 0; i < nc && spd; ++i)
+        for (int j = 0; j <= i; ++j) {
+          double sum = Ac[(size_t)i * nc + j];
+          for (int k = 0; k < j; ++k) sum = sum - G[(size_t)i * nc + k] * G[(size_t)j * nc + k];
+          if (i == j) {
+            if (!(sum > 0.0)) {
+              spd = false;
+              break;
+            }
+            G[(size_t)i * nc + i] = std::sqrt(sum);
+          } else {
+            G[(size_t)i * nc + j] = sum / G[(size_t)j * nc + j];
+          }
+        }
+      if (!spd) {
+        nc = 0;
+        std::fill(agg.begin(), agg.end(), 0);
+      } else {
+        for (int j = 0; j < nc; ++j) {
+          Gi[(size_t)j * nc + j] = 1.0 / G[(size_t)j * nc + j];
+          for (int i = j + 1; i < nc; ++i) {
+            double sum = 0.0;
+            for (int k = j; k < i; ++k) sum = sum - G[(size_t)i * nc + k] * Gi[(size_t)k * nc + j];
+            Gi[(size_t)i * nc + j] = sum / G[(size_t)i * nc + i];
+          }
+        }
+        Z.assign((size_t)nc * nc, 0.0);
+        for (int m = 0; m < nc; ++m)
+          for (int k = 0; k < nc; ++k) {
+            double sum = 0.0;
+            for (int q = std::max(m, k); q < nc; ++q) sum = sum + Gi[(size_t)q * nc + m] * Gi[(size_t)q * nc + k];
+            Z[(size_t)m * nc + k] = sum;
+          }
+      }
+    }
+    // aggregates of each natural block, block-partial slots of each aggregate
+    const int nblk = (int)blocks_for(n);
+    std::vector<int> blk_ptr(nblk + 1, 0), blk_agg;
+    for (int b = 0; b < nblk; ++b) {
+      std::vector<int> ms;
+      for (int64_t i = (int64_t)kBlock * b; i < std::min<int64_t>(n, (int64_t)kBlock * (b + 1)); ++i)
+        if (agg[i] < nc) ms.push_back(agg[i]);
+      std::sort(ms.begin(), ms.end());
+      ms.erase(std::unique(ms.begin(), ms.end()), ms.end());
+      blk_agg.insert(blk_agg.end(), ms.begin(), ms.end());
+      blk_ptr[b + 1] = (int)blk_agg.size();
+    }
+    const int np = (int)blk_agg.size();
+    std::vector<int> agg_ptr(nc + 1, 0), blk_slot(np, 0);
+    for (int m : blk_agg) agg_ptr[m + 1]++;
+    for (int m = 0; m < nc; ++m) agg_ptr[m + 1] += agg_ptr[m];
+    {
+      std::vector<int> fill(agg_ptr.begin(), agg_ptr.begin() + nc);
+      for (int q = 0; q < np; ++q) blk_slot[q] = fill[blk_agg[q]]++;
+    }
+    // aggregates each CTA reads: those of its rows and of their columns
+    std::vector<int> need_ptr(cg_res_grid + 1, 0), need;
+    if (nc > 0) {
+      std::vector<int> ci((size_t)nnz1);
+      CK(cudaMemcpyAsync(ci.data(), ci1, (size_t)nnz1 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      const int nblk_sell = (int)blocks_for(s1.nrows_pad);
+      for (int c = 0; c < cg_res_grid; ++c) {
+        const int b0 = std::min(nblk_sell, c * cg_res_bpc_sell), b1 = std::min(nblk_sell, b0 + cg_res_bpc_sell);
+        std::vector<int> ms;
+        for (int64_t i = (int64_t)kBlock * b0; i < std::min<int64_t>(n, (int64_t)kBlock * b1); ++i) {
+          if (agg[i] < nc) ms.push_back(agg[i]);
+          for (int k = h_rp1[i]; k < h_rp1[i + 1]; ++k)
+            if (agg[ci[k]] < nc) ms.push_back(agg[ci[k]]);
+        }
+        std::sort(ms.begin(), ms.end());
+        ms.erase(std::unique(ms.begin(), ms.end()), ms.end());
+        need.insert(need.end(), ms.begin(), ms.end());
+        need_ptr[c + 1] = (int)need.size();
+      }
+    }
+    CoarseView V{};
+    V.nc = nc;
+    V.agg = cupload(agg);
+    V.Z = cupload(Z);
+    V.blk_ptr = cupload(blk_ptr);
+    V.blk_agg = cupload(blk_agg);
+    V.agg_ptr = cupload(agg_ptr);
+    V.blk_slot = cupload(blk_slot);
+    V.need_ptr = cupload(need_ptr);
+    V.need = cupload(need);
+    V.np = np;
+    for (int q = 0; q < 2; ++q) V.part[q] = cupload(std::vector<double>((size_t)3 * std::max(np, 1), 0.0));
+    // shared memory: coarse arrays, row staging, then as many column indices as fit
+    int optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, k_cg2l_resident));
+    const int64_t coarse_bytes = (int64_t)(6 * nc + 2) * (int64_t)sizeof(double);
+    const int64_t row_bytes = (int64_t)3 * cg_res_bpc_sell * kBlock * (int64_t)sizeof(int);
+    const int64_t avail = (int64_t)optin - (int64_t)fa.sharedSizeBytes - coarse_bytes - row_bytes;
+    if (avail < 0) throw CudaError{"two-level pressure preconditioner: coarse space too large for shared memory"};
+    int max_entries = 0;
+    const int nblk_sell = (int)blocks_for(s1.nrows_pad);
+    for (int c = 0; c < cg_res_grid; ++c) {
+      const int b0 = std::min(nblk_sell, c * cg_res_bpc_sell), b1 = std::min(nblk_sell, b0 + cg_res_bpc_sell);
+      if (b1 > b0) max_entries = std::max(max_entries, s1.h_sptr[std::min(8 * b1, s1.nslices)] - s1.h_sptr[8 * b0]);
+    }
+    cg2l_col_cap = (int)std::min<int64_t>(max_entries, avail / (int64_t)sizeof(int));
+    cg2l_smem = (size_t)(coarse_bytes + row_bytes + (int64_t)cg2l_col_cap * (int64_t)sizeof(int));
+    CK(cudaFuncSetAttribute(k_cg2l_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cg2l_smem));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg2l_resident, kCgResThreads, cg2l_smem));
+    if (per_sm < 1) throw CudaError{"two-level pressure preconditioner: kernel does not fit on an SM"};
+    CK(cudaStreamSynchronize(stream));
+    coarse_view = V;
+    coarse_nc = nc;
+    coarse_np = np;
+    coarse_dirty = false;
+    graph_dirty = true;
   }
 
   // ------------------------------------------------------------------ Krylov loops
@@ -927,7 +1174,7 @@ struct cfsa_ns {
       else
         eager_while(body, [&] { return poll_bicg(bs_p); }, maxit_p);
       k_check_bicg<<<1, 1, 0, stream>>>(bs_p, 1, 1, s_out);
-    } else if (cg_persistent || krylov == CFSA_KRYLOV_CG1) {
+    } else if (cg_persistent || krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) {
       CgPersistentArgs c{};
       c.S = s1.view();
       c.Ls = Ls;
@@ -958,7 +1205,30 @@ struct cfsa_ns {
       attr[0].val.cooperative = 1;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
-      if (krylov == CFSA_KRYLOV_CG1) {
+      if (krylov == CFSA_KRYLOV_CG2L) {
+        CgResidentArgs rz{};
+        rz.P = c;
+        rz.nslices = s1.nslices;
+        rz.bpc_sell = cg_res_bpc_sell;
+        rz.bpc_nat = cg_res_bpc_nat;
+        rz.col_cap = cg2l_col_cap;
+        Cg2lArgs c2{};
+        c2.R = rz;
+        c2.V = coarse_view;
+        c2.r[0] = pr;
+        c2.r[1] = cg1_vec[0];
+        c2.w[0] = pq;
+        c2.w[1] = cg1_vec[1];
+        c2.s[0] = ps;
+        c2.s[1] = cg1_vec[2];
+        c2.p = pp;
+        CK(cudaMemsetAsync(pp, 0, (size_t)nv * sizeof(double), stream));
+        CK(cudaMemsetAsync(ps, 0, (size_t)nv * sizeof(double), stream));
+        cfg.gridDim = dim3((unsigned int)cg_res_grid);
+        cfg.blockDim = dim3(kCgResThreads);
+        cfg.dynamicSmemBytes = cg2l_smem;
+        CK(cudaLaunchKernelEx(&cfg, k_cg2l_resident, c2));
+      } else if (krylov == CFSA_KRYLOV_CG1) {
         CgResidentArgs rz{};
         rz.P = c;
         rz.nslices = s1.nslices;
@@ -1138,7 +1408,7 @@ struct cfsa_ns {
     CK(cudaEventSynchronize(ev1));
     CK(cudaStreamSynchronize(stream));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
-    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : ((cg_persistent || krylov == CFSA_KRYLOV_CG1) ? 1 : 3);
+    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : ((cg_persistent || krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) ? 1 : 3);
     // mixed momentum: 5 kernels per inner body, 3 per outer sweep (inner init, x update,
     // residual) plus the outer init kernel per step
     batch_launches = (int64_t)launched_steps * (launches_per_step + (precision == CFSA_PRECISION_MIXED ? 1 : 0)) +
@@ -1593,7 +1863,7 @@ struct cfsa_ns {
     adj_stats.momentum_iters = (int64_t)hs_adj.iters[0];
     adj_stats.pressure_iters = (int64_t)hs_adj.iters[1];
     adj_stats.backward_ms = ms;
-    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : ((cg_persistent || krylov == CFSA_KRYLOV_CG1) ? 1 : 3);
+    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : ((cg_persistent || krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) ? 1 : 3);
     adj_stats.kernel_launches = (int64_t)adj_steps * adj_launches_fixed + 5 * (int64_t)hs_adj.body_runs[0] +
                                 pressure_body * (int64_t)hs_adj.body_runs[1] +
                                 3 * (int64_t)hs_adj.body_runs[2];
@@ -1832,13 +2102,31 @@ int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u) {
 
 int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov) {
   if (!h) return CFSA_BAD_ARG;
-  if (krylov != CFSA_KRYLOV_CG && krylov != CFSA_KRYLOV_BICGSTAB && krylov != CFSA_KRYLOV_CG1)
+  if (krylov != CFSA_KRYLOV_CG && krylov != CFSA_KRYLOV_BICGSTAB && krylov != CFSA_KRYLOV_CG1 &&
+      krylov != CFSA_KRYLOV_CG2L)
     return fail(h, CFSA_BAD_ARG, "unknown Krylov method");
-  if (krylov == CFSA_KRYLOV_CG1 && !h->cg_resident)
+  if ((krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) && !h->cg_resident)
     return fail(h, CFSA_UNSUPPORTED, "single-reduction CG needs the shared-memory-resident grid on this device");
   h->krylov = krylov;
   h->graph_dirty = true;
   return CFSA_OK;
+}
+
+int cfsa_ns_set_coarse_target(cfsa_ns *h, int target) {
+  if (!h) return CFSA_BAD_ARG;
+  if (target < 1 || target > 2048) return fail(h, CFSA_BAD_ARG, "coarse target outside [1, 2048]");
+  if (target != h->coarse_target) h->coarse_dirty = h->graph_dirty = true;
+  h->coarse_target = target;
+  return CFSA_OK;
+}
+
+int cfsa_ns_get_coarse_size(cfsa_ns *h, int *nc) {
+  if (!h || !nc) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    if (h->krylov == CFSA_KRYLOV_CG2L) h->ensure_operators();
+    *nc = (h->krylov == CFSA_KRYLOV_CG2L) ? h->coarse_nc : 0;
+    return CFSA_OK;
+  });
 }
 
 int cfsa_ns_set_precision(cfsa_ns *h, int precision) {

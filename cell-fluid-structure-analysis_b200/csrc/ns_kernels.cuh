@@ -1335,9 +1335,9 @@ __device__ __forceinline__ void group_sync(int g) {
 }
 
 // block_partial for one 256-thread group of a larger CTA (named barrier 1 + g).
-template <int NV>
+template <int NV, int NS>
 __device__ __forceinline__ void group_partial(double (&v)[NV], double *__restrict__ partials, int b,
-                                              int g, double (*sm)[3][kBlock / 32]) {
+                                              int g, double (*sm)[NS][kBlock / 32]) {
   const int lt = threadIdx.x & (kBlock - 1), warp = lt >> 5, lane = lt & 31;
 #pragma unroll
   for (int j = 0; j < NV; ++j) {
@@ -1677,6 +1677,363 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg1_resident(Cg1Args C) {
     rn2 = A.scaled ? t[0] : t[2];
     cur ^= 1;
     if (isnan(t[0]) || isnan(t[1]) || isnan(t[2])) {
+      status = KS_BREAKDOWN;
+      break;
+    }
+    if (rn2 <= tol2) {
+      status = KS_CONVERGED;
+      break;
+    }
+    if (it >= maxit) {
+      status = KS_MAXIT;
+      break;
+    }
+    const double beta_new = t[0] / gamma;
+    const double den = t[1] - beta_new * t[0] / alpha;
+    if (den == 0.0) {
+      status = KS_BREAKDOWN;
+      break;
+    }
+    alpha = t[0] / den;
+    beta = beta_new;
+    gamma = t[0];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    CgState *c = A.cs;
+    c->iters = it;
+    c->rnorm2 = rn2;
+    c->alpha = alpha;
+    c->beta = beta;
+    c->absnew = gamma;
+    c->status = status;
+    c->active = 0;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Two-level single-reduction CG (CFSA_KRYLOV_CG2L): the recurrences of k_cg1_resident with the
+// preconditioner M r = D^-1 r + P Z P^T r, where P is the indicator matrix of geometric aggregates
+// (boxes of a uniform grid over the vertices, rows without a penalty only) and Z = (P^T A P)^-1 is
+// a dense nc x nc matrix built on the host. The coarse correction removes the smooth error
+// components that make Jacobi-CG slow on the Poisson operator (684 -> ~130 iterations on the
+// 1M-tet cylinder with ~256 aggregates), at the price of per-iteration aggregate sums and a small
+// dense product.
+//
+// One grid barrier per iteration is kept: the coarse input t = P^T r of the new residual is
+// formed after the barrier from the previous iteration's exact aggregate sums of r, w and s,
+//   t = T(r) - alpha (T(w) + beta T(s)),   c = Z t,
+// and each neighbour's new u = D^-1 r_new + c[agg] is then formed on the fly in the fused product,
+// as k_cg1_resident does for the Jacobi part. The aggregate sums are deterministic: per natural
+// block of 256 rows and per aggregate present in it, the block tree (8 warp butterflies in warp
+// order) of the masked values, then those block partials added in ascending block order by one
+// thread per aggregate; c[m] is a warp butterfly over lanes l of sum_{k = l mod 32} Z[m][k] t[k].
+// Each CTA forms c only for the aggregates that its rows and their neighbours belong to. The
+// oracle's cg2l() restates the same arithmetic, so GPU and oracle agree bit for bit.
+constexpr int kAggChunk = 8;  // aggregates of one block summed per pass
+
+struct CoarseView {
+  int nc;                          // aggregates (0: Jacobi only)
+  const int *agg;                  // [n] aggregate of each row; nc for rows without one
+  const double *Z;                 // [nc*nc] (P^T A P)^-1, symmetric
+  const int *blk_ptr, *blk_agg;    // aggregates present in each natural block, ascending
+  const int *blk_slot;             // slot of each (block, aggregate) partial: aggregate-major,
+                                   // ascending block inside an aggregate
+  const int *agg_ptr;              // slots [agg_ptr[m], agg_ptr[m+1]) hold aggregate m's partials
+  const int *need_ptr, *need;      // aggregates whose coarse value each CTA reads
+  double *part[2];                 // [parity][3 * np] aggregate partials of r, w, s
+  int np;                          // block-partial slots
+};
+
+struct Cg2lArgs {
+  CgResidentArgs R;
+  CoarseView V;
+  double *r[2], *w[2], *s[2];  // r[0] = b on entry
+  double *p;                   // zero on entry
+};
+
+// Aggregate block partials of NV vectors over this CTA's natural blocks [b0, b1); vector v's
+// partial of slot q goes to out[v * np + q].
+template <int NV>
+__device__ __forceinline__ void agg_partials(const double *const (&vec)[NV], const CoarseView &V,
+                                             double *__restrict__ out, int b0, int b1, int n, int g,
+                                             double (*sw)[kAggChunk][3][kBlock / 32]) {
+  const int lt = threadIdx.x & (kBlock - 1), warp = lt >> 5, lane = lt & 31;
+  for (int b = b0 + g; b < b1; b += kCgResGroups) {
+    const int i = b * kBlock + lt;
+    const bool in = i < n;
+    const int a = in ? __ldg(V.agg + i) : V.nc;
+    double x[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) x[v] = in ? __ldcg(vec[v] + i) : 0.0;
+    const int q0 = V.blk_ptr[b], q1 = V.blk_ptr[b + 1];
+    for (int qc = q0; qc < q1; qc += kAggChunk) {
+      const int nq = min(kAggChunk, q1 - qc);
+      for (int k = 0; k < nq; ++k) {
+        const int m = __ldg(V.blk_agg + qc + k);
+        const bool has = __any_sync(0xffffffffu, a == m);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          const double ws = has ? warp_sum((a == m) ? x[v] : 0.0) : 0.0;
+          if (lane == 0) sw[g][k][v][warp] = ws;
+        }
+      }
+      group_sync(g);
+      if (lt < nq * NV) {
+        const int k = lt / NV, v = lt % NV;
+        double sum = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) sum += sw[g][k][v][w];
+        __stcg(out + (size_t)v * V.np + __ldg(V.blk_slot + qc + k), sum);
+      }
+      group_sync(g);
+    }
+  }
+}
+
+// Aggregate sums of NV vectors from their block partials: one thread per (aggregate, vector),
+// its partials (contiguous, ascending block) loaded in batches of kSumBatch before they are added
+// in order, so that an aggregate costs one L2 round trip per batch.
+constexpr int kSumBatch = 8;
+
+template <int NV>
+__device__ __forceinline__ void agg_sums(const CoarseView &V, const double *__restrict__ part,
+                                         double *const (&dst)[NV]) {
+  for (int idx = threadIdx.x; idx < V.nc * NV; idx += blockDim.x) {
+    const int m = idx / NV, v = idx - m * NV;
+    const int q0 = __ldg(V.agg_ptr + m), q1 = __ldg(V.agg_ptr + m + 1);
+    const double *pv = part + (size_t)v * V.np;
+    double sum = 0.0;
+    for (int q = q0; q < q1; q += kSumBatch) {
+      double x[kSumBatch];
+#pragma unroll
+      for (int u = 0; u < kSumBatch; ++u) x[u] = (q + u < q1) ? __ldcg(pv + q + u) : 0.0;
+#pragma unroll
+      for (int u = 0; u < kSumBatch; ++u)
+        if (q + u < q1) sum += x[u];
+    }
+    dst[v][m] = sum;
+  }
+}
+
+// c[m] = Z[m] . t for the aggregates this CTA reads: one warp per aggregate, lane l adding
+// k = l, l + 32, ... in order (Z loads issued kSumBatch at a time), then a warp butterfly.
+__device__ __forceinline__ void coarse_values(const CoarseView &V, const double *__restrict__ t,
+                                              double *__restrict__ c) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int q0 = __ldg(V.need_ptr + blockIdx.x), q1 = __ldg(V.need_ptr + blockIdx.x + 1);
+  const int nc = V.nc;
+  for (int q = q0 + warp; q < q1; q += nw) {
+    const int m = __ldg(V.need + q);
+    const double *zr = V.Z + (size_t)m * nc;
+    double sum = 0.0;
+    for (int k0 = lane; k0 < nc; k0 += 32 * kSumBatch) {
+      double z[kSumBatch];
+#pragma unroll
+      for (int u = 0; u < kSumBatch; ++u) z[u] = (k0 + 32 * u < nc) ? __ldg(zr + k0 + 32 * u) : 0.0;
+#pragma unroll
+      for (int u = 0; u < kSumBatch; ++u)
+        if (k0 + 32 * u < nc) sum += z[u] * t[k0 + 32 * u];
+    }
+    sum = warp_sum(sum);
+    if (lane == 0) c[m] = sum;
+  }
+}
+
+__global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) {
+  extern __shared__ double s_dbl[];
+  __shared__ double s_grp[kCgResGroups][4][kBlock / 32];
+  __shared__ double s_tree[4][kBlock / 32];
+  __shared__ double s_agw[kCgResGroups][kAggChunk][3][kBlock / 32];
+  const CgResidentArgs &R = C.R;
+  const CgPersistentArgs &A = R.P;
+  const CoarseView &V = C.V;
+  if (A.st && A.st->halt) return;
+  if (!A.cs->active) return;
+  const int g = threadIdx.x / kBlock, lt = threadIdx.x & (kBlock - 1);
+  const int b0 = min(A.nblk_sell, (int)blockIdx.x * R.bpc_sell);
+  const int b1 = min(A.nblk_sell, b0 + R.bpc_sell);
+  const int nc = V.nc, n = A.n;
+  // shared memory: aggregate sums of r, w, s, the coarse input t, coarse values (two
+  // generations, entry nc = 0 for rows without aggregate), then the row staging of k_cg1_resident
+  double *cR = s_dbl, *cW = cR + nc, *cS = cW + nc, *ct = cS + nc;
+  double *cc[2] = {ct + nc, ct + 2 * nc + 1};
+  int *s_row = reinterpret_cast<int *>(ct + 3 * nc + 2);
+  int *s_len = s_row + R.bpc_sell * kBlock;
+  int *s_base = s_len + R.bpc_sell * kBlock;
+  int *s_col = s_base + R.bpc_sell * kBlock;
+  const int e0 = (b0 < b1) ? A.S.sptr[8 * b0] : 0;
+  int bs = b0;
+  while (bs < b1 && A.S.sptr[min(8 * (bs + 1), R.nslices)] - e0 <= R.col_cap) ++bs;
+  const int e1 = (bs > b0) ? A.S.sptr[min(8 * bs, R.nslices)] : e0;
+  for (int e = e0 + (int)threadIdx.x; e < e1; e += kCgResThreads) s_col[e - e0] = A.S.col[e];
+  for (int q = threadIdx.x; q < (b1 - b0) * kBlock; q += kCgResThreads) {
+    const int r = b0 * kBlock + q;
+    const bool in = r < A.S.nrows_pad;
+    s_row[q] = in ? A.S.perm[r] : -1;
+    s_len[q] = in ? A.S.len[r] : 0;
+    s_base[q] = in ? A.S.sptr[r >> 5] + (r & 31) : 0;
+  }
+  if (threadIdx.x == 0) {
+    cc[0][nc] = 0.0;
+    cc[1][nc] = 0.0;
+  }
+  for (int m = threadIdx.x; m < nc; m += kCgResThreads) cS[m] = 0.0;
+  __syncthreads();
+  const double tol2 = A.cs->tol2;
+  const int maxit = A.cs->maxit;
+  double gamma = 0.0, alpha = 0.0, beta = 0.0, rn2 = A.cs->bnorm2;
+  int it = 0, status = KS_RUNNING, cur = 0, pc = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[1] += 1;
+  const double *bvec = C.r[0];
+  // start: c0 = Z T(b)
+  if (nc > 0) {
+    const double *const vb[1] = {bvec};
+    agg_partials<1>(vb, V, V.part[0], b0, b1, n, g, s_agw);
+    if (!grid_sync(A.bar)) return;
+    double *const dR[1] = {cR};
+    agg_sums<1>(V, V.part[0], dR);
+    __syncthreads();
+    coarse_values(V, cR, cc[0]);
+    __syncthreads();
+  }
+  // w0 = A u0 with u0 = D^-1 b + c0[agg]; delta0 = w0.u0, gamma0 = b.u0 (product order)
+  for (int b = b0 + g; b < b1; b += kCgResGroups) {
+    const int lp = (b - b0) * kBlock + lt;
+    const int i = s_row[lp];
+    double v[2] = {0.0, 0.0};
+    if (i >= 0) {
+      const int base = s_base[lp], len = s_len[lp];
+      const bool staged = b < bs;
+      double acc = 0.0;
+      for (int k = 0; k < len; ++k) {
+        const int pos = base + k * kSellC;
+        const int jj = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+        const double uj = __ldg(A.invL + jj) * __ldcg(bvec + jj) + cc[0][__ldg(V.agg + jj)];
+        acc += __ldg(A.Ls + pos) * uj;
+      }
+      const double bi = __ldcg(bvec + i);
+      const double ui = __ldg(A.invL + i) * bi + cc[0][__ldg(V.agg + i)];
+      __stcg(C.w[0] + i, acc);
+      v[0] = acc * ui;
+      v[1] = bi * ui;
+    }
+    group_partial<2>(v, A.part_a, b, g, s_grp);
+  }
+  if (nc > 0) {
+    __syncthreads();  // this CTA's w0 rows are written
+    const double *const vw[1] = {C.w[0]};
+    agg_partials<1>(vw, V, V.part[0] + V.np, b0, b1, n, g, s_agw);
+  }
+  if (!grid_sync(A.bar)) return;
+  {
+    double d0[2];
+    tree_total_cta<2>(A.part_a, A.nblk_sell, d0, s_tree);
+    if (d0[0] == 0.0 || isnan(d0[0]) || isnan(d0[1]))
+      status = KS_BREAKDOWN;
+    else
+      alpha = d0[1] / d0[0];
+    gamma = d0[1];
+    if (nc > 0) {
+      double *const dW[1] = {cW};
+      agg_sums<1>(V, V.part[0] + V.np, dW);
+      __syncthreads();
+    }
+  }
+  while (status == KS_RUNNING) {
+    double *part = (it & 1) ? A.part_a : A.part_b;
+    double *apart = V.part[(it + 1) & 1];
+    const double *ro = C.r[cur], *wo = C.w[cur], *so = C.s[cur];
+    double *rn = C.r[cur ^ 1], *wn = C.w[cur ^ 1], *sn = C.s[cur ^ 1];
+    // coarse input of the new residual and its coarse values
+    if (nc > 0) {
+      for (int m = threadIdx.x; m < nc; m += kCgResThreads) {
+        const double sm = cW[m] + beta * cS[m];
+        ct[m] = cR[m] - alpha * sm;
+      }
+      __syncthreads();
+      coarse_values(V, ct, cc[pc ^ 1]);
+      __syncthreads();
+    }
+    const double *cold = cc[pc], *cnew = cc[pc ^ 1];
+    for (int b = b0 + g; b < b1; b += kCgResGroups) {
+      const int lp = (b - b0) * kBlock + lt;
+      const int i = s_row[lp];
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
+      if (i >= 0) {
+        const int base = s_base[lp], len = s_len[lp];
+        const bool staged = b < bs;
+        double acc = 0.0;
+        int k = 0;
+        for (; k + kCgChunk <= len; k += kCgChunk) {
+          int jj[kCgChunk], aj[kCgChunk];
+          double a[kCgChunk], rr_[kCgChunk], ww[kCgChunk], ss[kCgChunk], mm[kCgChunk];
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            const int pos = base + (k + q) * kSellC;
+            jj[q] = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+            a[q] = __ldg(A.Ls + pos);
+          }
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            rr_[q] = __ldcg(ro + jj[q]);
+            ww[q] = __ldcg(wo + jj[q]);
+            ss[q] = __ldcg(so + jj[q]);
+            mm[q] = __ldg(A.invL + jj[q]);
+            aj[q] = __ldg(V.agg + jj[q]);
+          }
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            const double sj = ww[q] + beta * ss[q];
+            const double rj = rr_[q] - alpha * sj;
+            acc += a[q] * (mm[q] * rj + cnew[aj[q]]);
+          }
+        }
+        for (; k < len; ++k) {
+          const int pos = base + k * kSellC;
+          const int jj = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+          const double sj = __ldcg(wo + jj) + beta * __ldcg(so + jj);
+          const double rj = __ldcg(ro + jj) - alpha * sj;
+          acc += __ldg(A.Ls + pos) * (__ldg(A.invL + jj) * rj + cnew[__ldg(V.agg + jj)]);
+        }
+        // own row
+        const int ai = __ldg(V.agg + i);
+        const double mi = __ldg(A.invL + i);
+        const double roi = __ldcg(ro + i);
+        const double uoi = mi * roi + cold[ai];
+        const double pi = uoi + beta * __ldcg(C.p + i);
+        const double si = __ldcg(wo + i) + beta * __ldcg(so + i);
+        const double xi = __ldcg(A.x + i) + alpha * pi;
+        const double ri = roi - alpha * si;
+        const double ui = mi * ri + cnew[ai];
+        __stcg(C.p + i, pi);
+        __stcg(sn + i, si);
+        __stcg(A.x + i, xi);
+        __stcg(rn + i, ri);
+        __stcg(wn + i, acc);
+        v[0] = ri * ui;
+        v[1] = acc * ui;
+        v[2] = ri * ri;
+        v[3] = ri * (mi * ri);
+      }
+      group_partial<4>(v, part, b, g, s_grp);
+    }
+    if (nc > 0) {
+      __syncthreads();  // this CTA's new r, w, s rows are written
+      const double *const vv[3] = {rn, wn, sn};
+      agg_partials<3>(vv, V, apart, b0, b1, n, g, s_agw);
+    }
+    if (!grid_sync(A.bar)) return;
+    double t[4];
+    tree_total_cta<4>(part, A.nblk_sell, t, s_tree);
+    if (nc > 0) {
+      double *const d3[3] = {cR, cW, cS};
+      agg_sums<3>(V, apart, d3);
+      __syncthreads();
+    }
+    ++it;
+    pc ^= 1;
+    rn2 = A.scaled ? t[3] : t[2];
+    cur ^= 1;
+    if (isnan(t[0]) || isnan(t[1]) || isnan(t[2]) || isnan(t[3])) {
       status = KS_BREAKDOWN;
       break;
     }

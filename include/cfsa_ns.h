@@ -51,6 +51,11 @@ extern "C" {
 /* CG with one reduction per iteration (Chronopoulos & Gear 1989): CG's iterates in exact
  * arithmetic, one fused product-and-reduction pass and one grid synchronisation per iteration */
 #define CFSA_KRYLOV_CG1 2
+/* CFSA_KRYLOV_CG1's recurrences with a two-level preconditioner: Jacobi plus an additive coarse
+ * correction on geometric aggregates (boxes over the vertices, ~cfsa_ns_set_coarse_target of
+ * them), M r = D^-1 r + P (P^T A P)^-1 P^T r. Same system and stopping rule, several times fewer
+ * iterations on the Poisson operator; still one grid synchronisation per iteration. */
+#define CFSA_KRYLOV_CG2L 3
 
 /* arithmetic of the Krylov solves */
 #define CFSA_PRECISION_FP64 0
@@ -139,6 +144,12 @@ int cfsa_ns_set_reference_node(cfsa_ns *h, int node);                      /* se
 int cfsa_ns_set_inlet_uniform(cfsa_ns *h, const double u[3]);             /* setMeanInletVelocity */
 int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u /*[N2][3]*/);   /* new: per-node inlet */
 int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov);                   /* new: CG or BiCGSTAB */
+/* new: aggregate count the CFSA_KRYLOV_CG2L coarse space aims for (default 256, 1..2048); the
+ * coarse space is rebuilt with the Poisson operator */
+int cfsa_ns_set_coarse_target(cfsa_ns *h, int target);
+/* new: aggregates of the current CFSA_KRYLOV_CG2L coarse space (built on demand; 0 for the other
+ * methods or when the coarse operator was not SPD) */
+int cfsa_ns_get_coarse_size(cfsa_ns *h, int *nc);
 int cfsa_ns_set_precision(cfsa_ns *h, int precision);                      /* new: FP64 or mixed */
 int cfsa_ns_set_convergence_norm(cfsa_ns *h, int norm);                     /* new: see CFSA_NORM_* */
 /* Fluid viscosity; stiffness (scaled by 1/viscosity, NavierStokes.cpp:153) is re-assembled. */

@@ -451,6 +451,303 @@ SolveInfo cg1(const CSR &A, const std::vector<double> &b, std::vector<double> &x
   return info;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Two-level preconditioner of the pressure CG (pressure_solver 3). Not in the reference, which
+// solves the Poisson problem with Jacobi-preconditioned BiCGSTAB; this is a faster solver of the
+// same system (the CUDA solver's CFSA_KRYLOV_CG2L), restated here so that the device iterates can
+// be checked bit for bit.
+//   M r = D^-1 r + P Z P^T r,   Z = (P^T A P)^-1,
+// P the indicator matrix of geometric aggregates (boxes of a uniform grid over the vertices) on the
+// rows without a penalty (Dirichlet outlet rows, or the Neumann reference row, belong to no
+// aggregate). Additive two-level Schwarz with a piecewise-constant coarse space: the coarse solve
+// removes the smooth error components that Jacobi-CG converges slowly on (684 -> 134 CG iterations
+// on the 1M-tet cylinder with ~256 aggregates).
+//
+// Aggregation: box edge h_k = e * c^k (e = largest extent of the vertex bounding box,
+// c = 2^-1/4, k the smallest exponent in [0, 64] for which the number of occupied boxes reaches
+// `target`, found by bisection); boxes are numbered in order of their first vertex.
+// Z from the Cholesky factor G of A_c (row-wise Cholesky-Banachiewicz, then the lower-triangular
+// inverse by columns, then Z = G^-T G^-1 summed over ascending rows); A_c entries summed over the
+// CSR in row-major order. A non-SPD A_c (a pivot <= 0) disables the coarse part (nc = 0).
+// Aggregate sums of a vector v: per natural block b of 256 rows and per aggregate m present in it,
+// the block tree of the masked values (agg[row] == m ? v[row] : 0) -- 8 warp butterflies over
+// rows 256b + 32w .. +31, added in warp order -- then these block partials added in ascending block
+// order. Coarse values c[m] = butterfly over lanes l of (sum over k = l, l+32, ... of Z[m][k] t[k]).
+struct CoarseSpace {
+  int nc = 0;
+  std::vector<int> agg;                // [n], nc for rows without aggregate
+  std::vector<double> Z;               // [nc*nc], symmetric
+  std::vector<int> blk_ptr, blk_agg;   // aggregates present in each natural block, ascending
+  std::vector<int> agg_ptr, agg_part;  // block-partial slots of each aggregate, ascending block
+};
+
+constexpr double kBoxShrink = 0.8408964152537145;  // 2^-1/4
+
+int count_boxes(const std::vector<V3> &xyz, const std::vector<char> &pen, int64_t n, double h,
+                const V3 &lo, std::vector<int64_t> *keys_out = nullptr) {
+  std::vector<int64_t> keys;
+  keys.reserve(n);
+  for (int64_t i = 0; i < n; ++i) {
+    if (pen[i]) continue;
+    const int64_t ix = (int64_t)std::floor((xyz[i].x - lo.x) / h);
+    const int64_t iy = (int64_t)std::floor((xyz[i].y - lo.y) / h);
+    const int64_t iz = (int64_t)std::floor((xyz[i].z - lo.z) / h);
+    keys.push_back((ix * 2097152 + iy) * 2097152 + iz);
+  }
+  if (keys_out) *keys_out = keys;
+  std::sort(keys.begin(), keys.end());
+  return (int)(std::unique(keys.begin(), keys.end()) - keys.begin());
+}
+
+CoarseSpace build_coarse(const CSR &A, const std::vector<V3> &xyz, const std::vector<char> &pen,
+                         int target) {
+  CoarseSpace cs;
+  const int64_t n = A.n;
+  cs.agg.assign(n, 0);
+  V3 lo{0, 0, 0}, hi{0, 0, 0};
+  bool any = false;
+  for (int64_t i = 0; i < n; ++i) {
+    if (pen[i]) continue;
+    if (!any) {
+      lo = hi = xyz[i];
+      any = true;
+    }
+    lo.x = std::min(lo.x, xyz[i].x), lo.y = std::min(lo.y, xyz[i].y), lo.z = std::min(lo.z, xyz[i].z);
+    hi.x = std::max(hi.x, xyz[i].x), hi.y = std::max(hi.y, xyz[i].y), hi.z = std::max(hi.z, xyz[i].z);
+  }
+  const double e = std::max(hi.x - lo.x, std::max(hi.y - lo.y, hi.z - lo.z));
+  if (!any || !(e > 0.0) || target < 1) {
+    cs.nc = 0;  // no coarse space: every row maps to the zero coarse value
+  } else {
+    auto h_of = [&](int k) {
+      double h = e;
+      for (int q = 0; q < k; ++q) h = h * kBoxShrink;
+      return h;
+    };
+    int klo = 0, khi = 64;  // count(h_klo) < target unless klo == 0; count(h_khi) >= target assumed
+    while (klo < khi) {
+      const int km = (klo + khi) / 2;
+      if (count_boxes(xyz, pen, n, h_of(km), lo) >= target)
+        khi = km;
+      else
+        klo = km + 1;
+    }
+    std::vector<int64_t> keys;
+    count_boxes(xyz, pen, n, h_of(klo), lo, &keys);
+    // number boxes by first vertex
+    std::vector<std::pair<int64_t, int>> kv(keys.size());
+    for (size_t q = 0; q < keys.size(); ++q) kv[q] = {keys[q], (int)q};
+    std::stable_sort(kv.begin(), kv.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+    std::vector<int> first_of(keys.size());  // box rank by first vertex
+    std::vector<std::pair<int, int>> firsts;  // (first q, group start)
+    for (size_t q = 0; q < kv.size();) {
+      size_t r = q;
+      while (r < kv.size() && kv[r].first == kv[q].first) ++r;
+      firsts.push_back({kv[q].second, (int)q});
+      q = r;
+    }
+    std::sort(firsts.begin(), firsts.end());
+    std::vector<int> id_of_sorted(kv.size());
+    for (size_t g = 0; g < firsts.size(); ++g) {
+      size_t q = firsts[g].second;
+      const int64_t key = kv[q].first;
+      while (q < kv.size() && kv[q].first == key) id_of_sorted[q++] = (int)g;
+    }
+    std::vector<int> id_of_q(keys.size());
+    for (size_t q = 0; q < kv.size(); ++q) id_of_q[kv[q].second] = id_of_sorted[q];
+    cs.nc = (int)firsts.size();
+    size_t q = 0;
+    for (int64_t i = 0; i < n; ++i) cs.agg[i] = pen[i] ? cs.nc : id_of_q[q++];
+  }
+  const int nc = cs.nc;
+  if (nc > 0) {
+    std::vector<double> Ac((size_t)nc * nc, 0.0), G((size_t)nc * nc, 0.0), Gi((size_t)nc * nc, 0.0);
+    for (int64_t i = 0; i < n; ++i) {
+      if (cs.agg[i] >= nc) continue;
+      for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) {
+        const int j = A.col[k];
+        if (cs.agg[j] >= nc) continue;
+        double &a = Ac[(size_t)cs.agg[i] * nc + cs.agg[j]];
+        a = a + A.val[k];
+      }
+    }
+    bool spd = true;
+    for (int i = 0; i < nc && spd; ++i)
+      for (int j = 0; j <= i; ++j) {
+        double s = Ac[(size_t)i * nc + j];
+        for (int k = 0; k < j; ++k) s = s - G[(size_t)i * nc + k] * G[(size_t)j * nc + k];
+        if (i == j) {
+          if (!(s > 0.0)) {
+            spd = false;
+            break;
+          }
+          G[(size_t)i * nc + i] = std::sqrt(s);
+        } else {
+          G[(size_t)i * nc + j] = s / G[(size_t)j * nc + j];
+        }
+      }
+    if (!spd) {
+      cs.nc = 0;
+      for (auto &a : cs.agg) a = 0;
+    } else {
+      for (int j = 0; j < nc; ++j) {
+        Gi[(size_t)j * nc + j] = 1.0 / G[(size_t)j * nc + j];
+        for (int i = j + 1; i < nc; ++i) {
+          double s = 0.0;
+          for (int k = j; k < i; ++k) s = s - G[(size_t)i * nc + k] * Gi[(size_t)k * nc + j];
+          Gi[(size_t)i * nc + j] = s / G[(size_t)i * nc + i];
+        }
+      }
+      cs.Z.assign((size_t)nc * nc, 0.0);
+      for (int m = 0; m < nc; ++m)
+        for (int k = 0; k < nc; ++k) {
+          double s = 0.0;
+          for (int q = std::max(m, k); q < nc; ++q) s = s + Gi[(size_t)q * nc + m] * Gi[(size_t)q * nc + k];
+          cs.Z[(size_t)m * nc + k] = s;
+        }
+    }
+  }
+  // block lists
+  const int64_t nblk = (n + 255) / 256;
+  cs.blk_ptr.assign(nblk + 1, 0);
+  cs.blk_agg.clear();
+  for (int64_t b = 0; b < nblk; ++b) {
+    std::vector<int> ms;
+    for (int64_t i = 256 * b; i < std::min(n, 256 * (b + 1)); ++i)
+      if (cs.agg[i] < cs.nc) ms.push_back(cs.agg[i]);
+    std::sort(ms.begin(), ms.end());
+    ms.erase(std::unique(ms.begin(), ms.end()), ms.end());
+    cs.blk_agg.insert(cs.blk_agg.end(), ms.begin(), ms.end());
+    cs.blk_ptr[b + 1] = (int)cs.blk_agg.size();
+  }
+  cs.agg_ptr.assign(cs.nc + 1, 0);
+  for (int m : cs.blk_agg) cs.agg_ptr[m + 1]++;
+  for (int m = 0; m < cs.nc; ++m) cs.agg_ptr[m + 1] += cs.agg_ptr[m];
+  cs.agg_part.assign(cs.blk_agg.size(), 0);
+  std::vector<int> fill(cs.agg_ptr.begin(), cs.agg_ptr.end() - (cs.nc > 0 ? 1 : 0));
+  for (size_t q = 0; q < cs.blk_agg.size(); ++q) cs.agg_part[fill[cs.blk_agg[q]]++] = (int)q;
+  return cs;
+}
+
+// aggregate sums of v (size nc)
+std::vector<double> aggregate_sums(const CoarseSpace &cs, const std::vector<double> &v) {
+  const int64_t n = (int64_t)v.size();
+  std::vector<double> part(cs.blk_agg.size());
+  const int64_t nblk = (int64_t)cs.blk_ptr.size() - 1;
+#pragma omp parallel for schedule(static)
+  for (int64_t b = 0; b < nblk; ++b)
+    for (int q = cs.blk_ptr[b]; q < cs.blk_ptr[b + 1]; ++q) {
+      const int m = cs.blk_agg[q];
+      double s = 0.0;
+      for (int w = 0; w < 8; ++w) {
+        double x[32];
+        for (int l = 0; l < 32; ++l) {
+          const int64_t i = 256 * b + 32 * w + l;
+          x[l] = (i < n && cs.agg[i] == m) ? v[i] : 0.0;
+        }
+        s += warp_butterfly(x);
+      }
+      part[q] = s;
+    }
+  std::vector<double> T(cs.nc, 0.0);
+  for (int m = 0; m < cs.nc; ++m) {
+    double s = 0.0;
+    for (int q = cs.agg_ptr[m]; q < cs.agg_ptr[m + 1]; ++q) s += part[cs.agg_part[q]];
+    T[m] = s;
+  }
+  return T;
+}
+
+// c = Z t (size nc + 1, c[nc] = 0 for rows without aggregate)
+std::vector<double> coarse_values(const CoarseSpace &cs, const std::vector<double> &t) {
+  const int nc = cs.nc;
+  std::vector<double> c(nc + 1, 0.0);
+  for (int m = 0; m < nc; ++m) {
+    double lanes[32];
+    for (int l = 0; l < 32; ++l) {
+      double s = 0.0;
+      for (int k = l; k < nc; k += 32) s += cs.Z[(size_t)m * nc + k] * t[k];
+      lanes[l] = s;
+    }
+    c[m] = warp_butterfly(lanes);
+  }
+  return c;
+}
+
+// Single-reduction CG (the recurrences of cg1) preconditioned by M r = D^-1 r + P Z P^T r.
+// t = P^T r of the new residual comes from the previous iteration's exact aggregate sums of r, w
+// and s (t = T(r) - alpha (T(w) + beta T(s))), so the device needs one grid barrier per iteration.
+// Start: u = M b, w = A u, gamma = b.u and delta = w.u in product order. The stopping rule is
+// cg1's: ||r||^2 or, scaled, sum r_i (r_i / a_ii) (the Jacobi-scaled norm, not r.u).
+SolveInfo cg2l(const CSR &A, const std::vector<double> &b, std::vector<double> &x, double tol,
+               int maxit, const RedOrder &sell, const RedOrder &nat, bool scaled,
+               const CoarseSpace &cs) {
+  const int64_t n = A.n;
+  SolveInfo info;
+  const std::vector<double> invdiag = inverse_diagonal(A);
+  x.assign(n, 0.0);
+  std::vector<double> r(b), u(n), w(n), p(n, 0.0), s(n, 0.0);
+  const double b2 = odot(nat, b.data(), b.data());
+  const double bz = tree_sum(nat, [&](int i) { return b[i] * (invdiag[i] * b[i]); });
+  const double bnorm2 = scaled ? bz : b2;
+  const double thr = tol * tol * bnorm2;
+  if (std::isnan(bnorm2) || std::isnan(b2)) return info;
+  double rn2 = bnorm2;
+  int it = 0;
+  if (!(bnorm2 == 0.0 || bnorm2 <= thr)) {
+    std::vector<double> R = aggregate_sums(cs, r), S(cs.nc, 0.0);
+    std::vector<double> c = coarse_values(cs, R);
+    for (int64_t k = 0; k < n; ++k) u[k] = invdiag[k] * r[k] + c[cs.agg[k]];
+    spmv(A, u.data(), w.data());
+    const double delta0 = odot(sell, w.data(), u.data());
+    double gamma = odot(sell, r.data(), u.data());
+    std::vector<double> W = aggregate_sums(cs, w);
+    if (delta0 == 0.0 || std::isnan(delta0) || std::isnan(gamma)) {
+      info.rel_res = 1.0;
+      return info;
+    }
+    double alpha = gamma / delta0, beta = 0.0;
+    std::vector<double> t(cs.nc);
+    while (true) {
+      for (int m = 0; m < cs.nc; ++m) {
+        const double sm = W[m] + beta * S[m];
+        t[m] = R[m] - alpha * sm;
+      }
+      c = coarse_values(cs, t);
+      for (int64_t k = 0; k < n; ++k) {
+        p[k] = u[k] + beta * p[k];
+        s[k] = w[k] + beta * s[k];
+        x[k] += alpha * p[k];
+        r[k] = r[k] - alpha * s[k];
+        u[k] = invdiag[k] * r[k] + c[cs.agg[k]];
+      }
+      spmv(A, u.data(), w.data());
+      const double g_new = odot(sell, r.data(), u.data());
+      const double delta = odot(sell, w.data(), u.data());
+      const double rr = odot(sell, r.data(), r.data());
+      const double rz = tree_sum(sell, [&](int i) { return r[i] * (invdiag[i] * r[i]); });
+      R = aggregate_sums(cs, r);
+      W = aggregate_sums(cs, w);
+      S = aggregate_sums(cs, s);
+      rn2 = scaled ? rz : rr;
+      ++it;
+      if (std::isnan(g_new) || std::isnan(delta) || std::isnan(rr) || std::isnan(rz)) break;
+      if (rn2 <= thr) break;
+      if (it >= maxit) break;
+      const double beta_new = g_new / gamma;
+      const double den = delta - beta_new * g_new / alpha;
+      if (den == 0.0) break;
+      alpha = g_new / den;
+      beta = beta_new;
+      gamma = g_new;
+    }
+  }
+  info.iters = it;
+  info.rel_res = std::sqrt(rn2 / bnorm2);
+  info.converged = rn2 <= thr;
+  return info;
+}
+
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -476,7 +773,8 @@ struct Oracle {
   int outlet_type = kDirichlet;
   double outlet_pressure = 0.0;
   int reference_node = -1;
-  int pressure_solver = 0;  // 0 = BiCGSTAB (reference), 1 = CG, 2 = CG with one reduction
+  int pressure_solver = 0;  // 0 = BiCGSTAB (reference), 1 = CG, 2 = CG with one reduction,
+                            // 3 = the latter with the two-level preconditioner
   int conv_norm = 0;        // 0 = ||r|| (reference), 1 = ||D^-1/2 r||
   std::vector<V3> inlet;    // per P2-node inlet velocity (the reference: one mean vector)
   std::vector<V3> u, ustar;
@@ -849,6 +1147,31 @@ struct Oracle {
     }
   }
 
+  // Pressure Krylov solve with the selected method (0 BiCGSTAB as the reference, 1 CG, 2 CG with
+  // one reduction, 3 the same with the two-level preconditioner). The coarse space depends on the
+  // penalised rows only through the boundary setup, so it is built once.
+  CoarseSpace coarse;
+  bool coarse_built = false;
+  int coarse_target = 256;
+  SolveInfo solve_pressure(const CSR &Lbc, const std::vector<double> &rhs, std::vector<double> &x) {
+    if (pressure_solver == 1) return cg(Lbc, rhs, x, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1);
+    if (pressure_solver == 2) return cg1(Lbc, rhs, x, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1);
+    if (pressure_solver == 3) {
+      if (!coarse_built) {
+        std::vector<char> pen(nv, 0);
+        if (outlet_type == kNeumann) {
+          if (reference_node >= 0 && reference_node < (int)nv) pen[reference_node] = 1;
+        } else if (outlet_type == kDirichlet) {
+          for (size_t i = 0; i < nv; ++i) pen[i] = p1bc[i] == kOutlet;
+        }
+        coarse = build_coarse(Lbc, vertices, pen, coarse_target);
+        coarse_built = true;
+      }
+      return cg2l(Lbc, rhs, x, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1, coarse);
+    }
+    return bicgstab(Lbc, rhs, x, tol_p, maxit_p, order_nv, order_p1, order_nv, conv_norm == 1);
+  }
+
   // solvePressurePoisson (NavierStokes.cpp:586-668)
   bool pressure() {
     const double t0 = now_s();
@@ -873,12 +1196,7 @@ struct Oracle {
           rhs[i] += penalty * outlet_pressure;
         }
     }
-    SolveInfo si = (pressure_solver == 1)
-                       ? cg(Lbc, rhs, x, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1)
-                   : (pressure_solver == 2)
-                       ? cg1(Lbc, rhs, x, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1)
-                       : bicgstab(Lbc, rhs, x, tol_p, maxit_p, order_nv, order_p1, order_nv,
-                                  conv_norm == 1);
+    SolveInfo si = solve_pressure(Lbc, rhs, x);
     it_p = si.iters;
     res_p = si.rel_res;
     if (!si.converged) {
@@ -1218,12 +1536,7 @@ struct Oracle {
       for (size_t i = 0; i < nv; ++i) rhs[i] = ((t0[i] + t1[i]) + t2[i]) + lpp[i];
       // pressure Poisson solve (L symmetric)
       {
-        SolveInfo si = (pressure_solver == 1)
-                           ? cg(Lbc, rhs, mu_p, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1)
-                       : (pressure_solver == 2)
-                           ? cg1(Lbc, rhs, mu_p, tol_p, maxit_p, order_p1, order_nv, conv_norm == 1)
-                           : bicgstab(Lbc, rhs, mu_p, tol_p, maxit_p, order_nv, order_p1, order_nv,
-                                      conv_norm == 1);
+        SolveInfo si = solve_pressure(Lbc, rhs, mu_p);
         adj_it_p += si.iters;
         if (!si.converged) return 1;
       }
@@ -1397,7 +1710,8 @@ void orc_set_fluid(void *h, double density, double viscosity) {
 }
 // Parameters: dt, momentum tol, pressure tol, momentum maxit, pressure maxit, corrections,
 // relax_u, relax_p, outlet type, outlet pressure, reference node, pressure solver (0 BiCGSTAB,
-// 1 CG, 2 single-reduction CG), convergence norm (0 ||r||, 1 ||D^-1/2 r||).
+// 1 CG, 2 single-reduction CG, 3 single-reduction CG with the two-level preconditioner),
+// convergence norm (0 ||r||, 1 ||D^-1/2 r||).
 void orc_set_params(void *h, double dt, double tol_mom, double tol_p, int maxit_mom, int maxit_p,
                     int n_corr, double relax_u, double relax_p, int outlet_type,
                     double outlet_pressure, int reference_node, int pressure_solver, int conv_norm) {
@@ -1415,7 +1729,16 @@ void orc_set_params(void *h, double dt, double tol_mom, double tol_p, int maxit_
   o->outlet_pressure = outlet_pressure;
   o->reference_node = reference_node;
   o->pressure_solver = pressure_solver;
+  o->coarse_built = false;
 }
+// Target number of aggregates of the two-level pressure preconditioner (default 256).
+void orc_set_coarse_target(void *h, int target) {
+  Oracle *o = static_cast<Oracle *>(h);
+  o->coarse_target = target;
+  o->coarse_built = false;
+}
+// Aggregates of the coarse space last built (0 before the first two-level solve).
+int orc_coarse_size(void *h) { return static_cast<Oracle *>(h)->coarse.nc; }
 // Per-node inlet velocity [N2][3] (P1 nodes first, then P2 edge nodes).
 void orc_set_inlet(void *h, const double *vals) {
   Oracle *o = static_cast<Oracle *>(h);

@@ -40,6 +40,8 @@ def lib() -> C.CDLL:
         "orc_set_fluid": (None, [vp, dbl, dbl]),
         "orc_set_params": (None, [vp, dbl, dbl, dbl, i32, i32, i32, dbl, dbl, i32, dbl, i32, i32, i32]),
         "orc_set_inlet": (None, [vp, vp]),
+        "orc_set_coarse_target": (None, [vp, i32]),
+        "orc_coarse_size": (i32, [vp]),
         "orc_initialize": (None, [vp]),
         "orc_reference_node": (i32, [vp]),
         "orc_piso_step": (i32, [vp]),
@@ -127,6 +129,13 @@ class Oracle:
                               float(p["relax_u"]), float(p["relax_p"]), int(p["outlet_type"]),
                               float(p["outlet_pressure"]), int(p["reference_node"]),
                               int(p["pressure_solver"]), int(p["conv_norm"]))
+
+    def set_coarse_target(self, target: int):
+        """Aggregate count the two-level pressure preconditioner (pressure_solver 3) aims for."""
+        self.L.orc_set_coarse_target(self.h, int(target))
+
+    def coarse_size(self) -> int:
+        return self.L.orc_coarse_size(self.h)
 
     def set_inlet(self, per_node):
         v = np.ascontiguousarray(per_node, np.float64).reshape(self.N2, 3)

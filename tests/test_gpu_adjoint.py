@@ -42,7 +42,7 @@ def oracle(po, m, prof, *, tol=1e-13, nu=NU, krylov=0):
     o = po.Oracle(m.vertices(), m.tets())
     o.set_fluid(RHO, nu)
     o.set_params(dt=DT, tol_mom=tol, tol_p=tol, maxit_mom=20000, maxit_p=50000,
-                 pressure_solver={0: 1, 1: 0, 2: 2}[krylov], conv_norm=1)
+                 pressure_solver={0: 1, 1: 0, 2: 2, 3: 3}[krylov], conv_norm=1)
     o.initialize()
     o.set_inlet(prof)
     return o
@@ -56,7 +56,7 @@ def small(cf):
 
 
 @pytest.mark.parametrize("obj", [WSS, PDROP], ids=["wall_shear_patch", "pressure_drop"])
-@pytest.mark.parametrize("krylov", [0, 1, 2], ids=["cg", "bicgstab", "cg1"])
+@pytest.mark.parametrize("krylov", [0, 1, 2, 3], ids=["cg", "bicgstab", "cg1", "cg2l"])
 def test_adjoint_bit_exact_vs_oracle(cf, po, small, obj, krylov):
     m, prof = small
     n = 4

@@ -48,7 +48,7 @@ def make_pair(cf, po, m, *, tol=1e-12, krylov=0, dt=0.01, inlet=0.5, profile=Non
     o.set_params(dt=dt, tol_mom=tol, tol_p=tol, maxit_mom=maxit[0], maxit_p=maxit[1],
                  n_corr=ncorr, relax_u=relax[0], relax_p=relax[1], outlet_type=outlet,
                  outlet_pressure=outlet_p, reference_node=s.reference_node,
-                 pressure_solver={0: 1, 1: 0, 2: 2}[krylov], conv_norm=norm)
+                 pressure_solver={0: 1, 1: 0, 2: 2, 3: 3}[krylov], conv_norm=norm)
     o.initialize()
     if profile is not None:
         s.setInletVelocityProfile(profile)
@@ -127,7 +127,7 @@ def run_both(s, o, steps):
     return states
 
 
-@pytest.mark.parametrize("krylov", [0, 1, 2], ids=["cg", "bicgstab", "cg1"])
+@pytest.mark.parametrize("krylov", [0, 1, 2, 3], ids=["cg", "bicgstab", "cg1", "cg2l"])
 def test_piso_parity_tight(cf, po, krylov):
     m = make_mesh(cf, 3, 12)
     s, o = make_pair(cf, po, m, tol=1e-13, krylov=krylov)
@@ -195,10 +195,13 @@ def test_reference_default_tolerances(cf, po):
     assert rel_l2(s.getPressure(), o.state()["p"]) < 1e-8
 
 
-@pytest.mark.parametrize("case", ["neumann", "two_correctors", "relaxed", "parabolic", "outlet_p"])
+@pytest.mark.parametrize("case", ["neumann", "two_correctors", "relaxed", "parabolic", "outlet_p",
+                                  "neumann_cg2l"])
 def test_variants_parity(cf, po, case):
     m = make_mesh(cf, 3, 12)
     kw = dict(tol=1e-13)
+    if case == "neumann_cg2l":
+        kw.update(outlet=1, krylov=cf.KRYLOV_CG2L)
     if case == "neumann":
         kw.update(outlet=1)
     elif case == "two_correctors":
@@ -210,7 +213,7 @@ def test_variants_parity(cf, po, case):
     elif case == "outlet_p":
         kw.update(outlet_p=10.0)
     s, o = make_pair(cf, po, m, **kw)
-    if case == "neumann":
+    if case.startswith("neumann"):
         assert s.reference_node >= 0 and o.reference_node() == s.reference_node
     for u, p, st in run_both(s, o, 3):
         assert rel_l2(u, st["u"]) < 1e-8, case
@@ -315,7 +318,7 @@ def test_reassembly_after_vertex_motion(cf, po):
         assert csr_equal(s.matrix(which), o2.matrix(name)), name
 
 
-@pytest.mark.parametrize("krylov", [0, 1, 2], ids=["cg", "bicgstab", "cg1"])
+@pytest.mark.parametrize("krylov", [0, 1, 2, 3], ids=["cg", "bicgstab", "cg1", "cg2l"])
 def test_trajectory_bit_exact(cf, po, krylov):
     """The oracle reduces its Krylov dot products in the device's fixed tree and applies the
     same column-scaled operator, so FP64 trajectories agree bit for bit, iteration counts too."""
@@ -371,7 +374,7 @@ def test_resident_cg_equals_persistent_cg(cf, po, layers):
         assert out[0][2] == o[2]
 
 
-@pytest.mark.parametrize("krylov", [0, 1, 2], ids=["cg", "bicgstab", "cg1"])
+@pytest.mark.parametrize("krylov", [0, 1, 2, 3], ids=["cg", "bicgstab", "cg1", "cg2l"])
 def test_jacobi_norm_trajectory_bit_exact(cf, po, krylov):
     """The Jacobi-scaled convergence norm, oracle and device in the same reduction tree."""
     m = make_mesh(cf, 3, 12)
@@ -403,3 +406,53 @@ def test_single_reduction_cg_matches_cg(cf, po):
         else:
             assert rel_l2(out[1][0], out[0][0]) <= 1e-9
             assert rel_l2(out[1][1], out[0][1]) <= 1e-9
+
+
+@pytest.mark.parametrize("target", [16, 256])
+def test_two_level_cg_bit_exact_many_blocks(cf, po, target):
+    """CFSA_KRYLOV_CG2L on a mesh where every CTA of the resident grid owns several blocks and
+    aggregates span several CTAs: same coarse space (aggregate count), same iteration counts and
+    the same bits as the oracle's cg2l, for a coarse and a fine aggregation."""
+    m = make_mesh(cf, 6, 300)
+    s, o = make_pair(cf, po, m, tol=1e-10, krylov=cf.KRYLOV_CG2L, norm=cf.NORM_JACOBI)
+    s.setCoarseTarget(target)
+    o.set_coarse_target(target)
+    for k in range(2):
+        assert s.pisoStep() and o.piso_step() == 0
+        assert s.stats()["pressure_iters"] == o.stats()["pressure_iters"], k
+        st = o.state()
+        assert np.array_equal(s.getPressureCorrection(), st["pcorr"]), k
+        assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"]), k
+    assert s.coarseSize() == o.coarse_size() >= target
+
+
+def test_two_level_cg_matches_cg(cf, po):
+    """The two-level preconditioner changes the iterates, not the solution: u and p within 1e-8 of
+    Jacobi CG (the FP64 parity bar) at a tight tolerance, in several times fewer pressure
+    iterations."""
+    m = make_mesh(cf, 6, 300)
+    out = []
+    for krylov in (cf.KRYLOV_CG, cf.KRYLOV_CG2L):
+        s, _ = make_pair(cf, po, m, tol=1e-13, krylov=krylov, norm=cf.NORM_JACOBI)
+        ok, done = s.pisoSteps(3)
+        assert ok and done == 3
+        out.append((s.getVelocity(), s.getPressure(), s.stats()["pressure_iters"]))
+    assert rel_l2(out[1][0], out[0][0]) <= 1e-8
+    assert rel_l2(out[1][1], out[0][1]) <= 1e-8
+    assert out[1][2] * 2 < out[0][2], (out[0][2], out[1][2])
+
+
+def test_two_level_cg_graph_equals_eager(cf, po):
+    m = make_mesh(cf, 4, 40)
+    res = []
+    for env in ({"CFSA_NO_GRAPH": "1"}, {}):
+        os.environ.update(env)
+        try:
+            s, _ = make_pair(cf, po, m, tol=1e-10, krylov=cf.KRYLOV_CG2L)
+        finally:
+            for k in env:
+                os.environ.pop(k, None)
+        ok, done = s.pisoSteps(3)
+        assert ok and done == 3
+        res.append((s.getVelocity(), s.getPressure()))
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
