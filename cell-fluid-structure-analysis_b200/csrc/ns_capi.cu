@@ -163,7 +163,7 @@ struct cfsa_ns {
   // two-level pressure preconditioner of k_cg2l_resident (rebuilt with the Poisson operator)
   int coarse_target = 256;
   bool coarse_dirty = true;
-  int coarse_nc = 0, coarse_np = 0;
+  int coarse_nc = 0;
   std::vector<void *> coarse_allocs;
   CoarseView coarse_view{};
   int cg2l_col_cap = 0;
@@ -766,70 +766,68 @@ struct cfsa_ns {
           }
       }
     }
-    // aggregates of each natural block, block-partial slots of each aggregate
-    const int nblk = (int)blocks_for(n);
-    std::vector<int> blk_ptr(nblk + 1, 0), blk_agg;
-    for (int b = 0; b < nblk; ++b) {
-      std::vector<int> ms;
-      for (int64_t i = (int64_t)kBlock * b; i < std::min<int64_t>(n, (int64_t)kBlock * (b + 1)); ++i)
-        if (agg[i] < nc) ms.push_back(agg[i]);
-      std::sort(ms.begin(), ms.end());
-      ms.erase(std::unique(ms.begin(), ms.end()), ms.end());
-      blk_agg.insert(blk_agg.end(), ms.begin(), ms.end());
-      blk_ptr[b + 1] = (int)blk_agg.size();
-    }
-    const int np = (int)blk_agg.size();
-    std::vector<int> agg_ptr(nc + 1, 0), blk_slot(np, 0);
-    for (int m : blk_agg) agg_ptr[m + 1]++;
-    for (int m = 0; m < nc; ++m) agg_ptr[m + 1] += agg_ptr[m];
-    {
-      std::vector<int> fill(agg_ptr.begin(), agg_ptr.begin() + nc);
-      for (int q = 0; q < np; ++q) blk_slot[q] = fill[blk_agg[q]]++;
-    }
-    // aggregates each CTA reads: those of its rows and of their columns
-    std::vector<int> need_ptr(cg_res_grid + 1, 0), need;
+    // per CTA: its rows sorted by aggregate (staging positions, one segment per aggregate) and
+    // the aggregates of its rows' columns (coarse values it reads)
+    const int nblk_sell = (int)blocks_for(s1.nrows_pad);
+    std::vector<int> row_pos(n, -1), own_ptr(cg_res_grid + 1, 0), own, seg_lo, seg_hi,
+        need_ptr(cg_res_grid + 1, 0), need;
+    int npos_max = 0;
     if (nc > 0) {
       std::vector<int> ci((size_t)nnz1);
       CK(cudaMemcpyAsync(ci.data(), ci1, (size_t)nnz1 * sizeof(int), cudaMemcpyDeviceToHost, stream));
       CK(cudaStreamSynchronize(stream));
-      const int nblk_sell = (int)blocks_for(s1.nrows_pad);
       for (int c = 0; c < cg_res_grid; ++c) {
         const int b0 = std::min(nblk_sell, c * cg_res_bpc_sell), b1 = std::min(nblk_sell, b0 + cg_res_bpc_sell);
-        std::vector<int> ms;
-        for (int64_t i = (int64_t)kBlock * b0; i < std::min<int64_t>(n, (int64_t)kBlock * b1); ++i) {
-          if (agg[i] < nc) ms.push_back(agg[i]);
+        const int64_t r0 = (int64_t)kBlock * b0, r1 = std::min<int64_t>(n, (int64_t)kBlock * b1);
+        std::vector<std::pair<int, int>> rows;  // (aggregate, row)
+        std::vector<int> mn;
+        for (int64_t i = r0; i < r1; ++i) {
+          if (agg[i] < nc) rows.push_back({agg[i], (int)i});
           for (int k = h_rp1[i]; k < h_rp1[i + 1]; ++k)
-            if (agg[ci[k]] < nc) ms.push_back(agg[ci[k]]);
+            if (agg[ci[k]] < nc) mn.push_back(agg[ci[k]]);
         }
-        std::sort(ms.begin(), ms.end());
-        ms.erase(std::unique(ms.begin(), ms.end()), ms.end());
-        need.insert(need.end(), ms.begin(), ms.end());
+        std::sort(rows.begin(), rows.end());
+        for (size_t q = 0; q < rows.size(); ++q) {
+          row_pos[rows[q].second] = (int)q;
+          if (q == 0 || rows[q].first != rows[q - 1].first) {
+            own.push_back(rows[q].first);
+            seg_lo.push_back((int)q);
+            seg_hi.push_back((int)q);
+            mn.push_back(rows[q].first);
+          }
+          seg_hi.back() = (int)q + 1;
+        }
+        own_ptr[c + 1] = (int)own.size();
+        std::sort(mn.begin(), mn.end());
+        mn.erase(std::unique(mn.begin(), mn.end()), mn.end());
+        need.insert(need.end(), mn.begin(), mn.end());
         need_ptr[c + 1] = (int)need.size();
+        npos_max = std::max(npos_max, (int)rows.size());
       }
     }
     CoarseView V{};
     V.nc = nc;
     V.agg = cupload(agg);
     V.Z = cupload(Z);
-    V.blk_ptr = cupload(blk_ptr);
-    V.blk_agg = cupload(blk_agg);
-    V.agg_ptr = cupload(agg_ptr);
-    V.blk_slot = cupload(blk_slot);
+    V.row_pos = cupload(row_pos);
+    V.own_ptr = cupload(own_ptr);
+    V.own = cupload(own);
+    V.seg_lo = cupload(seg_lo);
+    V.seg_hi = cupload(seg_hi);
     V.need_ptr = cupload(need_ptr);
     V.need = cupload(need);
-    V.np = np;
-    for (int q = 0; q < 2; ++q) V.part[q] = cupload(std::vector<double>((size_t)3 * std::max(np, 1), 0.0));
+    V.gacc = cupload(std::vector<unsigned long long>((size_t)18 * std::max(nc, 1), 0ull));
+    V.npos_max = npos_max;
     // shared memory: coarse arrays, row staging, then as many column indices as fit
     int optin = 0;
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     cudaFuncAttributes fa{};
     CK(cudaFuncGetAttributes(&fa, k_cg2l_resident));
-    const int64_t coarse_bytes = (int64_t)(6 * nc + 2) * (int64_t)sizeof(double);
+    const int64_t coarse_bytes = (int64_t)(6 * nc + 2 + 2 * npos_max) * (int64_t)sizeof(double);
     const int64_t row_bytes = (int64_t)3 * cg_res_bpc_sell * kBlock * (int64_t)sizeof(int);
     const int64_t avail = (int64_t)optin - (int64_t)fa.sharedSizeBytes - coarse_bytes - row_bytes;
     if (avail < 0) throw CudaError{"two-level pressure preconditioner: coarse space too large for shared memory"};
     int max_entries = 0;
-    const int nblk_sell = (int)blocks_for(s1.nrows_pad);
     for (int c = 0; c < cg_res_grid; ++c) {
       const int b0 = std::min(nblk_sell, c * cg_res_bpc_sell), b1 = std::min(nblk_sell, b0 + cg_res_bpc_sell);
       if (b1 > b0) max_entries = std::max(max_entries, s1.h_sptr[std::min(8 * b1, s1.nslices)] - s1.h_sptr[8 * b0]);
@@ -843,7 +841,6 @@ struct cfsa_ns {
     CK(cudaStreamSynchronize(stream));
     coarse_view = V;
     coarse_nc = nc;
-    coarse_np = np;
     coarse_dirty = false;
     graph_dirty = true;
   }
@@ -1222,6 +1219,8 @@ struct cfsa_ns {
         c2.s[0] = ps;
         c2.s[1] = cg1_vec[2];
         c2.p = pp;
+        if (coarse_view.nc > 0)
+          CK(cudaMemsetAsync(coarse_view.gacc, 0, (size_t)18 * coarse_view.nc * sizeof(unsigned long long), stream));
         CK(cudaMemsetAsync(pp, 0, (size_t)nv * sizeof(double), stream));
         CK(cudaMemsetAsync(ps, 0, (size_t)nv * sizeof(double), stream));
         cfg.gridDim = dim3((unsigned int)cg_res_grid);

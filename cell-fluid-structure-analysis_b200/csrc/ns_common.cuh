@@ -60,6 +60,7 @@ struct BicgState {
 
 struct CgState {
   double absnew, alpha, beta, bnorm2, tol2, rnorm2;
+  double bb;  // b.b of the solve's right-hand side (scale of the two-level CG's fixed-point sums)
   int iters, status, active, maxit;
 };
 

@@ -949,6 +949,7 @@ __global__ void k_pressure_rhs(PressureRhsArgs A) {
       c->rnorm2 = crit;
       c->tol2 = tol2;
       c->absnew = tot[1];
+      c->bb = tot[0];
       c->iters = 0;
       c->maxit = A.maxit;
       c->status = done ? final_status : KS_RUNNING;
@@ -1715,33 +1716,37 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg1_resident(Cg1Args C) {
 // preconditioner M r = D^-1 r + P Z P^T r, where P is the indicator matrix of geometric aggregates
 // (boxes of a uniform grid over the vertices, rows without a penalty only) and Z = (P^T A P)^-1 is
 // a dense nc x nc matrix built on the host. The coarse correction removes the smooth error
-// components that make Jacobi-CG slow on the Poisson operator (684 -> ~130 iterations on the
-// 1M-tet cylinder with ~256 aggregates), at the price of per-iteration aggregate sums and a small
-// dense product.
+// components that make Jacobi-CG slow on the Poisson operator (681 -> 127 iterations on the
+// 1M-tet cylinder with ~256 aggregates requested).
 //
 // One grid barrier per iteration is kept: the coarse input t = P^T r of the new residual is
-// formed after the barrier from the previous iteration's exact aggregate sums of r, w and s,
-//   t = T(r) - alpha (T(w) + beta T(s)),   c = Z t,
+// formed after the barrier from the previous iteration's aggregate sums of r and w and the
+// aggregate-level recurrence for s,
+//   T(s) <- T(w) + beta T(s),   t = T(r) - alpha T(s),   c = Z t,
 // and each neighbour's new u = D^-1 r_new + c[agg] is then formed on the fly in the fused product,
-// as k_cg1_resident does for the Jacobi part. The aggregate sums are deterministic: per natural
-// block of 256 rows and per aggregate present in it, the block tree (8 warp butterflies in warp
-// order) of the masked values, then those block partials added in ascending block order by one
-// thread per aggregate; c[m] is a warp butterfly over lanes l of sum_{k = l mod 32} Z[m][k] t[k].
-// Each CTA forms c only for the aggregates that its rows and their neighbours belong to. The
+// as k_cg1_resident does for the Jacobi part.
+//
+// Aggregate sums are exact fixed-point sums, so their order does not matter and they cost a few
+// atomics instead of a reduction tree: each value x becomes the 128-bit integer floor(x 2^S)
+// (S = 80 - floor(log2(b.b) / 2), clamped to +-2^100). A CTA stages its rows' values in shared
+// memory sorted by aggregate, one warp per aggregate sums a segment exactly and adds it into a
+// global accumulator (two 64-bit atomics with the carry of the low word), and after the barrier a
+// sum converts back as (hi 2^64 + lo) 2^-S.
+// Global accumulators rotate over three buffers; the buffer of the next phase is cleared while no
+// CTA can still read it. c[m] is a warp butterfly over lanes l of sum_{k = l mod 32} Z[m][k]
+// t[k]. Each CTA forms c only for the aggregates its rows and their neighbours belong to. The
 // oracle's cg2l() restates the same arithmetic, so GPU and oracle agree bit for bit.
-constexpr int kAggChunk = 8;  // aggregates of one block summed per pass
-
 struct CoarseView {
-  int nc;                          // aggregates (0: Jacobi only)
-  const int *agg;                  // [n] aggregate of each row; nc for rows without one
-  const double *Z;                 // [nc*nc] (P^T A P)^-1, symmetric
-  const int *blk_ptr, *blk_agg;    // aggregates present in each natural block, ascending
-  const int *blk_slot;             // slot of each (block, aggregate) partial: aggregate-major,
-                                   // ascending block inside an aggregate
-  const int *agg_ptr;              // slots [agg_ptr[m], agg_ptr[m+1]) hold aggregate m's partials
-  const int *need_ptr, *need;      // aggregates whose coarse value each CTA reads
-  double *part[2];                 // [parity][3 * np] aggregate partials of r, w, s
-  int np;                          // block-partial slots
+  int nc;                       // aggregates (0: Jacobi only)
+  const int *agg;               // [n] aggregate of each row; nc for rows without one
+  const double *Z;              // [nc*nc] (P^T A P)^-1, symmetric
+  const int *row_pos;           // [n] position of the row in its CTA's aggregate-sorted staging
+                                // order, -1 for rows without aggregate
+  const int *own_ptr, *own;     // aggregates of each CTA's rows (ascending)
+  const int *seg_lo, *seg_hi;   // staging positions of each own aggregate's rows
+  const int *need_ptr, *need;   // aggregates whose coarse value each CTA reads
+  unsigned long long *gacc;     // [3 buffers][3 vectors][nc][lo, hi] fixed-point sums
+  int npos_max;                 // largest staging list (shared-memory doubles per vector)
 };
 
 struct Cg2lArgs {
@@ -1751,71 +1756,95 @@ struct Cg2lArgs {
   double *p;                   // zero on entry
 };
 
-// Aggregate block partials of NV vectors over this CTA's natural blocks [b0, b1); vector v's
-// partial of slot q goes to out[v * np + q].
+// floor(x 2^S) as a two's-complement 128-bit integer (lo, hi); x 2^S is clamped to +-2^100 and a
+// NaN counts as 0.
+__device__ __forceinline__ void fixed128(double x, double scale, unsigned long long &lo,
+                                         unsigned long long &hi) {
+  double y = x * scale;
+  if (!(y == y)) y = 0.0;
+  y = fmin(fmax(y, -0x1p100), 0x1p100);
+  const double t = floor(y);
+  if (fabs(t) < 0x1p63) {
+    const long long v = (long long)t;
+    lo = (unsigned long long)v;
+    hi = (v < 0) ? ~0ull : 0ull;
+  } else {
+    const double hd = floor(t * 0x1p-64);
+    hi = (unsigned long long)(long long)hd;
+    lo = (unsigned long long)(t - hd * 0x1p64);
+  }
+}
+
+__device__ __forceinline__ void add128(unsigned long long *p, unsigned long long lo, unsigned long long hi) {
+  const unsigned long long old = atomicAdd(p, lo);
+  atomicAdd(p + 1, hi + ((old + lo < old) ? 1ull : 0ull));
+}
+
+__device__ __forceinline__ double unfixed128(unsigned long long lo, unsigned long long hi, double iscale) {
+  return ((double)(long long)hi * 0x1p64 + (double)lo) * iscale;
+}
+
+// Sums of this CTA's staged values per own aggregate into global buffer `buf`: one warp per
+// aggregate segment. Each lane adds its values exactly as 128-bit integers offset by 2^100 (so
+// that they are non-negative); the lane sums are cut into five 26-bit limbs, each limb summed by a
+// warp reduction (32 x 2^26 < 2^32), and lane 0 re-assembles the total, removes count x 2^100 and
+// adds it to the global accumulator.
 template <int NV>
-__device__ __forceinline__ void agg_partials(const double *const (&vec)[NV], const CoarseView &V,
-                                             double *__restrict__ out, int b0, int b1, int n, int g,
-                                             double (*sw)[kAggChunk][3][kBlock / 32]) {
-  const int lt = threadIdx.x & (kBlock - 1), warp = lt >> 5, lane = lt & 31;
-  for (int b = b0 + g; b < b1; b += kCgResGroups) {
-    const int i = b * kBlock + lt;
-    const bool in = i < n;
-    const int a = in ? __ldg(V.agg + i) : V.nc;
-    double x[NV];
+__device__ __forceinline__ void seg_sums(const CoarseView &V, const double *__restrict__ stage,
+                                         int buf, const int (&vi)[NV], double scale) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int q0 = __ldg(V.own_ptr + blockIdx.x), q1 = __ldg(V.own_ptr + blockIdx.x + 1);
+  for (int q = q0 + warp; q < q1; q += nw) {
+    const int p0 = __ldg(V.seg_lo + q), p1 = __ldg(V.seg_hi + q), m = __ldg(V.own + q);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) x[v] = in ? __ldcg(vec[v] + i) : 0.0;
-    const int q0 = V.blk_ptr[b], q1 = V.blk_ptr[b + 1];
-    for (int qc = q0; qc < q1; qc += kAggChunk) {
-      const int nq = min(kAggChunk, q1 - qc);
-      for (int k = 0; k < nq; ++k) {
-        const int m = __ldg(V.blk_agg + qc + k);
-        const bool has = __any_sync(0xffffffffu, a == m);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          const double ws = has ? warp_sum((a == m) ? x[v] : 0.0) : 0.0;
-          if (lane == 0) sw[g][k][v][warp] = ws;
-        }
+    for (int v = 0; v < NV; ++v) {
+      const double *sv = stage + (size_t)v * V.npos_max;
+      unsigned long long al = 0ull, ah = 0ull;
+      for (int p = p0 + lane; p < p1; p += 32) {
+        unsigned long long l, h;
+        fixed128(sv[p], scale, l, h);
+        h += 1ull << 36;  // + 2^100
+        al += l;
+        ah += h + ((al < l) ? 1ull : 0ull);
       }
-      group_sync(g);
-      if (lt < nq * NV) {
-        const int k = lt / NV, v = lt % NV;
-        double sum = 0.0;
-        for (int w = 0; w < kBlock / 32; ++w) sum += sw[g][k][v][w];
-        __stcg(out + (size_t)v * V.np + __ldg(V.blk_slot + qc + k), sum);
+      const unsigned m26 = (1u << 26) - 1u;
+      const unsigned long long s0 = __reduce_add_sync(0xffffffffu, (unsigned)(al & m26));
+      const unsigned long long s1 = __reduce_add_sync(0xffffffffu, (unsigned)((al >> 26) & m26));
+      const unsigned long long s2 = __reduce_add_sync(0xffffffffu, (unsigned)(((al >> 52) | (ah << 12)) & m26));
+      const unsigned long long s3 = __reduce_add_sync(0xffffffffu, (unsigned)((ah >> 14) & m26));
+      const unsigned long long s4 = __reduce_add_sync(0xffffffffu, (unsigned)((ah >> 40) & m26));
+      if (lane == 0) {
+        const unsigned long long l1 = s0 + (s1 << 26);
+        const unsigned long long l2 = l1 + (s2 << 52);
+        const unsigned long long h = (s2 >> 12) + (s3 << 14) + (s4 << 40) + ((l2 < l1) ? 1ull : 0ull) -
+                                     ((unsigned long long)(p1 - p0) << 36);
+        add128(V.gacc + 2 * ((size_t)(3 * buf + vi[v]) * V.nc + m), l2, h);
       }
-      group_sync(g);
     }
   }
 }
 
-// Aggregate sums of NV vectors from their block partials: one thread per (aggregate, vector),
-// its partials (contiguous, ascending block) loaded in batches of kSumBatch before they are added
-// in order, so that an aggregate costs one L2 round trip per batch.
-constexpr int kSumBatch = 8;
+// Clears global buffer `buf` (every CTA a share).
+__device__ __forceinline__ void clear_acc(const CoarseView &V, int buf) {
+  unsigned long long *g = V.gacc + (size_t)2 * 3 * V.nc * buf;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 6 * V.nc; k += gridDim.x * blockDim.x) g[k] = 0ull;
+}
 
+// Aggregate sums of vectors [v0, v0 + NV) from global buffer `buf`.
 template <int NV>
-__device__ __forceinline__ void agg_sums(const CoarseView &V, const double *__restrict__ part,
-                                         double *const (&dst)[NV]) {
-  for (int idx = threadIdx.x; idx < V.nc * NV; idx += blockDim.x) {
-    const int m = idx / NV, v = idx - m * NV;
-    const int q0 = __ldg(V.agg_ptr + m), q1 = __ldg(V.agg_ptr + m + 1);
-    const double *pv = part + (size_t)v * V.np;
-    double sum = 0.0;
-    for (int q = q0; q < q1; q += kSumBatch) {
-      double x[kSumBatch];
-#pragma unroll
-      for (int u = 0; u < kSumBatch; ++u) x[u] = (q + u < q1) ? __ldcg(pv + q + u) : 0.0;
-#pragma unroll
-      for (int u = 0; u < kSumBatch; ++u)
-        if (q + u < q1) sum += x[u];
-    }
-    dst[v][m] = sum;
+__device__ __forceinline__ void read_sums(const CoarseView &V, int buf, int v0, double iscale,
+                                          double *const (&dst)[NV]) {
+  for (int idx = threadIdx.x; idx < NV * V.nc; idx += blockDim.x) {
+    const int v = idx / V.nc, m = idx - v * V.nc;
+    const unsigned long long *a = V.gacc + 2 * ((size_t)(3 * buf + v0 + v) * V.nc + m);
+    dst[v][m] = unfixed128(__ldcg(a), __ldcg(a + 1), iscale);
   }
 }
 
 // c[m] = Z[m] . t for the aggregates this CTA reads: one warp per aggregate, lane l adding
-// k = l, l + 32, ... in order (Z loads issued kSumBatch at a time), then a warp butterfly.
+// k = l, l + 32, ... in order, then a warp butterfly.
+constexpr int kZBatch = 8;
+
 __device__ __forceinline__ void coarse_values(const CoarseView &V, const double *__restrict__ t,
                                               double *__restrict__ c) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -1825,12 +1854,12 @@ __device__ __forceinline__ void coarse_values(const CoarseView &V, const double 
     const int m = __ldg(V.need + q);
     const double *zr = V.Z + (size_t)m * nc;
     double sum = 0.0;
-    for (int k0 = lane; k0 < nc; k0 += 32 * kSumBatch) {
-      double z[kSumBatch];
+    for (int k0 = lane; k0 < nc; k0 += 32 * kZBatch) {
+      double z[kZBatch];
 #pragma unroll
-      for (int u = 0; u < kSumBatch; ++u) z[u] = (k0 + 32 * u < nc) ? __ldg(zr + k0 + 32 * u) : 0.0;
+      for (int u = 0; u < kZBatch; ++u) z[u] = (k0 + 32 * u < nc) ? __ldg(zr + k0 + 32 * u) : 0.0;
 #pragma unroll
-      for (int u = 0; u < kSumBatch; ++u)
+      for (int u = 0; u < kZBatch; ++u)
         if (k0 + 32 * u < nc) sum += z[u] * t[k0 + 32 * u];
     }
     sum = warp_sum(sum);
@@ -1842,7 +1871,6 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
   extern __shared__ double s_dbl[];
   __shared__ double s_grp[kCgResGroups][4][kBlock / 32];
   __shared__ double s_tree[4][kBlock / 32];
-  __shared__ double s_agw[kCgResGroups][kAggChunk][3][kBlock / 32];
   const CgResidentArgs &R = C.R;
   const CgPersistentArgs &A = R.P;
   const CoarseView &V = C.V;
@@ -1853,10 +1881,12 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
   const int b1 = min(A.nblk_sell, b0 + R.bpc_sell);
   const int nc = V.nc, n = A.n;
   // shared memory: aggregate sums of r, w, s, the coarse input t, coarse values (two
-  // generations, entry nc = 0 for rows without aggregate), then the row staging of k_cg1_resident
+  // generations, entry nc = 0 for rows without aggregate), the aggregate-sorted staging of two
+  // row vectors, then the row staging of k_cg1_resident
   double *cR = s_dbl, *cW = cR + nc, *cS = cW + nc, *ct = cS + nc;
   double *cc[2] = {ct + nc, ct + 2 * nc + 1};
-  int *s_row = reinterpret_cast<int *>(ct + 3 * nc + 2);
+  double *s_stage = ct + 3 * nc + 2;
+  int *s_row = reinterpret_cast<int *>(s_stage + 2 * V.npos_max);
   int *s_len = s_row + R.bpc_sell * kBlock;
   int *s_base = s_len + R.bpc_sell * kBlock;
   int *s_col = s_base + R.bpc_sell * kBlock;
@@ -1872,30 +1902,45 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
     s_len[q] = in ? A.S.len[r] : 0;
     s_base[q] = in ? A.S.sptr[r >> 5] + (r & 31) : 0;
   }
-  if (threadIdx.x == 0) {
-    cc[0][nc] = 0.0;
-    cc[1][nc] = 0.0;
+  for (int m = threadIdx.x; m <= nc; m += kCgResThreads) {
+    cc[0][m] = 0.0;
+    cc[1][m] = 0.0;
+    if (m < nc) cS[m] = 0.0;
   }
-  for (int m = threadIdx.x; m < nc; m += kCgResThreads) cS[m] = 0.0;
   __syncthreads();
   const double tol2 = A.cs->tol2;
   const int maxit = A.cs->maxit;
+  // fixed-point scale of the aggregate sums: 2^S with S = 80 - floor(log2(b.b) / 2)
+  int S = 80;
+  {
+    const double bb = A.cs->bb;
+    if (bb > 0.0 && bb <= 1.7976931348623157e308) {
+      const int e2 = ilogb(bb);
+      S = 80 - ((e2 >= 0) ? e2 / 2 : -((1 - e2) / 2));
+    }
+  }
+  const double scale = scalbn(1.0, S), iscale = scalbn(1.0, -S);
   double gamma = 0.0, alpha = 0.0, beta = 0.0, rn2 = A.cs->bnorm2;
   int it = 0, status = KS_RUNNING, cur = 0, pc = 0;
   if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[1] += 1;
   const double *bvec = C.r[0];
-  // start: c0 = Z T(b)
+  const int v_r[1] = {0}, v_w[1] = {1}, v_rw[2] = {0, 1};
+  // start: c0 = Z T(b) (phase 0, buffer 0)
   if (nc > 0) {
-    const double *const vb[1] = {bvec};
-    agg_partials<1>(vb, V, V.part[0], b0, b1, n, g, s_agw);
+    for (int i = b0 * kBlock + (int)threadIdx.x; i < min(n, b1 * kBlock); i += kCgResThreads) {
+      const int ps = __ldg(V.row_pos + i);
+      if (ps >= 0) s_stage[ps] = __ldcg(bvec + i);
+    }
+    __syncthreads();
+    seg_sums<1>(V, s_stage, 0, v_r, scale);
     if (!grid_sync(A.bar)) return;
     double *const dR[1] = {cR};
-    agg_sums<1>(V, V.part[0], dR);
+    read_sums<1>(V, 0, 0, iscale, dR);
     __syncthreads();
     coarse_values(V, cR, cc[0]);
     __syncthreads();
   }
-  // w0 = A u0 with u0 = D^-1 b + c0[agg]; delta0 = w0.u0, gamma0 = b.u0 (product order)
+  // phase 1 (buffer 1): w0 = A u0 with u0 = D^-1 b + c0[agg]; delta0 = w0.u0, gamma0 = b.u0
   for (int b = b0 + g; b < b1; b += kCgResGroups) {
     const int lp = (b - b0) * kBlock + lt;
     const int i = s_row[lp];
@@ -1915,13 +1960,16 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
       __stcg(C.w[0] + i, acc);
       v[0] = acc * ui;
       v[1] = bi * ui;
+      if (nc > 0) {
+        const int ps = __ldg(V.row_pos + i);
+        if (ps >= 0) s_stage[ps] = acc;
+      }
     }
     group_partial<2>(v, A.part_a, b, g, s_grp);
   }
   if (nc > 0) {
-    __syncthreads();  // this CTA's w0 rows are written
-    const double *const vw[1] = {C.w[0]};
-    agg_partials<1>(vw, V, V.part[0] + V.np, b0, b1, n, g, s_agw);
+    __syncthreads();
+    seg_sums<1>(V, s_stage, 1, v_w, scale);
   }
   if (!grid_sync(A.bar)) return;
   {
@@ -1934,19 +1982,21 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
     gamma = d0[1];
     if (nc > 0) {
       double *const dW[1] = {cW};
-      agg_sums<1>(V, V.part[0] + V.np, dW);
+      read_sums<1>(V, 1, 1, iscale, dW);
       __syncthreads();
     }
   }
   while (status == KS_RUNNING) {
     double *part = (it & 1) ? A.part_a : A.part_b;
-    double *apart = V.part[(it + 1) & 1];
+    const int buf = (it + 2) % 3;  // phase it + 2
     const double *ro = C.r[cur], *wo = C.w[cur], *so = C.s[cur];
     double *rn = C.r[cur ^ 1], *wn = C.w[cur ^ 1], *sn = C.s[cur ^ 1];
     // coarse input of the new residual and its coarse values
     if (nc > 0) {
+      clear_acc(V, (it + 3) % 3);  // buffer of the next phase; last read before the previous barrier
       for (int m = threadIdx.x; m < nc; m += kCgResThreads) {
-        const double sm = cW[m] + beta * cS[m];
+        const double sm = cW[m] + beta * cS[m];  // T(s) of the new s, by recurrence
+        cS[m] = sm;
         ct[m] = cR[m] - alpha * sm;
       }
       __syncthreads();
@@ -2013,20 +2063,26 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
         v[1] = acc * ui;
         v[2] = ri * ri;
         v[3] = ri * (mi * ri);
+        if (nc > 0) {
+          const int ps = __ldg(V.row_pos + i);
+          if (ps >= 0) {
+            s_stage[ps] = ri;
+            s_stage[V.npos_max + ps] = acc;
+          }
+        }
       }
       group_partial<4>(v, part, b, g, s_grp);
     }
     if (nc > 0) {
-      __syncthreads();  // this CTA's new r, w, s rows are written
-      const double *const vv[3] = {rn, wn, sn};
-      agg_partials<3>(vv, V, apart, b0, b1, n, g, s_agw);
+      __syncthreads();
+      seg_sums<2>(V, s_stage, buf, v_rw, scale);
     }
     if (!grid_sync(A.bar)) return;
     double t[4];
     tree_total_cta<4>(part, A.nblk_sell, t, s_tree);
     if (nc > 0) {
-      double *const d3[3] = {cR, cW, cS};
-      agg_sums<3>(V, apart, d3);
+      double *const d2[2] = {cR, cW};
+      read_sums<2>(V, buf, 0, iscale, d2);
       __syncthreads();
     }
     ++it;

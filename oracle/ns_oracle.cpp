@@ -469,16 +469,15 @@ SolveInfo cg1(const CSR &A, const std::vector<double> &b, std::vector<double> &x
 // Z from the Cholesky factor G of A_c (row-wise Cholesky-Banachiewicz, then the lower-triangular
 // inverse by columns, then Z = G^-T G^-1 summed over ascending rows); A_c entries summed over the
 // CSR in row-major order. A non-SPD A_c (a pivot <= 0) disables the coarse part (nc = 0).
-// Aggregate sums of a vector v: per natural block b of 256 rows and per aggregate m present in it,
-// the block tree of the masked values (agg[row] == m ? v[row] : 0) -- 8 warp butterflies over
-// rows 256b + 32w .. +31, added in warp order -- then these block partials added in ascending block
-// order. Coarse values c[m] = butterfly over lanes l of (sum over k = l, l+32, ... of Z[m][k] t[k]).
+// Aggregate sums are exact fixed-point sums: x -> floor(x 2^S) as a 128-bit integer (x 2^S
+// clamped to +-2^100, NaN -> 0), S = 80 - floor(log2(b.b) / 2) for the solve's right-hand side b,
+// summed exactly and converted back as (hi 2^64 + lo) 2^-S with hi the upper 64 bits (signed) and
+// lo the lower 64 bits (unsigned). Coarse values c[m] = butterfly over lanes l of
+// (sum over k = l, l+32, ... of Z[m][k] t[k]).
 struct CoarseSpace {
   int nc = 0;
   std::vector<int> agg;                // [n], nc for rows without aggregate
   std::vector<double> Z;               // [nc*nc], symmetric
-  std::vector<int> blk_ptr, blk_agg;   // aggregates present in each natural block, ascending
-  std::vector<int> agg_ptr, agg_part;  // block-partial slots of each aggregate, ascending block
 };
 
 constexpr double kBoxShrink = 0.8408964152537145;  // 2^-1/4
@@ -607,54 +606,42 @@ CoarseSpace build_coarse(const CSR &A, const std::vector<V3> &xyz, const std::ve
         }
     }
   }
-  // block lists
-  const int64_t nblk = (n + 255) / 256;
-  cs.blk_ptr.assign(nblk + 1, 0);
-  cs.blk_agg.clear();
-  for (int64_t b = 0; b < nblk; ++b) {
-    std::vector<int> ms;
-    for (int64_t i = 256 * b; i < std::min(n, 256 * (b + 1)); ++i)
-      if (cs.agg[i] < cs.nc) ms.push_back(cs.agg[i]);
-    std::sort(ms.begin(), ms.end());
-    ms.erase(std::unique(ms.begin(), ms.end()), ms.end());
-    cs.blk_agg.insert(cs.blk_agg.end(), ms.begin(), ms.end());
-    cs.blk_ptr[b + 1] = (int)cs.blk_agg.size();
-  }
-  cs.agg_ptr.assign(cs.nc + 1, 0);
-  for (int m : cs.blk_agg) cs.agg_ptr[m + 1]++;
-  for (int m = 0; m < cs.nc; ++m) cs.agg_ptr[m + 1] += cs.agg_ptr[m];
-  cs.agg_part.assign(cs.blk_agg.size(), 0);
-  std::vector<int> fill(cs.agg_ptr.begin(), cs.agg_ptr.end() - (cs.nc > 0 ? 1 : 0));
-  for (size_t q = 0; q < cs.blk_agg.size(); ++q) cs.agg_part[fill[cs.blk_agg[q]]++] = (int)q;
   return cs;
 }
 
+// fixed-point scale exponent of a solve with right-hand side norm^2 b2
+int fixed_scale(double b2) {
+  if (!(b2 > 0.0) || !(b2 <= std::numeric_limits<double>::max())) return 80;
+  const int e2 = std::ilogb(b2);
+  return 80 - ((e2 >= 0) ? e2 / 2 : -((1 - e2) / 2));
+}
+
+__int128 fixed128(double x, double scale) {
+  double y = x * scale;
+  if (!(y == y)) y = 0.0;
+  y = std::fmin(std::fmax(y, -0x1p100), 0x1p100);
+  const double t = std::floor(y);
+  if (std::fabs(t) < 0x1p63) return (__int128)(long long)t;
+  const double hd = std::floor(t * 0x1p-64);
+  const unsigned long long hi = (unsigned long long)(long long)hd;
+  const unsigned long long lo = (unsigned long long)(t - hd * 0x1p64);
+  return (__int128)(((unsigned __int128)hi << 64) | (unsigned __int128)lo);
+}
+
+double unfixed128(__int128 v, double iscale) {
+  const long long hi = (long long)(v >> 64);
+  const unsigned long long lo = (unsigned long long)v;
+  return ((double)hi * 0x1p64 + (double)lo) * iscale;
+}
+
 // aggregate sums of v (size nc)
-std::vector<double> aggregate_sums(const CoarseSpace &cs, const std::vector<double> &v) {
-  const int64_t n = (int64_t)v.size();
-  std::vector<double> part(cs.blk_agg.size());
-  const int64_t nblk = (int64_t)cs.blk_ptr.size() - 1;
-#pragma omp parallel for schedule(static)
-  for (int64_t b = 0; b < nblk; ++b)
-    for (int q = cs.blk_ptr[b]; q < cs.blk_ptr[b + 1]; ++q) {
-      const int m = cs.blk_agg[q];
-      double s = 0.0;
-      for (int w = 0; w < 8; ++w) {
-        double x[32];
-        for (int l = 0; l < 32; ++l) {
-          const int64_t i = 256 * b + 32 * w + l;
-          x[l] = (i < n && cs.agg[i] == m) ? v[i] : 0.0;
-        }
-        s += warp_butterfly(x);
-      }
-      part[q] = s;
-    }
-  std::vector<double> T(cs.nc, 0.0);
-  for (int m = 0; m < cs.nc; ++m) {
-    double s = 0.0;
-    for (int q = cs.agg_ptr[m]; q < cs.agg_ptr[m + 1]; ++q) s += part[cs.agg_part[q]];
-    T[m] = s;
-  }
+std::vector<double> aggregate_sums(const CoarseSpace &cs, const std::vector<double> &v, int S) {
+  const double scale = std::scalbn(1.0, S), iscale = std::scalbn(1.0, -S);
+  std::vector<__int128> acc(cs.nc, 0);
+  for (size_t i = 0; i < v.size(); ++i)
+    if (cs.agg[i] < cs.nc) acc[cs.agg[i]] += fixed128(v[i], scale);
+  std::vector<double> T(cs.nc);
+  for (int m = 0; m < cs.nc; ++m) T[m] = unfixed128(acc[m], iscale);
   return T;
 }
 
@@ -675,8 +662,9 @@ std::vector<double> coarse_values(const CoarseSpace &cs, const std::vector<doubl
 }
 
 // Single-reduction CG (the recurrences of cg1) preconditioned by M r = D^-1 r + P Z P^T r.
-// t = P^T r of the new residual comes from the previous iteration's exact aggregate sums of r, w
-// and s (t = T(r) - alpha (T(w) + beta T(s))), so the device needs one grid barrier per iteration.
+// t = P^T r of the new residual comes from the previous iteration's aggregate sums of r and w and
+// the aggregate-level recurrence T(s) <- T(w) + beta T(s), t = T(r) - alpha T(s), so the device
+// needs one grid barrier per iteration.
 // Start: u = M b, w = A u, gamma = b.u and delta = w.u in product order. The stopping rule is
 // cg1's: ||r||^2 or, scaled, sum r_i (r_i / a_ii) (the Jacobi-scaled norm, not r.u).
 SolveInfo cg2l(const CSR &A, const std::vector<double> &b, std::vector<double> &x, double tol,
@@ -695,13 +683,14 @@ SolveInfo cg2l(const CSR &A, const std::vector<double> &b, std::vector<double> &
   double rn2 = bnorm2;
   int it = 0;
   if (!(bnorm2 == 0.0 || bnorm2 <= thr)) {
-    std::vector<double> R = aggregate_sums(cs, r), S(cs.nc, 0.0);
+    const int sc = fixed_scale(b2);
+    std::vector<double> R = aggregate_sums(cs, r, sc), S(cs.nc, 0.0);
     std::vector<double> c = coarse_values(cs, R);
     for (int64_t k = 0; k < n; ++k) u[k] = invdiag[k] * r[k] + c[cs.agg[k]];
     spmv(A, u.data(), w.data());
     const double delta0 = odot(sell, w.data(), u.data());
     double gamma = odot(sell, r.data(), u.data());
-    std::vector<double> W = aggregate_sums(cs, w);
+    std::vector<double> W = aggregate_sums(cs, w, sc);
     if (delta0 == 0.0 || std::isnan(delta0) || std::isnan(gamma)) {
       info.rel_res = 1.0;
       return info;
@@ -710,7 +699,8 @@ SolveInfo cg2l(const CSR &A, const std::vector<double> &b, std::vector<double> &
     std::vector<double> t(cs.nc);
     while (true) {
       for (int m = 0; m < cs.nc; ++m) {
-        const double sm = W[m] + beta * S[m];
+        const double sm = W[m] + beta * S[m];  // T(s) of the new s, by recurrence
+        S[m] = sm;
         t[m] = R[m] - alpha * sm;
       }
       c = coarse_values(cs, t);
@@ -726,9 +716,8 @@ SolveInfo cg2l(const CSR &A, const std::vector<double> &b, std::vector<double> &
       const double delta = odot(sell, w.data(), u.data());
       const double rr = odot(sell, r.data(), r.data());
       const double rz = tree_sum(sell, [&](int i) { return r[i] * (invdiag[i] * r[i]); });
-      R = aggregate_sums(cs, r);
-      W = aggregate_sums(cs, w);
-      S = aggregate_sums(cs, s);
+      R = aggregate_sums(cs, r, sc);
+      W = aggregate_sums(cs, w, sc);
       rn2 = scaled ? rz : rr;
       ++it;
       if (std::isnan(g_new) || std::isnan(delta) || std::isnan(rr) || std::isnan(rz)) break;
