@@ -80,7 +80,9 @@ int main(int argc, char **argv) {
   ns->setNumberOfCorrections(N.n_corrections);
   ns->setPressureSolver(N.pressure_solver == "bicgstab" ? CFSA_KRYLOV_BICGSTAB
                         : N.pressure_solver == "cg"     ? CFSA_KRYLOV_CG
-                                                        : CFSA_KRYLOV_CG1);
+                        : N.pressure_solver == "cg1"    ? CFSA_KRYLOV_CG1
+                                                        : CFSA_KRYLOV_CG2L);
+  ns->setCoarseTarget(N.coarse_aggregates);
   ns->setPrecision(N.precision == "mixed" ? CFSA_PRECISION_MIXED : CFSA_PRECISION_FP64);
   ns->setConvergenceNorm(N.convergence_norm == "jacobi" ? CFSA_NORM_JACOBI : CFSA_NORM_REFERENCE);
   ns->initialize(mesh, fluid);

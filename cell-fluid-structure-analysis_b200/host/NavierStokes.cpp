@@ -53,6 +53,7 @@ void NavierStokesSolver::pushParameters() {
   status(cfsa_ns_set_outlet(h_, (int)outlet_type_, outlet_pressure_), "setOutlet");
   status(cfsa_ns_set_reference_node(h_, reference_node_), "setReferencePressureNode");
   status(cfsa_ns_set_pressure_solver(h_, krylov_), "setPressureSolver");
+  status(cfsa_ns_set_coarse_target(h_, coarse_target_), "setCoarseTarget");
   status(cfsa_ns_set_precision(h_, precision_), "setPrecision");
   status(cfsa_ns_set_convergence_norm(h_, conv_norm_), "setConvergenceNorm");
   pushInlet();
@@ -342,6 +343,11 @@ void NavierStokesSolver::setMaxIterations(int momentum, int pressure) {
 void NavierStokesSolver::setPressureSolver(int krylov) {
   krylov_ = krylov;
   if (h_) status(cfsa_ns_set_pressure_solver(h_, krylov), "setPressureSolver");
+}
+
+void NavierStokesSolver::setCoarseTarget(int target) {
+  coarse_target_ = target;
+  if (h_) status(cfsa_ns_set_coarse_target(h_, target), "setCoarseTarget");
 }
 
 void NavierStokesSolver::setPrecision(int precision) {

@@ -31,6 +31,7 @@ class NavierStokesSolver {
   double relax_p_ = 1.0;
   double dt_ = 1e-4;
   int krylov_ = CFSA_KRYLOV_CG;
+  int coarse_target_ = 256;
   int precision_ = CFSA_PRECISION_FP64;
   int conv_norm_ = CFSA_NORM_REFERENCE;
 
@@ -138,7 +139,8 @@ class NavierStokesSolver {
   // new
   void setKrylovTolerances(double momentum, double pressure);
   void setMaxIterations(int momentum, int pressure);
-  void setPressureSolver(int krylov);  // CFSA_KRYLOV_CG or CFSA_KRYLOV_BICGSTAB
+  void setPressureSolver(int krylov);  // CFSA_KRYLOV_CG, _BICGSTAB, _CG1 or _CG2L
+  void setCoarseTarget(int target);    // aggregates of the CFSA_KRYLOV_CG2L coarse space (default 256)
   void setPrecision(int precision);    // CFSA_PRECISION_FP64 or CFSA_PRECISION_MIXED
   void setConvergenceNorm(int norm);   // CFSA_NORM_REFERENCE or CFSA_NORM_JACOBI
   void setInletVelocityProfile(const std::vector<Vec3> &per_node);

@@ -233,7 +233,12 @@ SimulationConfig parseConfig(const std::string &text) {
         }
       });
       opt(ns, "precision", [&](const Node *n, const std::string &k) { N.precision = n->scalar; one_of(N.precision, {"fp64", "mixed"}, k); });
-      opt(ns, "pressure_solver", [&](const Node *n, const std::string &k) { N.pressure_solver = n->scalar; one_of(N.pressure_solver, {"bicgstab", "cg", "cg1"}, k); });
+      opt(ns, "pressure_solver", [&](const Node *n, const std::string &k) { N.pressure_solver = n->scalar; one_of(N.pressure_solver, {"bicgstab", "cg", "cg1", "cg2l"}, k); });
+      opt(ns, "coarse_aggregates", [&](const Node *n, const std::string &k) {
+        N.coarse_aggregates = as_int(n, k);
+        if (N.coarse_aggregates < 1 || N.coarse_aggregates > 2048)
+          throw std::runtime_error("navier_stokes.coarse_aggregates must be in [1, 2048]");
+      });
       opt(ns, "convergence_norm", [&](const Node *n, const std::string &k) { N.convergence_norm = n->scalar; one_of(N.convergence_norm, {"reference", "jacobi"}, k); });
       opt(ns, "inlet_profile", [&](const Node *n, const std::string &k) { N.inlet_profile = n->scalar; one_of(N.inlet_profile, {"uniform", "parabolic"}, k); });
     }
@@ -293,6 +298,7 @@ std::string describe(const SimulationConfig &c) {
     << "\nnavier_stokes.tolerance = " << N.tolerance << "\nnavier_stokes.max_iterations = " << N.max_iterations[0]
     << " " << N.max_iterations[1] << "\nnavier_stokes.n_corrections = " << N.n_corrections
     << "\nnavier_stokes.precision = " << N.precision << "\nnavier_stokes.pressure_solver = " << N.pressure_solver
+    << "\nnavier_stokes.coarse_aggregates = " << N.coarse_aggregates
     << "\nnavier_stokes.convergence_norm = " << N.convergence_norm << "\nnavier_stokes.inlet_profile = "
     << N.inlet_profile << "\noutput.prefix = " << c.output.output_prefix << "\noutput.total_steps = "
     << c.output.total_steps << "\noutput.output_frequency = " << c.output.output_frequency

@@ -32,7 +32,8 @@ navier_stokes:
   tolerance: 1e-10
   max_iterations: [4000, 20000]
   precision: mixed
-  pressure_solver: cg1
+  pressure_solver: cg2l
+  coarse_aggregates: 128
   convergence_norm: jacobi
   inlet_profile: parabolic
 
@@ -73,7 +74,8 @@ def test_config_keys_resolved(tmp_path):
     assert d["navier_stokes.inlet_velocity"] == "0.25 0 0" and float(d["navier_stokes.outlet_pressure"]) == 2.5
     assert float(d["navier_stokes.dt"]) == 0.005 and float(d["navier_stokes.relax_p"]) == 0.7
     assert float(d["navier_stokes.tolerance"]) == 1e-10 and d["navier_stokes.max_iterations"] == "4000 20000"
-    assert d["navier_stokes.precision"] == "mixed" and d["navier_stokes.pressure_solver"] == "cg1"
+    assert d["navier_stokes.precision"] == "mixed" and d["navier_stokes.pressure_solver"] == "cg2l"
+    assert d["navier_stokes.coarse_aggregates"] == "128"
     assert d["navier_stokes.convergence_norm"] == "jacobi" and d["navier_stokes.inlet_profile"] == "parabolic"
     assert d["output.prefix"] == "run #1" and d["output.total_steps"] == "7" and d["output.output_frequency"] == "3"
     assert d["adjoint.enabled"] == "1" and d["adjoint.objective"] == "pressure_drop"
@@ -104,6 +106,7 @@ def test_config_defaults_are_the_references(tmp_path):
     ("mesh:\n  type: cylinder\n    radius: 2\n", "unexpected indentation"),
     ("mesh:\n  type: msh\n", "msh_file required"),
     ("mesh:\n  type: cylinder\nnavier_stokes:\n  enabled: true\n  precision: fp16\n", "unknown value 'fp16'"),
+    ("mesh:\n  type: cylinder\nnavier_stokes:\n  enabled: true\n  coarse_aggregates: 0\n", "coarse_aggregates must be in"),
 ])
 def test_config_errors(tmp_path, text, msg):
     r = dry_run(tmp_path, text)
