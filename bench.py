@@ -218,7 +218,7 @@ def adjoint_section(cf, args, barrier):
     s.setKrylovTolerances(ADJ_TOL, ADJ_TOL)
     s.setConvergenceNorm(cf.NORM_JACOBI)
     s.setMaxIterations(50000, 200000)
-    s.setPressureSolver(cf.KRYLOV_CG1)
+    s.setPressureSolver(cf.KRYLOV_CG2L)
     s.setDt(DT)
     s.initialize(m, cf.Fluid(*FLUID))
     s.setInletVelocityProfile(prof)
