@@ -456,3 +456,31 @@ def test_two_level_cg_graph_equals_eager(cf, po):
         assert ok and done == 3
         res.append((s.getVelocity(), s.getPressure()))
     assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+def test_two_level_cg_bit_exact_y_bifurcation(cf, po):
+    """The two-level CG on the Y-bifurcation (lattice vertex numbering, two outlets, boxes that cut
+    across the branches): same coarse space, iteration counts and bits as the oracle."""
+    m = cf.Mesh.yBifurcation(cell=0.4)
+    prof = cf.parabolic_inlet(m.nodePositions(), 1.0, 2.0)
+    s = cf.NavierStokesSolver()
+    s.setKrylovTolerances(1e-10, 1e-10)
+    s.setMaxIterations(5000, 20000)
+    s.setPressureSolver(cf.KRYLOV_CG2L)
+    s.setConvergenceNorm(cf.NORM_JACOBI)
+    s.setDt(0.01)
+    s.initialize(m, cf.Fluid(RHO, NU))
+    s.setInletVelocityProfile(prof)
+    o = po.Oracle(m.vertices(), m.tets(), apply_bc=False)
+    o.set_bc(*m.fluidBC())  # the generator's tags (inlet cap, both daughter caps outlet)
+    o.set_fluid(RHO, NU)
+    o.set_params(dt=0.01, tol_mom=1e-10, tol_p=1e-10, maxit_mom=5000, maxit_p=20000, pressure_solver=3,
+                 conv_norm=1)
+    o.initialize()
+    o.set_inlet(prof)
+    for k in range(2):
+        assert s.pisoStep() and o.piso_step() == 0
+        assert s.stats()["pressure_iters"] == o.stats()["pressure_iters"], k
+        st = o.state()
+        assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"]), k
+    assert s.coarseSize() == o.coarse_size() > 0
