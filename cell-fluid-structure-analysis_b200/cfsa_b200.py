@@ -722,6 +722,9 @@ class NavierStokesSolver:
             self._check(self._lib.cfsa_ns_set_max_iterations(self._h, *self.maxit))
 
     def setPressureSolver(self, krylov: int):
+        """Pressure Krylov method: KRYLOV_BICGSTAB (the reference's), KRYLOV_CG, KRYLOV_CG1
+        (one reduction per iteration) or KRYLOV_CG2L (KRYLOV_CG1 with the two-level
+        Jacobi + aggregation coarse-correction preconditioner, the fastest)."""
         self.krylov = int(krylov)
         if self._h is not None:
             self._check(self._lib.cfsa_ns_set_pressure_solver(self._h, self.krylov))

@@ -145,7 +145,10 @@ int cfsa_ns_set_inlet_uniform(cfsa_ns *h, const double u[3]);             /* set
 int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u /*[N2][3]*/);   /* new: per-node inlet */
 int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov);                   /* new: CG or BiCGSTAB */
 /* new: aggregate count the CFSA_KRYLOV_CG2L coarse space aims for (default 256, 1..2048); the
- * coarse space is rebuilt with the Poisson operator */
+ * coarse space is rebuilt with the Poisson operator. Its per-aggregate arrays (6 doubles each) share
+ * the solve kernel's shared memory with the row staging: a coarse space that does not fit (very
+ * large targets on very large meshes) fails the next step with CFSA_CUDA_ERROR and says so in
+ * cfsa_ns_last_error. */
 int cfsa_ns_set_coarse_target(cfsa_ns *h, int target);
 /* new: aggregates of the current CFSA_KRYLOV_CG2L coarse space (built on demand; 0 for the other
  * methods or when the coarse operator was not SPD) */
