@@ -443,7 +443,7 @@ __global__ void k_gather_div(int nv, const int *__restrict__ adj_ptr, const int 
 // in flight per thread; the products are still accumulated in ascending column order, so the
 // result is bit-identical to the sequential CSR row sum. Matrix entries are streamed once per
 // product (evict-first), the gathered vector stays cacheable.
-template <int NC, int U = 8>
+template <int NC, int U = 8, int MASK = (1 << NC) - 1>
 __device__ __forceinline__ void sell_spmv_row(const SellView &S, const double *__restrict__ val,
                                               const double *__restrict__ x, int64_t n, int r,
                                               double acc[NC]) {
@@ -464,18 +464,43 @@ __device__ __forceinline__ void sell_spmv_row(const SellView &S, const double *_
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
-      for (int c = 0; c < NC; ++c) xv[u][c] = __ldg(x + c * n + j[u]);
+      for (int c = 0; c < NC; ++c)
+        if ((MASK >> c) & 1) xv[u][c] = __ldg(x + c * n + j[u]);
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
-      for (int c = 0; c < NC; ++c) acc[c] += a[u] * xv[u][c];
+      for (int c = 0; c < NC; ++c)
+        if ((MASK >> c) & 1) acc[c] += a[u] * xv[u][c];
   }
   for (; k < len; ++k) {
     const int pos = base + k * kSellC;
     const int j = __ldcs(S.col + pos);
     const double a = __ldcs(val + pos);
 #pragma unroll
-    for (int c = 0; c < NC; ++c) acc[c] += a * __ldg(x + c * n + j);
+    for (int c = 0; c < NC; ++c)
+      if ((MASK >> c) & 1) acc[c] += a * __ldg(x + c * n + j);
+  }
+}
+
+// The batched product for the right-hand sides still active in `mask`: compile-time variants for
+// the cases with two active components (one converged first, typically the penalty-dominated
+// streamwise one), so that a converged component costs no gathers; other masks use the full
+// product. Active components get the same sums in the same order in every variant.
+template <int NC>
+__device__ __forceinline__ void sell_spmv_row_active(const SellView &S, const double *__restrict__ val,
+                                                     const double *__restrict__ x, int64_t n, int r,
+                                                     double acc[NC], int mask) {
+  if constexpr (NC == 3) {
+    if (mask == 6)
+      sell_spmv_row<3, 8, 6>(S, val, x, n, r, acc);
+    else if (mask == 5)
+      sell_spmv_row<3, 8, 5>(S, val, x, n, r, acc);
+    else if (mask == 3)
+      sell_spmv_row<3, 8, 3>(S, val, x, n, r, acc);
+    else
+      sell_spmv_row<3>(S, val, x, n, r, acc);
+  } else {
+    sell_spmv_row<NC>(S, val, x, n, r, acc);
   }
 }
 
@@ -698,7 +723,7 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_bicg_v(BicgArgs A) {
     for (int c = 0; c < NC; ++c) part[c] = 0.0;
     if (i >= 0) {
       double acc[NC];
-      sell_spmv_row<NC>(A.S, A.At, A.pk, n, r, acc);
+      sell_spmv_row_active<NC>(A.S, A.At, A.pk, n, r, acc, active);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         if (!((active >> c) & 1)) continue;
@@ -754,7 +779,7 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_bicg_t(BicgArgs A) {
     for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
     if (i >= 0) {
       double acc[NC];
-      sell_spmv_row<NC>(A.S, A.At, A.s, n, r, acc);
+      sell_spmv_row_active<NC>(A.S, A.At, A.s, n, r, acc, active);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         if (!((active >> c) & 1)) continue;

@@ -49,7 +49,7 @@ struct MixedArgs {
   const float *cw32;  // the same for the inner solve
 };
 
-template <int U = 8>
+template <int U = 8, int MASK = 7>
 __device__ __forceinline__ void sell_spmv_row_f32x3(const SellView &S, const float *__restrict__ val,
                                                     const float *__restrict__ x, int64_t n, int r,
                                                     float acc[3]) {
@@ -69,19 +69,36 @@ __device__ __forceinline__ void sell_spmv_row_f32x3(const SellView &S, const flo
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xv[u][c] = __ldg(x + c * n + j[u]);
+      for (int c = 0; c < 3; ++c)
+        if ((MASK >> c) & 1) xv[u][c] = __ldg(x + c * n + j[u]);
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) acc[c] += a[u] * xv[u][c];
+      for (int c = 0; c < 3; ++c)
+        if ((MASK >> c) & 1) acc[c] += a[u] * xv[u][c];
   }
   for (; k < len; ++k) {
     const int pos = base + k * kSellC;
     const int j = __ldcs(S.col + pos);
     const float a = __ldcs(val + pos);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) acc[c] += a * __ldg(x + c * n + j);
+    for (int c = 0; c < 3; ++c)
+      if ((MASK >> c) & 1) acc[c] += a * __ldg(x + c * n + j);
   }
+}
+
+// sell_spmv_row_f32x3 for the components still active in `mask` (see sell_spmv_row_active).
+__device__ __forceinline__ void sell_spmv_row_f32x3_active(const SellView &S, const float *__restrict__ val,
+                                                           const float *__restrict__ x, int64_t n, int r,
+                                                           float acc[3], int mask) {
+  if (mask == 6)
+    sell_spmv_row_f32x3<8, 6>(S, val, x, n, r, acc);
+  else if (mask == 5)
+    sell_spmv_row_f32x3<8, 5>(S, val, x, n, r, acc);
+  else if (mask == 3)
+    sell_spmv_row_f32x3<8, 3>(S, val, x, n, r, acc);
+  else
+    sell_spmv_row_f32x3(S, val, x, n, r, acc);
 }
 
 // Outer init (after k_momentum_rhs wrote b and x = 0): r64 = b, ||b||^2 per component.
@@ -209,7 +226,7 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_v(MixedArgs A) {
     double part[3] = {0.0, 0.0, 0.0};
     if (i >= 0) {
       float acc[3];
-      sell_spmv_row_f32x3(A.S, A.At32, A.p, n, r, acc);
+      sell_spmv_row_f32x3_active(A.S, A.At32, A.p, n, r, acc, act);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         if (!((act >> c) & 1)) continue;
@@ -258,7 +275,7 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_t(MixedArgs A) {
     double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (i >= 0) {
       float acc[3];
-      sell_spmv_row_f32x3(A.S, A.At32, A.s, n, r, acc);
+      sell_spmv_row_f32x3_active(A.S, A.At32, A.s, n, r, acc, act);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         if (!((act >> c) & 1)) continue;
@@ -368,7 +385,7 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_residual(MixedArgs A) {
     double part[3] = {0.0, 0.0, 0.0};
     if (i >= 0) {
       double acc[3];
-      sell_spmv_row<3>(A.S, A.At64, A.xs, n, r, acc);
+      sell_spmv_row_active<3>(A.S, A.At64, A.xs, n, r, acc, active);
       const double w = A.cw ? A.cw[i] : 1.0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
