@@ -484,3 +484,27 @@ def test_two_level_cg_bit_exact_y_bifurcation(cf, po):
         st = o.state()
         assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"]), k
     assert s.coarseSize() == o.coarse_size() > 0
+
+
+@pytest.mark.parametrize("case", ["one_aggregate", "two_correctors_relaxed", "retarget_between_steps"])
+def test_two_level_cg_edge_cases(cf, po, case):
+    """Two-level CG against the oracle bit for bit: a single aggregate (a one-dimensional coarse
+    space), two correctors with under-relaxation, and a coarse target changed between steps
+    (coarse space and step graph rebuilt on both sides)."""
+    m = make_mesh(cf, 4, 40)
+    kw = dict(tol=1e-10, krylov=cf.KRYLOV_CG2L, norm=cf.NORM_JACOBI)
+    if case == "two_correctors_relaxed":
+        kw.update(ncorr=2, relax=(0.7, 0.6))
+    s, o = make_pair(cf, po, m, **kw)
+    if case == "one_aggregate":
+        s.setCoarseTarget(1)
+        o.set_coarse_target(1)
+    for k in range(3):
+        if case == "retarget_between_steps" and k == 1:
+            s.setCoarseTarget(64)
+            o.set_coarse_target(64)
+        assert s.pisoStep() and o.piso_step() == 0
+        assert s.stats()["pressure_iters"] == o.stats()["pressure_iters"], k
+        st = o.state()
+        assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"]), k
+    assert s.coarseSize() == o.coarse_size()
