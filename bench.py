@@ -483,15 +483,20 @@ def main():
     value = world * args.steps / (ms_max / 1e3)
 
     # end to end through the public API with host buffers: per step upload the inlet profile
-    # (H2D), pisoStep, read back u and p (D2H)
+    # (H2D), pisoStep, read back u and p (D2H); the host buffers are pinned, as an application
+    # streaming fields every step would hold them
+    prof_host = torch.empty(profile.shape, dtype=torch.float64, pin_memory=True).numpy()
+    prof_host[:] = profile
+    u_host = torch.empty((s.N2, 3), dtype=torch.float64, pin_memory=True).numpy()
+    p_host = torch.empty((s.nv,), dtype=torch.float64, pin_memory=True).numpy()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        s.setInletVelocityProfile(profile)
+        s.setInletVelocityProfile(prof_host)
         if not s.pisoStep():
             raise SystemExit("e2e step failed")
-        u = s.getVelocity()
-        p = s.getPressure()
+        u = s.getVelocity(out=u_host)
+        p = s.getPressure(out=p_host)
     barrier()
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")

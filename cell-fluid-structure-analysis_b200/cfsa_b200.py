@@ -529,9 +529,19 @@ class NavierStokesSolver:
         return out
 
     # getters (NavierStokes.hpp:146-189)
-    def getVelocity(self) -> np.ndarray:
-        out = np.empty((self.N2, 3))
+    def getVelocity(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Velocity [N2, 3] (P1 vertices first). `out`: a C-contiguous float64 [N2, 3] array to
+        fill instead of a new one (e.g. a pinned buffer for fast repeated reads)."""
+        out = self._out((self.N2, 3), out)
         self._check(self._lib.cfsa_ns_get_velocity(self._h, _ptr(out)))
+        return out
+
+    @staticmethod
+    def _out(shape, out):
+        if out is None:
+            return np.empty(shape)
+        if out.shape != shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float64 array of shape {shape}")
         return out
 
     def getVelocityStar(self) -> np.ndarray:
@@ -539,8 +549,8 @@ class NavierStokesSolver:
         self._check(self._lib.cfsa_ns_get_velocity_star(self._h, _ptr(out)))
         return out
 
-    def getPressure(self) -> np.ndarray:
-        out = np.empty(self.nv)
+    def getPressure(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = self._out((self.nv,), out)
         self._check(self._lib.cfsa_ns_get_pressure(self._h, _ptr(out)))
         return out
 

@@ -147,6 +147,8 @@ struct cfsa_ns {
   BicgState *h_bs = nullptr;
   CgState *h_cs = nullptr;
   double *h_stage = nullptr;  // pinned [3][N2] staging for host transfers
+  double *d_vec3 = nullptr;   // device [N2][3] staging of vector-field transfers
+  bool h_inlet_stale = false;  // h_inlet behind the device inlet (set from a device-side split)
   BicgState *bs_prof = nullptr;
   CgState *cs_prof = nullptr;
   // persistent CG
@@ -456,6 +458,7 @@ struct cfsa_ns {
     CK(cudaMallocHost(&h_bs, 2 * sizeof(BicgState)));
     CK(cudaMallocHost(&h_cs, sizeof(CgState)));
     CK(cudaMallocHost(&h_stage, n3 * sizeof(double)));
+    d_vec3 = dalloc<double>(n3);
     CK(cudaMallocHost(&h_ms, sizeof(MixedState)));
     At32 = dalloc<float>((size_t)s2.nentries);
     invA32 = dalloc<float>((size_t)N2);
@@ -1447,33 +1450,35 @@ struct cfsa_ns {
   }
 
   // [N2][3] host layout <-> component-major device layout through pinned staging.
+  // [3][N2] device field -> caller's [N2][3] host array (one copy; fast when the caller's memory
+  // is pinned, staged by the driver otherwise)
   void download_vec3(const double *d, double *out) {
-    CK(cudaMemcpyAsync(h_stage, d, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    k_vec3_interleave<<<blocks_for(3 * N2), kBlock, 0, stream>>>(N2, d, d_vec3);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, d_vec3, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
-    const double *hx = h_stage, *hy = h_stage + N2, *hz = h_stage + 2 * N2;
-    for (int64_t i = 0; i < N2; ++i) {
-      out[3 * i] = hx[i];
-      out[3 * i + 1] = hy[i];
-      out[3 * i + 2] = hz[i];
-    }
   }
   void upload_vec3(const double *in, double *d) {
-    CK(cudaStreamSynchronize(stream));  // staging may still feed an earlier copy
-    double *hx = h_stage, *hy = h_stage + N2, *hz = h_stage + 2 * N2;
-    for (int64_t i = 0; i < N2; ++i) {
-      hx[i] = in[3 * i];
-      hy[i] = in[3 * i + 1];
-      hz[i] = in[3 * i + 2];
-    }
-    CK(cudaMemcpyAsync(d, h_stage, (size_t)3 * N2 * sizeof(double), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(d_vec3, in, (size_t)3 * N2 * sizeof(double), cudaMemcpyHostToDevice, stream));
+    k_vec3_split<<<blocks_for(3 * N2), kBlock, 0, stream>>>(N2, d_vec3, d);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(stream));
+  }
+  // the host mirror of the inlet values (fingerprint, field initialisation)
+  const std::vector<double> &host_inlet() {
+    if (h_inlet_stale) {
+      CK(cudaMemcpyAsync(h_inlet.data(), inlet, h_inlet.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      h_inlet_stale = false;
+    }
+    return h_inlet;
   }
 
   // ------------------------------------------------------------------ discrete adjoint
   // Everything the recorded forward pass depends on besides the state: parameters, inlet
   // values, boundary tags and the geometry generation. The backward pass refuses to run when
   // it differs from the value taken at recording time.
-  uint64_t adjoint_fingerprint() const {
+  uint64_t adjoint_fingerprint() {
     uint64_t hsh = 1469598103934665603ull;
     auto mix = [&](const void *ptr, size_t nb) {
       const unsigned char *b = static_cast<const unsigned char *>(ptr);
@@ -1485,7 +1490,8 @@ struct cfsa_ns {
                          conv_norm, geom_gen, mixed_inner_maxit, (int64_t)cg_persistent};
     mix(d, sizeof(d));
     mix(k, sizeof(k));
-    mix(h_inlet.data(), h_inlet.size() * sizeof(double));
+    const std::vector<double> &hin = host_inlet();
+    mix(hin.data(), hin.size() * sizeof(double));
     mix(h_bc.data(), h_bc.size());
     return hsh;
   }
@@ -2080,6 +2086,7 @@ int cfsa_ns_set_inlet_uniform(cfsa_ns *h, const double u[3]) {
   return guarded(h, [&] {
     for (int c = 0; c < 3; ++c)
       std::fill(h->h_inlet.begin() + (size_t)c * h->N2, h->h_inlet.begin() + (size_t)(c + 1) * h->N2, u[c]);
+    h->h_inlet_stale = false;
     CK(cudaMemcpyAsync(h->inlet, h->h_inlet.data(), h->h_inlet.size() * sizeof(double),
                        cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -2090,11 +2097,8 @@ int cfsa_ns_set_inlet_uniform(cfsa_ns *h, const double u[3]) {
 int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u) {
   if (!h || !u) return CFSA_BAD_ARG;
   return guarded(h, [&] {
-    for (int64_t i = 0; i < h->N2; ++i)
-      for (int c = 0; c < 3; ++c) h->h_inlet[(size_t)c * h->N2 + i] = u[3 * i + c];
-    CK(cudaMemcpyAsync(h->inlet, h->h_inlet.data(), h->h_inlet.size() * sizeof(double),
-                       cudaMemcpyHostToDevice, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    h->upload_vec3(u, h->inlet);
+    h->h_inlet_stale = true;
     return CFSA_OK;
   });
 }
@@ -2163,9 +2167,10 @@ int cfsa_ns_initialize_fields(cfsa_ns *h) {
   return guarded(h, [&] {
     const size_t n3 = (size_t)3 * h->N2;
     std::vector<double> u0(n3, 0.0);
+    const std::vector<double> &hin = h->host_inlet();
     for (int64_t i = 0; i < h->N2; ++i)
       if (h->h_bc[i] == BC_INLET)
-        for (int c = 0; c < 3; ++c) u0[(size_t)c * h->N2 + i] = h->h_inlet[(size_t)c * h->N2 + i];
+        for (int c = 0; c < 3; ++c) u0[(size_t)c * h->N2 + i] = hin[(size_t)c * h->N2 + i];
     CK(cudaMemcpyAsync(h->u, u0.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemsetAsync(h->ustar, 0, n3 * sizeof(double), h->stream));
     CK(cudaMemsetAsync(h->p, 0, h->nv * sizeof(double), h->stream));

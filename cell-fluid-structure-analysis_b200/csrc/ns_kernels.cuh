@@ -2149,6 +2149,23 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
 }
 
 // ------------------------------------------------------------------------------------------
+// Host transfers of vector fields: the API's [N][3] node-major layout <-> the device's
+// component-major [3][N], converted on the device so that the host side is one straight copy.
+__global__ void k_vec3_interleave(int64_t n, const double *__restrict__ src, double *__restrict__ dst) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 3 * n) return;
+  const int64_t i = k / 3, c = k - 3 * i;
+  dst[k] = src[c * n + i];
+}
+
+__global__ void k_vec3_split(int64_t n, const double *__restrict__ src, double *__restrict__ dst) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 3 * n) return;
+  const int64_t c = k / n, i = k - c * n;
+  dst[k] = src[3 * i + c];
+}
+
+// ------------------------------------------------------------------------------------------
 // p += relax_p p'; Dirichlet outlet reset (NavierStokes.cpp:652-662, reinforcePressureBCs
 // :1011-1024). The pressure correction p' is the Krylov solution.
 __global__ void k_pressure_update(int nv, double relax_p, int outlet_type, double outlet_pressure,
