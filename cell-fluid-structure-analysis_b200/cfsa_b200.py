@@ -178,6 +178,8 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "cfsa_ns_set_inlet_profile": (i32, [vp, vp]),
         "cfsa_ns_set_pressure_solver": (i32, [vp, i32]),
         "cfsa_ns_set_coarse_target": (i32, [vp, i32]),
+        "cfsa_ns_save_state": (i32, [vp, C.c_char_p]),
+        "cfsa_ns_load_state": (i32, [vp, C.c_char_p]),
         "cfsa_ns_get_coarse_size": (i32, [vp, vp]),
         "cfsa_ns_set_precision": (i32, [vp, i32]),
         "cfsa_ns_set_convergence_norm": (i32, [vp, i32]),
@@ -590,6 +592,15 @@ class NavierStokesSolver:
         b = None if p is None else _c(p, np.float64).reshape(self.nv)
         self._check(self._lib.cfsa_ns_set_fields(self._h, None if a is None else _ptr(a),
                                                  None if b is None else _ptr(b)))
+
+    def saveState(self, path: str):
+        """Write u, p, time and step count to a binary restart file (new: the reference's VTK
+        output cannot be read back)."""
+        self._check(self._lib.cfsa_ns_save_state(self._h, os.fsencode(path)))
+
+    def loadState(self, path: str):
+        """Restore u, p, time and step count from saveState's file (same mesh sizes)."""
+        self._check(self._lib.cfsa_ns_load_state(self._h, os.fsencode(path)))
 
     def stats(self) -> dict:
         s = Stats()

@@ -2317,6 +2317,59 @@ int cfsa_ns_set_fields(cfsa_ns *h, const double *u, const double *p) {
   });
 }
 
+namespace {
+constexpr char kStateTag[8] = {'C', 'F', 'S', 'A', 'S', 'T', '0', '1'};
+}
+
+int cfsa_ns_save_state(cfsa_ns *h, const char *path) {
+  if (!h || !path) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    std::vector<double> u((size_t)3 * h->N2), p((size_t)h->nv);
+    h->download_vec3(h->u, u.data());
+    CK(cudaMemcpyAsync(p.data(), h->p, p.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(h, CFSA_BAD_ARG, std::string("cannot open ") + path + " for writing");
+    const int64_t sizes[2] = {h->N2, h->nv};
+    const int64_t steps = h->steps;
+    bool ok = std::fwrite(kStateTag, 1, 8, f) == 8 && std::fwrite(sizes, sizeof(int64_t), 2, f) == 2 &&
+              std::fwrite(&h->time, sizeof(double), 1, f) == 1 && std::fwrite(&steps, sizeof(int64_t), 1, f) == 1 &&
+              std::fwrite(u.data(), sizeof(double), u.size(), f) == u.size() &&
+              std::fwrite(p.data(), sizeof(double), p.size(), f) == p.size();
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? CFSA_OK : fail(h, CFSA_BAD_ARG, std::string("write error on ") + path);
+  });
+}
+
+int cfsa_ns_load_state(cfsa_ns *h, const char *path) {
+  if (!h || !path) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(h, CFSA_BAD_ARG, std::string("cannot open ") + path);
+    char tag[8];
+    int64_t sizes[2] = {0, 0}, steps = 0;
+    double t = 0.0;
+    bool ok = std::fread(tag, 1, 8, f) == 8 && std::memcmp(tag, kStateTag, 8) == 0 &&
+              std::fread(sizes, sizeof(int64_t), 2, f) == 2 && std::fread(&t, sizeof(double), 1, f) == 1 &&
+              std::fread(&steps, sizeof(int64_t), 1, f) == 1;
+    if (!ok || sizes[0] != h->N2 || sizes[1] != h->nv) {
+      std::fclose(f);
+      return fail(h, CFSA_BAD_ARG, std::string(path) + ": not a state file of this mesh (N2/nv differ or bad header)");
+    }
+    std::vector<double> u((size_t)3 * h->N2), p((size_t)h->nv);
+    ok = std::fread(u.data(), sizeof(double), u.size(), f) == u.size() &&
+         std::fread(p.data(), sizeof(double), p.size(), f) == p.size();
+    std::fclose(f);
+    if (!ok) return fail(h, CFSA_BAD_ARG, std::string(path) + ": truncated state file");
+    h->upload_vec3(u.data(), h->u);
+    CK(cudaMemcpyAsync(h->p, p.data(), p.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->time = t;
+    h->steps = steps;
+    return CFSA_OK;
+  });
+}
+
 int cfsa_ns_get_time(const cfsa_ns *h, double *t) {
   if (!h || !t) return CFSA_BAD_ARG;
   *t = h->time;

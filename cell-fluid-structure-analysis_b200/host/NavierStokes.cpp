@@ -345,6 +345,18 @@ void NavierStokesSolver::setPressureSolver(int krylov) {
   if (h_) status(cfsa_ns_set_pressure_solver(h_, krylov), "setPressureSolver");
 }
 
+bool NavierStokesSolver::saveState(const std::string &path) {
+  if (!h_) return false;
+  return status(cfsa_ns_save_state(h_, path.c_str()), "saveState");
+}
+
+bool NavierStokesSolver::loadState(const std::string &path) {
+  if (!h_) return false;
+  const bool ok = status(cfsa_ns_load_state(h_, path.c_str()), "loadState");
+  invalidateMirrors();
+  return ok;
+}
+
 void NavierStokesSolver::setCoarseTarget(int target) {
   coarse_target_ = target;
   if (h_) status(cfsa_ns_set_coarse_target(h_, target), "setCoarseTarget");

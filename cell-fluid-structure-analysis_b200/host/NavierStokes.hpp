@@ -141,6 +141,9 @@ class NavierStokesSolver {
   void setMaxIterations(int momentum, int pressure);
   void setPressureSolver(int krylov);  // CFSA_KRYLOV_CG, _BICGSTAB, _CG1 or _CG2L
   void setCoarseTarget(int target);    // aggregates of the CFSA_KRYLOV_CG2L coarse space (default 256)
+  // new: binary restart file of u, p, time and step count (cfsa_ns_save_state / _load_state)
+  bool saveState(const std::string &path);
+  bool loadState(const std::string &path);
   void setPrecision(int precision);    // CFSA_PRECISION_FP64 or CFSA_PRECISION_MIXED
   void setConvergenceNorm(int norm);   // CFSA_NORM_REFERENCE or CFSA_NORM_JACOBI
   void setInletVelocityProfile(const std::vector<Vec3> &per_node);

@@ -186,6 +186,13 @@ int cfsa_ns_get_pressure(cfsa_ns *h, double *p /*[nv]*/);             /* getPres
 int cfsa_ns_get_pressure_correction(cfsa_ns *h, double *p /*[nv]*/);
 int cfsa_ns_set_fields(cfsa_ns *h, const double *u /*[N2][3] or NULL*/, const double *p /*[nv] or NULL*/);
 int cfsa_ns_get_time(const cfsa_ns *h, double *t);                    /* getTime */
+/* new: binary state file for restarts (the reference has none: its VTK output cannot be read
+ * back). cfsa_ns_save_state writes u ([N2][3]), p ([nv]), the time and the step count after a
+ * header holding a format tag, N2 and nv; cfsa_ns_load_state reads such a file into a handle
+ * whose mesh has the same N2 and nv (CFSA_BAD_ARG otherwise, or on an I/O error, with the reason
+ * in cfsa_ns_last_error). Operators, parameters and the inlet are not part of the file. */
+int cfsa_ns_save_state(cfsa_ns *h, const char *path);
+int cfsa_ns_load_state(cfsa_ns *h, const char *path);
 int cfsa_ns_get_stats(const cfsa_ns *h, cfsa_ns_stats *s);
 
 /* ---- operators ---- */

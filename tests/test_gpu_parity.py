@@ -271,30 +271,33 @@ def test_batched_steps_equal_single_steps(cf, po):
     assert a.getTime() == b.getTime()
 
 
-def test_not_converged_is_reported(cf, po):
+@pytest.mark.parametrize("krylov", [0, 3], ids=["cg", "cg2l"])
+def test_not_converged_is_reported(cf, po, krylov):
     """maxit = 1 with a tight tolerance: pisoStep returns false, time does not advance (the
     reference returns before time_ += dt, NavierStokes.cpp:387-390)."""
     m = make_mesh(cf, 3, 12)
-    s, _ = make_pair(cf, po, m, tol=1e-14, maxit=(1, 1))
+    s, _ = make_pair(cf, po, m, tol=1e-14, maxit=(1, 1), krylov=krylov)
     assert not s.pisoStep()
     assert s.getTime() == 0.0
     ok, done = s.pisoSteps(3)
     assert not ok and done == 0
 
 
-def test_nan_is_reported(cf, po):
+@pytest.mark.parametrize("krylov", [0, 3], ids=["cg", "cg2l"])
+def test_nan_is_reported(cf, po, krylov):
     """A NaN relaxation factor poisons u in the corrector: the step completes (time advances, as
     in the reference) and pisoStep returns false through the hasNans() check."""
     m = make_mesh(cf, 3, 12)
-    s, _ = make_pair(cf, po, m, tol=1e-12, relax=(float("nan"), 1.0))
+    s, _ = make_pair(cf, po, m, tol=1e-12, relax=(float("nan"), 1.0), krylov=krylov)
     assert not s.pisoStep()
     assert s.getTime() == pytest.approx(0.01)
     assert np.isnan(s.getVelocity()).any()
 
 
-def test_nan_input_fails_fast(cf, po):
+@pytest.mark.parametrize("krylov", [0, 3], ids=["cg", "cg2l"])
+def test_nan_input_fails_fast(cf, po, krylov):
     m = make_mesh(cf, 3, 12)
-    s, _ = make_pair(cf, po, m, tol=1e-12)
+    s, _ = make_pair(cf, po, m, tol=1e-12, krylov=krylov)
     p = np.zeros(s.nv)
     p[5] = np.nan
     s.setFields(None, p)
@@ -508,3 +511,27 @@ def test_two_level_cg_edge_cases(cf, po, case):
         st = o.state()
         assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"]), k
     assert s.coarseSize() == o.coarse_size()
+
+
+def test_state_file_restart(cf, po, tmp_path):
+    """saveState / loadState: a run restarted from the file after two steps continues bit for bit
+    like the uninterrupted run (same u, p, time, step count); a file of another mesh is refused."""
+    m = make_mesh(cf, 3, 12)
+    a, _ = make_pair(cf, po, m, tol=1e-10, krylov=cf.KRYLOV_CG2L)
+    ok, _ = a.pisoSteps(2)
+    assert ok
+    path = str(tmp_path / "state.bin")
+    a.saveState(path)
+    ok, _ = a.pisoSteps(2)
+    assert ok
+    b, _ = make_pair(cf, po, m, tol=1e-10, krylov=cf.KRYLOV_CG2L)
+    b.loadState(path)
+    assert b.getTime() == pytest.approx(0.02)
+    ok, _ = b.pisoSteps(2)
+    assert ok
+    assert np.array_equal(a.getVelocity(), b.getVelocity()) and np.array_equal(a.getPressure(), b.getPressure())
+    assert a.getTime() == b.getTime() and a.stats()["steps"] == b.stats()["steps"]
+    other, _ = make_pair(cf, po, make_mesh(cf, 3, 13), tol=1e-10)
+    with pytest.raises(cf.CfsaError) as ei:
+        other.loadState(path)
+    assert ei.value.code == cf.BAD_ARG
