@@ -9,6 +9,8 @@
 #include "ns_kernels.cuh"
 #include "ns_mixed.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -26,6 +28,13 @@
 using namespace cfsa;
 
 namespace {
+
+// NVTX range over a host-side phase (set-up, a batch of steps, an adjoint pass); free unless a
+// profiler is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 struct Sell {
   int *sptr = nullptr, *col = nullptr, *len = nullptr, *perm = nullptr, *posmap = nullptr;
@@ -583,6 +592,7 @@ struct cfsa_ns {
 
   // buildMassMatrix + buildStiffnessMatrix + buildGradientMatrices + buildPoissonMatrix
   void assemble() {
+    NvtxRange nvtx_("cfsa assemble");
     ++geom_gen;
     k_geometry<<<blocks_for(nt), kBlock, 0, stream>>>((int)nt, xyz, tnode, vol, grad);
     k_assemble_p2<<<blocks_for(N2), kBlock, 0, stream>>>((int)N2, (int)nt, density, 1.0 / viscosity,
@@ -650,6 +660,7 @@ struct cfsa_ns {
   }
 
   void build_coarse() {
+    NvtxRange nvtx_("cfsa two-level coarse space");
     CK(cudaStreamSynchronize(stream));
     for (void *q : coarse_allocs) CK(cudaFree(q));
     coarse_allocs.clear();
@@ -1425,6 +1436,7 @@ struct cfsa_ns {
   }
 
   int run_steps(int n, int *n_done, bool simple) {
+    NvtxRange nvtx_("cfsa steps");
     ensure_operators();
     reset_status();
     int launched = 0;
@@ -1585,6 +1597,7 @@ struct cfsa_ns {
   }
 
   int adjoint_forward(int nsteps, int C, int *n_done) {
+    NvtxRange nvtx_("cfsa adjoint forward");
     if (ncorr < 1) throw CudaError{"the adjoint needs at least one pressure corrector"};
     ensure_operators();
     ensure_adjoint_work();
@@ -1821,6 +1834,7 @@ struct cfsa_ns {
 
   // Backward pass. The seed is already in a_lu / a_lp / a_scal[0].
   int adjoint_backward_core(double *grad_inlet, double *grad_viscosity, double *grad_u0, double *grad_p0) {
+    NvtxRange nvtx_("cfsa adjoint backward");
     const size_t n3 = (size_t)3 * N2;
     CK(cudaMemsetAsync(a_gin, 0, n3 * sizeof(double), stream));
     CK(cudaMemsetAsync(st_adj, 0, sizeof(DevStatus), stream));
