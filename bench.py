@@ -459,6 +459,10 @@ def main():
     ok, done = s.pisoSteps(max(args.warmup, 3))
     if not ok:
         raise SystemExit(f"warm-up failed after {done} steps: {s.stats()}")
+    # the end-to-end loop below replays the same steps as the device-timed loop, from this state
+    import tempfile
+    snap = os.path.join(tempfile.gettempdir(), f"cfsa_bench_state_{os.getpid()}.bin")
+    s.saveState(snap)
 
     def barrier():
         torch.cuda.synchronize()
@@ -484,7 +488,9 @@ def main():
 
     # end to end through the public API with host buffers: per step upload the inlet profile
     # (H2D), pisoStep, read back u and p (D2H); the host buffers are pinned, as an application
-    # streaming fields every step would hold them
+    # streaming fields every step would hold them. Same steps as the timed loop (restored state).
+    s.loadState(snap)
+    os.remove(snap)
     prof_host = torch.empty(profile.shape, dtype=torch.float64, pin_memory=True).numpy()
     prof_host[:] = profile
     u_host = torch.empty((s.N2, 3), dtype=torch.float64, pin_memory=True).numpy()
