@@ -388,6 +388,17 @@ def cpu_baseline(xyz, tets, profile, n_threads):
                       f"FP64 oracle port of the reference algorithm (BiCGSTAB pressure) with OpenMP on {cores} threads"}
 
 
+def max_over_ranks(value: float, dist, device: str = "cuda") -> float:
+    """The largest value over all ranks (times are reported as the slowest rank's); `dist` is
+    torch.distributed or None for a single process."""
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -480,10 +491,7 @@ def main():
     if not ok:
         raise SystemExit(f"timed steps failed after {done} steps: {st}")
     ms_total = st["last_step_ms"]
-    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms_total, dist)
     value = world * args.steps / (ms_max / 1e3)
 
     # end to end through the public API with host buffers: per step upload the inlet profile
@@ -505,10 +513,7 @@ def main():
         p = s.getPressure(out=p_host)
     barrier()
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps / float(te.item())
+    e2e_value = world * args.steps / max_over_ranks(e2e_s, dist)
 
     # roofline of the step's SpMV kernels on live data (CUDA events on the solver's stream)
     peak, peak_kind = measured_peak()
@@ -546,10 +551,8 @@ def main():
             ok_b, _ = sx.pisoSteps(args.steps)
             stx = sx.stats()
             barrier()
-            t = torch.tensor([stx["last_step_ms"]], dtype=torch.float64, device="cuda")
-            if dist is not None:
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            out = (sx.getVelocity(), sx.getPressure(), stx, float(t.item()), bool(ok_a and ok_b))
+            out = (sx.getVelocity(), sx.getPressure(), stx, max_over_ranks(stx["last_step_ms"], dist),
+                   bool(ok_a and ok_b))
             del sx
             return out
 
