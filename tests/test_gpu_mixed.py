@@ -3,7 +3,7 @@
 The momentum right-hand side is dominated by the 1e10 penalty rows, so the reference's criterion
 ||r|| <= tol ||b|| leaves the interior loosely determined at tol = 1e-10: FP64 solves at 1e-10
 and at 1e-14 differ by ~1e-3 after one step on the 30k-tet cylinder. Mixed precision is therefore
-checked against a converged FP64 reference (tol 1e-14): the north star's bar, relative L2 <= 1e-6
+checked against a converged FP64 reference (tol 1e-14): the mixed-precision bar, relative L2 <= 1e-6
 on u and p, holds with the outer tolerance at 1e-12 (tested on the true FP64 residual).
 """
 import os
