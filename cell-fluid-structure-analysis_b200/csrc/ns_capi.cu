@@ -2132,7 +2132,7 @@ int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov) {
 
 int cfsa_ns_set_coarse_target(cfsa_ns *h, int target) {
   if (!h) return CFSA_BAD_ARG;
-  if (target < 1 || target > 2048) return fail(h, CFSA_BAD_ARG, "coarse target outside [1, 2048]");
+  if (target < 1 || target > 1024) return fail(h, CFSA_BAD_ARG, "coarse target outside [1, 1024]");
   if (target != h->coarse_target) h->coarse_dirty = h->graph_dirty = true;
   h->coarse_target = target;
   return CFSA_OK;

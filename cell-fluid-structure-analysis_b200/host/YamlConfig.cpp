@@ -236,8 +236,8 @@ SimulationConfig parseConfig(const std::string &text) {
       opt(ns, "pressure_solver", [&](const Node *n, const std::string &k) { N.pressure_solver = n->scalar; one_of(N.pressure_solver, {"bicgstab", "cg", "cg1", "cg2l"}, k); });
       opt(ns, "coarse_aggregates", [&](const Node *n, const std::string &k) {
         N.coarse_aggregates = as_int(n, k);
-        if (N.coarse_aggregates < 1 || N.coarse_aggregates > 2048)
-          throw std::runtime_error("navier_stokes.coarse_aggregates must be in [1, 2048]");
+        if (N.coarse_aggregates < 1 || N.coarse_aggregates > 1024)
+          throw std::runtime_error("navier_stokes.coarse_aggregates must be in [1, 1024]");
       });
       opt(ns, "convergence_norm", [&](const Node *n, const std::string &k) { N.convergence_norm = n->scalar; one_of(N.convergence_norm, {"reference", "jacobi"}, k); });
       opt(ns, "inlet_profile", [&](const Node *n, const std::string &k) { N.inlet_profile = n->scalar; one_of(N.inlet_profile, {"uniform", "parabolic"}, k); });

@@ -144,7 +144,9 @@ int cfsa_ns_set_reference_node(cfsa_ns *h, int node);                      /* se
 int cfsa_ns_set_inlet_uniform(cfsa_ns *h, const double u[3]);             /* setMeanInletVelocity */
 int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u /*[N2][3]*/);   /* new: per-node inlet */
 int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov);                   /* new: CG or BiCGSTAB */
-/* new: aggregate count the CFSA_KRYLOV_CG2L coarse space aims for (default 256, 1..2048); the
+/* new: aggregate count the CFSA_KRYLOV_CG2L coarse space aims for (default 256, 1..1024; the host
+ * Cholesky of the coarse matrix grows with the cube of the count: ~0.1 s at 256, ~0.8 s at 1024
+ * on the 1M-tet cylinder); the
  * coarse space is rebuilt with the Poisson operator. Its per-aggregate arrays (6 doubles each) share
  * the solve kernel's shared memory with the row staging: a coarse space that does not fit (very
  * large targets on very large meshes) fails the next step with CFSA_CUDA_ERROR and says so in
