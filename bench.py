@@ -30,6 +30,7 @@ PKG = ROOT / "cell-fluid-structure-analysis_b200"
 sys.path.insert(0, str(PKG))
 
 METRIC = "PISO steps/s at 1M tets (FP64 GPU step)"
+DATA = "synthetic: procedural cylinder mesh (TetGen unavailable), random-free"
 UNIT = "steps/s"
 GEOM = dict(length=30.0, radius=2.0, rings=16, layers=217)
 FLUID = (1060.0, 0.004)
@@ -103,20 +104,31 @@ def parse():
     ap.add_argument("--adjoint-fd-nodes", type=int, default=ADJ_NODES,
                     help="seeded inlet nodes checked against central finite differences")
     ap.add_argument("--reference-budget-s", type=float, default=120.0,
-                    help="cap on the timed CPU work of --impl reference")
+                    help="cap on each timed CPU loop of --impl reference")
+    ap.add_argument("--reference-single-core-steps", type=int, default=5,
+                    help="steps of the 1-thread figure of --impl reference (0: skip)")
     return ap.parse_args()
 
 
-def workload_desc(m, rings, layers):
-    nv, nt, ne, _, _ = m.sizes
+def workload_desc(sizes, rings, layers, world):
+    """The workload both arms run (mesh, boundary conditions, fluid, time step, stopping rule);
+    each arm names its Krylov methods in its own "solver" key. sizes = (nv, nt, ne)."""
+    nv, nt, ne = sizes
     return {
         "workload": f"cylinder L=30 R=2, {nt} tets ({rings} rings x {layers} layers), "
-                    f"N2={nv + ne} P2 nodes, nv={nv}; FP64 PISO, two-level CG pressure (~256 aggregates) + batched BiCGSTAB "
-                    f"momentum to 1e-10, parabolic inlet peak 1.0, rho 1060, nu 0.004, dt 0.01",
+                    f"N2={nv + ne} P2 nodes, nv={nv}; FP64 PISO from rest, parabolic inlet peak 1.0, no-slip wall, "
+                    f"p=0 outlet, rho 1060, nu 0.004, dt 0.01, Krylov solves to 1e-10 relative residual",
         "tets": nt, "p2_nodes": nv + ne, "pressure_dofs": nv,
         "velocity_dofs": 3 * (nv + ne),
         "l2": "no flush: momentum operator ~0.5 GB and M ~0.3 GB stream through the 126 MB L2 every step",
+        "parallelism": f"replicas x{world}",
     }
+
+
+GPU_SOLVER = ("two-level CG pressure (single-reduction CG, Jacobi + ~256-aggregate coarse correction) + "
+              "batched 3-component BiCGSTAB momentum, FP64, on the GPU")
+REF_SOLVER = ("reference algorithm (src/FEM/NavierStokes.cpp:416-668): Jacobi BiCGSTAB pressure + per-component "
+              "Jacobi BiCGSTAB momentum, FP64, oracle port on the host cores")
 
 
 def make_mesh(cf, rings, layers):
@@ -366,26 +378,51 @@ def ybif_section(cf, args, barrier):
     return out
 
 
-def cpu_baseline(xyz, tets, profile, n_threads):
-    """Oracle port (test infrastructure) timed on the host cores: the 2nd step from rest of the
-    same workload (setup and the 1st step untimed)."""
+def oracle_cylinder(rings, layers, pressure_solver):
+    """Oracle (test infrastructure) set up on the benchmark workload from its own mesher, so that
+    a CPU-only run maps no product library: the 999,936-tet cylinder with the parabolic inlet."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle as po
 
-    cores = po.set_threads(n_threads)
+    xyz, tets = po.cylinder(GEOM["length"], GEOM["radius"], rings, layers)
     o = po.Oracle(xyz, tets)
     o.set_fluid(*FLUID)
-    o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=0)
+    o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1],
+                 pressure_solver=pressure_solver)
     o.initialize()
-    o.set_inlet(profile)
+    o.set_inlet(po.parabolic_inlet(o, INLET_PEAK, GEOM["radius"]))
+    return po, o
+
+
+def time_oracle_steps(po, o, threads, nsteps, budget_s):
+    """Wall time of up to `nsteps` oracle PISO steps on `threads` host threads, stopping early
+    once `budget_s` seconds of steps have run. Returns (steps done, seconds, threads used)."""
+    cores = po.set_threads(threads)
+    done, t0 = 0, time.perf_counter()
+    while done < nsteps:
+        if o.piso_step() != 0:
+            break
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    return done, time.perf_counter() - t0, cores
+
+
+def cpu_baseline(rings, layers, n_threads, steps=5, budget_s=30.0):
+    """Oracle port of the reference algorithm (BiCGSTAB pressure and momentum) timed on the host
+    cores: steps 2.. of the same workload from rest (set-up and the first step untimed), up to
+    `steps` steps or `budget_s` seconds, all host threads."""
+    po, o = oracle_cylinder(rings, layers, pressure_solver=0)
+    po.set_threads(n_threads)
     if o.piso_step() != 0:
         return None
-    t = time.perf_counter()
-    code = o.piso_step()
-    dt = time.perf_counter() - t
-    return {"value": (1.0 / dt) if code == 0 else 0.0, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"1 PISO step (2nd from rest) of the {len(tets)}-tet workload, {dt:.2f} s, "
-                      f"FP64 oracle port of the reference algorithm (BiCGSTAB pressure) with OpenMP on {cores} threads"}
+    done, el, cores = time_oracle_steps(po, o, n_threads, steps, budget_s)
+    if done == 0:
+        return None
+    return {"value": done / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{done} PISO steps (steps 2-{done + 1} from rest) of the {o.nt}-tet workload, {el:.1f} s, "
+                      f"FP64 oracle port of the reference algorithm (BiCGSTAB pressure and momentum) "
+                      f"with OpenMP on {cores} threads"}
 
 
 def max_over_ranks(value: float, dist, device: str = "cuda") -> float:
@@ -400,43 +437,39 @@ def max_over_ranks(value: float, dist, device: str = "cuda") -> float:
 
 
 def run_reference(args):
+    """The reference arm: the reference algorithm (oracle port, BiCGSTAB pressure and momentum)
+    on the host cores, on the same workload, metric and unit as the GPU arm. It builds its mesh
+    with the oracle's own mesher and loads no product library. All host threads over the
+    requested steps (after the same warm-up steps as the GPU arm), then the same solver on one
+    thread over `--reference-single-core-steps` steps, as the reference itself runs (its build has
+    no OpenMP and Eigen's sparse products are serial)."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    import cfsa_b200 as cf  # mesh generation only (host C++), no device work
-
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pyoracle as po
-
+    warm = max(args.warmup, 3)
+    po, o = oracle_cylinder(args.rings, args.layers, pressure_solver=0)
     cores = po.set_threads(os.cpu_count() or 1)
-    m = make_mesh(cf, args.rings, args.layers)
-    xyz, tets = m.vertices(), m.tets()
-    profile = cf.parabolic_inlet(m.nodePositions(), INLET_PEAK, GEOM["radius"])
-    o = po.Oracle(xyz, tets)
-    o.set_fluid(*FLUID)
-    o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=0)
-    o.initialize()
-    o.set_inlet(profile)
-    for _ in range(max(1, min(args.warmup, 3))):
+    for _ in range(warm):
         o.piso_step()
-    done, t0 = 0, time.perf_counter()
-    while done < args.steps:
-        if o.piso_step() != 0:
-            break
-        done += 1
-        if time.perf_counter() - t0 > args.reference_budget_s:
-            break
-    el = time.perf_counter() - t0
+    done, el, cores = time_oracle_steps(po, o, os.cpu_count() or 1, args.steps, args.reference_budget_s)
     value = done / el if el > 0 else 0.0
-    sample = (f"{done} of {args.steps} requested PISO steps after {max(1, min(args.warmup, 3))} warm-up "
-              f"steps, FP64 oracle port of the reference algorithm (BiCGSTAB pressure) with OpenMP on {cores} threads, capped at "
-              f"{args.reference_budget_s:.0f} s of timed work")
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-            "steps": done, "warmup": max(1, min(args.warmup, 3)),
+    one = None
+    if args.reference_single_core_steps > 0:
+        d1, e1, c1 = time_oracle_steps(po, o, 1, args.reference_single_core_steps, args.reference_budget_s)
+        one = {"value": d1 / e1 if e1 > 0 else 0.0, "unit": UNIT, "cores": c1, "steps": d1,
+               "sample": f"{d1} PISO steps right after the all-thread ones, same solver on 1 thread"}
+    sample = (f"{done} of {args.steps} requested PISO steps after {warm} warm-up steps from rest, FP64 "
+              f"oracle port of the reference algorithm (BiCGSTAB pressure and momentum) with OpenMP on "
+              f"{cores} threads, capped at {args.reference_budget_s:.0f} s of timed work")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": done, "warmup": warm,
             "ms_per_step": 1e3 * el / max(done, 1), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic: procedural cylinder mesh",
-            "config": workload_desc(m, args.rings, args.layers),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "config": workload_desc((o.nv, o.nt, o.ne), args.rings, args.layers, world),
+            "solver": REF_SOLVER,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                             "single_core": one},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -592,15 +625,16 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(m.vertices(), m.tets(), profile, os.cpu_count() or 1)
+        cpu = cpu_baseline(args.rings, args.layers, os.cpu_count() or 1)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: procedural cylinder mesh (TetGen unavailable), random-free",
-            "config": dict(workload_desc(m, args.rings, args.layers), parallelism=f"replicas x{world}"),
+            "data": DATA,
+            "config": workload_desc((nv, nt, ne), args.rings, args.layers, world),
+            "solver": GPU_SOLVER,
             "dof_updates_per_s": value * (3 * N2 + nv),
             "krylov_iters_per_step": [st["krylov_iters"][0] / args.steps, st["krylov_iters"][1] / args.steps],
             "gpu_launches": int(st["kernel_launches"]),

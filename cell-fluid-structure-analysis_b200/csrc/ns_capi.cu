@@ -2763,6 +2763,24 @@ int noalloc_scratch(cfsa_ns *h, double **out) {
   *out = g_noalloc_ptr[dev];
   return CFSA_OK;
 }
+
+// Makes `dev` current for the lifetime of the guard and puts the caller's device back on every
+// return path, so a multi-GPU caller's later CUDA calls run where it expects.
+struct DeviceGuard {
+  int prev = -1;
+  bool switched = false;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) {
+      ok = (cudaSetDevice(dev) == cudaSuccess);
+      switched = ok && prev >= 0;
+    }
+  }
+  ~DeviceGuard() {
+    if (switched) cudaSetDevice(prev);
+  }
+};
 }  // namespace
 
 extern "C" int cfsa_ns_compute_divergence_noalloc(cfsa_ns *h, const double *u_dev, double *div_dev) {
@@ -2771,10 +2789,8 @@ extern "C" int cfsa_ns_compute_divergence_noalloc(cfsa_ns *h, const double *u_de
     return fail(h, CFSA_BAD_ARG,
                 "cfsa_ns_compute_divergence_noalloc: mesh has " + std::to_string(h->nt) +
                     " tets, the static scratch holds at most " + std::to_string(kNoAllocMaxTets));
-  int cur = -1;
-  if (cudaGetDevice(&cur) != cudaSuccess || cur != h->device) {
-    if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, CFSA_CUDA_ERROR, "cannot select the handle's device");
-  }
+  DeviceGuard guard(h->device);
+  if (!guard.ok) return fail(h, CFSA_CUDA_ERROR, "cannot select the handle's device");
   double *scratch = nullptr;
   const int code = noalloc_scratch(h, &scratch);
   if (code != CFSA_OK) return code;

@@ -144,10 +144,11 @@ int cfsa_ns_set_reference_node(cfsa_ns *h, int node);                      /* se
 int cfsa_ns_set_inlet_uniform(cfsa_ns *h, const double u[3]);             /* setMeanInletVelocity */
 int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u /*[N2][3]*/);   /* new: per-node inlet */
 int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov);                   /* new: CG or BiCGSTAB */
-/* new: aggregate count the CFSA_KRYLOV_CG2L coarse space aims for (default 256, 1..1024; the host
- * Cholesky of the coarse matrix grows with the cube of the count: ~0.1 s at 256, ~0.8 s at 1024
- * on the 1M-tet cylinder); the
- * coarse space is rebuilt with the Poisson operator. Its per-aggregate arrays (6 doubles each) share
+/* new: aggregate count the CFSA_KRYLOV_CG2L coarse space aims for (default 256, 1..1024, others
+ * are rejected with CFSA_BAD_ARG). The aggregates are boxes of a uniform grid, so the number
+ * actually occupied can exceed the target (256 requested gives 432 on the 1M-tet cylinder); the
+ * host Cholesky of the coarse matrix grows with the cube of the occupied count (~0.1 s at 432 on
+ * that mesh). The coarse space is rebuilt with the Poisson operator. Its per-aggregate arrays (6 doubles each) share
  * the solve kernel's shared memory with the row staging: a coarse space that does not fit (very
  * large targets on very large meshes) fails the next step with CFSA_CUDA_ERROR and says so in
  * cfsa_ns_last_error. */
@@ -223,17 +224,20 @@ int cfsa_ns_profile_kernel(cfsa_ns *h, int which, int iters, double *avg_ms, dou
 
 /* ---- allocation-free operator (no counterpart in the reference) ---- */
 /* Divergence (the computeDivergence operator above) for callers that cannot allocate device
- * memory at call time: code running while a CUDA graph is being captured (cudaMalloc is not
- * allowed then), hosts whose memory pool has reserved the whole device, and tight coupling loops
- * that must not pay allocation latency. Inputs and outputs are the caller's device arrays:
- * u_dev [3][N2] component-major doubles (all x, then all y, then all z), div_dev [nv] doubles.
- * The per-tet intermediate lives in a file-scope static device array of 1,048,576 doubles (8 MiB),
- * held by every GPU that loads this library until the process exits; meshes with more tets are
- * rejected with CFSA_BAD_ARG. The first call on a device looks that array's address up, so make
- * the first call before any stream capture. Every call shares the one array and every entry a
- * call reads is written by the same call first, so nothing needs clearing; calls that overlap on
- * the GPU (other threads or other handles) race on it. Runs on the handle's stream and returns
- * once div_dev is written. */
+ * memory when they call it: a host framework whose caching pool allocator has already reserved
+ * the whole device (cudaMalloc then fails with out-of-memory although the pool has room), and
+ * coupling loops that call the operator many times per step, where cudaMalloc/cudaFree would
+ * synchronise the device and stall the caller's other streams. Inputs and outputs are the
+ * caller's device arrays: u_dev [3][N2] component-major doubles (all x, then all y, then all z),
+ * div_dev [nv] doubles. The per-tet intermediate lives in a file-scope static device array of
+ * 1,048,576 doubles (8 MiB), held by every GPU that loads this library until the process exits;
+ * meshes with more tets are rejected with CFSA_BAD_ARG. The first call on a device looks that
+ * array's address up, so make the first call before any stream capture. Every call shares the one
+ * array and every entry a call reads is written by the same call first, so nothing needs
+ * clearing; calls that overlap on the GPU (other threads or other handles) race on it.
+ * The kernels run on the handle's stream, not on the caller's: finish writing u_dev first (for
+ * example, synchronise the stream that produced it). The call returns once div_dev is written and
+ * leaves the caller's current device as it found it. */
 int cfsa_ns_compute_divergence_noalloc(cfsa_ns *h, const double *u_dev, double *div_dev);
 
 /* ---- output ---- */

@@ -1720,11 +1720,14 @@ void orc_set_params(void *h, double dt, double tol_mom, double tol_p, int maxit_
   o->pressure_solver = pressure_solver;
   o->coarse_built = false;
 }
-// Target number of aggregates of the two-level pressure preconditioner (default 256).
-void orc_set_coarse_target(void *h, int target) {
+// Target number of aggregates of the two-level pressure preconditioner (default 256). Returns 0,
+// or 1 (target unchanged) outside [1, 1024], the range the device solver accepts.
+int orc_set_coarse_target(void *h, int target) {
+  if (target < 1 || target > 1024) return 1;
   Oracle *o = static_cast<Oracle *>(h);
   o->coarse_target = target;
   o->coarse_built = false;
+  return 0;
 }
 // Aggregates of the coarse space last built (0 before the first two-level solve).
 int orc_coarse_size(void *h) { return static_cast<Oracle *>(h)->coarse.nc; }
@@ -1845,6 +1848,99 @@ int orc_adjoint_backward(void *h, double *lu, double *lp, double dnu_explicit, d
   std::copy(P.begin(), P.end(), lp);
   return 0;
 }
+// Synthetic cylinder input (the reference meshes with TetGen, absent here): the same vertex and
+// tet arrays as the product's procedural mesher, produced here so that a CPU run of the oracle
+// needs no product library. Disk: centre point, then ring k = 1..rings of 6k points at radius
+// R k / rings; rings k-1 and k are stitched by a merge walk over their angular positions. Axis x:
+// `layers` equal prism layers on [0, L]. Each prism splits into 3 tets around its minimum-index
+// vertex (Dompierre et al. 1999, so shared quad faces get the same diagonal); tets are oriented
+// to positive signed volume. Sizes: nv = (1 + 3 rings (rings+1)) (layers+1), nt = 3 * 6 rings^2
+// * layers. Returns 0, or 1 for invalid sizes.
+int orc_cylinder(double length, double radius, int rings, int layers, double *xyz, int *tets) {
+  if (rings < 1 || layers < 1 || !(length > 0.0) || !(radius > 0.0)) return 1;
+  std::vector<double> dy{0.0}, dz{0.0};
+  std::vector<int> first(rings + 1, 0), count(rings + 1, 1);
+  for (int k = 1; k <= rings; ++k) {
+    first[k] = (int)dy.size();
+    count[k] = 6 * k;
+    const double rad = radius * (double)k / (double)rings;
+    for (int j = 0; j < count[k]; ++j) {
+      const double th = 2.0 * M_PI * (double)j / (double)count[k];
+      dy.push_back(rad * std::cos(th));
+      dz.push_back(rad * std::sin(th));
+    }
+  }
+  std::vector<std::array<int, 3>> tri;
+  for (int k = 1; k <= rings; ++k) {
+    const int na = count[k - 1], nb = count[k], fa = first[k - 1], fb = first[k];
+    int i = 0, j = 0;
+    while (i < na || j < nb) {
+      // position of the next point on each ring as a fraction of a turn; the centre never moves
+      const double ta = (k == 1) ? 2.0 : (double)(i + 1) / (double)na;
+      const double tb = (double)(j + 1) / (double)nb;
+      const bool inner = (j >= nb) || (i < na && k > 1 && ta < tb);
+      if (inner) {
+        tri.push_back({fa + i % na, fb + j % nb, fa + (i + 1) % na});
+        ++i;
+      } else {
+        tri.push_back({fa + i % na, fb + j % nb, fb + (j + 1) % nb});
+        ++j;
+      }
+      if (k == 1 && j >= nb) break;
+    }
+  }
+  const int np = (int)dy.size();
+  for (int l = 0; l <= layers; ++l) {
+    const double x = length * (double)l / (double)layers;
+    for (int q = 0; q < np; ++q) {
+      double *v = xyz + 3 * ((size_t)l * np + q);
+      v[0] = x;
+      v[1] = dy[q];
+      v[2] = dz[q];
+    }
+  }
+  // vertex order of the prism (bottom 0,1,2 / top 3,4,5) rotated so the smallest index comes first
+  static const int rot[6][6] = {{0, 1, 2, 3, 4, 5}, {1, 2, 0, 4, 5, 3}, {2, 0, 1, 5, 3, 4},
+                                {3, 5, 4, 0, 2, 1}, {4, 3, 5, 1, 0, 2}, {5, 4, 3, 2, 1, 0}};
+  size_t t = 0;
+  for (int l = 0; l < layers; ++l)
+    for (const auto &tr : tri) {
+      int P[6];
+      for (int a = 0; a < 3; ++a) {
+        P[a] = l * np + tr[a];
+        P[a + 3] = (l + 1) * np + tr[a];
+      }
+      int m = 0;
+      for (int a = 1; a < 6; ++a)
+        if (P[a] < P[m]) m = a;
+      int V[6];
+      for (int a = 0; a < 6; ++a) V[a] = P[rot[m][a]];
+      int T[3][4];
+      if (std::min(V[1], V[5]) < std::min(V[2], V[4])) {
+        const int c[3][4] = {{V[0], V[1], V[2], V[5]}, {V[0], V[1], V[5], V[4]}, {V[0], V[4], V[5], V[3]}};
+        std::memcpy(T, c, sizeof(T));
+      } else {
+        const int c[3][4] = {{V[0], V[1], V[2], V[4]}, {V[0], V[4], V[2], V[5]}, {V[0], V[4], V[5], V[3]}};
+        std::memcpy(T, c, sizeof(T));
+      }
+      for (auto &c : T) {
+        const double *a = xyz + 3 * (size_t)c[0], *b = xyz + 3 * (size_t)c[1], *e = xyz + 3 * (size_t)c[2],
+                     *d = xyz + 3 * (size_t)c[3];
+        const double u[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+        const double w[3] = {e[0] - a[0], e[1] - a[1], e[2] - a[2]};
+        const double s[3] = {d[0] - a[0], d[1] - a[1], d[2] - a[2]};
+        const double det = (u[1] * w[2] - u[2] * w[1]) * s[0] + (u[2] * w[0] - u[0] * w[2]) * s[1] +
+                           (u[0] * w[1] - u[1] * w[0]) * s[2];
+        int *o = tets + 4 * t++;
+        o[0] = c[0];
+        o[1] = c[1];
+        o[2] = det < 0.0 ? c[3] : c[2];
+        o[3] = det < 0.0 ? c[2] : c[3];
+      }
+    }
+  return 0;
+}
+
 int orc_set_threads(int n) {
 #ifdef _OPENMP
   if (n > 0) omp_set_num_threads(n);

@@ -40,7 +40,7 @@ def lib() -> C.CDLL:
         "orc_set_fluid": (None, [vp, dbl, dbl]),
         "orc_set_params": (None, [vp, dbl, dbl, dbl, i32, i32, i32, dbl, dbl, i32, dbl, i32, i32, i32]),
         "orc_set_inlet": (None, [vp, vp]),
-        "orc_set_coarse_target": (None, [vp, i32]),
+        "orc_set_coarse_target": (i32, [vp, i32]),
         "orc_coarse_size": (i32, [vp]),
         "orc_initialize": (None, [vp]),
         "orc_reference_node": (i32, [vp]),
@@ -60,6 +60,7 @@ def lib() -> C.CDLL:
         "orc_shear_stress": (None, [vp, vp]),
         "orc_stats": (None, [vp, vp, vp, vp]),
         "orc_set_threads": (i32, [i32]),
+        "orc_cylinder": (i32, [dbl, dbl, i32, i32, vp, vp]),
         "orc_adjoint_forward": (i32, [vp, i32]),
         "orc_objective": (i32, [vp, i32, i32, dbl, dbl, vp, vp, vp, vp]),
         "orc_adjoint_backward": (i32, [vp, vp, vp, dbl, vp, vp, vp]),
@@ -80,6 +81,29 @@ def set_threads(n: int) -> int:
     return lib().orc_set_threads(int(n))
 
 
+def cylinder(length: float, radius: float, rings: int, layers: int):
+    """Synthetic cylinder along x (vertices [nv][3], tets [nt][4]): the same arrays as the
+    product's procedural mesher, built here so that CPU runs of the oracle load no product
+    library."""
+    np_disk = 1 + 3 * rings * (rings + 1)
+    xyz = np.empty((np_disk * (layers + 1), 3), np.float64)
+    tets = np.empty((18 * rings * rings * layers, 4), np.int32)
+    if lib().orc_cylinder(float(length), float(radius), int(rings), int(layers), _p(xyz), _p(tets)) != 0:
+        raise ValueError("cylinder: rings, layers >= 1 and positive length/radius required")
+    return xyz, tets
+
+
+def parabolic_inlet(o: "Oracle", peak: float, radius: float, axis: int = 0) -> np.ndarray:
+    """u_axis = peak (1 - r^2 / R^2) at every P1 vertex and P2 edge node of the oracle mesh, r the
+    distance from the axis through the origin; other components zero. [N2, 3]."""
+    nodes = np.concatenate([o.vertices, o.mesh()["edge_xyz"]])
+    other = [a for a in range(3) if a != axis]
+    r2 = nodes[:, other[0]] ** 2 + nodes[:, other[1]] ** 2
+    out = np.zeros_like(nodes)
+    out[:, axis] = peak * (1.0 - r2 / (radius * radius))
+    return out
+
+
 class Oracle:
     """FP64 CPU restatement of the reference NavierStokesSolver on a raw (xyz, tets) mesh."""
 
@@ -87,6 +111,7 @@ class Oracle:
         self.L = lib()
         xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
         tets = np.ascontiguousarray(tets, np.int32).reshape(-1, 4)
+        self.vertices = xyz
         d = np.ascontiguousarray(direction, np.float64)
         self.h = C.c_void_p(self.L.orc_create(len(xyz), _p(xyz), len(tets), _p(tets),
                                               1 if apply_bc else 0, _p(d), float(coverage)))
@@ -131,8 +156,10 @@ class Oracle:
                               int(p["pressure_solver"]), int(p["conv_norm"]))
 
     def set_coarse_target(self, target: int):
-        """Aggregate count the two-level pressure preconditioner (pressure_solver 3) aims for."""
-        self.L.orc_set_coarse_target(self.h, int(target))
+        """Aggregate count the two-level pressure preconditioner (pressure_solver 3) aims for,
+        1..1024 as on the device."""
+        if self.L.orc_set_coarse_target(self.h, int(target)) != 0:
+            raise ValueError(f"coarse target {target} outside [1, 1024]")
 
     def coarse_size(self) -> int:
         return self.L.orc_coarse_size(self.h)

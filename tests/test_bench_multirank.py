@@ -64,3 +64,24 @@ def test_reference_arm_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["steps"] == 1 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["config"]["parallelism"] == "replicas x2" and "BiCGSTAB pressure" in d["solver"]
+
+
+def test_reference_arm_maps_no_product_library():
+    """The reference arm builds its mesh with the oracle's mesher: the process never maps the
+    product's libcfsa.so, and it runs the same warm-up as the GPU arm."""
+    code = (
+        "import sys, json, io, contextlib; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', "
+        "'--warmup', '5', '--rings', '2', '--layers', '6', '--reference-single-core-steps', '1']; "
+        "sys.path.insert(0, '.'); import bench; buf = io.StringIO()\n"
+        "with contextlib.redirect_stdout(buf): bench.main()\n"
+        "maps = open('/proc/self/maps').read(); d = json.loads(buf.getvalue())\n"
+        "print(json.dumps({'libcfsa': 'libcfsa' in maps, 'oracle': 'liboracle_ns' in maps, "
+        "'cfsa_module': 'cfsa_b200' in sys.modules, 'warmup': d['warmup'], "
+        "'single': d['cpu_baseline']['single_core']['cores']}))"
+    )
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600,
+                       cwd=str(ROOT), env=dict(os.environ, OMP_NUM_THREADS="2"))
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d == {"libcfsa": False, "oracle": True, "cfsa_module": False, "warmup": 5, "single": 1}

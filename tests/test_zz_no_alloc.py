@@ -2,11 +2,12 @@
 computeDivergence entry point.
 
 The no-alloc variant exists for callers that cannot allocate device memory when they call it:
-code running during CUDA graph capture, hosts whose memory pool already owns the device, and
-coupling loops that must not pay allocation latency. It takes the caller's device arrays and keeps
-its per-tet intermediate in a static device array; these checks call it through the C ABI twice in
-a row (different inputs) and require the same bits as the regular operator, whose own parity with
-the oracle is bit-exact.
+hosts whose pool allocator has already reserved the whole device, and coupling loops where
+cudaMalloc/cudaFree would synchronise the device on every call. It takes the caller's device
+arrays and keeps its per-tet intermediate in a static device array; these checks call it through
+the C ABI twice in a row (different inputs) and require the same bits as the regular operator,
+whose own parity with the oracle is bit-exact. The call runs on the handle's stream, so the test
+finishes writing the input (synchronize) before each call.
 """
 import ctypes
 
