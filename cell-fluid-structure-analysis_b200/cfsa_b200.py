@@ -210,6 +210,8 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "cfsa_ns_get_matrix": (i32, [vp, i32, vp, vp, vp]),
         "cfsa_ns_get_inv_lumped_mass": (i32, [vp, vp]),
         "cfsa_ns_profile_kernel": (i32, [vp, i32, i32, vp, vp]),
+        "cfsa_ns_set_barrier_spin_limit": (i32, [vp, C.c_int64]),
+        "cfsa_ns_solve_pressure_bicgstab": (i32, [vp, vp, vp, dbl, i32]),
         "cfsa_ns_compute_divergence_noalloc": (i32, [vp, vp, vp]),
         "cfsa_ns_objective": (i32, [vp, vp, vp]),
         "cfsa_ns_write_vtk": (i32, [vp, C.c_char_p, C.c_double, i32]),
@@ -395,7 +397,7 @@ class NavierStokesSolver:
         self.reference_node = -1
         self.mean_inlet_velocity = np.zeros(3)
         self.inlet_profile = None
-        self.krylov = KRYLOV_CG
+        self.krylov = KRYLOV_BICGSTAB  # the reference's pressure method; CG variants opt-in
         self.coarse_target = 256
         self.precision = PRECISION_FP64
         self.conv_norm = NORM_REFERENCE
@@ -498,6 +500,16 @@ class NavierStokesSolver:
 
     def correctVelocity(self) -> bool:
         return self._status(self._lib.cfsa_ns_correct_velocity(self._h))
+
+    def solvePressureBiCGSTAB(self, rhs, x=None, tol: float = 1e-8, maxit: int = 1000):
+        """solvePressureBiCGSTAB (NavierStokes.cpp:773-802): Jacobi BiCGSTAB on the raw Poisson
+        matrix from a zero guess; returns (ok, x) with x the [nv] iterate."""
+        b = np.ascontiguousarray(rhs, np.float64)
+        if b.shape != (self.nv,):
+            raise ValueError(f"rhs must have {self.nv} entries")
+        out = np.empty(self.nv) if x is None else x
+        ok = self._status(self._lib.cfsa_ns_solve_pressure_bicgstab(self._h, _ptr(b), _ptr(out), float(tol), int(maxit)))
+        return ok, out
 
     def computeDivergence(self, u) -> np.ndarray:
         u = _c(u, np.float64).reshape(self.N2, 3)
@@ -671,6 +683,11 @@ class NavierStokesSolver:
         ms, by = C.c_double(), C.c_double()
         self._check(self._lib.cfsa_ns_profile_kernel(self._h, int(which), int(iters), C.byref(ms), C.byref(by)))
         return ms.value, by.value
+
+    def setBarrierSpinLimit(self, polls: int):
+        """Polls a waiting CTA of the resident pressure solvers makes at a grid barrier before it
+        gives up (the step then fails with CUDA_ERROR); < 0 restores the default."""
+        self._check(self._lib.cfsa_ns_set_barrier_spin_limit(self._h, int(polls)))
 
     def invLumpedMass(self) -> np.ndarray:
         out = np.empty(self.N2)

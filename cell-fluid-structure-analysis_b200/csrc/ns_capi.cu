@@ -108,7 +108,7 @@ struct cfsa_ns {
   int outlet_type = CFSA_OUTLET_DIRICHLET;
   double outlet_pressure = 0.0;
   int ref_node = -1;
-  int krylov = CFSA_KRYLOV_CG;
+  int krylov = CFSA_KRYLOV_BICGSTAB;  // the reference's pressure method (NavierStokes.cpp:633)
   int precision = CFSA_PRECISION_FP64;
   int conv_norm = CFSA_NORM_REFERENCE;
   double time = 0.0;
@@ -171,6 +171,11 @@ struct cfsa_ns {
   size_t cg_res_smem = 0;
   unsigned int *bar_count = nullptr, *bar_gen = nullptr;
   int *bar_err = nullptr;
+  long long bar_spin_limit = kBarrierSpinLimit;
+  // raw Poisson operator of solvePressureBiCGSTAB (no penalty rows), column-scaled by its inverse
+  // diagonal like Lt; built on first use and again after the geometry changed
+  double *Lraw_t = nullptr, *diag_raw = nullptr, *inv_raw = nullptr;
+  int64_t raw_gen = -1;
   // two-level pressure preconditioner of k_cg2l_resident (rebuilt with the Poisson operator)
   int coarse_target = 256;
   bool coarse_dirty = true;
@@ -1204,7 +1209,7 @@ struct cfsa_ns {
       c.part_b = cg_part_b;
       c.cs = cs;
       c.st = s_out;
-      c.bar = GridBarrier{bar_count, bar_gen, bar_err};
+      c.bar = GridBarrier{bar_count, bar_gen, bar_err, bar_spin_limit};
       c.scaled = (conv_norm == CFSA_NORM_JACOBI) ? 1 : 0;
       CK(cudaMemsetAsync(bar_count, 0, (1 + kBarrierGroups) * sizeof(unsigned int), stream));
       CK(cudaMemsetAsync(bar_err, 0, sizeof(int), stream));
@@ -1310,6 +1315,70 @@ struct cfsa_ns {
       k_check_cg<<<1, 1, 0, stream>>>(cs, s_out, nullptr);
     }
     CK(cudaGetLastError());
+  }
+
+  // NavierStokesSolver::solvePressureBiCGSTAB (src/FEM/NavierStokes.cpp:773-802): Jacobi
+  // BiCGSTAB on the raw Poisson matrix, zero initial guess, stopping rule ||r|| <= tol ||b||.
+  // Uses the pressure solve's work vectors and leaves the solver's fields untouched.
+  int solve_poisson_raw(const double *rhs, double *x_host, double tol, int maxit) {
+    ensure_operators();
+    if (!Lraw_t) {
+      Lraw_t = dalloc<double>((size_t)s1.nentries);
+      diag_raw = dalloc<double>((size_t)nv);
+      inv_raw = dalloc<double>((size_t)nv);
+      CK(cudaMemsetAsync(Lraw_t, 0, (size_t)s1.nentries * sizeof(double), stream));
+    }
+    if (raw_gen != geom_gen) {
+      k_poisson_diag<<<blocks_for(nv), kBlock, 0, stream>>>((int)nv, -1, -1, dpos1, Lv, bc, diag_raw, inv_raw);
+      k_poisson_sell<<<blocks_for(nnz1), kBlock, 0, stream>>>(nnz1, -1, -1, s1.posmap, rows1, ci1, Lv, bc,
+                                                              inv_raw, nullptr, Lraw_t);
+      CK(cudaGetLastError());
+      raw_gen = geom_gen;
+    }
+    double *d_b = d_vec3, *d_x = d_vec3 + nv;  // staging buffer, 3 N2 >= 2 nv doubles
+    CK(cudaMemcpyAsync(d_b, rhs, (size_t)nv * sizeof(double), cudaMemcpyHostToDevice, stream));
+    reset_status();
+    PressureRhsArgs a = pressure_rhs_args(d_x, st);
+    a.given_b = d_b;
+    a.invL = inv_raw;
+    a.tol = tol;
+    a.maxit = maxit;
+    a.krylov = 1;
+    a.scaled = 0;
+    k_pressure_rhs<<<blocks_for(nv), kBlock, 0, stream>>>(a);
+    CK(cudaGetLastError());
+    BicgArgs b{};
+    b.S = s1.view();
+    b.At = Lraw_t;
+    b.diagA = diag_raw;
+    b.invA = inv_raw;
+    b.b = pb;
+    b.x = d_x;
+    b.r = pr;
+    b.r0 = pz;
+    b.pk = pp;
+    b.v = pv;
+    b.s = ps;
+    b.t = pt;
+    b.n = (int)nv;
+    b.bs = bs_p;
+    b.red = red;
+    b.st = st;
+    b.slot = 1;
+    b.cw = nullptr;
+    auto body = [&](cudaStream_t s, cudaGraphConditionalHandle hc, int use) {
+      BicgArgs c = b;
+      c.cond = hc;
+      c.use_cond = use;
+      bicg_body<1>(c, s, s1, (int)nv);
+    };
+    eager_while(body, [&] { return poll_bicg(bs_p); }, maxit);
+    k_check_bicg<<<1, 1, 0, stream>>>(bs_p, 1, 1, st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(x_host, d_x, (size_t)nv * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    return h_st->code;
   }
 
   void enqueue_pressure_update() {
@@ -2230,12 +2299,19 @@ int cfsa_ns_update_boundary_tags(cfsa_ns *h, const int8_t *p1_bc, const int8_t *
   });
 }
 
+// Message of a failed stepping call (status from the device status word).
+static std::string step_failure(int code) {
+  std::string m = "step failed with status " + std::to_string(code);
+  if (code == CFSA_CUDA_ERROR) m += ": the pressure solve gave up waiting at a grid barrier";
+  return m;
+}
+
 int cfsa_ns_piso_steps(cfsa_ns *h, int n, int *n_done) {
   if (!h) return CFSA_BAD_ARG;
   if (n < 0) return fail(h, CFSA_BAD_ARG, "negative step count");
   return guarded(h, [&] {
     const int code = h->run_steps(n, n_done, false);
-    if (code != CFSA_OK) h->err = "step failed with status " + std::to_string(code);
+    if (code != CFSA_OK) h->err = step_failure(code);
     return code;
   });
 }
@@ -2246,7 +2322,7 @@ int cfsa_ns_simple_step(cfsa_ns *h) {
   if (!h) return CFSA_BAD_ARG;
   return guarded(h, [&] {
     const int code = h->run_steps(1, nullptr, true);
-    if (code != CFSA_OK) h->err = "step failed with status " + std::to_string(code);
+    if (code != CFSA_OK) h->err = step_failure(code);
     return code;
   });
 }
@@ -2273,6 +2349,17 @@ int cfsa_ns_pressure_poisson(cfsa_ns *h) {
     CK(cudaMemcpyAsync(h->h_st, h->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return h->h_st->code;
+  });
+}
+
+int cfsa_ns_solve_pressure_bicgstab(cfsa_ns *h, const double *rhs, double *x, double tol, int maxit) {
+  if (!h || !rhs || !x) return CFSA_BAD_ARG;
+  if (!(tol >= 0.0) || maxit < 1) return fail(h, CFSA_BAD_ARG, "solvePressureBiCGSTAB: tol >= 0 and maxit >= 1 required");
+  return guarded(h, [&] {
+    const int code = h->solve_poisson_raw(rhs, x, tol, maxit);
+    if (code == CFSA_NOT_CONVERGED) h->err = "BiCGSTAB failed: no convergence within the iteration cap";
+    if (code == CFSA_BREAKDOWN) h->err = "BiCGSTAB failed: breakdown";
+    return code;
   });
 }
 
@@ -2724,6 +2811,14 @@ int cfsa_ns_get_adjoint_stats(cfsa_ns *h, cfsa_adjoint_stats *out) {
 }
 
 }  // extern "C"
+
+extern "C" int cfsa_ns_set_barrier_spin_limit(cfsa_ns *h, int64_t polls) {
+  if (!h) return CFSA_BAD_ARG;
+  const long long lim = polls < 0 ? kBarrierSpinLimit : (long long)polls;
+  if (lim != h->bar_spin_limit) h->graph_dirty = true;  // the limit is a captured launch argument
+  h->bar_spin_limit = lim;
+  return CFSA_OK;
+}
 
 extern "C" int cfsa_ns_profile_kernel(cfsa_ns *h, int which, int iters, double *avg_ms,
                                       double *alg_bytes) {

@@ -308,6 +308,7 @@ __global__ void k_row_of_slot(int n, const int *__restrict__ rp, int *__restrict
 
 // Poisson operator with the outlet / reference penalty (NavierStokes.cpp:604-626) in SELL
 // layout: Ls = Lbc (for CG), Lt = Lbc * diag(invL) (for BiCGSTAB); diagonal inverse invL.
+// outlet_type -1 adds no penalty (the raw operator of solvePressureBiCGSTAB, :773-802).
 __global__ void k_poisson_diag(int n, int outlet_type, int ref_node, const int *__restrict__ dpos,
                                const double *__restrict__ Lv, const signed char *__restrict__ bc,
                                double *__restrict__ diagL, double *__restrict__ invL) {
@@ -333,7 +334,7 @@ __global__ void k_poisson_sell(int64_t nnz, int outlet_type, int ref_node,
   if (i == j && ((outlet_type == 1 && i == ref_node) || (outlet_type == 0 && bc[i] == BC_OUTLET)))
     a += kPoissonPenalty;
   const int pos = posmap[k];
-  Ls[pos] = a;
+  if (Ls) Ls[pos] = a;
   Lt[pos] = a * invL[j];
 }
 
@@ -919,6 +920,9 @@ struct PressureRhsArgs {
   Reduce red;
   // Adjoint mode (adj_q != nullptr): b = sum_a G_a^T q_a + adj_lpp (q_a = adj_q + a*nv).
   const double *adj_q, *adj_lpp;
+  // Given right-hand side (given_b != nullptr): b = given_b, no divergence and no penalty term
+  // (the raw Poisson solve of solvePressureBiCGSTAB).
+  const double *given_b;
   CsrView G;
   const int *tpos;
   const double *Gv;
@@ -931,7 +935,9 @@ __global__ void k_pressure_rhs(PressureRhsArgs A) {
   double part[2] = {0.0, 0.0};
   if (i < A.nv) {
     double b;
-    if (A.adj_q) {
+    if (A.given_b) {
+      b = A.given_b[i];
+    } else if (A.adj_q) {
       double g[3];
       gt_row3(i, A.G.rp, A.G.ci, A.tpos, A.Gv, A.nnz1, A.adj_q, A.adj_q + A.nv,
               A.adj_q + 2 * (int64_t)A.nv, g);
@@ -1096,12 +1102,15 @@ __global__ void k_cg_p(CgArgs A) {
 // all CTAs take the same decisions and the iterates equal those of k_cg_q / k_cg_xr / k_cg_p bit
 // for bit. Data written by other CTAs inside the launch is read with L1-bypassing loads.
 // Barriers spin with a bound; on expiry the kernel records an error and every CTA returns.
+// The bound is a launch argument (default kBarrierSpinLimit polls, over a second), so that a
+// test can make a wait run out on purpose and check that the step reports it.
 constexpr long long kBarrierSpinLimit = 1LL << 25;
 
 struct GridBarrier {
   unsigned int *count;  // [1 + kBarrierGroups]: top counter, then one counter per group of CTAs
   unsigned int *gen;
   int *err;
+  long long spin_limit;  // polls of the generation word before a waiting CTA gives up
 };
 constexpr int kBarrierGroupSize = 32;  // CTAs per first-level counter
 constexpr int kBarrierGroups = 64;     // supports grids of up to 2048 CTAs
@@ -1138,7 +1147,7 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier &B) {
           ok = 0;
           break;
         }
-        if (++spins > kBarrierSpinLimit) {
+        if (++spins > B.spin_limit) {
           atomicExch(B.err, 1);
           ok = 0;
           break;

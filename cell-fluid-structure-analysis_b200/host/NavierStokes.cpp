@@ -184,10 +184,26 @@ bool NavierStokesSolver::solvePressureCG(const std::vector<double> &, std::vecto
   return false;
 }
 
-bool NavierStokesSolver::solvePressureBiCGSTAB(const std::vector<double> &, std::vector<double> &) {
-  std::cerr << "[NS] solvePressureBiCGSTAB: raw Poisson solves outside the step are not provided"
-            << std::endl;
-  return false;
+// src/FEM/NavierStokes.cpp:773-802: Jacobi BiCGSTAB (tol 1e-8, maxit 1000, zero initial guess)
+// on the raw Poisson matrix, no boundary penalty. As in the reference, the first x.size()
+// entries of the solution are copied into x.
+bool NavierStokesSolver::solvePressureBiCGSTAB(const std::vector<double> &rhs, std::vector<double> &x) {
+  if (!h_) {
+    std::cerr << "[NS] Error: solver not initialized" << std::endl;
+    return false;
+  }
+  if (rhs.size() != pressure_.size() || x.size() > pressure_.size()) {
+    std::cerr << "[NS] solvePressureBiCGSTAB: rhs needs one entry per pressure node" << std::endl;
+    return false;
+  }
+  std::vector<double> sol(pressure_.size(), 0.0);
+  const int code = cfsa_ns_solve_pressure_bicgstab(h_, rhs.data(), sol.data(), 1e-8, 1000);
+  if (code != CFSA_OK) {
+    std::cerr << "[NS] " << cfsa_ns_last_error(h_) << std::endl;
+    return false;
+  }
+  std::copy(sol.begin(), sol.begin() + (std::ptrdiff_t)x.size(), x.begin());
+  return true;
 }
 
 void NavierStokesSolver::computeDivergence(const std::vector<Vec3> &u, std::vector<double> &div_out) {

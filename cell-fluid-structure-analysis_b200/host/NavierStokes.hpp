@@ -30,7 +30,7 @@ class NavierStokesSolver {
   double relax_u_ = 1.0;
   double relax_p_ = 1.0;
   double dt_ = 1e-4;
-  int krylov_ = CFSA_KRYLOV_CG;
+  int krylov_ = CFSA_KRYLOV_BICGSTAB;  // NavierStokes.cpp:633; the CG variants are opt-in
   int coarse_target_ = 256;
   int precision_ = CFSA_PRECISION_FP64;
   int conv_norm_ = CFSA_NORM_REFERENCE;
@@ -77,9 +77,10 @@ class NavierStokesSolver {
   std::vector<Vec3> computeAdvectionRHS();
   bool correctVelocity();
   bool solvePressurePoisson();
-  // Declared but never defined by the reference (NavierStokes.hpp:111-113); the GPU build does
-  // not offer raw Poisson solves outside the step: both return false.
+  // Declared but never defined by the reference (NavierStokes.hpp:111): returns false.
   bool solvePressureCG(const std::vector<double> &rhs, std::vector<double> &x);
+  // NavierStokes.cpp:773-802: Jacobi BiCGSTAB (tol 1e-8, maxit 1000) on the raw Poisson matrix
+  // (no boundary penalty) from a zero guess, on the device.
   bool solvePressureBiCGSTAB(const std::vector<double> &rhs, std::vector<double> &x);
   bool normalizePressire();
 

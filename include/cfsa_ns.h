@@ -44,8 +44,9 @@ extern "C" {
 #define CFSA_OUTLET_DIRICHLET 0
 #define CFSA_OUTLET_NEUMANN 1
 
-/* pressure Krylov method: the reference uses BiCGSTAB (src/FEM/NavierStokes.cpp:633); the
- * Poisson matrix with penalty rows is SPD, so CG is offered and is the default here. */
+/* pressure Krylov method: the reference uses BiCGSTAB (src/FEM/NavierStokes.cpp:633), which is the
+ * default here too; the Poisson matrix with penalty rows is SPD, so the CG variants are offered
+ * (same system and stopping rule, fewer products; CFSA_KRYLOV_CG2L is the fastest). */
 #define CFSA_KRYLOV_CG 0
 #define CFSA_KRYLOV_BICGSTAB 1
 /* CG with one reduction per iteration (Chronopoulos & Gear 1989): CG's iterates in exact
@@ -180,6 +181,12 @@ int cfsa_ns_piso_steps(cfsa_ns *h, int n, int *n_done);     /* n x pisoStep, one
 int cfsa_ns_simple_step(cfsa_ns *h);                        /* simpleStep, NavierStokes.cpp:968-1009 */
 int cfsa_ns_momentum_predictor(cfsa_ns *h);                 /* solveMomentumPredictor, :416-524 */
 int cfsa_ns_pressure_poisson(cfsa_ns *h);                   /* solvePressurePoisson, :586-668 */
+/* solvePressureBiCGSTAB (src/FEM/NavierStokes.cpp:773-802): solves L x = rhs with Jacobi BiCGSTAB
+ * on the raw Poisson matrix (no outlet or reference penalty) from a zero initial guess, stopping at
+ * ||r|| <= tol ||rhs|| or after maxit iterations (the reference uses tol 1e-8, maxit 1000).
+ * rhs, x: [nv] host arrays; x receives the last iterate. Returns CFSA_NOT_CONVERGED or
+ * CFSA_BREAKDOWN when the solve fails (the reference's false). The solver's fields are unchanged. */
+int cfsa_ns_solve_pressure_bicgstab(cfsa_ns *h, const double *rhs, double *x, double tol, int maxit);
 int cfsa_ns_correct_velocity(cfsa_ns *h);                   /* correctVelocity, :702-771 */
 
 /* ---- fields ---- */
@@ -221,6 +228,12 @@ int cfsa_ns_get_inv_lumped_mass(cfsa_ns *h, double *out /*[N2]*/);
  * launch; alg_bytes: algorithmic bytes one launch must move (matrix values and column indices,
  * row metadata, each vector element read or written once). */
 int cfsa_ns_profile_kernel(cfsa_ns *h, int which, int iters, double *avg_ms, double *alg_bytes);
+/* Bound on the polls a CTA of the resident pressure solvers (CG, CFSA_KRYLOV_CG1, CG2L) makes at
+ * a grid barrier before it gives up: the solve then stops, the step fails with CFSA_CUDA_ERROR
+ * ("gave up waiting at a grid barrier"), time does not advance, and the handle stays usable.
+ * polls < 0 restores the default (2^25 polls, over a second); 0 gives up at the first wait, which
+ * tests use to exercise the failure path. */
+int cfsa_ns_set_barrier_spin_limit(cfsa_ns *h, int64_t polls);
 
 /* ---- allocation-free operator (no counterpart in the reference) ---- */
 /* Divergence (the computeDivergence operator above) for callers that cannot allocate device

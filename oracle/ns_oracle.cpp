@@ -1720,6 +1720,18 @@ void orc_set_params(void *h, double dt, double tol_mom, double tol_p, int maxit_
   o->pressure_solver = pressure_solver;
   o->coarse_built = false;
 }
+// NavierStokesSolver::solvePressureBiCGSTAB (src/FEM/NavierStokes.cpp:773-802): BiCGSTAB with
+// Jacobi on the raw Poisson matrix L (no boundary penalty), zero initial guess (Eigen's solve),
+// stopping at tol / maxit; x [nv] receives the iterate. Returns 0 when converged, 1 otherwise.
+int orc_solve_poisson_raw(void *h, const double *rhs, double *x, double tol, int maxit, int *iters) {
+  Oracle *o = static_cast<Oracle *>(h);
+  std::vector<double> b(rhs, rhs + o->nv), xv;
+  SolveInfo si = bicgstab(o->L, b, xv, tol, maxit, o->order_nv, o->order_p1, o->order_nv, false);
+  std::copy(xv.begin(), xv.end(), x);
+  if (iters) *iters = si.iters;
+  return si.converged ? 0 : 1;
+}
+
 // Target number of aggregates of the two-level pressure preconditioner (default 256). Returns 0,
 // or 1 (target unchanged) outside [1, 1024], the range the device solver accepts.
 int orc_set_coarse_target(void *h, int target) {

@@ -61,6 +61,7 @@ def lib() -> C.CDLL:
         "orc_stats": (None, [vp, vp, vp, vp]),
         "orc_set_threads": (i32, [i32]),
         "orc_cylinder": (i32, [dbl, dbl, i32, i32, vp, vp]),
+        "orc_solve_poisson_raw": (i32, [vp, vp, vp, dbl, i32, vp]),
         "orc_adjoint_forward": (i32, [vp, i32]),
         "orc_objective": (i32, [vp, i32, i32, dbl, dbl, vp, vp, vp, vp]),
         "orc_adjoint_backward": (i32, [vp, vp, vp, dbl, vp, vp, vp]),
@@ -160,6 +161,15 @@ class Oracle:
         1..1024 as on the device."""
         if self.L.orc_set_coarse_target(self.h, int(target)) != 0:
             raise ValueError(f"coarse target {target} outside [1, 1024]")
+
+    def solve_poisson_raw(self, rhs, tol=1e-8, maxit=1000):
+        """solvePressureBiCGSTAB: (converged, x, iterations) of Jacobi BiCGSTAB on the raw Poisson
+        matrix (no boundary penalty) from a zero guess."""
+        b = np.ascontiguousarray(rhs, np.float64)
+        x = np.zeros(self.nv)
+        it = C.c_int(0)
+        code = self.L.orc_solve_poisson_raw(self.h, _p(b), _p(x), float(tol), int(maxit), C.byref(it))
+        return code == 0, x, it.value
 
     def coarse_size(self) -> int:
         return self.L.orc_coarse_size(self.h)

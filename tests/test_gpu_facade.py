@@ -35,7 +35,7 @@ def test_cpp_example_matches_oracle(cf, po, tmp_path):
     o = po.Oracle(m.vertices(), m.tets())
     o.set_fluid(1060.0, 0.004)
     o.set_params(dt=0.01, tol_mom=1e-10, tol_p=1e-10, maxit_mom=5000, maxit_p=50000,
-                 relax_u=0.5, relax_p=0.5, pressure_solver=1)
+                 relax_u=0.5, relax_p=0.5, pressure_solver=0)  # the default: BiCGSTAB, as the reference
     inl = np.zeros((o.N2, 3))
     inl[:, 0] = 0.5
     o.set_inlet(inl)  # before initialize, as in the example

@@ -306,6 +306,61 @@ def test_nan_input_fails_fast(cf, po, krylov):
     assert max(st["momentum_iters"]) <= 1
 
 
+@pytest.mark.parametrize("krylov", [0, 2, 3], ids=["cg", "cg1", "cg2l"])
+def test_grid_barrier_wait_runs_out(cf, po, krylov):
+    """The resident pressure solvers wait at grid barriers with a bounded number of polls. With
+    the bound at 0 the first CTA to wait gives up: every CTA leaves the kernel, the step reports
+    CFSA_CUDA_ERROR through the C ABI (the facade's pisoStep() is false), time does not advance,
+    and after the default bound is restored the same handle steps on from the unchanged state
+    bit for bit with the oracle's first step. No GPU fault is involved: the wait ends on its own
+    and the host reads the status word."""
+    m = make_mesh(cf, 3, 12)
+    s, o = make_pair(cf, po, m, tol=1e-12, krylov=krylov)
+    lib = cf.load_library()
+    u0, p0 = s.getVelocity().copy(), s.getPressure().copy()
+    s.setBarrierSpinLimit(0)
+    code = lib.cfsa_ns_piso_step(s._h)
+    assert code == cf.CUDA_ERROR
+    assert "grid barrier" in lib.cfsa_ns_last_error(s._h).decode()
+    assert s.getTime() == 0.0
+    assert np.array_equal(s.getVelocity(), u0) and np.array_equal(s.getPressure(), p0)
+    s.setBarrierSpinLimit(-1)
+    assert s.pisoStep()
+    assert o.piso_step() == 0
+    st = o.state()
+    assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"])
+    assert s.getTime() == st["time"]
+
+
+def test_solve_pressure_bicgstab_matches_oracle(cf, po):
+    """solvePressureBiCGSTAB (NavierStokes.cpp:773-802): raw Poisson matrix, no boundary penalty,
+    tol 1e-8, maxit 1000, zero guess. A consistent right-hand side (L y) converges; the GPU iterate
+    equals the oracle's bit for bit (same reduction tree). An inconsistent one with a small cap
+    fails on both sides with the same last iterate. The solver's fields are left unchanged."""
+    m = make_mesh(cf, 3, 12)
+    s, o = make_pair(cf, po, m, tol=1e-12, krylov=1)
+    rng = np.random.default_rng(11)
+    rp, ci, vals = s.matrix(5)
+    L = np.zeros((s.nv, s.nv))
+    for i in range(s.nv):
+        L[i, ci[rp[i]:rp[i + 1]]] = vals[rp[i]:rp[i + 1]]
+    rhs = L @ rng.standard_normal(s.nv)
+    u0, p0 = s.getVelocity().copy(), s.getPressure().copy()
+    ok, x = s.solvePressureBiCGSTAB(rhs)
+    ok_o, x_o, it_o = o.solve_poisson_raw(rhs)
+    assert ok and ok_o and it_o > 1
+    assert np.array_equal(x, x_o)
+    assert np.linalg.norm(L @ x - rhs) <= 1e-8 * np.linalg.norm(rhs) * (1 + 1e-6)
+    assert np.array_equal(s.getVelocity(), u0) and np.array_equal(s.getPressure(), p0)
+    bad = rng.standard_normal(s.nv)  # not in the range of the singular L: stays unconverged
+    ok, x = s.solvePressureBiCGSTAB(bad, maxit=5)
+    ok_o, x_o, it_o = o.solve_poisson_raw(bad, maxit=5)
+    assert not ok and not ok_o and it_o == 5
+    assert np.array_equal(x, x_o)
+    ok, x = s.solvePressureBiCGSTAB(np.zeros(s.nv))
+    assert ok and not x.any()
+
+
 def test_reassembly_after_vertex_motion(cf, po):
     """build_sparse_matrices after the mesh moved (coupled path): device re-assembly equals the
     oracle built on the moved mesh."""
