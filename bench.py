@@ -96,10 +96,15 @@ def parse():
     ap.add_argument("--rings", type=int, default=GEOM["rings"])
     ap.add_argument("--layers", type=int, default=GEOM["layers"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-oracle", action="store_true",
+                    help="skip every oracle run (parity at 1M tets, config-2 CPU comparison, CPU baseline)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
+    ap.add_argument("--mixed-marks", default="1,50,200", help="steps at which config 2 compares fields")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint run")
-    ap.add_argument("--y-bifurcation", action="store_true",
-                    help="also run config 4 (Y-bifurcation, ~4M tets, mixed precision + adjoint)")
+    ap.add_argument("--no-y-bifurcation", action="store_true",
+                    help="skip config 4 (Y-bifurcation, ~4M tets, mixed precision + adjoint)")
+    ap.add_argument("--y-steps", type=int, default=20, help="steps of each config-4 run")
+    ap.add_argument("--y-checkpoint", type=int, default=5, help="checkpoint interval of the config-4 adjoint")
     ap.add_argument("--y-cell", type=float, default=0.081, help="lattice edge of the Y-bifurcation mesh")
     ap.add_argument("--adjoint-fd-nodes", type=int, default=ADJ_NODES,
                     help="seeded inlet nodes checked against central finite differences")
@@ -299,82 +304,82 @@ def adjoint_section(cf, args, barrier):
 
 
 Y_CELL = 0.081  # Kuhn lattice edge of the Y-bifurcation: ~4M tets (mean volume ~1e-4)
-Y_STEPS, Y_CHECKPOINT = 100, 20
 
 
-def ybif_section(cf, args, barrier):
+def ybif_section(cf, args, barrier, peak):
     """Config 4: Y-bifurcation (parent R=2 L=15, daughters R=1.5 L=12 at +-35 deg, blend 0.5),
-    ~4M tets, parabolic inlet peak 1.0, both outlets p=0, 100 steps from rest. FP64 and mixed
-    precision forward runs (Jacobi-scaled criterion, tol 1e-10), then the mixed-precision
-    forward/backward pair with checkpoints every 20 steps for the pressure-drop objective
-    differentiated with respect to the inlet profile."""
-    import torch
-
+    ~4M tets, parabolic inlet peak 1.0, both outlets p=0, from rest; FP64 and mixed-precision
+    forward runs (Jacobi-scaled criterion, tol 1e-10) over `--y-steps` steps (the configuration
+    names 100; the default budget keeps the whole benchmark within minutes), the pressure solve's
+    achieved bandwidth where its operator no longer fits in L2, then the mixed-precision
+    forward/backward pair of the pressure-drop objective differentiated with respect to the inlet
+    profile, checkpointing every `--y-checkpoint` steps."""
     t0 = time.perf_counter()
     m = cf.Mesh.yBifurcation(cell=args.y_cell)
     mesh_s = time.perf_counter() - t0
     nv, nt, ne, _, _ = m.sizes
     prof = cf.parabolic_inlet(m.nodePositions(), INLET_PEAK, 2.0)
     p1, p2 = m.fluidBC()
+    n = args.y_steps
 
     def solver(precision):
-        s = cf.NavierStokesSolver()
-        s.setKrylovTolerances(TOL, TOL)
-        s.setConvergenceNorm(cf.NORM_JACOBI)
-        s.setMaxIterations(*MAXIT)
-        s.setPressureSolver(cf.KRYLOV_CG2L)
-        s.setPrecision(precision)
-        s.setDt(DT)
-        s.initialize(m, cf.Fluid(*FLUID))
-        s.setInletVelocityProfile(prof)
-        return s
+        return make_solver_with(cf, m, prof, tol=TOL, norm=cf.NORM_JACOBI, precision=precision)
 
     out = {"workload": f"config 4: Y-bifurcation, {nt} tets, N2={nv + ne}, nv={nv} (Kuhn lattice cell "
-                       f"{args.y_cell}); {Y_STEPS} steps from rest, parabolic inlet peak 1.0, both outlets "
-                       f"p=0, Krylov tol {TOL:g} Jacobi-scaled",
-           "tets": nt, "p2_nodes": nv + ne, "inlet_vertices": int((p1 == 1).sum()),
-           "outlet_vertices": int((p1 == 2).sum()), "mesh_seconds": mesh_s}
+                       f"{args.y_cell}); {n} steps from rest (budget; the configuration names 100), parabolic "
+                       f"inlet peak 1.0, both outlets p=0, Krylov tol {TOL:g} Jacobi-scaled, two-level CG pressure",
+           "tets": nt, "p2_nodes": nv + ne, "pressure_dofs": nv, "inlet_vertices": int((p1 == 1).sum()),
+           "outlet_vertices": int((p1 == 2).sum()), "mesh_seconds": mesh_s, "steps": n}
     res = {}
     for name, prec in (("fp64", cf.PRECISION_FP64), ("mixed", cf.PRECISION_MIXED)):
         s = solver(prec)
         barrier()
-        ok, done = s.pisoSteps(Y_STEPS)
+        ok, done = s.pisoSteps(n)
         st = s.stats()
         barrier()
-        res[name] = dict(ok=bool(ok), steps=done, ms=st["last_step_ms"], u=s.getVelocity(), p=s.getPressure(),
+        res[name] = dict(ok=bool(ok), steps=done, ms=st["last_step_ms"], u=s.getVelocity().copy(),
+                         p=s.getPressure().copy(),
                          iters=[st["krylov_iters"][0] / max(done, 1), st["krylov_iters"][1] / max(done, 1)],
                          phase_ms=st["phase_ms"])
+        if name == "fp64":
+            ms, by = s.profileKernel(cf.KERNEL_PRESSURE_SOLVE, 3)
+            gbs = by / (ms * 1e-3) / 1e9
+            out["pressure_cg_solve"] = {
+                "avg_ms": ms, "alg_bytes": by, "achieved_gbs": gbs, "frac_of_peak": gbs / peak,
+                "iterations": s.stats()["pressure_iters"],
+                "note": "whole two-level CG solve in one resident kernel; Poisson operator of "
+                        f"{nv} rows does not fit in the 126 MB L2 together with its vectors"}
         del s
+        import torch
+
         torch.cuda.empty_cache()
-    from numpy.linalg import norm as l2
     for name in ("fp64", "mixed"):
         r = res[name]
         out[name] = {"ok": r["ok"], "steps_per_s": r["steps"] / (r["ms"] / 1e3), "ms_per_step": r["ms"] / max(r["steps"], 1),
                      "krylov_iters_per_step": r["iters"], "phase_ms_last_step": r["phase_ms"],
                      "dof_updates_per_s": (3 * (nv + ne) + nv) * r["steps"] / (r["ms"] / 1e3)}
     out["mixed_speedup_vs_fp64"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
-    out["rel_l2_mixed_vs_fp64"] = {"u": float(l2(res["mixed"]["u"] - res["fp64"]["u"]) / l2(res["fp64"]["u"])),
-                                   "p": float(l2(res["mixed"]["p"] - res["fp64"]["p"]) / l2(res["fp64"]["p"]))}
-    # adjoint (mixed precision forward and adjoint solves)
+    out["rel_l2_mixed_vs_fp64"] = {"u": rel_l2(res["mixed"]["u"], res["fp64"]["u"]),
+                                   "p": rel_l2(res["mixed"]["p"], res["fp64"]["p"])}
+    # adjoint (mixed-precision forward and adjoint solves)
     s = solver(cf.PRECISION_MIXED)
     barrier()
-    ok = s.adjointForward(Y_STEPS, Y_CHECKPOINT)
+    ok = s.adjointForward(n, args.y_checkpoint)
     g = s.adjointBackward(kind=cf.OBJECTIVE_PRESSURE_DROP) if ok else None
     barrier()
     if g is not None:
-        ast = s.adjointStats()
+        ast_ = s.adjointStats()
         inl = np.concatenate([p1, p2]) == 1
-        out["adjoint"] = {"ok": True, "J_pressure_drop": g["J"], "forward_ms": ast["forward_ms"],
-                          "backward_ms": ast["backward_ms"], "recomputed_steps": ast["recomputed_steps"],
-                          "checkpoints": ast["checkpoints"], "record_gb": ast["record_bytes"] / 2**30,
-                          "adjoint_krylov_iters": [ast["momentum_iters"], ast["pressure_iters"]],
-                          "grad_inlet_axial_l2": float(l2(g["grad_inlet"][inl, 0])),
+        out["adjoint"] = {"ok": True, "J_pressure_drop": g["J"], "forward_ms": ast_["forward_ms"],
+                          "backward_ms": ast_["backward_ms"], "recomputed_steps": ast_["recomputed_steps"],
+                          "checkpoints": ast_["checkpoints"], "record_gb": ast_["record_bytes"] / 2**30,
+                          "adjoint_krylov_iters": [ast_["momentum_iters"], ast_["pressure_iters"]],
+                          "grad_inlet_axial_l2": float(np.linalg.norm(g["grad_inlet"][inl, 0])),
                           "grad_viscosity": g["grad_viscosity"],
-                          "steps_per_s_forward_plus_backward": Y_STEPS / ((ast["forward_ms"] + ast["backward_ms"]) / 1e3)}
+                          "steps_per_s_forward_plus_backward": n / ((ast_["forward_ms"] + ast_["backward_ms"]) / 1e3)}
     else:
         out["adjoint"] = {"ok": False}
     del s
-    torch.cuda.empty_cache()
     return out
 
 
@@ -475,6 +480,123 @@ def run_reference(args):
     return 0
 
 
+def rel_l2(a, b) -> float:
+    from numpy.linalg import norm
+
+    nb = norm(b)
+    return float(norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0))
+
+
+def trajectory(cf, m, profile, precision, tol, norm, marks):
+    """A solver from rest: device ms over all steps and (u, p, per-step stats) at each mark."""
+    s = make_solver_with(cf, m, profile, tol=tol, norm=norm, precision=precision)
+    out, ms, done, ok = {}, 0.0, 0, True
+    iters, upd = [0, 0], 0
+    for k in marks:
+        good, n = s.pisoSteps(k - done)
+        st = s.stats()
+        ok = ok and good and n == k - done
+        ms += st["last_step_ms"]
+        iters = [iters[0] + st["krylov_iters"][0], iters[1] + st["krylov_iters"][1]]
+        done = k
+        out[k] = (s.getVelocity().copy(), s.getPressure().copy(), st)
+    del s
+    return out, ms, ok, iters
+
+
+def make_solver_with(cf, m, profile, tol=TOL, norm=0, precision=0):
+    s = cf.NavierStokesSolver()
+    s.setKrylovTolerances(tol, tol)
+    s.setConvergenceNorm(norm)
+    s.setMaxIterations(*MAXIT)
+    s.setPressureSolver(cf.KRYLOV_CG2L)
+    s.setPrecision(precision)
+    s.setDt(DT)
+    s.initialize(m, cf.Fluid(*FLUID))
+    s.setInletVelocityProfile(profile)
+    return s
+
+
+def mixed_section(cf, m, profile, marks):
+    """Config 2 on the headline mesh and inputs: FP64 and mixed precision (FP32 BiCGSTAB with FP64
+    reliable updates) from rest over marks[-1] steps, both under the Jacobi-scaled criterion at
+    1e-10 (the reference's criterion is dominated by the 1e10 penalty rows and pins the interior
+    only loosely), and an FP64 run at 1e-14 in the same norm as the converged solution; fields at
+    every mark. Both paths run the two-level CG pressure solve in FP64."""
+    J = cf.NORM_JACOBI
+    f64, f_ms, f_ok, f_it = trajectory(cf, m, profile, cf.PRECISION_FP64, TOL, J, marks)
+    mix, m_ms, m_ok, m_it = trajectory(cf, m, profile, cf.PRECISION_MIXED, TOL, J, marks)
+    conv, _, c_ok, _ = trajectory(cf, m, profile, cf.PRECISION_FP64, 1e-14, J, marks)
+    n = marks[-1]
+    res = {"workload": f"config 2: the headline mesh and inputs, {n} steps from rest; FP32 operator and Krylov "
+                       f"vectors with FP64 reliable updates (true residual, solution, dots) vs FP64 BiCGSTAB "
+                       f"momentum; two-level CG pressure in FP64 in both; Jacobi-scaled criterion 1e-10",
+           "ok": bool(f_ok and m_ok and c_ok), "steps": n,
+           "value": n / (m_ms / 1e3), "unit": UNIT, "fp64_value": n / (f_ms / 1e3),
+           "speedup_vs_fp64": f_ms / m_ms, "ms_per_step": m_ms / n, "fp64_ms_per_step": f_ms / n,
+           "krylov_iters_per_step": {"mixed": [m_it[0] / n, m_it[1] / n], "fp64": [f_it[0] / n, f_it[1] / n]},
+           "at_step": {}}
+    for k in marks:
+        res["at_step"][str(k)] = {
+            "mixed_vs_fp64": {"u": rel_l2(mix[k][0], f64[k][0]), "p": rel_l2(mix[k][1], f64[k][1])},
+            "mixed_vs_converged": {"u": rel_l2(mix[k][0], conv[k][0]), "p": rel_l2(mix[k][1], conv[k][1])},
+            "fp64_vs_converged": {"u": rel_l2(f64[k][0], conv[k][0]), "p": rel_l2(f64[k][1], conv[k][1])},
+            "momentum_iters": {"mixed": mix[k][2]["momentum_iters"], "fp64": f64[k][2]["momentum_iters"]},
+            "reliable_updates": mix[k][2]["momentum_outer"],
+            "pressure_iters": mix[k][2]["pressure_iters"],
+        }
+    first = marks[0]
+    return res, {"mixed": mix[first][:2], "fp64": f64[first][:2]}
+
+
+def cpu_section(args, gpu_headline, gpu_step1_jacobi):
+    """Everything the oracle (test infrastructure) does in the GPU arm, on one oracle instance of
+    the headline workload, after the GPU sections: (1) parity of the headline FP64 path, the same
+    solver (two-level CG pressure, same coarse target, reference criterion 1e-10) from rest, at
+    steps 1 and 3; (2) config 2's CPU comparison, FP64 in the Jacobi-scaled criterion, step 1;
+    (3) the timed CPU baseline, the reference algorithm (BiCGSTAB pressure) on all host threads."""
+    po, o = oracle_cylinder(args.rings, args.layers, pressure_solver=3)
+    threads = po.set_threads(os.cpu_count() or 1)
+    zero_u, zero_p = np.zeros((o.N2, 3)), np.zeros(o.nv)
+    parity = {"workload": "headline FP64 step (two-level CG pressure, reference criterion 1e-10) from rest, "
+                          "GPU vs the oracle on the same mesh and inputs", "at_step": {}}
+    t0 = time.perf_counter()
+    for k in (1, 2, 3):
+        if o.piso_step() != 0:
+            parity["ok"] = False
+            break
+        if k in gpu_headline:
+            st = o.state()
+            gu, gp = gpu_headline[k]
+            parity["at_step"][str(k)] = {"u": rel_l2(gu, st["u"]), "p": rel_l2(gp, st["p"]),
+                                         "bit_exact": bool(np.array_equal(gu, st["u"]) and np.array_equal(gp, st["p"]))}
+    parity.setdefault("ok", all(v["u"] <= 1e-8 and v["p"] <= 1e-8 for v in parity["at_step"].values()))
+    parity["oracle_seconds"] = time.perf_counter() - t0
+    parity["oracle_threads"] = threads
+    mixed_cpu = None
+    if gpu_step1_jacobi is not None:
+        o.set_state(zero_u, zero_p)
+        o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=3,
+                     conv_norm=1)
+        if o.piso_step() == 0:
+            st = o.state()
+            mixed_cpu = {"reference": "FP64 oracle (CPU), Jacobi-scaled criterion 1e-10, step 1 from rest"}
+            for name, (gu, gp) in gpu_step1_jacobi.items():
+                mixed_cpu[name] = {"u": rel_l2(gu, st["u"]), "p": rel_l2(gp, st["p"])}
+    cpu = None
+    if not args.no_cpu_baseline:
+        o.set_state(zero_u, zero_p)
+        o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=0)
+        if o.piso_step() == 0:
+            done, el, cores = time_oracle_steps(po, o, os.cpu_count() or 1, 5, 30.0)
+            if done:
+                cpu = {"value": done / el, "unit": UNIT, "cores": cores, "kind": "port",
+                       "sample": f"{done} PISO steps (steps 2-{done + 1} from rest) of the {o.nt}-tet workload, "
+                                 f"{el:.1f} s, FP64 oracle port of the reference algorithm (BiCGSTAB pressure and "
+                                 f"momentum) with OpenMP on {cores} threads"}
+    return parity, mixed_cpu, cpu
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -499,11 +621,21 @@ def main():
     s, profile = make_solver(cf, m)
     nv, nt, ne, _, _ = m.sizes
     N2 = nv + ne
+    warm = max(args.warmup, 3)
 
-    ok, done = s.pisoSteps(max(args.warmup, 3))
-    if not ok:
-        raise SystemExit(f"warm-up failed after {done} steps: {s.stats()}")
-    # the end-to-end loop below replays the same steps as the device-timed loop, from this state
+    # warm-up from rest; its steps 1 and 3 are kept for the parity check against the oracle
+    headline_states = {}
+    done = 0
+    for k in (1, 3, warm):
+        if k == done:
+            continue
+        ok, n = s.pisoSteps(k - done)
+        if not ok:
+            raise SystemExit(f"warm-up failed at step {done + n}: {s.stats()}")
+        done = k
+        headline_states.setdefault(k, (s.getVelocity().copy(), s.getPressure().copy()))
+    headline_states = {k: v for k, v in headline_states.items() if k in (1, 3)}
+    # the end-to-end loop and the accuracy check below replay the timed steps from this state
     import tempfile
     snap = os.path.join(tempfile.gettempdir(), f"cfsa_bench_state_{os.getpid()}.bin")
     s.saveState(snap)
@@ -526,12 +658,12 @@ def main():
     ms_total = st["last_step_ms"]
     ms_max = max_over_ranks(ms_total, dist)
     value = world * args.steps / (ms_max / 1e3)
+    timed_u, timed_p = s.getVelocity().copy(), s.getPressure().copy()
 
     # end to end through the public API with host buffers: per step upload the inlet profile
     # (H2D), pisoStep, read back u and p (D2H); the host buffers are pinned, as an application
     # streaming fields every step would hold them. Same steps as the timed loop (restored state).
     s.loadState(snap)
-    os.remove(snap)
     prof_host = torch.empty(profile.shape, dtype=torch.float64, pin_memory=True).numpy()
     prof_host[:] = profile
     u_host = torch.empty((s.N2, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -548,17 +680,21 @@ def main():
     e2e_s = time.perf_counter() - t0
     e2e_value = world * args.steps / max_over_ranks(e2e_s, dist)
 
-    # roofline of the step's SpMV kernels on live data (CUDA events on the solver's stream)
+    # roofline of the step's kernels on live data (CUDA events on the solver's stream)
     peak, peak_kind = measured_peak()
     traffic = traffic_table()
     kernels = {}
     for name, which, per_step in (("momentum_spmv_3rhs", cf.KERNEL_MOMENTUM_SPMV, 2 * st["krylov_iters"][0]),
-                                  ("pressure_cg_spmv", cf.KERNEL_PRESSURE_SPMV, st["krylov_iters"][1])):
-        ms, by = s.profileKernel(which, 50)
+                                  ("pressure_cg_solve", cf.KERNEL_PRESSURE_SOLVE, args.steps)):
+        ms, by = s.profileKernel(which, 20 if which == cf.KERNEL_MOMENTUM_SPMV else 3)
         gbs = by / (ms * 1e-3) / 1e9
-        kernels[name] = {"avg_ms": ms, "alg_bytes": by, "achieved_gbs": gbs,
+        kernels[name] = {"avg_ms": ms, "alg_bytes": by, "achieved_gbs": gbs, "frac_of_peak": gbs / peak,
                          "launches_timed_region": int(per_step),
                          "time_share_est": None, "traffic": traffic.get(name)}
+    kernels["pressure_cg_solve"]["note"] = (
+        "one launch = one whole two-level CG solve (fused product, coarse correction and vector updates "
+        "in one resident kernel); alg_bytes = iterations x per-iteration bytes; the 1M-tet Poisson operator "
+        "and vectors (~50 MB) stay in the 126 MB L2, so this rate is L2-served, not HBM")
     total_ms = ms_max
     for k in kernels.values():
         k["time_share_est"] = k["avg_ms"] * k["launches_timed_region"] / total_ms
@@ -566,71 +702,51 @@ def main():
     dom = kernels[dom_name]
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": dom["achieved_gbs"], "peak": peak,
                 "unit": "GB/s", "frac": dom["achieved_gbs"] / peak, "peak_kind": peak_kind,
-                "traffic": dom["traffic"]}
+                "traffic": dom["traffic"],
+                "traffic_note": "ncu dram__bytes_read.sum + write.sum of one launch captured at 250k tets, "
+                                "scaled to this workload by the ratio of algorithmic bytes (profiles/)"}
 
-    # Config 2 (mixed precision) on the same mesh and inputs. The reference's criterion
-    # ||r|| <= tol ||b|| is dominated by the 1e10 penalty rows and pins the interior only loosely,
-    # so FP64 and mixed are compared under the Jacobi-scaled norm (||D^-1/2 r|| <= tol ||D^-1/2 b||),
-    # both timed over the same steps, both measured against a converged FP64 run (tol 1e-14).
-    mixed = None
+    # accuracy of the headline itself: the timed steps again from the same state with the Krylov
+    # solves converged (1e-14 in the Jacobi-scaled criterion, which sees the interior rows)
+    s.loadState(snap)
+    os.remove(snap)
+    s.setConvergenceNorm(cf.NORM_JACOBI)
+    s.setKrylovTolerances(1e-14, 1e-14)
+    ok_c, _ = s.pisoSteps(args.steps)
+    headline_accuracy = {
+        "reference": "same steps from the same state, FP64, Krylov tol 1e-14 in the Jacobi-scaled criterion",
+        "ok": bool(ok_c), "u": rel_l2(timed_u, s.getVelocity()), "p": rel_l2(timed_p, s.getPressure()),
+        "note": "the reference's criterion ||r|| <= 1e-10 ||b|| is dominated by the 1e10 penalty rows, so the "
+                "interior is solved loosely at the headline tolerance; this is the headline's own error"}
+    del s
+    torch.cuda.empty_cache()
+
+    mixed, step1 = None, None
     if not args.no_mixed:
-        nwarm = max(args.warmup, 3)
-
-        def timed_run(precision, tol):
-            sx, _ = make_solver(cf, m, tol=tol, norm=cf.NORM_JACOBI)
-            sx.setPrecision(precision)
-            ok_a, _ = sx.pisoSteps(nwarm)
-            barrier()
-            ok_b, _ = sx.pisoSteps(args.steps)
-            stx = sx.stats()
-            barrier()
-            out = (sx.getVelocity(), sx.getPressure(), stx, max_over_ranks(stx["last_step_ms"], dist),
-                   bool(ok_a and ok_b))
-            del sx
-            return out
-
-        from numpy.linalg import norm as l2
-
-        def rel(a, b):
-            return float(l2(a - b) / l2(b))
-
-        cu, cp_, _, _, _ = timed_run(cf.PRECISION_FP64, 1e-14)
-        fu, fp_, fst, fms, fok = timed_run(cf.PRECISION_FP64, TOL)
-        mu_, mp_, mst, mms, mok = timed_run(cf.PRECISION_MIXED, TOL)
-        fv_, mv_ = world * args.steps / (fms / 1e3), world * args.steps / (mms / 1e3)
-        mixed = {
-            "value": mv_, "unit": UNIT, "ok": mok and fok, "norm": "jacobi ||D^-1/2 r|| <= 1e-10 ||D^-1/2 b||",
-            "fp64_value": fv_, "speedup_vs_fp64": mv_ / fv_,
-            "ms_per_step": mms / args.steps, "fp64_ms_per_step": fms / args.steps,
-            "rel_l2_vs_converged": {"mixed": {"u": rel(mu_, cu), "p": rel(mp_, cp_)},
-                                    "fp64": {"u": rel(fu, cu), "p": rel(fp_, cp_)},
-                                    "after_steps": nwarm + args.steps,
-                                    "reference": "FP64 GPU, Krylov tol 1e-14, same norm"},
-            "rel_l2_mixed_vs_fp64": {"u": rel(mu_, fu), "p": rel(mp_, fp_)},
-            "krylov_iters_per_step": {"mixed": [mst["krylov_iters"][0] / args.steps, mst["krylov_iters"][1] / args.steps],
-                                      "fp64": [fst["krylov_iters"][0] / args.steps, fst["krylov_iters"][1] / args.steps]},
-            "outer_sweeps_last_step": mst["momentum_outer"],
-            "phase_ms_last_step": {"mixed": mst["phase_ms"], "fp64": fst["phase_ms"]},
-            "workload": "config 2: same mesh and inputs; momentum FP32 inner BiCGSTAB in FP64 defect "
-                        "correction (true FP64 residual) vs FP64 BiCGSTAB; pressure FP64 two-level CG in both",
-        }
+        marks = [int(x) for x in args.mixed_marks.split(",")]
+        mixed, step1 = mixed_section(cf, m, profile, marks)
+        torch.cuda.empty_cache()
 
     adjoint = None
     if not args.no_adjoint:
         adjoint = adjoint_section(cf, args, barrier)
+        torch.cuda.empty_cache()
 
     ybif = None
-    if args.y_bifurcation:
-        ybif = ybif_section(cf, args, barrier)
+    if not args.no_y_bifurcation:
+        ybif = ybif_section(cf, args, barrier, peak)
+        torch.cuda.empty_cache()
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.rings, args.layers, os.cpu_count() or 1)
+    parity, cpu = None, None
+    if rank == 0 and world == 1 and not args.no_oracle:
+        parity, mixed_cpu, cpu = cpu_section(args, headline_states, step1)
+        if mixed is not None:
+            mixed["vs_cpu_oracle_step1"] = mixed_cpu
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
+            "warmup": warm, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": DATA,
             "config": workload_desc((nv, nt, ne), args.rings, args.layers, world),
@@ -643,8 +759,8 @@ def main():
             "roofline": roofline, "kernels": kernels,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(profile.nbytes),
                     "d2h_bytes_per_step": int(u.nbytes + p.nbytes)},
-            "cpu_baseline": cpu, "clocks": clk, "mixed": mixed, "adjoint": adjoint,
-            "y_bifurcation": ybif,
+            "cpu_baseline": cpu, "clocks": clk, "parity": parity, "headline_accuracy": headline_accuracy,
+            "mixed": mixed, "adjoint": adjoint, "y_bifurcation": ybif,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -185,15 +185,15 @@ struct cfsa_ns {
   int cg2l_col_cap = 0;
   size_t cg2l_smem = 0;
   double *cg_part_a = nullptr, *cg_part_b = nullptr;
-  // mixed precision (FP32 inner Krylov in FP64 defect correction)
+  // mixed precision (FP32 BiCGSTAB with FP64 reliable updates)
   float *At32 = nullptr, *invA32 = nullptr;
   float *fr = nullptr, *fr0 = nullptr, *fp = nullptr, *fv = nullptr, *fs = nullptr, *ft = nullptr,
         *fdx = nullptr;  // [3][N2]
   MixedState *ms = nullptr;
   MixedState *h_ms = nullptr;
-  double mixed_inner_tol = 1e-2;  // measured best of 3e-2..1e-5: 1M-tet cylinder 18.99 vs 19.38 ms per
-                                  // step (4-5 outer sweeps), 1.2M-tet Y mesh 50.7 vs 79.9 ms
-  int mixed_inner_maxit = 300, mixed_max_outer = 30;
+  // reliable-update trigger of the mixed-precision BiCGSTAB: the FP64 residual replaces the FP32
+  // one when the latter has dropped by this factor since the previous update
+  double mixed_delta = 1e-3;
   // discrete adjoint (ns_adjoint.cuh): transposed P1 slots, vertex -> (boundary face, local
   // index in the face's tet) incidence, host vertex coordinates for objective patches
   int *tpos1 = nullptr, *vbf_ptr = nullptr, *vbf = nullptr;
@@ -481,8 +481,7 @@ struct cfsa_ns {
     for (float **w : {&fr, &fr0, &fp, &fv, &fs, &ft, &fdx}) *w = dalloc<float>(n3);
     ms = dalloc<MixedState>(1);
     CK(cudaMemsetAsync(ms, 0, sizeof(MixedState), stream));
-    if (const char *e = std::getenv("CFSA_MIXED_INNER_TOL")) mixed_inner_tol = std::atof(e);
-    if (const char *e = std::getenv("CFSA_MIXED_INNER_MAXIT")) mixed_inner_maxit = std::atoi(e);
+    if (const char *e = std::getenv("CFSA_MIXED_DELTA")) mixed_delta = std::atof(e);
     bs_prof = dalloc<BicgState>(1);
     cs_prof = dalloc<CgState>(1);
     // boundary faces
@@ -535,7 +534,7 @@ struct cfsa_ns {
         q((const void *)k_bicg_xr<3>);
         q((const void *)k_bicg_xr<1>);
         q((const void *)k_mp_xr);
-        q((const void *)k_mp_inner_init);
+        q((const void *)k_mp_init);
       }
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent, kBlock, 0));
       const int nblk_sell = (int)blocks_for(s1.nrows_pad), nblk_nat = (int)blocks_for(nv);
@@ -879,21 +878,29 @@ struct cfsa_ns {
     capture_while_with(cap, sub, new_cond_handle(cap), body);
   }
 
-  // Handle of a conditional node of the graph being captured on `cap`. Its default (1) is
-  // applied when the top-level graph is launched; a loop nested in another loop's body must be
-  // re-armed by a kernel upstream of it in the same body (k_mp_inner_init does this).
-  cudaGraphConditionalHandle new_cond_handle(cudaStream_t cap) {
+  // Handle of a conditional node of the graph being captured on `cap`. Its default is applied
+  // when the top-level graph is launched; a node nested in a loop body must be set by a kernel
+  // upstream of it in the same body (k_mp_xr sets the reliable-update IF node every iteration).
+  cudaGraphConditionalHandle new_cond_handle(cudaStream_t cap, unsigned int dflt = 1) {
     cudaStreamCaptureStatus cst;
     cudaGraph_t g = nullptr;
     CK(cudaStreamGetCaptureInfo(cap, &cst, nullptr, &g, nullptr, nullptr));
     if (cst != cudaStreamCaptureStatusActive) throw CudaError{"stream is not capturing"};
     cudaGraphConditionalHandle h;
-    CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    CK(cudaGraphConditionalHandleCreate(&h, g, dflt, cudaGraphCondAssignDefault));
     return h;
   }
 
   template <class Body>
   void capture_while_with(cudaStream_t cap, cudaStream_t sub, cudaGraphConditionalHandle h, Body body) {
+    capture_cond_with(cap, sub, h, cudaGraphCondTypeWhile, body);
+  }
+
+  // Conditional node (WHILE or IF) appended to the graph being captured on `cap`; its body is
+  // captured from `body` on `sub`.
+  template <class Body>
+  void capture_cond_with(cudaStream_t cap, cudaStream_t sub, cudaGraphConditionalHandle h,
+                         cudaGraphConditionalNodeType type, Body body) {
     cudaStreamCaptureStatus cst;
     cudaGraph_t g = nullptr;
     const cudaGraphNode_t *deps = nullptr;
@@ -902,7 +909,7 @@ struct cfsa_ns {
     if (cst != cudaStreamCaptureStatusActive) throw CudaError{"stream is not capturing"};
     cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
     cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.type = type;
     cp.conditional.size = 1;
     cudaGraphNode_t node;
     CK(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
@@ -1071,52 +1078,46 @@ struct cfsa_ns {
     return a;
   }
 
-  // FP32 inner BiCGSTAB sweeps inside FP64 defect correction (ns_mixed.cuh); outer and inner
-  // loops are nested WHILE nodes when captured.
+  // FP32 BiCGSTAB with FP64 reliable updates (ns_mixed.cuh). Captured: a WHILE node whose body
+  // is one iteration followed by an IF node holding the reliable update; eager: the update
+  // kernels run after every iteration and return at once when no component asked for one.
   void enqueue_momentum_mixed(bool capture, double *x, DevStatus *s_out) {
     const MixedArgs a = mixed_args(x, s_out);
     const unsigned int gp = blocks_for(N2);
-    k_mp_outer_init<<<gp, kBlock, 0, stream>>>(a, tol_mom, mixed_max_outer, mixed_inner_tol, mixed_inner_maxit);
+    k_mp_init<<<strided(k_mp_init, gp), kBlock, 0, stream>>>(a, tol_mom, maxit_mom, mixed_delta);
     CK(cudaGetLastError());
-    auto inner_body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
+    auto update_body = [&](cudaStream_t s, MixedArgs b) {
+      k_mp_xupdate<<<gp, kBlock, 0, s>>>(b);
+      k_mp_residual<<<s2.nruns, kRunThreads, 0, s>>>(b);
+    };
+    auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
       MixedArgs b = a;
       b.cond = h;
       b.use_cond = use;
+      if (use) b.cond_upd = new_cond_handle(s, 0);
       k_mp_p<<<gp, kBlock, 0, s>>>(b);
       k_mp_v<<<s2.nruns, kRunThreads, 0, s>>>(b);
       k_mp_s<<<gp, kBlock, 0, s>>>(b);
       k_mp_t<<<s2.nruns, kRunThreads, 0, s>>>(b);
       k_mp_xr<<<strided(k_mp_xr, gp), kBlock, 0, s>>>(b);
-    };
-    auto outer_body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
-      MixedArgs b = a;
-      if (use) {
-        const cudaGraphConditionalHandle hin = new_cond_handle(s);
-        b.cond = hin;
-        b.use_cond = 1;
-        k_mp_inner_init<<<strided(k_mp_inner_init, gp), kBlock, 0, s>>>(b);  // re-arms the inner loop every sweep
-        capture_while_with(s, body_stream2, hin, inner_body);
-      } else {
-        k_mp_inner_init<<<strided(k_mp_inner_init, gp), kBlock, 0, s>>>(b);
-        eager_while(inner_body, [&] { return poll_mixed(true); }, mixed_inner_maxit);
-      }
-      b.cond = h;
-      b.use_cond = use;
-      k_mp_xupdate<<<gp, kBlock, 0, s>>>(b);
-      k_mp_residual<<<s2.nruns, kRunThreads, 0, s>>>(b);
+      if (use)
+        capture_cond_with(s, body_stream2, b.cond_upd, cudaGraphCondTypeIf,
+                          [&](cudaStream_t ss, cudaGraphConditionalHandle, int) { update_body(ss, b); });
+      else
+        update_body(s, b);
     };
     if (capture)
-      capture_while(outer_body);
+      capture_while(body);
     else
-      eager_while(outer_body, [&] { return poll_mixed(false); }, mixed_max_outer);
+      eager_while(body, [&] { return poll_mixed(); }, maxit_mom);
     k_mp_check<<<1, 1, 0, stream>>>(ms, s_out);
     CK(cudaGetLastError());
   }
 
-  bool poll_mixed(bool inner) {
+  bool poll_mixed() {
     CK(cudaMemcpyAsync(h_ms, ms, sizeof(MixedState), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
-    return inner ? h_ms->in_active != 0 : h_ms->active != 0;
+    return h_ms->active != 0;
   }
 
   void enqueue_pressure_solve(bool capture) {
@@ -1492,11 +1493,11 @@ struct cfsa_ns {
     CK(cudaStreamSynchronize(stream));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
     const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : ((cg_persistent || krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) ? 1 : 3);
-    // mixed momentum: 5 kernels per inner body, 3 per outer sweep (inner init, x update,
-    // residual) plus the outer init kernel per step
+    // mixed momentum: 5 kernels per iteration, 2 per reliable update (x update, residual) plus
+    // the init kernel per step
     batch_launches = (int64_t)launched_steps * (launches_per_step + (precision == CFSA_PRECISION_MIXED ? 1 : 0)) +
                      5 * (int64_t)h_st->body_runs[0] + pressure_body * (int64_t)h_st->body_runs[1] +
-                     3 * (int64_t)h_st->body_runs[2];
+                     2 * (int64_t)h_st->body_runs[2];
     batch_iters[0] = (int64_t)h_st->iters[0];
     batch_iters[1] = (int64_t)h_st->iters[1];
     for (int64_t k = 0; k < h_st->steps_done; ++k) time += dt;
@@ -1567,9 +1568,9 @@ struct cfsa_ns {
       for (size_t k = 0; k < nb; ++k) hsh = (hsh ^ b[k]) * 1099511628211ull;
     };
     const double d[] = {dt, tol_mom, tol_p, relax_u, relax_p, outlet_pressure, viscosity, density,
-                        mixed_inner_tol};
+                        mixed_delta};
     const int64_t k[] = {maxit_mom, maxit_p, ncorr, outlet_type, ref_node, krylov, precision,
-                         conv_norm, geom_gen, mixed_inner_maxit, (int64_t)cg_persistent};
+                         conv_norm, geom_gen, (int64_t)cg_persistent};
     mix(d, sizeof(d));
     mix(k, sizeof(k));
     const std::vector<double> &hin = host_inlet();
@@ -1955,7 +1956,7 @@ struct cfsa_ns {
     const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : ((cg_persistent || krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) ? 1 : 3);
     adj_stats.kernel_launches = (int64_t)adj_steps * adj_launches_fixed + 5 * (int64_t)hs_adj.body_runs[0] +
                                 pressure_body * (int64_t)hs_adj.body_runs[1] +
-                                3 * (int64_t)hs_adj.body_runs[2];
+                                2 * (int64_t)hs_adj.body_runs[2];
     if (h_st->code != CFSA_OK) {
       err = "forward recomputation failed with status " + std::to_string(h_st->code);
       return h_st->code;
@@ -2028,6 +2029,38 @@ struct cfsa_ns {
       for (int k = 0; k < iters; ++k) k_cg_q<<<g, kBlock, 0, stream>>>(c);
       CK(cudaEventRecord(ev1, stream));
       *alg_bytes = 12.0 * (double)nnz1 + 8.0 * s1.nrows_pad + 4.0 * (s1.nslices + 1) + 16.0 * (double)nv;
+    } else if (which == CFSA_KERNEL_PRESSURE_SOLVE) {
+      // the whole resident pressure solve on the divergence of the current u* (the system of the
+      // last step), into scratch: the solver's fields and status are not touched
+      if (krylov != CFSA_KRYLOV_CG2L && krylov != CFSA_KRYLOV_CG1)
+        throw CudaError{"pressure-solve profile needs the resident CG solvers (CG1 or CG2L)"};
+      CK(cudaMemsetAsync(st_free, 0, sizeof(DevStatus), stream));
+      float total = 0.f;
+      int64_t its = 0;
+      for (int k = 0; k < iters; ++k) {
+        k_tet_div<<<blocks_for(nt), kBlock, 0, stream>>>((int)nt, N2, tnode, grad, ustar, divt, st_free);
+        const PressureRhsArgs a = pressure_rhs_args(pv, st_free);
+        k_pressure_rhs<<<blocks_for(nv), kBlock, 0, stream>>>(a);
+        CK(cudaEventRecord(ev0, stream));
+        enqueue_pressure_krylov(false, pv, st_free);
+        CK(cudaEventRecord(ev1, stream));
+        CK(cudaMemcpyAsync(h_cs, cs, sizeof(CgState), cudaMemcpyDeviceToHost, stream));
+        CK(cudaEventSynchronize(ev1));
+        CK(cudaStreamSynchronize(stream));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        total += ms;
+        its += h_cs->iters;
+      }
+      *avg_ms = (double)total / (double)iters;
+      // per iteration: operator values and columns, row metadata, the vectors each read or
+      // written once (r, w, s, p, x, D^-1 read; r, w, s, p, x written; aggregate ids and staging
+      // positions) and, with the coarse space, the dense coarse inverse once
+      const double per_it = 12.0 * (double)nnz1 + 8.0 * s1.nrows_pad + 4.0 * (s1.nslices + 1) +
+                            96.0 * (double)nv +
+                            (krylov == CFSA_KRYLOV_CG2L ? 8.0 * (double)coarse_nc * coarse_nc : 0.0);
+      *alg_bytes = per_it * (double)its / (double)iters;
+      return;
     } else {
       throw CudaError{"unknown kernel id"};
     }
@@ -2491,8 +2524,8 @@ int cfsa_ns_get_stats(const cfsa_ns *hc, cfsa_ns_stats *s) {
       CK(cudaMemcpyAsync(h->h_ms, h->ms, sizeof(MixedState), cudaMemcpyDeviceToHost, h->stream));
       CK(cudaStreamSynchronize(h->stream));
       for (int c = 0; c < 3; ++c) {
-        s->momentum_iters[c] = h->h_ms->total_iters[c];
-        s->momentum_outer[c] = h->h_ms->outer[c];
+        s->momentum_iters[c] = h->h_ms->iters[c];
+        s->momentum_outer[c] = h->h_ms->updates[c];
         const double b2 = h->h_ms->bnorm2[c];
         s->momentum_residual[c] = b2 > 0 ? std::sqrt(h->h_ms->rnorm2[c] / b2) : 0.0;
       }

@@ -70,7 +70,7 @@ struct DevStatus {
   int steps_done;  // completed steps in this batch
   int nan;         // NaN flag of the current step
   unsigned long long body_runs[3];  // loop bodies executed: [0] momentum Krylov, [1] pressure,
-                                    // [2] mixed-precision outer sweeps
+                                    // [2] mixed-precision reliable updates
   unsigned long long iters[2];      // Krylov iterations completed: [0] momentum (max over rhs), [1] pressure
 };
 

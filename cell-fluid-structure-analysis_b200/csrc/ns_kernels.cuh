@@ -484,22 +484,23 @@ __device__ __forceinline__ void sell_spmv_row(const SellView &S, const double *_
 }
 
 // The batched product for the right-hand sides still active in `mask`: compile-time variants for
-// the cases with two active components (one converged first, typically the penalty-dominated
-// streamwise one), so that a converged component costs no gathers; other masks use the full
-// product. Active components get the same sums in the same order in every variant.
+// the cases with one or two active components (the penalty-dominated streamwise one converges
+// first), so that a converged component costs no gathers; the full mask uses the full product.
+// Active components get the same sums in the same order in every variant.
 template <int NC>
 __device__ __forceinline__ void sell_spmv_row_active(const SellView &S, const double *__restrict__ val,
                                                      const double *__restrict__ x, int64_t n, int r,
                                                      double acc[NC], int mask) {
   if constexpr (NC == 3) {
-    if (mask == 6)
-      sell_spmv_row<3, 8, 6>(S, val, x, n, r, acc);
-    else if (mask == 5)
-      sell_spmv_row<3, 8, 5>(S, val, x, n, r, acc);
-    else if (mask == 3)
-      sell_spmv_row<3, 8, 3>(S, val, x, n, r, acc);
-    else
-      sell_spmv_row<3>(S, val, x, n, r, acc);
+    switch (mask) {
+      case 1: sell_spmv_row<3, 8, 1>(S, val, x, n, r, acc); break;
+      case 2: sell_spmv_row<3, 8, 2>(S, val, x, n, r, acc); break;
+      case 4: sell_spmv_row<3, 8, 4>(S, val, x, n, r, acc); break;
+      case 3: sell_spmv_row<3, 8, 3>(S, val, x, n, r, acc); break;
+      case 5: sell_spmv_row<3, 8, 5>(S, val, x, n, r, acc); break;
+      case 6: sell_spmv_row<3, 8, 6>(S, val, x, n, r, acc); break;
+      default: sell_spmv_row<3>(S, val, x, n, r, acc); break;
+    }
   } else {
     sell_spmv_row<NC>(S, val, x, n, r, acc);
   }

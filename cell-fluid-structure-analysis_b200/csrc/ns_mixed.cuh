@@ -1,16 +1,23 @@
-// Mixed-precision momentum solve: FP32 batched BiCGSTAB inside FP64 defect correction.
+// Mixed-precision momentum solve: one batched BiCGSTAB sequence in FP32 with reliable updates
+// of the solution and the residual in FP64 (residual replacement: van der Vorst & Ye, SIAM J. Sci.
+// Comput. 22(5), 2000; group-wise solution updates: Sleijpen & van der Vorst, Computing 56, 1996;
+// their mixed-precision GPU form: Clark et al., Comput. Phys. Commun. 181, 2010).
 //
-//   x = 0, r = b                                       (FP64, from k_momentum_rhs)
-//   repeat (outer sweep) while some component has ||r||^2 > tol^2 ||b||^2:
-//     solve At d = r approximately in FP32            (inner: FP32 operator values and vectors,
-//                                                      FP64 dot products and scalars, stop at
-//                                                      ||r_in|| <= tol_in ||r||, a cap or near-breakdown)
-//     x += D^-1 d                                     (FP64)
-//     r = b - A x                                     (FP64 operator, true residual)
-// At = A D^-1 is the right-Jacobi-scaled momentum operator (At32 is its FP32 copy); the penalty
-// rows (diagonal 1e10) have unit diagonal in At, so FP32 holds them without overflow or loss.
-// The convergence test is on the true FP64 residual, so the result meets the same tolerance as
-// the FP64 solve. Components are independent (per-component scalars and masks).
+//   FP64: b, x (solution), r64 (true residual), xs = diag(A) x
+//   FP32: r, r0, p, v, s, t (Krylov vectors), dx (correction accumulated since the last update)
+//   every iteration (FP32 operator At32 = FP32 copy of A D^-1, FP64 dot products and scalars):
+//     p = r + beta (p - omega v); v = At32 p; alpha = rho / (r0.v); s = r - alpha v;
+//     t = At32 s; omega = (t.s) / (t.t); dx += alpha D^-1 p + omega D^-1 s; r = s - omega t
+//   reliable update of component c when its iterated residual has dropped below delta times the
+//   largest one since its last update, meets the tolerance, hits the iteration cap or nears a
+//   breakdown:  x += dx; dx = 0; r64 = b - A x (FP64 operator); r = (float) r64
+// The Krylov space is kept across updates (p, r0 and the scalars carry on), so the iteration
+// count stays that of the FP64 solve instead of restarting with every correction. Convergence is
+// decided on the FP64 true residual only, with the FP64 solve's criterion. In a CUDA graph the
+// update is a conditional IF node inside the iteration's WHILE body, so iterations without an
+// update launch nothing extra. The penalty rows (diagonal 1e10) have unit diagonal in A D^-1, so
+// FP32 holds them without overflow or loss. Components are independent (per-component scalars,
+// masks and updates).
 #pragma once
 
 #include "ns_kernels.cuh"
@@ -18,17 +25,16 @@
 namespace cfsa {
 
 struct MixedState {
-  // outer (FP64)
-  double bnorm2[3], tol2[3], rnorm2[3];
-  int outer[3], status[3];
-  int active;  // components still sweeping
-  int max_outer;
-  // inner (FP32 vectors, FP64 scalars)
-  double rho[3], alpha[3], omega[3], beta[3], r0norm2[3], tol_in2[3], rin2[3];
-  int iters[3], total_iters[3];
-  int in_active;  // components iterating in the current sweep
-  int in_maxit;
-  double tol_in;
+  double bnorm2[3], tol2[3], rnorm2[3];  // FP64 criterion; rnorm2: true residual at the last update
+  double rho[3], alpha[3], omega[3], beta[3], r0norm2[3];
+  double rin2[3];   // iterated FP32 residual, same norm
+  double rmax2[3];  // largest iterated residual since the last update
+  int iters[3], status[3], updates[3];
+  int active;   // components iterating
+  int upd;      // components updated at the end of this iteration
+  int restart;  // components whose Krylov space restarts at that update (near-breakdown)
+  int maxit;
+  double delta2;  // update trigger: rin2 < delta2 * rmax2
 };
 
 struct MixedArgs {
@@ -37,16 +43,17 @@ struct MixedArgs {
   const double *At64, *diagA, *invA;
   const float *invA32;
   const double *b;
-  double *x, *r64, *xs;  // FP64 solution, residual, scaled solution D x
+  double *x, *r64, *xs;  // FP64 solution, true residual, scaled solution D x
   float *r, *r0, *p, *v, *s, *t, *dx;
   int n;
   MixedState *ms;
   DevStatus *st;
   Reduce red;
-  cudaGraphConditionalHandle cond;
+  cudaGraphConditionalHandle cond;      // WHILE node of the iteration
+  cudaGraphConditionalHandle cond_upd;  // IF node of the reliable update
   int use_cond;
   const double *cw;   // convergence-norm weights (diag(A)^-1), nullptr: unscaled ||r||
-  const float *cw32;  // the same for the inner solve
+  const float *cw32;  // the same for the FP32 residual
 };
 
 template <int U = 8, int MASK = 7>
@@ -91,46 +98,67 @@ __device__ __forceinline__ void sell_spmv_row_f32x3(const SellView &S, const flo
 __device__ __forceinline__ void sell_spmv_row_f32x3_active(const SellView &S, const float *__restrict__ val,
                                                            const float *__restrict__ x, int64_t n, int r,
                                                            float acc[3], int mask) {
-  if (mask == 6)
-    sell_spmv_row_f32x3<8, 6>(S, val, x, n, r, acc);
-  else if (mask == 5)
-    sell_spmv_row_f32x3<8, 5>(S, val, x, n, r, acc);
-  else if (mask == 3)
-    sell_spmv_row_f32x3<8, 3>(S, val, x, n, r, acc);
-  else
-    sell_spmv_row_f32x3(S, val, x, n, r, acc);
+  switch (mask) {
+    case 1: sell_spmv_row_f32x3<8, 1>(S, val, x, n, r, acc); break;
+    case 2: sell_spmv_row_f32x3<8, 2>(S, val, x, n, r, acc); break;
+    case 4: sell_spmv_row_f32x3<8, 4>(S, val, x, n, r, acc); break;
+    case 3: sell_spmv_row_f32x3<8, 3>(S, val, x, n, r, acc); break;
+    case 5: sell_spmv_row_f32x3<8, 5>(S, val, x, n, r, acc); break;
+    case 6: sell_spmv_row_f32x3<8, 6>(S, val, x, n, r, acc); break;
+    default: sell_spmv_row_f32x3(S, val, x, n, r, acc); break;
+  }
 }
 
-// Outer init (after k_momentum_rhs wrote b and x = 0): r64 = b, ||b||^2 per component.
-__global__ void k_mp_outer_init(MixedArgs A, double tol, int max_outer, double tol_in, int in_maxit) {
+// Init (after k_momentum_rhs wrote b and x = 0): r = r0 = (float) b, p = v = dx = 0;
+// FP64 ||b|| in the convergence norm, rho = r0 . r.
+__global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta) {
   if (A.st->halt) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n = A.n;
-  double part[3] = {0.0, 0.0, 0.0};
-  if (i < A.n) {
-    const double w = A.cw ? A.cw[i] : 1.0;
+  __shared__ WarpSums<6> S;
+  const int nblk = (A.n + kBlock - 1) / kBlock;
+  int slot = 0;
+  for (int bk = blockIdx.x; bk < nblk; bk += gridDim.x, ++slot) {
+    const int i = bk * kBlock + threadIdx.x;
+    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (i < A.n) {
+      const double w = A.cw ? A.cw[i] : 1.0;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const double bi = A.b[c * n + i];
-      A.r64[c * n + i] = bi;
-      part[c] = (bi * bi) * w;
+      for (int c = 0; c < 3; ++c) {
+        const int64_t o = c * n + i;
+        const double bi = A.b[o];
+        const float ri = (float)bi;
+        A.r[o] = ri;
+        A.r0[o] = ri;
+        A.p[o] = 0.f;
+        A.v[o] = 0.f;
+        A.dx[o] = 0.f;
+        part[c] = (bi * bi) * w;
+        part[3 + c] = (double)ri * (double)ri;
+      }
     }
+    warp_partial<6>(part, S, slot);
   }
-  double tot[3];
-  if (grid_reduce<3>(part, A.red, tot) && threadIdx.x == 0) {
+  double tot[6];
+  if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     MixedState *m = A.ms;
     m->active = 0;
-    m->max_outer = max_outer;
-    m->tol_in = tol_in;
-    m->in_maxit = in_maxit;
+    m->upd = 0;
+    m->restart = 0;
+    m->maxit = maxit;
+    m->delta2 = delta * delta;
     for (int c = 0; c < 3; ++c) {
       m->bnorm2[c] = tot[c];
       m->rnorm2[c] = tot[c];
+      m->rin2[c] = tot[c];
+      m->rmax2[c] = tot[c];
       m->tol2[c] = tol * tol * tot[c];
-      m->outer[c] = 0;
-      m->total_iters[c] = 0;
+      m->rho[c] = tot[3 + c];
+      m->r0norm2[c] = tot[3 + c];
+      m->alpha[c] = m->omega[c] = 1.0;
+      m->beta[c] = 0.0;
       m->iters[c] = 0;
-      if (isnan(tot[c])) {
+      m->updates[c] = 0;
+      if (isnan(tot[c]) || isnan(tot[3 + c])) {
         m->status[c] = KS_BREAKDOWN;
       } else if (tot[c] == 0.0 || tot[c] <= m->tol2[c]) {
         m->status[c] = KS_CONVERGED;
@@ -142,65 +170,9 @@ __global__ void k_mp_outer_init(MixedArgs A, double tol, int max_outer, double t
   }
 }
 
-// Inner init: r = r0 = (float) r64, p = v = dx = 0; rho = ||r||^2. When captured it also sets
-// the inner loop's condition (a nested loop is not re-armed by its handle's default value).
-__global__ void k_mp_inner_init(MixedArgs A) {
-  const int active = A.ms->active;
-  if (!active) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      A.ms->in_active = 0;
-      if (A.use_cond) cudaGraphSetConditional(A.cond, 0);
-    }
-    return;
-  }
-  const int64_t n = A.n;
-  __shared__ WarpSums<6> S;
-  const int nblk = (A.n + kBlock - 1) / kBlock;
-  int slot = 0;
-  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
-    const int i = b * kBlock + threadIdx.x;
-    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (i < A.n) {
-      const double w = A.cw32 ? (double)A.cw32[i] : 1.0;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const int64_t o = c * n + i;
-        const float ri = (float)A.r64[o];
-        A.r[o] = ri;
-        A.r0[o] = ri;
-        A.p[o] = 0.f;
-        A.v[o] = 0.f;
-        A.dx[o] = 0.f;
-        if ((active >> c) & 1) {
-          part[c] = (double)ri * (double)ri;
-          part[3 + c] = ((double)ri * (double)ri) * w;
-        }
-      }
-    }
-    warp_partial<6>(part, S, slot);
-  }
-  double tot[6];
-  if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
-    MixedState *m = A.ms;
-    m->in_active = 0;
-    for (int c = 0; c < 3; ++c) {
-      m->iters[c] = 0;
-      if (!((active >> c) & 1)) continue;
-      m->rho[c] = tot[c];
-      m->r0norm2[c] = tot[c];
-      m->rin2[c] = tot[3 + c];
-      m->tol_in2[c] = m->tol_in * m->tol_in * tot[3 + c];
-      m->alpha[c] = m->omega[c] = 1.0;
-      m->beta[c] = 0.0;
-      if (tot[c] > 0.0 && !isnan(tot[c])) m->in_active |= 1 << c;
-    }
-    if (A.use_cond) cudaGraphSetConditional(A.cond, m->in_active ? 1u : 0u);
-  }
-}
-
-// K1: p = r + beta (p - omega v)
+// K1: p = r + beta (p - omega v)  (beta = 0 after a restart: p = r)
 __global__ void k_mp_p(MixedArgs A) {
-  const int act = A.ms->in_active;
+  const int act = A.ms->active;
   if (!act) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
@@ -216,7 +188,7 @@ __global__ void k_mp_p(MixedArgs A) {
 
 // K2: v = At32 p, alpha = rho / (r0 . v)
 __global__ void __launch_bounds__(kRunThreads, 1) k_mp_v(MixedArgs A) {
-  const int act = A.ms->in_active;
+  const int act = A.ms->active;
   if (!act) return;
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
@@ -240,17 +212,19 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_v(MixedArgs A) {
   if (grid_reduce_runs<3>(A.S, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < 3; ++c) {
       if (!((act >> c) & 1)) continue;
-      if (tot[c] == 0.0 || isnan(tot[c]))
-        A.ms->in_active &= ~(1 << c);  // sweep ends; the outer residual restarts it
-      else
+      if (tot[c] == 0.0 || isnan(tot[c])) {
+        A.ms->status[c] = KS_BREAKDOWN;
+        A.ms->active &= ~(1 << c);
+      } else {
         A.ms->alpha[c] = A.ms->rho[c] / tot[c];
+      }
     }
   }
 }
 
 // K3: s = r - alpha v
 __global__ void k_mp_s(MixedArgs A) {
-  const int act = A.ms->in_active;
+  const int act = A.ms->active;
   if (!act) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
@@ -265,7 +239,7 @@ __global__ void k_mp_s(MixedArgs A) {
 
 // K4: t = At32 s, omega = (t . s) / (t . t)
 __global__ void __launch_bounds__(kRunThreads, 1) k_mp_t(MixedArgs A) {
-  const int act = A.ms->in_active;
+  const int act = A.ms->active;
   if (!act) return;
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
@@ -295,20 +269,24 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_t(MixedArgs A) {
   }
 }
 
-// K5: dx += alpha D^-1 p + omega D^-1 s, r = s - omega t; inner convergence, next beta.
+// K5: dx += alpha D^-1 p + omega D^-1 s, r = s - omega t; ||r||, r0 . r; which components take a
+// reliable update at the end of this iteration (IF node), next beta for the others.
 __global__ void k_mp_xr(MixedArgs A) {
-  const int act = A.ms->in_active;
+  const int act = A.ms->active;
   if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[0] += 1;
   if (!act) {
-    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0);
+    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) {
+      cudaGraphSetConditional(A.cond_upd, 0);
+      cudaGraphSetConditional(A.cond, 0);
+    }
     return;
   }
   const int64_t n = A.n;
   __shared__ WarpSums<6> S;
   const int nblk = (A.n + kBlock - 1) / kBlock;
   int slot = 0;
-  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
-    const int i = b * kBlock + threadIdx.x;
+  for (int bk = blockIdx.x; bk < nblk; bk += gridDim.x, ++slot) {
+    const int i = bk * kBlock + threadIdx.x;
     double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (i < A.n) {
       const float dinv = A.invA32[i];
@@ -331,90 +309,126 @@ __global__ void k_mp_xr(MixedArgs A) {
   if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     MixedState *m = A.ms;
     const double eps = 2.220446049250313e-16;
+    int upd = 0, rst = 0;
     for (int c = 0; c < 3; ++c) {
       if (!((act >> c) & 1)) continue;
       m->iters[c] += 1;
-      m->total_iters[c] += 1;
       m->rin2[c] = tot[c];
       const double rho_new = tot[3 + c];
-      if (isnan(tot[c]) || tot[c] <= m->tol_in2[c] || m->iters[c] >= m->in_maxit || m->omega[c] == 0.0 ||
-          fabs(rho_new) < eps * eps * m->r0norm2[c]) {
-        m->in_active &= ~(1 << c);
+      if (isnan(tot[c]) || isnan(rho_new)) {
+        m->status[c] = KS_BREAKDOWN;
+        m->active &= ~(1 << c);
+        continue;
+      }
+      const bool near_breakdown = fabs(rho_new) < eps * eps * m->r0norm2[c];
+      if (tot[c] <= m->tol2[c] || m->iters[c] >= m->maxit || tot[c] < m->delta2 * m->rmax2[c] ||
+          m->omega[c] == 0.0 || near_breakdown) {
+        upd |= 1 << c;
+        if (near_breakdown) rst |= 1 << c;
       } else {
         m->beta[c] = (rho_new / m->rho[c]) * (m->alpha[c] / m->omega[c]);
         m->rho[c] = rho_new;
+        m->rmax2[c] = fmax(m->rmax2[c], tot[c]);
       }
     }
-    if (A.use_cond) cudaGraphSetConditional(A.cond, m->in_active ? 1u : 0u);
+    m->upd = upd;
+    m->restart = rst;
+    if (A.use_cond) {
+      cudaGraphSetConditional(A.cond_upd, upd ? 1u : 0u);
+      cudaGraphSetConditional(A.cond, m->active ? 1u : 0u);
+    }
   }
 }
 
-// x += D^-1-scaled correction (FP64); xs = diag(A) x for the residual product.
+// Reliable update, part 1: x += dx (FP64), dx = 0, xs = diag(A) x for the updated components.
 __global__ void k_mp_xupdate(MixedArgs A) {
-  const int active = A.ms->active;
-  if (!active) return;
+  const int upd = A.ms->upd;
+  if (!upd) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const int64_t n = A.n;
   const double d = A.diagA[i];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
+    if (!((upd >> c) & 1)) continue;
     const int64_t o = c * n + i;
-    double xi = A.x[o];
-    if ((active >> c) & 1) {
-      xi += (double)A.dx[o];
-      A.x[o] = xi;
-    }
+    const double xi = A.x[o] + (double)A.dx[o];
+    A.x[o] = xi;
+    A.dx[o] = 0.f;
     A.xs[o] = d * xi;
   }
 }
 
-// r64 = b - At64 (D x) (FP64 true residual); outer convergence and loop condition.
+// Reliable update, part 2: r64 = b - At64 (D x) (FP64 true residual), r = (float) r64 (and r0 = r
+// for a restart); convergence on the true residual, next beta from the replaced residual.
 __global__ void __launch_bounds__(kRunThreads, 1) k_mp_residual(MixedArgs A) {
-  const int active = A.ms->active;
+  const int upd = A.ms->upd;
+  if (!upd) return;
+  const int rst = A.ms->restart;
   if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[2] += 1;
-  if (!active) {
-    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0);
-    return;
-  }
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
   for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
     const int r = sl * kSellC + (threadIdx.x & 31);
     const int i = A.S.perm[r];
-    double part[3] = {0.0, 0.0, 0.0};
+    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (i >= 0) {
       double acc[3];
-      sell_spmv_row_active<3>(A.S, A.At64, A.xs, n, r, acc, active);
+      sell_spmv_row_active<3>(A.S, A.At64, A.xs, n, r, acc, upd);
       const double w = A.cw ? A.cw[i] : 1.0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        if (!((active >> c) & 1)) continue;
-        const double ri = A.b[c * n + i] - acc[c];
-        A.r64[c * n + i] = ri;
+        if (!((upd >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        const double ri = A.b[o] - acc[c];
+        A.r64[o] = ri;
+        const float rf = (float)ri;
+        A.r[o] = rf;
+        float r0 = A.r0[o];
+        if ((rst >> c) & 1) {
+          r0 = rf;
+          A.r0[o] = rf;
+        }
         part[c] = (ri * ri) * w;
+        part[3 + c] = (double)r0 * (double)rf;
       }
     }
-    slice_partial<3>(part, A.S, sl);
+    slice_partial<6>(part, A.S, sl);
   }
-  double tot[3];
-  if (grid_reduce_runs<3>(A.S, A.red, tot) && threadIdx.x == 0) {
+  double tot[6];
+  if (grid_reduce_runs<6>(A.S, A.red, tot) && threadIdx.x == 0) {
     MixedState *m = A.ms;
     for (int c = 0; c < 3; ++c) {
-      if (!((active >> c) & 1)) continue;
-      m->outer[c] += 1;
+      if (!((upd >> c) & 1)) continue;
+      m->updates[c] += 1;
       m->rnorm2[c] = tot[c];
-      if (isnan(tot[c])) {
+      const double rho_new = tot[3 + c];
+      if (isnan(tot[c]) || isnan(rho_new)) {
         m->status[c] = KS_BREAKDOWN;
         m->active &= ~(1 << c);
       } else if (tot[c] <= m->tol2[c]) {
         m->status[c] = KS_CONVERGED;
         m->active &= ~(1 << c);
-      } else if (m->outer[c] >= m->max_outer) {
+      } else if (m->iters[c] >= m->maxit) {
         m->status[c] = KS_MAXIT;
         m->active &= ~(1 << c);
+      } else if (m->omega[c] == 0.0) {
+        m->status[c] = KS_BREAKDOWN;
+        m->active &= ~(1 << c);
+      } else {
+        if ((rst >> c) & 1) {
+          m->r0norm2[c] = rho_new;
+          m->beta[c] = 0.0;
+        } else {
+          m->beta[c] = (rho_new / m->rho[c]) * (m->alpha[c] / m->omega[c]);
+        }
+        m->rho[c] = rho_new;
+        m->rin2[c] = tot[c];
+        m->rmax2[c] = tot[c];
       }
     }
+    m->upd = 0;
+    m->restart = 0;
     if (A.use_cond) cudaGraphSetConditional(A.cond, m->active ? 1u : 0u);
   }
 }
@@ -423,7 +437,7 @@ __global__ void k_mp_check(const MixedState *__restrict__ m, DevStatus *st) {
   if (st->halt) return;
   int code = 0, it = 0;
   for (int c = 0; c < 3; ++c) {
-    it = max(it, m->total_iters[c]);
+    it = max(it, m->iters[c]);
     if (m->status[c] == KS_MAXIT && code == 0) code = 1;
     if (m->status[c] == KS_BREAKDOWN && code == 0) code = 2;
   }

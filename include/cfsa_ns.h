@@ -60,7 +60,9 @@ extern "C" {
 
 /* arithmetic of the Krylov solves */
 #define CFSA_PRECISION_FP64 0
-#define CFSA_PRECISION_MIXED 1 /* FP32 inner Krylov inside FP64 defect correction */
+/* FP32 operator and Krylov vectors; FP64 solution, true residual (reliable updates), dot
+ * products and scalars; convergence decided on the FP64 true residual */
+#define CFSA_PRECISION_MIXED 1
 
 /* Krylov convergence norm. REFERENCE: ||r|| <= tol ||b|| (NavierStokes.cpp:500,635). With the
  * 1e10 / 1e12 penalty rows in b this norm is dominated by the Dirichlet rows, so it constrains the
@@ -106,7 +108,7 @@ typedef struct {
   int32_t pressure_iters;     /* last corrector solve */
   double momentum_residual[3];/* ||r||/||b|| at exit */
   double pressure_residual;
-  int32_t momentum_outer[3];  /* defect-correction sweeps (mixed precision), else 0 */
+  int32_t momentum_outer[3];  /* FP64 reliable updates of x and r (mixed precision), else 0 */
   int32_t pressure_outer;
   int64_t steps;              /* PISO/SIMPLE steps taken since create */
   double time;                /* simulated time */
@@ -121,6 +123,10 @@ typedef struct {
 /* kernel ids for cfsa_ns_profile_kernel */
 #define CFSA_KERNEL_MOMENTUM_SPMV 0 /* 3-right-hand-side SELL product of the momentum BiCGSTAB */
 #define CFSA_KERNEL_PRESSURE_SPMV 1 /* SELL product of the pressure CG */
+/* the whole resident pressure solve (CFSA_KRYLOV_CG2L or _CG1) on the last step's system, fused
+ * product and vector updates inside one kernel: avg_ms per solve, alg_bytes = iterations x bytes
+ * per iteration (operator, row metadata, each vector read or written once, coarse inverse) */
+#define CFSA_KERNEL_PRESSURE_SOLVE 2
 
 /* NavierStokesSolver::initialize (include/FEM/NavierStokes.hpp:91-92; NavierStokes.cpp:10-68):
  * uploads the mesh, builds the CSR patterns, assembles M, K, G, L on the device and zeroes the

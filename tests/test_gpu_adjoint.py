@@ -197,7 +197,7 @@ def test_recording_invalidated_by_changes(cf, small):
 
 
 def test_mixed_precision_adjoint(cf, small):
-    """FP32-inner / FP64-defect-correction solves in forward and adjoint: gradients within 1e-6 of
+    """FP32 BiCGSTAB with FP64 reliable updates in forward and adjoint: gradients within 1e-6 of
     the FP64 adjoint (both to 1e-13 in the Jacobi-scaled norm)."""
     m, prof = small
     out = []

@@ -1,4 +1,4 @@
-"""Mixed precision (FP32 inner BiCGSTAB in FP64 defect correction) against the FP64 GPU path.
+"""Mixed precision (FP32 BiCGSTAB with FP64 reliable updates) against the FP64 GPU path.
 
 The momentum right-hand side is dominated by the 1e10 penalty rows, so the reference's criterion
 ||r|| <= tol ||b|| leaves the interior loosely determined at tol = 1e-10: FP64 solves at 1e-10
@@ -39,7 +39,7 @@ def test_mixed_matches_converged_fp64(cf, po, rings, layers):
     for k in (0, 4, 9):
         eu, ep = rel_l2(mix[k][0], ref[k][0]), rel_l2(mix[k][1], ref[k][1])
         print(f"step {k + 1}: mixed(1e-12) vs fp64(1e-14) rel L2 u {eu:.2e} p {ep:.2e}; "
-              f"inner iters {mix[k][2]['momentum_iters']} sweeps {mix[k][2]['momentum_outer']}")
+              f"iters {mix[k][2]['momentum_iters']} updates {mix[k][2]['momentum_outer']}")
         assert eu <= 1e-6 and ep <= 1e-6, (k, eu, ep)
     for _, _, st in mix:
         assert max(st["momentum_residual"]) <= 1e-12  # true FP64 residual
@@ -73,8 +73,9 @@ def test_mixed_graph_and_eager_identical(cf, po):
 
 
 def test_mixed_reports_non_convergence(cf, po):
-    """A tolerance below the FP64 residual floor cannot be met: the sweep cap ends the solve and
-    pisoStep returns false without advancing time."""
+    """A tolerance below the FP64 residual floor cannot be met: the iteration cap ends the solve
+    (the last reliable update finds the true residual above the tolerance) and pisoStep returns
+    false without advancing time."""
     m = make_mesh(cf, 2, 6)
     s, _ = make_pair(cf, po, m, tol=1e-20)
     s.setPrecision(cf.PRECISION_MIXED)
@@ -95,5 +96,5 @@ def test_jacobi_norm_makes_1e10_meaningful(cf, po):
         emx = (rel_l2(mix[k][0], ref[k][0]), rel_l2(mix[k][1], ref[k][1]))
         print(f"jacobi norm step {k + 1}: fp64(1e-10) u {e64[0]:.2e} p {e64[1]:.2e}; "
               f"mixed(1e-10) u {emx[0]:.2e} p {emx[1]:.2e}; iters fp64 {f64[k][2]['momentum_iters']} "
-              f"mixed {mix[k][2]['momentum_iters']} sweeps {mix[k][2]['momentum_outer']}")
+              f"mixed {mix[k][2]['momentum_iters']} updates {mix[k][2]['momentum_outer']}")
         assert max(emx) <= 1e-6, (k, emx)
