@@ -191,6 +191,14 @@ struct cfsa_ns {
         *fdx = nullptr;  // [3][N2]
   MixedState *ms = nullptr;
   MixedState *h_ms = nullptr;
+  // mixed-precision pressure (two-level CG in float storage inside FP64 defect correction)
+  float *Ls32 = nullptr, *invL32 = nullptr, *px32 = nullptr, *pp32 = nullptr;
+  float *pr32[2] = {nullptr, nullptr}, *pw32[2] = {nullptr, nullptr}, *ps32[2] = {nullptr, nullptr};
+  CgState *cs_in = nullptr;
+  PMixState *pmx = nullptr;
+  PMixState *h_pmx = nullptr;
+  double mixed_p_tol_in = 1e-5;  // inner reduction per sweep
+  int mixed_p_max_sweeps = 30;
   // reliable-update trigger of the mixed-precision BiCGSTAB: the FP64 residual replaces the FP32
   // one when the latter has dropped by this factor since the previous update
   double mixed_delta = 1e-3;
@@ -254,6 +262,7 @@ struct cfsa_ns {
     if (h_cs) cudaFreeHost(h_cs);
     if (h_stage) cudaFreeHost(h_stage);
     if (h_ms) cudaFreeHost(h_ms);
+    if (h_pmx) cudaFreeHost(h_pmx);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     for (cudaEvent_t e : ph)
@@ -481,6 +490,16 @@ struct cfsa_ns {
     for (float **w : {&fr, &fr0, &fp, &fv, &fs, &ft, &fdx}) *w = dalloc<float>(n3);
     ms = dalloc<MixedState>(1);
     CK(cudaMemsetAsync(ms, 0, sizeof(MixedState), stream));
+    Ls32 = dalloc<float>((size_t)s1.nentries);
+    CK(cudaMemsetAsync(Ls32, 0, (size_t)s1.nentries * sizeof(float), stream));
+    for (float **w : {&invL32, &px32, &pp32, &pr32[0], &pr32[1], &pw32[0], &pw32[1], &ps32[0], &ps32[1]})
+      *w = dalloc<float>((size_t)nv);
+    cs_in = dalloc<CgState>(1);
+    pmx = dalloc<PMixState>(1);
+    CK(cudaMemsetAsync(cs_in, 0, sizeof(CgState), stream));
+    CK(cudaMemsetAsync(pmx, 0, sizeof(PMixState), stream));
+    CK(cudaMallocHost(&h_pmx, sizeof(PMixState)));
+    if (const char *e = std::getenv("CFSA_MIXED_P_TOL_IN")) mixed_p_tol_in = std::atof(e);
     if (const char *e = std::getenv("CFSA_MIXED_DELTA")) mixed_delta = std::atof(e);
     bs_prof = dalloc<BicgState>(1);
     cs_prof = dalloc<CgState>(1);
@@ -535,6 +554,7 @@ struct cfsa_ns {
         q((const void *)k_bicg_xr<1>);
         q((const void *)k_mp_xr);
         q((const void *)k_mp_init);
+        q((const void *)k_pmx_prep);
       }
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent, kBlock, 0));
       const int nblk_sell = (int)blocks_for(s1.nrows_pad), nblk_nat = (int)blocks_for(nv);
@@ -623,6 +643,8 @@ struct cfsa_ns {
                                                             bc, diagL, invL);
       k_poisson_sell<<<blocks_for(nnz1), kBlock, 0, stream>>>(nnz1, outlet_type, ref_node, s1.posmap,
                                                               rows1, ci1, Lv, bc, invL, Ls, Lt);
+      k_to_f32<<<blocks_for(s1.nentries), kBlock, 0, stream>>>(s1.nentries, Ls, Ls32);
+      k_to_f32<<<blocks_for(nv), kBlock, 0, stream>>>(nv, invL, invL32);
       CK(cudaGetLastError());
       poisson_dirty = false;
       coarse_dirty = true;
@@ -841,7 +863,7 @@ struct cfsa_ns {
     int optin = 0;
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     cudaFuncAttributes fa{};
-    CK(cudaFuncGetAttributes(&fa, k_cg2l_resident));
+    CK(cudaFuncGetAttributes(&fa, k_cg2l_resident<double>));
     const int64_t coarse_bytes = (int64_t)(6 * nc + 2 + 2 * npos_max) * (int64_t)sizeof(double);
     const int64_t row_bytes = (int64_t)3 * cg_res_bpc_sell * kBlock * (int64_t)sizeof(int);
     const int64_t avail = (int64_t)optin - (int64_t)fa.sharedSizeBytes - coarse_bytes - row_bytes;
@@ -853,9 +875,17 @@ struct cfsa_ns {
     }
     cg2l_col_cap = (int)std::min<int64_t>(max_entries, avail / (int64_t)sizeof(int));
     cg2l_smem = (size_t)(coarse_bytes + row_bytes + (int64_t)cg2l_col_cap * (int64_t)sizeof(int));
-    CK(cudaFuncSetAttribute(k_cg2l_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cg2l_smem));
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg2l_resident, kCgResThreads, cg2l_smem));
+    int per_sm = 1;
+    for (const void *fn : {(const void *)k_cg2l_resident<double>, (const void *)k_cg2l_resident<float>}) {
+      cudaFuncAttributes fb{};
+      CK(cudaFuncGetAttributes(&fb, fn));
+      if (fb.sharedSizeBytes > fa.sharedSizeBytes)
+        throw CudaError{"two-level pressure preconditioner: float form needs more static shared memory"};
+      CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cg2l_smem));
+      int o = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, kCgResThreads, cg2l_smem));
+      per_sm = std::min(per_sm, o);
+    }
     if (per_sm < 1) throw CudaError{"two-level pressure preconditioner: kernel does not fit on an SM"};
     CK(cudaStreamSynchronize(stream));
     coarse_view = V;
@@ -1158,9 +1188,138 @@ struct cfsa_ns {
     return a;
   }
 
+  // Arguments of the resident two-level CG (FP64 form into x; the float form's vectors are the
+  // handle's FP32 pressure buffers).
+  Cg2lArgs cg2l_args(double *x, DevStatus *s_out, CgState *state) {
+    CgPersistentArgs c{};
+    c.S = s1.view();
+    c.Ls = Ls;
+    c.invL = invL;
+    c.x = x;
+    c.r = pr;
+    c.z = pz;
+    c.q = pq;
+    c.p[0] = pp;
+    c.p[1] = ps;
+    c.n = (int)nv;
+    c.nblk_sell = (int)blocks_for(s1.nrows_pad);
+    c.nblk_nat = (int)blocks_for(nv);
+    c.part_a = cg_part_a;
+    c.part_b = cg_part_b;
+    c.cs = state;
+    c.st = s_out;
+    c.bar = GridBarrier{bar_count, bar_gen, bar_err, bar_spin_limit};
+    c.scaled = (conv_norm == CFSA_NORM_JACOBI) ? 1 : 0;
+    CgResidentArgs rz{};
+    rz.P = c;
+    rz.nslices = s1.nslices;
+    rz.bpc_sell = cg_res_bpc_sell;
+    rz.bpc_nat = cg_res_bpc_nat;
+    rz.col_cap = cg2l_col_cap;
+    Cg2lArgs c2{};
+    c2.R = rz;
+    c2.V = coarse_view;
+    c2.r[0] = pr;
+    c2.r[1] = cg1_vec[0];
+    c2.w[0] = pq;
+    c2.w[1] = cg1_vec[1];
+    c2.s[0] = ps;
+    c2.s[1] = cg1_vec[2];
+    c2.p = pp;
+    c2.Ls32 = Ls32;
+    c2.invL32 = invL32;
+    c2.x32 = px32;
+    c2.p32 = pp32;
+    for (int q = 0; q < 2; ++q) {
+      c2.r32[q] = pr32[q];
+      c2.w32[q] = pw32[q];
+      c2.s32[q] = ps32[q];
+    }
+    return c2;
+  }
+
+  // One cooperative launch of the two-level CG on `s` (barrier words and coarse accumulators
+  // cleared first; the caller zeroes p and s[0] of the form it launches).
+  void launch_cg2l(const Cg2lArgs &c2, bool f32, cudaStream_t s) {
+    CK(cudaMemsetAsync(bar_count, 0, (1 + kBarrierGroups) * sizeof(unsigned int), s));
+    CK(cudaMemsetAsync(bar_err, 0, sizeof(int), s));
+    if (coarse_view.nc > 0)
+      CK(cudaMemsetAsync(coarse_view.gacc, 0, (size_t)18 * coarse_view.nc * sizeof(unsigned long long), s));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned int)cg_res_grid);
+    cfg.blockDim = dim3(kCgResThreads);
+    cfg.dynamicSmemBytes = cg2l_smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (f32)
+      CK(cudaLaunchKernelEx(&cfg, k_cg2l_resident<float>, c2));
+    else
+      CK(cudaLaunchKernelEx(&cfg, k_cg2l_resident<double>, c2));
+  }
+
+  // Mixed-precision pressure solve (ns_mixed.cuh): FP64 defect correction around the float
+  // two-level CG; the sweeps are a WHILE node when captured.
+  void enqueue_pressure_mixed(bool capture, double *x, DevStatus *s_out) {
+    PMixArgs a{};
+    a.S = s1.view();
+    a.Ls = Ls;
+    a.invL = invL;
+    a.invL32 = invL32;
+    a.b = pb;
+    a.x = x;
+    a.r = pr;
+    a.r32 = pr32[0];
+    a.x32 = px32;
+    a.p32 = pp32;
+    a.s32 = ps32[0];
+    a.n = (int)nv;
+    a.scaled = (conv_norm == CFSA_NORM_JACOBI) ? 1 : 0;
+    a.maxit = maxit_p;
+    a.cs = cs;
+    a.cs_in = cs_in;
+    a.pm = pmx;
+    a.st = s_out;
+    a.red = red;
+    a.bar_err = bar_err;
+    k_pmx_init<<<1, 1, 0, stream>>>(a, mixed_p_tol_in, mixed_p_max_sweeps);
+    CK(cudaGetLastError());
+    const Cg2lArgs c2 = cg2l_args(x, s_out, cs_in);
+    const unsigned int gp = blocks_for(nv);
+    auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
+      PMixArgs b = a;
+      b.cond = h;
+      b.use_cond = use;
+      k_pmx_prep<<<strided(k_pmx_prep, gp), kBlock, 0, s>>>(b);
+      launch_cg2l(c2, true, s);
+      k_pmx_xupdate<<<gp, kBlock, 0, s>>>(b);
+      k_pmx_residual<<<blocks_for(s1.nrows_pad), kBlock, 0, s>>>(b);
+    };
+    if (capture)
+      capture_while(body);
+    else
+      eager_while(body, [&] { return poll_pmx(); }, mixed_p_max_sweeps);
+    k_pmx_check<<<1, 1, 0, stream>>>(a, s_out);
+    CK(cudaGetLastError());
+  }
+
+  bool poll_pmx() {
+    CK(cudaMemcpyAsync(h_pmx, pmx, sizeof(PMixState), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    return h_pmx->active != 0;
+  }
+
   // Pressure Krylov solve (state set up by k_pressure_rhs) into x; failures and iteration
-  // counts go to `s_out`.
+  // counts go to `s_out`. Mixed precision applies to the two-level CG (the other methods solve
+  // in FP64 in both precisions).
   void enqueue_pressure_krylov(bool capture, double *x, DevStatus *s_out) {
+    if (precision == CFSA_PRECISION_MIXED && krylov == CFSA_KRYLOV_CG2L) {
+      enqueue_pressure_mixed(capture, x, s_out);
+      return;
+    }
     if (krylov == CFSA_KRYLOV_BICGSTAB) {
       BicgArgs b{};
       b.S = s1.view();
@@ -1224,30 +1383,9 @@ struct cfsa_ns {
       cfg.attrs = attr;
       cfg.numAttrs = 1;
       if (krylov == CFSA_KRYLOV_CG2L) {
-        CgResidentArgs rz{};
-        rz.P = c;
-        rz.nslices = s1.nslices;
-        rz.bpc_sell = cg_res_bpc_sell;
-        rz.bpc_nat = cg_res_bpc_nat;
-        rz.col_cap = cg2l_col_cap;
-        Cg2lArgs c2{};
-        c2.R = rz;
-        c2.V = coarse_view;
-        c2.r[0] = pr;
-        c2.r[1] = cg1_vec[0];
-        c2.w[0] = pq;
-        c2.w[1] = cg1_vec[1];
-        c2.s[0] = ps;
-        c2.s[1] = cg1_vec[2];
-        c2.p = pp;
-        if (coarse_view.nc > 0)
-          CK(cudaMemsetAsync(coarse_view.gacc, 0, (size_t)18 * coarse_view.nc * sizeof(unsigned long long), stream));
         CK(cudaMemsetAsync(pp, 0, (size_t)nv * sizeof(double), stream));
         CK(cudaMemsetAsync(ps, 0, (size_t)nv * sizeof(double), stream));
-        cfg.gridDim = dim3((unsigned int)cg_res_grid);
-        cfg.blockDim = dim3(kCgResThreads);
-        cfg.dynamicSmemBytes = cg2l_smem;
-        CK(cudaLaunchKernelEx(&cfg, k_cg2l_resident, c2));
+        launch_cg2l(cg2l_args(x, s_out, cs), false, stream);
       } else if (krylov == CFSA_KRYLOV_CG1) {
         CgResidentArgs rz{};
         rz.P = c;
@@ -1487,15 +1625,27 @@ struct cfsa_ns {
 
   void reset_status() { CK(cudaMemsetAsync(st, 0, sizeof(DevStatus), stream)); }
 
+  // Kernels of one pressure-solve body run (counted by DevStatus::body_runs[1]) and the extra
+  // fixed kernels of a mixed-precision step, for the launch counts.
+  bool pressure_mixed() const { return precision == CFSA_PRECISION_MIXED && krylov == CFSA_KRYLOV_CG2L; }
+  int pressure_body_kernels() const {
+    if (pressure_mixed()) return 4;  // prep, float two-level CG, x update, FP64 residual
+    if (krylov == CFSA_KRYLOV_BICGSTAB) return 5;
+    return (cg_persistent || krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) ? 1 : 3;
+  }
+  int mixed_fixed_kernels() const {
+    return (precision == CFSA_PRECISION_MIXED ? 1 : 0) + (pressure_mixed() ? 1 : 0);
+  }
+
   int finish_batch(int launched_steps) {
     CK(cudaMemcpyAsync(h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
     CK(cudaEventSynchronize(ev1));
     CK(cudaStreamSynchronize(stream));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
-    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : ((cg_persistent || krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) ? 1 : 3);
+    const int pressure_body = pressure_body_kernels();
     // mixed momentum: 5 kernels per iteration, 2 per reliable update (x update, residual) plus
-    // the init kernel per step
-    batch_launches = (int64_t)launched_steps * (launches_per_step + (precision == CFSA_PRECISION_MIXED ? 1 : 0)) +
+    // the init kernel per step; mixed two-level CG pressure: 4 kernels per sweep plus its init
+    batch_launches = (int64_t)launched_steps * (launches_per_step + mixed_fixed_kernels()) +
                      5 * (int64_t)h_st->body_runs[0] + pressure_body * (int64_t)h_st->body_runs[1] +
                      2 * (int64_t)h_st->body_runs[2];
     batch_iters[0] = (int64_t)h_st->iters[0];
@@ -1953,7 +2103,7 @@ struct cfsa_ns {
     adj_stats.momentum_iters = (int64_t)hs_adj.iters[0];
     adj_stats.pressure_iters = (int64_t)hs_adj.iters[1];
     adj_stats.backward_ms = ms;
-    const int pressure_body = (krylov == CFSA_KRYLOV_BICGSTAB) ? 5 : ((cg_persistent || krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) ? 1 : 3);
+    const int pressure_body = pressure_body_kernels();
     adj_stats.kernel_launches = (int64_t)adj_steps * adj_launches_fixed + 5 * (int64_t)hs_adj.body_runs[0] +
                                 pressure_body * (int64_t)hs_adj.body_runs[1] +
                                 2 * (int64_t)hs_adj.body_runs[2];
@@ -2544,6 +2694,11 @@ int cfsa_ns_get_stats(const cfsa_ns *hc, cfsa_ns_stats *s) {
       s->pressure_iters = h->h_cs->iters;
       const double b2 = h->h_cs->bnorm2;
       s->pressure_residual = b2 > 0 ? std::sqrt(h->h_cs->rnorm2 / b2) : 0.0;
+      if (h->pressure_mixed()) {
+        CK(cudaMemcpyAsync(h->h_pmx, h->pmx, sizeof(PMixState), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        s->pressure_outer = h->h_pmx->sweeps;
+      }
     }
     s->steps = h->steps;
     s->time = h->time;

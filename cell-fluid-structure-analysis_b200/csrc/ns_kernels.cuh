@@ -7,6 +7,8 @@
 // the reference's element loops while needing no atomics.
 #pragma once
 
+#include <type_traits>
+
 #include "ns_common.cuh"
 
 namespace cfsa {
@@ -1789,6 +1791,10 @@ struct Cg2lArgs {
   CoarseView V;
   double *r[2], *w[2], *s[2];  // r[0] = b on entry
   double *p;                   // zero on entry
+  // float storage of the mixed-precision inner solve (k_cg2l_resident<float>): operator values,
+  // inverse diagonal, solution and the same vectors (r32[0] = b, p32 = s32[0] = 0 on entry)
+  const float *Ls32, *invL32;
+  float *x32, *r32[2], *w32[2], *s32[2], *p32;
 };
 
 // floor(x 2^S) as a two's-complement 128-bit integer (lo, hi); x 2^S is clamped to +-2^100 and a
@@ -1902,6 +1908,13 @@ __device__ __forceinline__ void coarse_values(const CoarseView &V, const double 
   }
 }
 
+// TS: storage type of the operator values, inverse diagonal, solution and Krylov vectors. double:
+// the FP64 solve (bit-identical to the oracle's cg2l); float: the inner solve of the mixed-precision
+// pressure solve (half the bytes per entry). Arithmetic, dot products, aggregate sums and scalars
+// are FP64 in both; in the float form each updated vector entry is rounded to float once and the
+// rounded value is the one used in the dot products and aggregate sums, so they describe the
+// stored vectors.
+template <class TS>
 __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) {
   extern __shared__ double s_dbl[];
   __shared__ double s_grp[kCgResGroups][4][kBlock / 32];
@@ -1909,6 +1922,17 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
   const CgResidentArgs &R = C.R;
   const CgPersistentArgs &A = R.P;
   const CoarseView &V = C.V;
+  constexpr bool f32 = std::is_same<TS, float>::value;
+  const TS *Lsv, *invLv;
+  TS *xv, *pv, *rv0, *rv1, *wv0, *wv1, *sv0, *sv1;
+  if constexpr (f32) {
+    Lsv = C.Ls32, invLv = C.invL32, xv = C.x32, pv = C.p32;
+    rv0 = C.r32[0], rv1 = C.r32[1], wv0 = C.w32[0], wv1 = C.w32[1], sv0 = C.s32[0], sv1 = C.s32[1];
+  } else {
+    Lsv = A.Ls, invLv = A.invL, xv = A.x, pv = C.p;
+    rv0 = C.r[0], rv1 = C.r[1], wv0 = C.w[0], wv1 = C.w[1], sv0 = C.s[0], sv1 = C.s[1];
+  }
+  auto rnd = [](double v) { return (double)(TS)v; };  // storage rounding (identity for double)
   if (A.st && A.st->halt) return;
   if (!A.cs->active) return;
   const int g = threadIdx.x / kBlock, lt = threadIdx.x & (kBlock - 1);
@@ -1958,13 +1982,13 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
   double gamma = 0.0, alpha = 0.0, beta = 0.0, rn2 = A.cs->bnorm2;
   int it = 0, status = KS_RUNNING, cur = 0, pc = 0;
   if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[1] += 1;
-  const double *bvec = C.r[0];
+  const TS *bvec = rv0;
   const int v_r[1] = {0}, v_w[1] = {1}, v_rw[2] = {0, 1};
   // start: c0 = Z T(b) (phase 0, buffer 0)
   if (nc > 0) {
     for (int i = b0 * kBlock + (int)threadIdx.x; i < min(n, b1 * kBlock); i += kCgResThreads) {
       const int ps = __ldg(V.row_pos + i);
-      if (ps >= 0) s_stage[ps] = __ldcg(bvec + i);
+      if (ps >= 0) s_stage[ps] = (double)__ldcg(bvec + i);
     }
     __syncthreads();
     seg_sums<1>(V, s_stage, 0, v_r, scale);
@@ -1987,12 +2011,13 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
       for (int k = 0; k < len; ++k) {
         const int pos = base + k * kSellC;
         const int jj = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
-        const double uj = __ldg(A.invL + jj) * __ldcg(bvec + jj) + cc[0][__ldg(V.agg + jj)];
-        acc += __ldg(A.Ls + pos) * uj;
+        const double uj = (double)__ldg(invLv + jj) * (double)__ldcg(bvec + jj) + cc[0][__ldg(V.agg + jj)];
+        acc += (double)__ldg(Lsv + pos) * uj;
       }
-      const double bi = __ldcg(bvec + i);
-      const double ui = __ldg(A.invL + i) * bi + cc[0][__ldg(V.agg + i)];
-      __stcg(C.w[0] + i, acc);
+      acc = rnd(acc);
+      const double bi = (double)__ldcg(bvec + i);
+      const double ui = (double)__ldg(invLv + i) * bi + cc[0][__ldg(V.agg + i)];
+      __stcg(wv0 + i, (TS)acc);
       v[0] = acc * ui;
       v[1] = bi * ui;
       if (nc > 0) {
@@ -2024,8 +2049,8 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
   while (status == KS_RUNNING) {
     double *part = (it & 1) ? A.part_a : A.part_b;
     const int buf = (it + 2) % 3;  // phase it + 2
-    const double *ro = C.r[cur], *wo = C.w[cur], *so = C.s[cur];
-    double *rn = C.r[cur ^ 1], *wn = C.w[cur ^ 1], *sn = C.s[cur ^ 1];
+    const TS *ro = cur ? rv1 : rv0, *wo = cur ? wv1 : wv0, *so = cur ? sv1 : sv0;
+    TS *rn = cur ? rv0 : rv1, *wn = cur ? wv0 : wv1, *sn = cur ? sv0 : sv1;
     // coarse input of the new residual and its coarse values
     if (nc > 0) {
       clear_acc(V, (it + 3) % 3);  // buffer of the next phase; last read before the previous barrier
@@ -2055,14 +2080,14 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
           for (int q = 0; q < kCgChunk; ++q) {
             const int pos = base + (k + q) * kSellC;
             jj[q] = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
-            a[q] = __ldg(A.Ls + pos);
+            a[q] = (double)__ldg(Lsv + pos);
           }
 #pragma unroll
           for (int q = 0; q < kCgChunk; ++q) {
-            rr_[q] = __ldcg(ro + jj[q]);
-            ww[q] = __ldcg(wo + jj[q]);
-            ss[q] = __ldcg(so + jj[q]);
-            mm[q] = __ldg(A.invL + jj[q]);
+            rr_[q] = (double)__ldcg(ro + jj[q]);
+            ww[q] = (double)__ldcg(wo + jj[q]);
+            ss[q] = (double)__ldcg(so + jj[q]);
+            mm[q] = (double)__ldg(invLv + jj[q]);
             aj[q] = __ldg(V.agg + jj[q]);
           }
 #pragma unroll
@@ -2075,25 +2100,26 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
         for (; k < len; ++k) {
           const int pos = base + k * kSellC;
           const int jj = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
-          const double sj = __ldcg(wo + jj) + beta * __ldcg(so + jj);
-          const double rj = __ldcg(ro + jj) - alpha * sj;
-          acc += __ldg(A.Ls + pos) * (__ldg(A.invL + jj) * rj + cnew[__ldg(V.agg + jj)]);
+          const double sj = (double)__ldcg(wo + jj) + beta * (double)__ldcg(so + jj);
+          const double rj = (double)__ldcg(ro + jj) - alpha * sj;
+          acc += (double)__ldg(Lsv + pos) * ((double)__ldg(invLv + jj) * rj + cnew[__ldg(V.agg + jj)]);
         }
+        acc = rnd(acc);
         // own row
         const int ai = __ldg(V.agg + i);
-        const double mi = __ldg(A.invL + i);
-        const double roi = __ldcg(ro + i);
+        const double mi = (double)__ldg(invLv + i);
+        const double roi = (double)__ldcg(ro + i);
         const double uoi = mi * roi + cold[ai];
-        const double pi = uoi + beta * __ldcg(C.p + i);
-        const double si = __ldcg(wo + i) + beta * __ldcg(so + i);
-        const double xi = __ldcg(A.x + i) + alpha * pi;
-        const double ri = roi - alpha * si;
+        const double pi = rnd(uoi + beta * (double)__ldcg(pv + i));
+        const double si = rnd((double)__ldcg(wo + i) + beta * (double)__ldcg(so + i));
+        const double xi = (double)__ldcg(xv + i) + alpha * pi;
+        const double ri = rnd(roi - alpha * si);
         const double ui = mi * ri + cnew[ai];
-        __stcg(C.p + i, pi);
-        __stcg(sn + i, si);
-        __stcg(A.x + i, xi);
-        __stcg(rn + i, ri);
-        __stcg(wn + i, acc);
+        __stcg(pv + i, (TS)pi);
+        __stcg(sn + i, (TS)si);
+        __stcg(xv + i, (TS)xi);
+        __stcg(rn + i, (TS)ri);
+        __stcg(wn + i, (TS)acc);
         v[0] = ri * ui;
         v[1] = acc * ui;
         v[2] = ri * ri;

@@ -448,6 +448,176 @@ __global__ void k_mp_check(const MixedState *__restrict__ m, DevStatus *st) {
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Mixed-precision pressure solve: FP64 defect correction around the two-level CG with float
+// storage (k_cg2l_resident<float>: operator values, inverse diagonal and Krylov vectors in float,
+// arithmetic and reductions in FP64).
+//   x = 0, r = b                                  (FP64, from k_pressure_rhs)
+//   while ||r|| > tol ||b|| (the FP64 solve's criterion, on the FP64 true residual):
+//     solve Lbc d = r in float to tol_in relative  (k_cg2l_resident<float>, one cooperative launch)
+//     x += d;  r = b - Lbc x                       (FP64)
+// The operator is L2-resident at the benchmark sizes and the solve is bound by the latency of its
+// grid barriers, so float storage shortens the body of an iteration (half the bytes gathered per
+// entry) but not its barrier; the sweeps add one FP64 product each.
+struct PMixState {
+  double bnorm2, tol2, rnorm2;  // outer criterion on the FP64 true residual
+  int sweeps, status, active;
+  int iters;       // inner iterations over all sweeps
+  int bar_failed;  // an inner solve gave up at a grid barrier
+  int max_sweeps;
+  double tol_in;
+};
+
+struct PMixArgs {
+  SellView S;
+  const double *Ls, *invL;  // FP64 penalised operator (SELL) and its inverse diagonal
+  const float *invL32;
+  const double *b;
+  double *x, *r;            // FP64 solution and true residual (x = 0, r = b on entry)
+  float *r32, *x32, *p32, *s32;  // inner right-hand side, solution, and the two zero-on-entry vectors
+  int n, scaled, maxit;
+  CgState *cs;     // the FP64 solve's state (criterion of b from k_pressure_rhs; totals at the end)
+  CgState *cs_in;  // the inner float solve
+  PMixState *pm;
+  DevStatus *st;
+  Reduce red;
+  const int *bar_err;
+  cudaGraphConditionalHandle cond;
+  int use_cond;
+};
+
+__global__ void k_pmx_init(PMixArgs A, double tol_in, int max_sweeps) {
+  PMixState *m = A.pm;
+  const bool halted = A.st && A.st->halt;
+  m->bnorm2 = A.cs->bnorm2;
+  m->tol2 = A.cs->tol2;
+  m->rnorm2 = A.cs->bnorm2;
+  m->sweeps = 0;
+  m->iters = 0;
+  m->bar_failed = 0;
+  m->status = A.cs->status;
+  m->active = halted ? 0 : A.cs->active;
+  m->max_sweeps = max_sweeps;
+  m->tol_in = tol_in;
+}
+
+// Sweep start: inner right-hand side r32 = (float) r, x32 = p32 = s32 = 0, inner criterion.
+__global__ void k_pmx_prep(PMixArgs A) {
+  if (!A.pm->active) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      A.cs_in->active = 0;
+      if (A.use_cond) cudaGraphSetConditional(A.cond, 0);
+    }
+    return;
+  }
+  __shared__ WarpSums<2> S;
+  const int nblk = (A.n + kBlock - 1) / kBlock;
+  int slot = 0;
+  for (int bk = blockIdx.x; bk < nblk; bk += gridDim.x, ++slot) {
+    const int i = bk * kBlock + threadIdx.x;
+    double part[2] = {0.0, 0.0};
+    if (i < A.n) {
+      const float rf = (float)A.r[i];
+      A.r32[i] = rf;
+      A.x32[i] = 0.f;
+      A.p32[i] = 0.f;
+      A.s32[i] = 0.f;
+      const double rd = (double)rf;
+      part[0] = rd * rd;
+      part[1] = A.scaled ? rd * ((double)A.invL32[i] * rd) : rd * rd;
+    }
+    warp_partial<2>(part, S, slot);
+  }
+  double tot[2];
+  if (grid_reduce_strided<2>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
+    CgState *c = A.cs_in;
+    c->bb = tot[0];
+    c->bnorm2 = tot[1];
+    c->rnorm2 = tot[1];
+    c->tol2 = A.pm->tol_in * A.pm->tol_in * tot[1];
+    c->iters = 0;
+    c->maxit = A.maxit;
+    const bool run = tot[1] > 0.0 && !isnan(tot[1]);
+    c->status = run ? KS_RUNNING : KS_BREAKDOWN;
+    c->active = run ? 1 : 0;
+  }
+}
+
+// x += d (FP64)
+__global__ void k_pmx_xupdate(PMixArgs A) {
+  if (!A.pm->active) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < A.n) A.x[i] += (double)A.x32[i];
+}
+
+// r = b - Lbc x (FP64 true residual, rows in SELL order, one thread per row); outer criterion,
+// sweep count and loop condition.
+__global__ void k_pmx_residual(PMixArgs A) {
+  if (!A.pm->active) {
+    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0);
+    return;
+  }
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+  double part[1] = {0.0};
+  if (i >= 0) {
+    const int base = A.S.sptr[r >> 5] + (r & 31), len = A.S.len[r];
+    double acc = 0.0;
+    for (int k = 0; k < len; ++k) {
+      const int pos = base + k * kSellC;
+      acc += A.Ls[pos] * A.x[A.S.col[pos]];
+    }
+    const double ri = A.b[i] - acc;
+    A.r[i] = ri;
+    part[0] = A.scaled ? ri * (A.invL[i] * ri) : ri * ri;
+  }
+  double tot[1];
+  if (grid_reduce<1>(part, A.red, tot) && threadIdx.x == 0) {
+    PMixState *m = A.pm;
+    m->sweeps += 1;
+    m->iters += A.cs_in->iters;
+    m->rnorm2 = tot[0];
+    if (A.bar_err && *A.bar_err) {
+      m->bar_failed = 1;
+      m->status = KS_BREAKDOWN;
+      m->active = 0;
+    } else if (isnan(tot[0])) {
+      m->status = KS_BREAKDOWN;
+      m->active = 0;
+    } else if (tot[0] <= m->tol2) {
+      m->status = KS_CONVERGED;
+      m->active = 0;
+    } else if (A.cs_in->status == KS_BREAKDOWN) {
+      m->status = KS_BREAKDOWN;
+      m->active = 0;
+    } else if (m->sweeps >= m->max_sweeps) {
+      m->status = KS_MAXIT;
+      m->active = 0;
+    }
+    if (A.use_cond) cudaGraphSetConditional(A.cond, m->active ? 1u : 0u);
+  }
+}
+
+// After the sweeps: totals into the FP64 solve's state (for the statistics) and, on failure, the
+// step's status word (as k_check_cg does for the FP64 solve).
+__global__ void k_pmx_check(PMixArgs A, DevStatus *st) {
+  const PMixState *m = A.pm;
+  if (st->halt) return;
+  A.cs->iters = m->iters;
+  A.cs->rnorm2 = m->rnorm2;
+  A.cs->status = m->status;
+  A.cs->active = 0;
+  st->iters[1] += (unsigned long long)m->iters;
+  int code = 0;
+  if (m->status == KS_MAXIT) code = 1;
+  if (m->status == KS_BREAKDOWN) code = 2;
+  if (m->bar_failed) code = 4;
+  if (code) {
+    st->code = code;
+    st->halt = 1;
+  }
+}
+
 __global__ void k_to_f32(int64_t n, const double *__restrict__ src, float *__restrict__ dst) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) dst[k] = (float)src[k];

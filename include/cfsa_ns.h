@@ -109,7 +109,7 @@ typedef struct {
   double momentum_residual[3];/* ||r||/||b|| at exit */
   double pressure_residual;
   int32_t momentum_outer[3];  /* FP64 reliable updates of x and r (mixed precision), else 0 */
-  int32_t pressure_outer;
+  int32_t pressure_outer;     /* defect-correction sweeps of the mixed-precision pressure solve */
   int64_t steps;              /* PISO/SIMPLE steps taken since create */
   double time;                /* simulated time */
   double last_step_ms;        /* device time of the last stepping call, all its steps (CUDA events) */

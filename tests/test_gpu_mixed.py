@@ -98,3 +98,36 @@ def test_jacobi_norm_makes_1e10_meaningful(cf, po):
               f"mixed(1e-10) u {emx[0]:.2e} p {emx[1]:.2e}; iters fp64 {f64[k][2]['momentum_iters']} "
               f"mixed {mix[k][2]['momentum_iters']} updates {mix[k][2]['momentum_outer']}")
         assert max(emx) <= 1e-6, (k, emx)
+
+
+def test_mixed_pressure_two_level_cg(cf, po):
+    """Mixed precision with the two-level CG pressure: the pressure solve runs in float storage
+    inside FP64 defect correction (sweeps > 0, true FP64 residual at the tolerance); u and p stay
+    within 1e-6 of the converged FP64 solution under the Jacobi-scaled criterion."""
+    m = make_mesh(cf, 5, 68)
+    J, K = cf.NORM_JACOBI, cf.KRYLOV_CG2L
+    ref = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-14, norm=J, krylov=K)
+    mix = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-10, norm=J, krylov=K)
+    for k in (0, 4, 9):
+        eu, ep = rel_l2(mix[k][0], ref[k][0]), rel_l2(mix[k][1], ref[k][1])
+        st = mix[k][2]
+        print(f"step {k + 1}: mixed (float two-level CG pressure) vs fp64(1e-14) u {eu:.2e} p {ep:.2e}; "
+              f"pressure iters {st['pressure_iters']} sweeps {st['pressure_outer']}")
+        assert eu <= 1e-6 and ep <= 1e-6, (k, eu, ep)
+    for _, _, st in mix:
+        assert st["pressure_outer"] >= 1
+        assert st["pressure_residual"] <= 1e-10
+
+
+def test_mixed_pressure_graph_and_eager_identical(cf, po):
+    m = make_mesh(cf, 3, 12)
+    res = []
+    for ng in ("0", "1"):
+        os.environ["CFSA_NO_GRAPH"] = ng
+        try:
+            out = run(cf, po, m, cf.PRECISION_MIXED, 3, 1e-12, krylov=cf.KRYLOV_CG2L)
+        finally:
+            os.environ.pop("CFSA_NO_GRAPH", None)
+        res.append(out[-1])
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+    assert res[0][2]["pressure_outer"] == res[1][2]["pressure_outer"] >= 1
