@@ -590,3 +590,33 @@ def test_state_file_restart(cf, po, tmp_path):
     with pytest.raises(cf.CfsaError) as ei:
         other.loadState(path)
     assert ei.value.code == cf.BAD_ARG
+
+
+def test_headline_config_parity_1m_tets(cf, po):
+    """The benchmark's own configuration: 999,936-tet cylinder, parabolic inlet (peak 1.0), FP64,
+    two-level CG pressure (256-aggregate target) and batched BiCGSTAB momentum to 1e-10 in the
+    reference's criterion, from rest. The oracle runs the same solver on the same mesh (its own
+    mesher, identical arrays) and inputs; the first two steps agree bit for bit."""
+    m = make_mesh(cf, 16, 217)
+    assert m.nTets() == 999936
+    prof = cf.parabolic_inlet(m.nodePositions(), 1.0, 2.0)
+    s = cf.NavierStokesSolver()
+    s.setKrylovTolerances(1e-10, 1e-10)
+    s.setMaxIterations(5000, 50000)
+    s.setPressureSolver(cf.KRYLOV_CG2L)
+    s.setDt(0.01)
+    s.initialize(m, cf.Fluid(RHO, NU))
+    s.setInletVelocityProfile(prof)
+    xyz, tets = po.cylinder(30.0, 2.0, 16, 217)
+    assert np.array_equal(xyz, m.vertices()) and np.array_equal(tets, m.tets())
+    o = po.Oracle(xyz, tets)
+    o.set_fluid(RHO, NU)
+    o.set_params(dt=0.01, tol_mom=1e-10, tol_p=1e-10, maxit_mom=5000, maxit_p=50000, pressure_solver=3)
+    o.initialize()
+    o.set_inlet(prof)
+    for k in range(2):
+        assert s.pisoStep() and o.piso_step() == 0
+        st = o.state()
+        eu, ep = rel_l2(s.getVelocity(), st["u"]), rel_l2(s.getPressure(), st["p"])
+        print(f"1M tets step {k + 1}: rel L2 u {eu:.2e} p {ep:.2e}")
+        assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"])
