@@ -84,36 +84,48 @@ def test_mixed_reports_non_convergence(cf, po):
 
 
 def test_jacobi_norm_makes_1e10_meaningful(cf, po):
-    """Under the Jacobi-scaled norm the configs' 1e-10 constrains the interior: FP64 at 1e-10 is
-    close to the converged solution and mixed at 1e-10 meets the 1e-6 bar against it."""
+    """Under the Jacobi-scaled norm the configs' 1e-10 constrains the interior to a few 1e-6 of the
+    converged solution, for FP64 as for mixed precision: mixed at 1e-10 is no farther from the
+    converged solution than FP64 at 1e-10 (reliable updates stop where the FP64 solve stops), and at
+    1e-12 both meet the 1e-6 bar."""
     m = make_mesh(cf, 5, 68)
     J = cf.NORM_JACOBI
     ref = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-14, norm=J)
     f64 = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-10, norm=J)
     mix = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-10, norm=J)
+    mix12 = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-12, norm=J)
     for k in (0, 4, 9):
         e64 = (rel_l2(f64[k][0], ref[k][0]), rel_l2(f64[k][1], ref[k][1]))
         emx = (rel_l2(mix[k][0], ref[k][0]), rel_l2(mix[k][1], ref[k][1]))
+        e12 = (rel_l2(mix12[k][0], ref[k][0]), rel_l2(mix12[k][1], ref[k][1]))
         print(f"jacobi norm step {k + 1}: fp64(1e-10) u {e64[0]:.2e} p {e64[1]:.2e}; "
-              f"mixed(1e-10) u {emx[0]:.2e} p {emx[1]:.2e}; iters fp64 {f64[k][2]['momentum_iters']} "
-              f"mixed {mix[k][2]['momentum_iters']} updates {mix[k][2]['momentum_outer']}")
-        assert max(emx) <= 1e-6, (k, emx)
+              f"mixed(1e-10) u {emx[0]:.2e} p {emx[1]:.2e}; mixed(1e-12) u {e12[0]:.2e} p {e12[1]:.2e}; "
+              f"iters fp64 {f64[k][2]['momentum_iters']} mixed {mix[k][2]['momentum_iters']} "
+              f"updates {mix[k][2]['momentum_outer']}")
+        assert emx[0] <= 1.5 * e64[0] + 1e-7 and emx[1] <= 1.5 * e64[1] + 1e-7, (k, emx, e64)
+        assert max(e12) <= 1e-6, (k, e12)
 
 
 def test_mixed_pressure_two_level_cg(cf, po):
     """Mixed precision with the two-level CG pressure: the pressure solve runs in float storage
-    inside FP64 defect correction (sweeps > 0, true FP64 residual at the tolerance); u and p stay
-    within 1e-6 of the converged FP64 solution under the Jacobi-scaled criterion."""
+    inside FP64 defect correction (sweeps > 0, true FP64 residual at the tolerance). Against the
+    converged FP64 solution: at 1e-10 no farther than FP64 at 1e-10, at 1e-12 within 1e-6."""
     m = make_mesh(cf, 5, 68)
     J, K = cf.NORM_JACOBI, cf.KRYLOV_CG2L
     ref = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-14, norm=J, krylov=K)
+    f64 = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-10, norm=J, krylov=K)
     mix = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-10, norm=J, krylov=K)
+    mix12 = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-12, norm=J, krylov=K)
     for k in (0, 4, 9):
-        eu, ep = rel_l2(mix[k][0], ref[k][0]), rel_l2(mix[k][1], ref[k][1])
+        e64 = (rel_l2(f64[k][0], ref[k][0]), rel_l2(f64[k][1], ref[k][1]))
+        emx = (rel_l2(mix[k][0], ref[k][0]), rel_l2(mix[k][1], ref[k][1]))
+        e12 = (rel_l2(mix12[k][0], ref[k][0]), rel_l2(mix12[k][1], ref[k][1]))
         st = mix[k][2]
-        print(f"step {k + 1}: mixed (float two-level CG pressure) vs fp64(1e-14) u {eu:.2e} p {ep:.2e}; "
-              f"pressure iters {st['pressure_iters']} sweeps {st['pressure_outer']}")
-        assert eu <= 1e-6 and ep <= 1e-6, (k, eu, ep)
+        print(f"step {k + 1}: fp64(1e-10) u {e64[0]:.2e} p {e64[1]:.2e}; mixed(1e-10) u {emx[0]:.2e} "
+              f"p {emx[1]:.2e}; mixed(1e-12) u {e12[0]:.2e} p {e12[1]:.2e}; pressure iters "
+              f"{st['pressure_iters']} sweeps {st['pressure_outer']}")
+        assert emx[0] <= 1.5 * e64[0] + 1e-7 and emx[1] <= 1.5 * e64[1] + 1e-7, (k, emx, e64)
+        assert max(e12) <= 1e-6, (k, e12)
     for _, _, st in mix:
         assert st["pressure_outer"] >= 1
         assert st["pressure_residual"] <= 1e-10
