@@ -26,7 +26,7 @@ OK, NOT_CONVERGED, BREAKDOWN, NAN, CUDA_ERROR, BAD_ARG, NOT_INITIALIZED, UNSUPPO
 MAT_MASS, MAT_STIFFNESS, MAT_GRAD_X, MAT_GRAD_Y, MAT_GRAD_Z, MAT_POISSON, MAT_MOMENTUM, MAT_POISSON_BC = range(8)
 KERNEL_MOMENTUM_SPMV, KERNEL_PRESSURE_SPMV, KERNEL_PRESSURE_SOLVE = 0, 1, 2
 KRYLOV_CG, KRYLOV_BICGSTAB, KRYLOV_CG1, KRYLOV_CG2L = 0, 1, 2, 3
-PRECISION_FP64, PRECISION_MIXED = 0, 1
+PRECISION_FP64, PRECISION_MIXED, PRECISION_MIXED_FULL = 0, 1, 2
 NORM_REFERENCE, NORM_JACOBI = 0, 1
 OBJECTIVE_WALL_SHEAR, OBJECTIVE_PRESSURE_DROP = 0, 1
 VTK_SHEAR_STRESS, VTK_PRESSURE_FORCES = 1, 2

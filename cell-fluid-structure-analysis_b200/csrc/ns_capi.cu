@@ -1061,7 +1061,7 @@ struct cfsa_ns {
   // Batched momentum Krylov solve (x = 0, r = b in wb set up by k_momentum_rhs) into x; the
   // check kernel records failures and iteration counts in `s`.
   void enqueue_momentum_krylov(bool capture, double *x, DevStatus *s_out) {
-    if (precision == CFSA_PRECISION_MIXED) {
+    if (momentum_mixed()) {
       enqueue_momentum_mixed(capture, x, s_out);
       return;
     }
@@ -1316,7 +1316,7 @@ struct cfsa_ns {
   // counts go to `s_out`. Mixed precision applies to the two-level CG (the other methods solve
   // in FP64 in both precisions).
   void enqueue_pressure_krylov(bool capture, double *x, DevStatus *s_out) {
-    if (precision == CFSA_PRECISION_MIXED && krylov == CFSA_KRYLOV_CG2L) {
+    if (pressure_mixed()) {
       enqueue_pressure_mixed(capture, x, s_out);
       return;
     }
@@ -1627,14 +1627,15 @@ struct cfsa_ns {
 
   // Kernels of one pressure-solve body run (counted by DevStatus::body_runs[1]) and the extra
   // fixed kernels of a mixed-precision step, for the launch counts.
-  bool pressure_mixed() const { return precision == CFSA_PRECISION_MIXED && krylov == CFSA_KRYLOV_CG2L; }
+  bool momentum_mixed() const { return precision != CFSA_PRECISION_FP64; }
+  bool pressure_mixed() const { return precision == CFSA_PRECISION_MIXED_FULL && krylov == CFSA_KRYLOV_CG2L; }
   int pressure_body_kernels() const {
     if (pressure_mixed()) return 4;  // prep, float two-level CG, x update, FP64 residual
     if (krylov == CFSA_KRYLOV_BICGSTAB) return 5;
     return (cg_persistent || krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) ? 1 : 3;
   }
   int mixed_fixed_kernels() const {
-    return (precision == CFSA_PRECISION_MIXED ? 1 : 0) + (pressure_mixed() ? 1 : 0);
+    return (momentum_mixed() ? 1 : 0) + (pressure_mixed() ? 1 : 0);
   }
 
   int finish_batch(int launched_steps) {
@@ -2027,8 +2028,7 @@ struct cfsa_ns {
     CK(cudaGetLastError());
     // correct, [sum,] chain per corrector, pressure rhs + check, momentum rhs + check,
     // conv_tet, mom_out (Krylov loop bodies counted from the status)
-    adj_launches_fixed = 1 + ncorr * (normalize ? 2 : 1) + 2 + 2 + 2 +
-                         (precision == CFSA_PRECISION_MIXED ? 1 : 0);
+    adj_launches_fixed = 1 + ncorr * (normalize ? 2 : 1) + 2 + 2 + 2 + mixed_fixed_kernels();
   }
 
   void ensure_adj_graph() {
@@ -2401,7 +2401,8 @@ int cfsa_ns_get_coarse_size(cfsa_ns *h, int *nc) {
 
 int cfsa_ns_set_precision(cfsa_ns *h, int precision) {
   if (!h) return CFSA_BAD_ARG;
-  if (precision != CFSA_PRECISION_FP64 && precision != CFSA_PRECISION_MIXED)
+  if (precision != CFSA_PRECISION_FP64 && precision != CFSA_PRECISION_MIXED &&
+      precision != CFSA_PRECISION_MIXED_FULL)
     return fail(h, CFSA_BAD_ARG, "unknown precision");
   if (precision != h->precision) h->graph_dirty = true;
   h->precision = precision;
@@ -2670,7 +2671,7 @@ int cfsa_ns_get_stats(const cfsa_ns *hc, cfsa_ns_stats *s) {
     CK(cudaMemcpyAsync(h->h_cs, h->cs, sizeof(CgState), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     std::memset(s, 0, sizeof(*s));
-    if (h->precision == CFSA_PRECISION_MIXED) {
+    if (h->momentum_mixed()) {
       CK(cudaMemcpyAsync(h->h_ms, h->ms, sizeof(MixedState), cudaMemcpyDeviceToHost, h->stream));
       CK(cudaStreamSynchronize(h->stream));
       for (int c = 0; c < 3; ++c) {

@@ -24,6 +24,8 @@
 
 namespace cfsa {
 
+constexpr double kMixedDrift2 = 100.0;  // true / iterated residual (squared) that restarts the space
+
 struct MixedState {
   double bnorm2[3], tol2[3], rnorm2[3];  // FP64 criterion; rnorm2: true residual at the last update
   double rho[3], alpha[3], omega[3], beta[3], r0norm2[3];
@@ -33,8 +35,11 @@ struct MixedState {
   int active;   // components iterating
   int upd;      // components updated at the end of this iteration
   int restart;  // components whose Krylov space restarts at that update (near-breakdown)
+  int restart_next;  // components restarting at the next iteration (the FP32 recurrence drifted)
   int maxit;
   double delta2;  // update trigger: rin2 < delta2 * rmax2
+  double delta;   // companions of a triggered update: rin2 < delta * rmax2 (halfway, in norm)
+  int drift_restarts[3];
 };
 
 struct MixedArgs {
@@ -144,8 +149,10 @@ __global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta) {
     m->active = 0;
     m->upd = 0;
     m->restart = 0;
+    m->restart_next = 0;
     m->maxit = maxit;
     m->delta2 = delta * delta;
+    m->delta = delta;
     for (int c = 0; c < 3; ++c) {
       m->bnorm2[c] = tot[c];
       m->rnorm2[c] = tot[c];
@@ -158,6 +165,7 @@ __global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta) {
       m->beta[c] = 0.0;
       m->iters[c] = 0;
       m->updates[c] = 0;
+      m->drift_restarts[c] = 0;
       if (isnan(tot[c]) || isnan(tot[3 + c])) {
         m->status[c] = KS_BREAKDOWN;
       } else if (tot[c] == 0.0 || tot[c] <= m->tol2[c]) {
@@ -170,19 +178,43 @@ __global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta) {
   }
 }
 
-// K1: p = r + beta (p - omega v)  (beta = 0 after a restart: p = r)
+// K1: p = r + beta (p - omega v)  (beta = 0 after a restart: p = r). Components whose FP32
+// recurrence drifted from the true residual (flagged by the last update) restart here instead:
+// r0 = p = r and rho = r0 . r, the one reduction of this kernel (taken only when a restart is due).
 __global__ void k_mp_p(MixedArgs A) {
   const int act = A.ms->active;
   if (!act) return;
+  const int rs = A.ms->restart_next & act;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
   const int64_t n = A.n;
+  double part[3] = {0.0, 0.0, 0.0};
+  if (i < A.n) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    if (!((act >> c) & 1)) continue;
-    const int64_t o = c * n + i;
-    const float beta = (float)A.ms->beta[c], omega = (float)A.ms->omega[c];
-    A.p[o] = A.r[o] + beta * (A.p[o] - omega * A.v[o]);
+    for (int c = 0; c < 3; ++c) {
+      if (!((act >> c) & 1)) continue;
+      const int64_t o = c * n + i;
+      if ((rs >> c) & 1) {
+        const float ri = A.r[o];
+        A.p[o] = ri;
+        A.r0[o] = ri;
+        part[c] = (double)ri * (double)ri;
+      } else {
+        const float beta = (float)A.ms->beta[c], omega = (float)A.ms->omega[c];
+        A.p[o] = A.r[o] + beta * (A.p[o] - omega * A.v[o]);
+      }
+    }
+  }
+  if (!rs) return;
+  double tot[3];
+  if (grid_reduce<3>(part, A.red, tot) && threadIdx.x == 0) {
+    MixedState *m = A.ms;
+    for (int c = 0; c < 3; ++c)
+      if ((rs >> c) & 1) {
+        m->rho[c] = tot[c];
+        m->r0norm2[c] = tot[c];
+        m->drift_restarts[c] += 1;
+      }
+    m->restart_next = 0;
   }
 }
 
@@ -309,7 +341,7 @@ __global__ void k_mp_xr(MixedArgs A) {
   if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     MixedState *m = A.ms;
     const double eps = 2.220446049250313e-16;
-    int upd = 0, rst = 0;
+    int upd = 0, rst = 0, live = 0;
     for (int c = 0; c < 3; ++c) {
       if (!((act >> c) & 1)) continue;
       m->iters[c] += 1;
@@ -320,16 +352,25 @@ __global__ void k_mp_xr(MixedArgs A) {
         m->active &= ~(1 << c);
         continue;
       }
+      live |= 1 << c;
       const bool near_breakdown = fabs(rho_new) < eps * eps * m->r0norm2[c];
       if (tot[c] <= m->tol2[c] || m->iters[c] >= m->maxit || tot[c] < m->delta2 * m->rmax2[c] ||
           m->omega[c] == 0.0 || near_breakdown) {
         upd |= 1 << c;
         if (near_breakdown) rst |= 1 << c;
-      } else {
-        m->beta[c] = (rho_new / m->rho[c]) * (m->alpha[c] / m->omega[c]);
-        m->rho[c] = rho_new;
-        m->rmax2[c] = fmax(m->rmax2[c], tot[c]);
       }
+    }
+    // an update's FP64 product streams the whole operator whichever components it serves, so the
+    // components that are halfway (in norm) to their own trigger join it
+    if (upd)
+      for (int c = 0; c < 3; ++c)
+        if (((live & ~upd) >> c) & 1 && tot[c] < m->delta * m->rmax2[c]) upd |= 1 << c;
+    for (int c = 0; c < 3; ++c) {
+      if (!(((live & ~upd) >> c) & 1)) continue;
+      const double rho_new = tot[3 + c];
+      m->beta[c] = (rho_new / m->rho[c]) * (m->alpha[c] / m->omega[c]);
+      m->rho[c] = rho_new;
+      m->rmax2[c] = fmax(m->rmax2[c], tot[c]);
     }
     m->upd = upd;
     m->restart = rst;
@@ -421,6 +462,9 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_residual(MixedArgs A) {
           m->beta[c] = 0.0;
         } else {
           m->beta[c] = (rho_new / m->rho[c]) * (m->alpha[c] / m->omega[c]);
+          // the true residual is more than 10x (in norm) the FP32 recurrence's: its Krylov space
+          // has drifted; the next iteration restarts it from the replaced residual
+          if (tot[c] > kMixedDrift2 * m->rin2[c]) m->restart_next |= 1 << c;
         }
         m->rho[c] = rho_new;
         m->rin2[c] = tot[c];

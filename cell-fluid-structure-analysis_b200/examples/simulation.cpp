@@ -83,7 +83,9 @@ int main(int argc, char **argv) {
                         : N.pressure_solver == "cg1"    ? CFSA_KRYLOV_CG1
                                                         : CFSA_KRYLOV_CG2L);
   ns->setCoarseTarget(N.coarse_aggregates);
-  ns->setPrecision(N.precision == "mixed" ? CFSA_PRECISION_MIXED : CFSA_PRECISION_FP64);
+  ns->setPrecision(N.precision == "mixed"        ? CFSA_PRECISION_MIXED
+                   : N.precision == "mixed_full" ? CFSA_PRECISION_MIXED_FULL
+                                                 : CFSA_PRECISION_FP64);
   ns->setConvergenceNorm(N.convergence_norm == "jacobi" ? CFSA_NORM_JACOBI : CFSA_NORM_REFERENCE);
   ns->initialize(mesh, fluid);
   if (N.inlet_profile == "parabolic") {

@@ -145,7 +145,7 @@ class NavierStokesSolver {
   // new: binary restart file of u, p, time and step count (cfsa_ns_save_state / _load_state)
   bool saveState(const std::string &path);
   bool loadState(const std::string &path);
-  void setPrecision(int precision);    // CFSA_PRECISION_FP64 or CFSA_PRECISION_MIXED
+  void setPrecision(int precision);    // CFSA_PRECISION_FP64, _MIXED or _MIXED_FULL
   void setConvergenceNorm(int norm);   // CFSA_NORM_REFERENCE or CFSA_NORM_JACOBI
   void setInletVelocityProfile(const std::vector<Vec3> &per_node);
   bool pisoSteps(int n, int *n_done = nullptr);  // n steps, one host synchronisation

@@ -232,7 +232,7 @@ SimulationConfig parseConfig(const std::string &text) {
           N.max_iterations[0] = N.max_iterations[1] = as_int(n, k);
         }
       });
-      opt(ns, "precision", [&](const Node *n, const std::string &k) { N.precision = n->scalar; one_of(N.precision, {"fp64", "mixed"}, k); });
+      opt(ns, "precision", [&](const Node *n, const std::string &k) { N.precision = n->scalar; one_of(N.precision, {"fp64", "mixed", "mixed_full"}, k); });
       opt(ns, "pressure_solver", [&](const Node *n, const std::string &k) { N.pressure_solver = n->scalar; one_of(N.pressure_solver, {"bicgstab", "cg", "cg1", "cg2l"}, k); });
       opt(ns, "coarse_aggregates", [&](const Node *n, const std::string &k) {
         N.coarse_aggregates = as_int(n, k);

@@ -13,7 +13,7 @@
 //   navier_stokes.tolerance          Krylov tolerance of both solves (reference: 1e-6 / 1e-8)
 //   navier_stokes.max_iterations     [momentum, pressure] iteration caps (reference: 1000, 1000)
 //   navier_stokes.n_corrections      PISO correctors (reference: 1)
-//   navier_stokes.precision          fp64 | mixed
+//   navier_stokes.precision          fp64 | mixed | mixed_full
 //   navier_stokes.pressure_solver    bicgstab | cg | cg1 | cg2l (reference: bicgstab)
 //   navier_stokes.coarse_aggregates  aggregates of the cg2l coarse space (default 256)
 //   navier_stokes.convergence_norm   reference | jacobi

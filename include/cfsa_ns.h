@@ -60,9 +60,13 @@ extern "C" {
 
 /* arithmetic of the Krylov solves */
 #define CFSA_PRECISION_FP64 0
-/* FP32 operator and Krylov vectors; FP64 solution, true residual (reliable updates), dot
- * products and scalars; convergence decided on the FP64 true residual */
+/* momentum: FP32 operator and Krylov vectors; FP64 solution, true residual (reliable updates), dot
+ * products and scalars; convergence decided on the FP64 true residual. Pressure in FP64. */
 #define CFSA_PRECISION_MIXED 1
+/* CFSA_PRECISION_MIXED plus, with CFSA_KRYLOV_CG2L, the pressure solve in float storage inside
+ * FP64 defect correction. Each sweep restarts the CG, so the pressure solve takes more iterations
+ * than in FP64 (1.8x on the 1M-tet cylinder), which costs more than float storage saves. */
+#define CFSA_PRECISION_MIXED_FULL 2
 
 /* Krylov convergence norm. REFERENCE: ||r|| <= tol ||b|| (NavierStokes.cpp:500,635). With the
  * 1e10 / 1e12 penalty rows in b this norm is dominated by the Dirichlet rows, so it constrains the

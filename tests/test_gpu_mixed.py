@@ -107,15 +107,15 @@ def test_jacobi_norm_makes_1e10_meaningful(cf, po):
 
 
 def test_mixed_pressure_two_level_cg(cf, po):
-    """Mixed precision with the two-level CG pressure: the pressure solve runs in float storage
+    """CFSA_PRECISION_MIXED_FULL with the two-level CG pressure: the pressure solve runs in float storage
     inside FP64 defect correction (sweeps > 0, true FP64 residual at the tolerance). Against the
     converged FP64 solution: at 1e-10 no farther than FP64 at 1e-10, at 1e-12 within 1e-6."""
     m = make_mesh(cf, 5, 68)
     J, K = cf.NORM_JACOBI, cf.KRYLOV_CG2L
     ref = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-14, norm=J, krylov=K)
     f64 = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-10, norm=J, krylov=K)
-    mix = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-10, norm=J, krylov=K)
-    mix12 = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-12, norm=J, krylov=K)
+    mix = run(cf, po, m, cf.PRECISION_MIXED_FULL, 10, 1e-10, norm=J, krylov=K)
+    mix12 = run(cf, po, m, cf.PRECISION_MIXED_FULL, 10, 1e-12, norm=J, krylov=K)
     for k in (0, 4, 9):
         e64 = (rel_l2(f64[k][0], ref[k][0]), rel_l2(f64[k][1], ref[k][1]))
         emx = (rel_l2(mix[k][0], ref[k][0]), rel_l2(mix[k][1], ref[k][1]))
@@ -137,9 +137,18 @@ def test_mixed_pressure_graph_and_eager_identical(cf, po):
     for ng in ("0", "1"):
         os.environ["CFSA_NO_GRAPH"] = ng
         try:
-            out = run(cf, po, m, cf.PRECISION_MIXED, 3, 1e-12, krylov=cf.KRYLOV_CG2L)
+            out = run(cf, po, m, cf.PRECISION_MIXED_FULL, 3, 1e-12, krylov=cf.KRYLOV_CG2L)
         finally:
             os.environ.pop("CFSA_NO_GRAPH", None)
         res.append(out[-1])
     assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
     assert res[0][2]["pressure_outer"] == res[1][2]["pressure_outer"] >= 1
+
+
+def test_mixed_keeps_fp64_pressure(cf, po):
+    """CFSA_PRECISION_MIXED runs only the momentum solve in FP32: its pressure solve is the FP64
+    two-level CG (no defect-correction sweeps)."""
+    m = make_mesh(cf, 3, 12)
+    out = run(cf, po, m, cf.PRECISION_MIXED, 2, 1e-12, krylov=cf.KRYLOV_CG2L)
+    for _, _, st in out:
+        assert st["pressure_outer"] == 0 and max(st["momentum_outer"]) >= 1
