@@ -201,7 +201,8 @@ struct cfsa_ns {
   int mixed_p_max_sweeps = 30;
   // reliable-update trigger of the mixed-precision BiCGSTAB: the FP64 residual replaces the FP32
   // one when the latter has dropped by this factor since the previous update
-  double mixed_delta = 1e-3;
+  double mixed_delta = 1e-2;
+  bool mixed_if = true;  // reliable update behind an IF node (else its kernels run every iteration)
   // discrete adjoint (ns_adjoint.cuh): transposed P1 slots, vertex -> (boundary face, local
   // index in the face's tet) incidence, host vertex coordinates for objective patches
   int *tpos1 = nullptr, *vbf_ptr = nullptr, *vbf = nullptr;
@@ -501,6 +502,7 @@ struct cfsa_ns {
     CK(cudaMallocHost(&h_pmx, sizeof(PMixState)));
     if (const char *e = std::getenv("CFSA_MIXED_P_TOL_IN")) mixed_p_tol_in = std::atof(e);
     if (const char *e = std::getenv("CFSA_MIXED_DELTA")) mixed_delta = std::atof(e);
+    if (const char *e = std::getenv("CFSA_MIXED_IF")) mixed_if = (std::atoi(e) != 0);
     bs_prof = dalloc<BicgState>(1);
     cs_prof = dalloc<CgState>(1);
     // boundary faces
@@ -1124,13 +1126,14 @@ struct cfsa_ns {
       MixedArgs b = a;
       b.cond = h;
       b.use_cond = use;
-      if (use) b.cond_upd = new_cond_handle(s, 0);
+      b.use_if = (use && mixed_if) ? 1 : 0;
+      if (b.use_if) b.cond_upd = new_cond_handle(s, 0);
       k_mp_p<<<gp, kBlock, 0, s>>>(b);
       k_mp_v<<<s2.nruns, kRunThreads, 0, s>>>(b);
       k_mp_s<<<gp, kBlock, 0, s>>>(b);
       k_mp_t<<<s2.nruns, kRunThreads, 0, s>>>(b);
       k_mp_xr<<<strided(k_mp_xr, gp), kBlock, 0, s>>>(b);
-      if (use)
+      if (b.use_if)
         capture_cond_with(s, body_stream2, b.cond_upd, cudaGraphCondTypeIf,
                           [&](cudaStream_t ss, cudaGraphConditionalHandle, int) { update_body(ss, b); });
       else

@@ -36,6 +36,7 @@ struct MixedState {
   int upd;      // components updated at the end of this iteration
   int restart;  // components whose Krylov space restarts at that update (near-breakdown)
   int restart_next;  // components restarting at the next iteration (the FP32 recurrence drifted)
+  int force;         // components whose r0 . v vanished: update and restart at this iteration's end
   int maxit;
   double delta2;  // update trigger: rin2 < delta2 * rmax2
   double delta;   // companions of a triggered update: rin2 < delta * rmax2 (halfway, in norm)
@@ -57,6 +58,7 @@ struct MixedArgs {
   cudaGraphConditionalHandle cond;      // WHILE node of the iteration
   cudaGraphConditionalHandle cond_upd;  // IF node of the reliable update
   int use_cond;
+  int use_if;  // cond_upd is a live IF node (otherwise the update kernels run every iteration)
   const double *cw;   // convergence-norm weights (diag(A)^-1), nullptr: unscaled ||r||
   const float *cw32;  // the same for the FP32 residual
 };
@@ -150,6 +152,7 @@ __global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta) {
     m->upd = 0;
     m->restart = 0;
     m->restart_next = 0;
+    m->force = 0;
     m->maxit = maxit;
     m->delta2 = delta * delta;
     m->delta = delta;
@@ -244,9 +247,13 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_v(MixedArgs A) {
   if (grid_reduce_runs<3>(A.S, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < 3; ++c) {
       if (!((act >> c) & 1)) continue;
-      if (tot[c] == 0.0 || isnan(tot[c])) {
+      if (isnan(tot[c])) {
         A.ms->status[c] = KS_BREAKDOWN;
         A.ms->active &= ~(1 << c);
+      } else if (tot[c] == 0.0) {
+        // r0 . v vanished: no step along p; the iteration ends in an update and a restart
+        A.ms->alpha[c] = 0.0;
+        A.ms->force |= 1 << c;
       } else {
         A.ms->alpha[c] = A.ms->rho[c] / tot[c];
       }
@@ -308,7 +315,7 @@ __global__ void k_mp_xr(MixedArgs A) {
   if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[0] += 1;
   if (!act) {
     if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) {
-      cudaGraphSetConditional(A.cond_upd, 0);
+      if (A.use_if) cudaGraphSetConditional(A.cond_upd, 0);
       cudaGraphSetConditional(A.cond, 0);
     }
     return;
@@ -353,11 +360,13 @@ __global__ void k_mp_xr(MixedArgs A) {
         continue;
       }
       live |= 1 << c;
-      const bool near_breakdown = fabs(rho_new) < eps * eps * m->r0norm2[c];
-      if (tot[c] <= m->tol2[c] || m->iters[c] >= m->maxit || tot[c] < m->delta2 * m->rmax2[c] ||
-          m->omega[c] == 0.0 || near_breakdown) {
+      // near-breakdown, a vanished omega or r0 . v: the FP32 space is exhausted; the update
+      // replaces the residual and the Krylov space restarts from it
+      const bool restart = fabs(rho_new) < eps * eps * m->r0norm2[c] || m->omega[c] == 0.0 ||
+                           ((m->force >> c) & 1);
+      if (tot[c] <= m->tol2[c] || m->iters[c] >= m->maxit || tot[c] < m->delta2 * m->rmax2[c] || restart) {
         upd |= 1 << c;
-        if (near_breakdown) rst |= 1 << c;
+        if (restart) rst |= 1 << c;
       }
     }
     // an update's FP64 product streams the whole operator whichever components it serves, so the
@@ -374,8 +383,9 @@ __global__ void k_mp_xr(MixedArgs A) {
     }
     m->upd = upd;
     m->restart = rst;
+    m->force = 0;
     if (A.use_cond) {
-      cudaGraphSetConditional(A.cond_upd, upd ? 1u : 0u);
+      if (A.use_if) cudaGraphSetConditional(A.cond_upd, upd ? 1u : 0u);
       cudaGraphSetConditional(A.cond, m->active ? 1u : 0u);
     }
   }
@@ -452,9 +462,6 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_residual(MixedArgs A) {
         m->active &= ~(1 << c);
       } else if (m->iters[c] >= m->maxit) {
         m->status[c] = KS_MAXIT;
-        m->active &= ~(1 << c);
-      } else if (m->omega[c] == 0.0) {
-        m->status[c] = KS_BREAKDOWN;
         m->active &= ~(1 << c);
       } else {
         if ((rst >> c) & 1) {
