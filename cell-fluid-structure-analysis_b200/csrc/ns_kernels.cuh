@@ -669,6 +669,10 @@ __global__ void k_bicg_p(BicgArgs A) {
   const int active = A.bs->active;
   if (!active) return;
   const int restart = A.bs->restart;
+  // the scalars are read once, before any store the compiler could not prove disjoint from them
+  double beta_c[NC], omega_c[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) beta_c[c] = A.bs->beta[c], omega_c[c] = A.bs->omega[c];
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
   const int64_t n = A.n;
@@ -694,8 +698,7 @@ __global__ void k_bicg_p(BicgArgs A) {
         A.pk[o] = ri;
         part[c] = ri * ri;
       } else {
-        const double beta = A.bs->beta[c], omega = A.bs->omega[c];
-        A.pk[o] = A.r[o] + beta * (A.pk[o] - omega * A.v[o]);
+        A.pk[o] = A.r[o] + beta_c[c] * (A.pk[o] - omega_c[c] * A.v[o]);
       }
     }
   }
@@ -760,12 +763,15 @@ __global__ void k_bicg_s(BicgArgs A) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const int64_t n = A.n;
+  double alpha[NC], rv[NC], vv[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
-    if (!((active >> c) & 1)) continue;
-    const int64_t o = c * n + i;
-    A.s[o] = A.r[o] - A.bs->alpha[c] * A.v[o];
+    alpha[c] = A.bs->alpha[c];
+    if ((active >> c) & 1) rv[c] = A.r[c * n + i], vv[c] = A.v[c * n + i];
   }
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+    if ((active >> c) & 1) A.s[c * n + i] = rv[c] - alpha[c] * vv[c];
 }
 
 // K4: t = At s, omega = (t . s) / (t . t) (0 when t . t == 0)
@@ -816,6 +822,9 @@ __global__ void k_bicg_xr(BicgArgs A) {
   __shared__ WarpSums<2 * NC> S;
   const int nblk = (A.n + kBlock - 1) / kBlock;
   const int64_t n = A.n;
+  double alpha_c[NC], omega_c[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) alpha_c[c] = A.bs->alpha[c], omega_c[c] = A.bs->omega[c];
   int slot = 0;
   for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
     const int i = b * kBlock + threadIdx.x;
@@ -825,18 +834,24 @@ __global__ void k_bicg_xr(BicgArgs A) {
     if (i < A.n) {
       const double dinv = A.invA[i];
       const double w = A.cw ? A.cw[i] : 1.0;
+      double pv[NC], sv[NC], tv[NC], xv[NC], r0v[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         if (!((active >> c) & 1)) continue;
         const int64_t o = c * n + i;
-        const double alpha = A.bs->alpha[c], omega = A.bs->omega[c];
-        const double y = dinv * A.pk[o];
-        const double z = dinv * A.s[o];
-        A.x[o] += alpha * y + omega * z;
-        const double ri = A.s[o] - omega * A.t[o];
+        pv[c] = A.pk[o], sv[c] = A.s[o], tv[c] = A.t[o], xv[c] = A.x[o], r0v[c] = A.r0[o];
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        if (!((active >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        const double y = dinv * pv[c];
+        const double z = dinv * sv[c];
+        A.x[o] = xv[c] + (alpha_c[c] * y + omega_c[c] * z);
+        const double ri = sv[c] - omega_c[c] * tv[c];
         A.r[o] = ri;
         part[c] = (ri * ri) * w;
-        part[NC + c] = A.r0[o] * ri;
+        part[NC + c] = r0v[c] * ri;
       }
     }
     warp_partial<2 * NC>(part, S, slot);

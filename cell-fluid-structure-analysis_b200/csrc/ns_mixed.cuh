@@ -188,22 +188,27 @@ __global__ void k_mp_p(MixedArgs A) {
   const int act = A.ms->active;
   if (!act) return;
   const int rs = A.ms->restart_next & act;
+  float beta[3], omega[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) beta[c] = (float)A.ms->beta[c], omega[c] = (float)A.ms->omega[c];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n = A.n;
   double part[3] = {0.0, 0.0, 0.0};
   if (i < A.n) {
+    float rv[3], pv[3], vv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      if ((act >> c) & 1) rv[c] = A.r[c * n + i], pv[c] = A.p[c * n + i], vv[c] = A.v[c * n + i];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       if (!((act >> c) & 1)) continue;
       const int64_t o = c * n + i;
       if ((rs >> c) & 1) {
-        const float ri = A.r[o];
-        A.p[o] = ri;
-        A.r0[o] = ri;
-        part[c] = (double)ri * (double)ri;
+        A.p[o] = rv[c];
+        A.r0[o] = rv[c];
+        part[c] = (double)rv[c] * (double)rv[c];
       } else {
-        const float beta = (float)A.ms->beta[c], omega = (float)A.ms->omega[c];
-        A.p[o] = A.r[o] + beta * (A.p[o] - omega * A.v[o]);
+        A.p[o] = rv[c] + beta[c] * (pv[c] - omega[c] * vv[c]);
       }
     }
   }
@@ -268,12 +273,15 @@ __global__ void k_mp_s(MixedArgs A) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const int64_t n = A.n;
+  float alpha[3], rv[3], vv[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    if (!((act >> c) & 1)) continue;
-    const int64_t o = c * n + i;
-    A.s[o] = A.r[o] - (float)A.ms->alpha[c] * A.v[o];
+    alpha[c] = (float)A.ms->alpha[c];
+    if ((act >> c) & 1) rv[c] = A.r[c * n + i], vv[c] = A.v[c * n + i];
   }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    if ((act >> c) & 1) A.s[c * n + i] = rv[c] - alpha[c] * vv[c];
 }
 
 // K4: t = At32 s, omega = (t . s) / (t . t)
@@ -323,6 +331,9 @@ __global__ void k_mp_xr(MixedArgs A) {
   const int64_t n = A.n;
   __shared__ WarpSums<6> S;
   const int nblk = (A.n + kBlock - 1) / kBlock;
+  float alpha_c[3], omega_c[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) alpha_c[c] = (float)A.ms->alpha[c], omega_c[c] = (float)A.ms->omega[c];
   int slot = 0;
   for (int bk = blockIdx.x; bk < nblk; bk += gridDim.x, ++slot) {
     const int i = bk * kBlock + threadIdx.x;
@@ -330,16 +341,22 @@ __global__ void k_mp_xr(MixedArgs A) {
     if (i < A.n) {
       const float dinv = A.invA32[i];
       const double w = A.cw32 ? (double)A.cw32[i] : 1.0;
+      float pv[3], sv[3], tv[3], dxv[3], r0v[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         if (!((act >> c) & 1)) continue;
         const int64_t o = c * n + i;
-        const float alpha = (float)A.ms->alpha[c], omega = (float)A.ms->omega[c];
-        A.dx[o] += alpha * (dinv * A.p[o]) + omega * (dinv * A.s[o]);
-        const float ri = A.s[o] - omega * A.t[o];
+        pv[c] = A.p[o], sv[c] = A.s[o], tv[c] = A.t[o], dxv[c] = A.dx[o], r0v[c] = A.r0[o];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (!((act >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        A.dx[o] = dxv[c] + (alpha_c[c] * (dinv * pv[c]) + omega_c[c] * (dinv * sv[c]));
+        const float ri = sv[c] - omega_c[c] * tv[c];
         A.r[o] = ri;
         part[c] = ((double)ri * (double)ri) * w;
-        part[3 + c] = (double)A.r0[o] * (double)ri;
+        part[3 + c] = (double)r0v[c] * (double)ri;
       }
     }
     warp_partial<6>(part, S, slot);
