@@ -24,8 +24,6 @@
 
 namespace cfsa {
 
-constexpr double kMixedDrift2 = 100.0;  // true / iterated residual (squared) that restarts the space
-
 struct MixedState {
   double bnorm2[3], tol2[3], rnorm2[3];  // FP64 criterion; rnorm2: true residual at the last update
   double rho[3], alpha[3], omega[3], beta[3], r0norm2[3];
@@ -40,7 +38,13 @@ struct MixedState {
   int maxit;
   double delta2;  // update trigger: rin2 < delta2 * rmax2
   double delta;   // companions of a triggered update: rin2 < delta * rmax2 (halfway, in norm)
+  double drift2;  // true / iterated residual (squared) above which the Krylov space restarts
+  int companions; // components halfway to their trigger join an update
   int drift_restarts[3];
+  // diagnostics of the last solve: updates by cause (tolerance, delta, restart, companion) and the
+  // iterated / true residual of the first updates of each component
+  int cause[3][4];
+  double hist[3][16][2];
 };
 
 struct MixedArgs {
@@ -101,24 +105,10 @@ __device__ __forceinline__ void sell_spmv_row_f32x3(const SellView &S, const flo
   }
 }
 
-// sell_spmv_row_f32x3 for the components still active in `mask` (see sell_spmv_row_active).
-__device__ __forceinline__ void sell_spmv_row_f32x3_active(const SellView &S, const float *__restrict__ val,
-                                                           const float *__restrict__ x, int64_t n, int r,
-                                                           float acc[3], int mask) {
-  switch (mask) {
-    case 1: sell_spmv_row_f32x3<8, 1>(S, val, x, n, r, acc); break;
-    case 2: sell_spmv_row_f32x3<8, 2>(S, val, x, n, r, acc); break;
-    case 4: sell_spmv_row_f32x3<8, 4>(S, val, x, n, r, acc); break;
-    case 3: sell_spmv_row_f32x3<8, 3>(S, val, x, n, r, acc); break;
-    case 5: sell_spmv_row_f32x3<8, 5>(S, val, x, n, r, acc); break;
-    case 6: sell_spmv_row_f32x3<8, 6>(S, val, x, n, r, acc); break;
-    default: sell_spmv_row_f32x3(S, val, x, n, r, acc); break;
-  }
-}
 
 // Init (after k_momentum_rhs wrote b and x = 0): r = r0 = (float) b, p = v = dx = 0;
 // FP64 ||b|| in the convergence norm, rho = r0 . r.
-__global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta) {
+__global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta, double drift2, int companions) {
   if (A.st->halt) return;
   const int64_t n = A.n;
   __shared__ WarpSums<6> S;
@@ -156,6 +146,10 @@ __global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta) {
     m->maxit = maxit;
     m->delta2 = delta * delta;
     m->delta = delta;
+    m->drift2 = drift2;
+    m->companions = companions;
+    for (int c = 0; c < 3; ++c)
+      for (int q = 0; q < 4; ++q) m->cause[c][q] = 0;
     for (int c = 0; c < 3; ++c) {
       m->bnorm2[c] = tot[c];
       m->rnorm2[c] = tot[c];
@@ -232,22 +226,25 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_v(MixedArgs A) {
   if (!act) return;
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
-  for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
-    const int r = sl * kSellC + (threadIdx.x & 31);
-    const int i = A.S.perm[r];
-    double part[3] = {0.0, 0.0, 0.0};
-    if (i >= 0) {
-      float acc[3];
-      sell_spmv_row_f32x3_active(A.S, A.At32, A.p, n, r, acc, act);
+  with_mask<3>(act, [&](auto mk) {
+    constexpr int MASK = decltype(mk)::value;
+    for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+      const int r = sl * kSellC + (threadIdx.x & 31);
+      const int i = A.S.perm[r];
+      double part[3] = {0.0, 0.0, 0.0};
+      if (i >= 0) {
+        float acc[3];
+        sell_spmv_row_f32x3<8, MASK>(A.S, A.At32, A.p, n, r, acc);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (!((act >> c) & 1)) continue;
-        A.v[c * n + i] = acc[c];
-        part[c] = (double)A.r0[c * n + i] * (double)acc[c];
+        for (int c = 0; c < 3; ++c) {
+          if (!((MASK >> c) & 1)) continue;
+          A.v[c * n + i] = acc[c];
+          part[c] = (double)A.r0[c * n + i] * (double)acc[c];
+        }
       }
+      slice_partial<3>(part, A.S, sl);
     }
-    slice_partial<3>(part, A.S, sl);
-  }
+  });
   double tot[3];
   if (grid_reduce_runs<3>(A.S, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < 3; ++c) {
@@ -290,23 +287,26 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_t(MixedArgs A) {
   if (!act) return;
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
-  for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
-    const int r = sl * kSellC + (threadIdx.x & 31);
-    const int i = A.S.perm[r];
-    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (i >= 0) {
-      float acc[3];
-      sell_spmv_row_f32x3_active(A.S, A.At32, A.s, n, r, acc, act);
+  with_mask<3>(act, [&](auto mk) {
+    constexpr int MASK = decltype(mk)::value;
+    for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+      const int r = sl * kSellC + (threadIdx.x & 31);
+      const int i = A.S.perm[r];
+      double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      if (i >= 0) {
+        float acc[3];
+        sell_spmv_row_f32x3<8, MASK>(A.S, A.At32, A.s, n, r, acc);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (!((act >> c) & 1)) continue;
-        A.t[c * n + i] = acc[c];
-        part[c] = (double)acc[c] * (double)acc[c];
-        part[3 + c] = (double)acc[c] * (double)A.s[c * n + i];
+        for (int c = 0; c < 3; ++c) {
+          if (!((MASK >> c) & 1)) continue;
+          A.t[c * n + i] = acc[c];
+          part[c] = (double)acc[c] * (double)acc[c];
+          part[3 + c] = (double)acc[c] * (double)A.s[c * n + i];
+        }
       }
+      slice_partial<6>(part, A.S, sl);
     }
-    slice_partial<6>(part, A.S, sl);
-  }
+  });
   double tot[6];
   if (grid_reduce_runs<6>(A.S, A.red, tot) && threadIdx.x == 0) {
     for (int c = 0; c < 3; ++c) {
@@ -384,13 +384,17 @@ __global__ void k_mp_xr(MixedArgs A) {
       if (tot[c] <= m->tol2[c] || m->iters[c] >= m->maxit || tot[c] < m->delta2 * m->rmax2[c] || restart) {
         upd |= 1 << c;
         if (restart) rst |= 1 << c;
+        m->cause[c][restart ? 2 : (tot[c] <= m->tol2[c] ? 0 : 1)] += 1;
       }
     }
     // an update's FP64 product streams the whole operator whichever components it serves, so the
     // components that are halfway (in norm) to their own trigger join it
-    if (upd)
+    if (upd && m->companions)
       for (int c = 0; c < 3; ++c)
-        if (((live & ~upd) >> c) & 1 && tot[c] < m->delta * m->rmax2[c]) upd |= 1 << c;
+        if (((live & ~upd) >> c) & 1 && tot[c] < m->delta * m->rmax2[c]) {
+          upd |= 1 << c;
+          m->cause[c][3] += 1;
+        }
     for (int c = 0; c < 3; ++c) {
       if (!(((live & ~upd) >> c) & 1)) continue;
       const double rho_new = tot[3 + c];
@@ -436,38 +440,45 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_residual(MixedArgs A) {
   if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[2] += 1;
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
-  for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
-    const int r = sl * kSellC + (threadIdx.x & 31);
-    const int i = A.S.perm[r];
-    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (i >= 0) {
-      double acc[3];
-      sell_spmv_row_active<3>(A.S, A.At64, A.xs, n, r, acc, upd);
-      const double w = A.cw ? A.cw[i] : 1.0;
+  with_mask<3>(upd, [&](auto mk) {
+    constexpr int MASK = decltype(mk)::value;
+    for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+      const int r = sl * kSellC + (threadIdx.x & 31);
+      const int i = A.S.perm[r];
+      double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      if (i >= 0) {
+        double acc[3];
+        sell_spmv_row<3, kU64, MASK>(A.S, A.At64, A.xs, n, r, acc);
+        const double w = A.cw ? A.cw[i] : 1.0;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (!((upd >> c) & 1)) continue;
-        const int64_t o = c * n + i;
-        const double ri = A.b[o] - acc[c];
-        A.r64[o] = ri;
-        const float rf = (float)ri;
-        A.r[o] = rf;
-        float r0 = A.r0[o];
-        if ((rst >> c) & 1) {
-          r0 = rf;
-          A.r0[o] = rf;
+        for (int c = 0; c < 3; ++c) {
+          if (!((MASK >> c) & 1)) continue;
+          const int64_t o = c * n + i;
+          const double ri = A.b[o] - acc[c];
+          A.r64[o] = ri;
+          const float rf = (float)ri;
+          A.r[o] = rf;
+          float r0 = A.r0[o];
+          if ((rst >> c) & 1) {
+            r0 = rf;
+            A.r0[o] = rf;
+          }
+          part[c] = (ri * ri) * w;
+          part[3 + c] = (double)r0 * (double)rf;
         }
-        part[c] = (ri * ri) * w;
-        part[3 + c] = (double)r0 * (double)rf;
       }
+      slice_partial<6>(part, A.S, sl);
     }
-    slice_partial<6>(part, A.S, sl);
-  }
+  });
   double tot[6];
   if (grid_reduce_runs<6>(A.S, A.red, tot) && threadIdx.x == 0) {
     MixedState *m = A.ms;
     for (int c = 0; c < 3; ++c) {
       if (!((upd >> c) & 1)) continue;
+      if (m->updates[c] < 16) {
+        m->hist[c][m->updates[c]][0] = m->rin2[c];
+        m->hist[c][m->updates[c]][1] = tot[c];
+      }
       m->updates[c] += 1;
       m->rnorm2[c] = tot[c];
       const double rho_new = tot[3 + c];
@@ -488,7 +499,7 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_residual(MixedArgs A) {
           m->beta[c] = (rho_new / m->rho[c]) * (m->alpha[c] / m->omega[c]);
           // the true residual is more than 10x (in norm) the FP32 recurrence's: its Krylov space
           // has drifted; the next iteration restarts it from the replaced residual
-          if (tot[c] > kMixedDrift2 * m->rin2[c]) m->restart_next |= 1 << c;
+          if (tot[c] > m->drift2 * m->rin2[c]) m->restart_next |= 1 << c;
         }
         m->rho[c] = rho_new;
         m->rin2[c] = tot[c];
