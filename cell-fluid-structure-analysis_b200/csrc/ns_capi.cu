@@ -202,9 +202,7 @@ struct cfsa_ns {
   // reliable-update trigger of the mixed-precision BiCGSTAB: the FP64 residual replaces the FP32
   // one when the latter has dropped by this factor since the previous update
   double mixed_delta = 1e-2;
-  bool mixed_if = true;  // reliable update behind an IF node (else its kernels run every iteration)
-  double mixed_drift2 = 100.0;  // true / iterated residual (squared) that restarts the FP32 space
-  bool mixed_companions = true;
+
   // discrete adjoint (ns_adjoint.cuh): transposed P1 slots, vertex -> (boundary face, local
   // index in the face's tet) incidence, host vertex coordinates for objective patches
   int *tpos1 = nullptr, *vbf_ptr = nullptr, *vbf = nullptr;
@@ -504,9 +502,7 @@ struct cfsa_ns {
     CK(cudaMallocHost(&h_pmx, sizeof(PMixState)));
     if (const char *e = std::getenv("CFSA_MIXED_P_TOL_IN")) mixed_p_tol_in = std::atof(e);
     if (const char *e = std::getenv("CFSA_MIXED_DELTA")) mixed_delta = std::atof(e);
-    if (const char *e = std::getenv("CFSA_MIXED_IF")) mixed_if = (std::atoi(e) != 0);
-    if (const char *e = std::getenv("CFSA_MIXED_DRIFT")) mixed_drift2 = std::atof(e);
-    if (const char *e = std::getenv("CFSA_MIXED_COMPANIONS")) mixed_companions = (std::atoi(e) != 0);
+
     bs_prof = dalloc<BicgState>(1);
     cs_prof = dalloc<CgState>(1);
     // boundary faces
@@ -1120,8 +1116,7 @@ struct cfsa_ns {
   void enqueue_momentum_mixed(bool capture, double *x, DevStatus *s_out) {
     const MixedArgs a = mixed_args(x, s_out);
     const unsigned int gp = blocks_for(N2);
-    k_mp_init<<<strided(k_mp_init, gp), kBlock, 0, stream>>>(a, tol_mom, maxit_mom, mixed_delta, mixed_drift2,
-                                                             mixed_companions ? 1 : 0);
+    k_mp_init<<<strided(k_mp_init, gp), kBlock, 0, stream>>>(a, tol_mom, maxit_mom, mixed_delta);
     CK(cudaGetLastError());
     auto update_body = [&](cudaStream_t s, MixedArgs b) {
       k_mp_xupdate<<<gp, kBlock, 0, s>>>(b);
@@ -1131,7 +1126,7 @@ struct cfsa_ns {
       MixedArgs b = a;
       b.cond = h;
       b.use_cond = use;
-      b.use_if = (use && mixed_if) ? 1 : 0;
+      b.use_if = use;
       if (b.use_if) b.cond_upd = new_cond_handle(s, 0);
       k_mp_p<<<gp, kBlock, 0, s>>>(b);
       k_mp_v<<<s2.nruns, kRunThreads, 0, s>>>(b);

@@ -24,6 +24,8 @@
 
 namespace cfsa {
 
+constexpr double kMixedDrift2 = 100.0;  // true / iterated residual (squared) that restarts the space
+
 struct MixedState {
   double bnorm2[3], tol2[3], rnorm2[3];  // FP64 criterion; rnorm2: true residual at the last update
   double rho[3], alpha[3], omega[3], beta[3], r0norm2[3];
@@ -37,14 +39,7 @@ struct MixedState {
   int force;         // components whose r0 . v vanished: update and restart at this iteration's end
   int maxit;
   double delta2;  // update trigger: rin2 < delta2 * rmax2
-  double delta;   // companions of a triggered update: rin2 < delta * rmax2 (halfway, in norm)
-  double drift2;  // true / iterated residual (squared) above which the Krylov space restarts
-  int companions; // components halfway to their trigger join an update
-  int drift_restarts[3];
-  // diagnostics of the last solve: updates by cause (tolerance, delta, restart, companion) and the
-  // iterated / true residual of the first updates of each component
-  int cause[3][4];
-  double hist[3][16][2];
+  int restarts[3];  // Krylov-space restarts (drift or a growing true residual)
 };
 
 struct MixedArgs {
@@ -108,7 +103,7 @@ __device__ __forceinline__ void sell_spmv_row_f32x3(const SellView &S, const flo
 
 // Init (after k_momentum_rhs wrote b and x = 0): r = r0 = (float) b, p = v = dx = 0;
 // FP64 ||b|| in the convergence norm, rho = r0 . r.
-__global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta, double drift2, int companions) {
+__global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta) {
   if (A.st->halt) return;
   const int64_t n = A.n;
   __shared__ WarpSums<6> S;
@@ -145,11 +140,6 @@ __global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta, doub
     m->force = 0;
     m->maxit = maxit;
     m->delta2 = delta * delta;
-    m->delta = delta;
-    m->drift2 = drift2;
-    m->companions = companions;
-    for (int c = 0; c < 3; ++c)
-      for (int q = 0; q < 4; ++q) m->cause[c][q] = 0;
     for (int c = 0; c < 3; ++c) {
       m->bnorm2[c] = tot[c];
       m->rnorm2[c] = tot[c];
@@ -162,7 +152,7 @@ __global__ void k_mp_init(MixedArgs A, double tol, int maxit, double delta, doub
       m->beta[c] = 0.0;
       m->iters[c] = 0;
       m->updates[c] = 0;
-      m->drift_restarts[c] = 0;
+      m->restarts[c] = 0;
       if (isnan(tot[c]) || isnan(tot[3 + c])) {
         m->status[c] = KS_BREAKDOWN;
       } else if (tot[c] == 0.0 || tot[c] <= m->tol2[c]) {
@@ -214,7 +204,7 @@ __global__ void k_mp_p(MixedArgs A) {
       if ((rs >> c) & 1) {
         m->rho[c] = tot[c];
         m->r0norm2[c] = tot[c];
-        m->drift_restarts[c] += 1;
+        m->restarts[c] += 1;
       }
     m->restart_next = 0;
   }
@@ -384,17 +374,11 @@ __global__ void k_mp_xr(MixedArgs A) {
       if (tot[c] <= m->tol2[c] || m->iters[c] >= m->maxit || tot[c] < m->delta2 * m->rmax2[c] || restart) {
         upd |= 1 << c;
         if (restart) rst |= 1 << c;
-        m->cause[c][restart ? 2 : (tot[c] <= m->tol2[c] ? 0 : 1)] += 1;
       }
     }
-    // an update's FP64 product streams the whole operator whichever components it serves, so the
-    // components that are halfway (in norm) to their own trigger join it
-    if (upd && m->companions)
-      for (int c = 0; c < 3; ++c)
-        if (((live & ~upd) >> c) & 1 && tot[c] < m->delta * m->rmax2[c]) {
-          upd |= 1 << c;
-          m->cause[c][3] += 1;
-        }
+    // Components update on their own triggers only: replacing a residual before it has dropped by
+    // delta perturbs BiCGSTAB's recurrences, and on the 4M-tet Y-bifurcation updates brought
+    // forward to share one FP64 product made the iteration erratic until it hit the cap.
     for (int c = 0; c < 3; ++c) {
       if (!(((live & ~upd) >> c) & 1)) continue;
       const double rho_new = tot[3 + c];
@@ -475,11 +459,8 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_residual(MixedArgs A) {
     MixedState *m = A.ms;
     for (int c = 0; c < 3; ++c) {
       if (!((upd >> c) & 1)) continue;
-      if (m->updates[c] < 16) {
-        m->hist[c][m->updates[c]][0] = m->rin2[c];
-        m->hist[c][m->updates[c]][1] = tot[c];
-      }
       m->updates[c] += 1;
+      const double prev2 = m->rnorm2[c];  // true residual at the previous update
       m->rnorm2[c] = tot[c];
       const double rho_new = tot[3 + c];
       if (isnan(tot[c]) || isnan(rho_new)) {
@@ -497,9 +478,10 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_residual(MixedArgs A) {
           m->beta[c] = 0.0;
         } else {
           m->beta[c] = (rho_new / m->rho[c]) * (m->alpha[c] / m->omega[c]);
-          // the true residual is more than 10x (in norm) the FP32 recurrence's: its Krylov space
-          // has drifted; the next iteration restarts it from the replaced residual
-          if (tot[c] > m->drift2 * m->rin2[c]) m->restart_next |= 1 << c;
+          // the true residual is more than 10x (in norm) the FP32 recurrence's (its Krylov space
+          // has drifted), or it grew since the previous update (erratic convergence): the next
+          // iteration restarts the space from the replaced residual
+          if (tot[c] > kMixedDrift2 * m->rin2[c] || tot[c] > prev2) m->restart_next |= 1 << c;
         }
         m->rho[c] = rho_new;
         m->rin2[c] = tot[c];
