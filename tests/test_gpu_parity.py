@@ -620,3 +620,19 @@ def test_headline_config_parity_1m_tets(cf, po):
         eu, ep = rel_l2(s.getVelocity(), st["u"]), rel_l2(s.getPressure(), st["p"])
         print(f"1M tets step {k + 1}: rel L2 u {eu:.2e} p {ep:.2e}")
         assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"])
+
+
+def test_profile_kernel_leaves_the_solver_state(cf, po):
+    """cfsa_ns_profile_kernel (momentum product, pressure product, whole pressure solve) runs on
+    scratch buffers: the fields are unchanged and the next step is still bit-exact with the oracle."""
+    m = make_mesh(cf, 3, 12)
+    s, o = make_pair(cf, po, m, tol=1e-12, krylov=cf.KRYLOV_CG2L)
+    assert s.pisoStep() and o.piso_step() == 0
+    u, p = s.getVelocity().copy(), s.getPressure().copy()
+    for which in (cf.KERNEL_MOMENTUM_SPMV, cf.KERNEL_PRESSURE_SPMV, cf.KERNEL_PRESSURE_SOLVE):
+        ms, by = s.profileKernel(which, 3)
+        assert ms > 0.0 and by > 0.0, which
+    assert np.array_equal(s.getVelocity(), u) and np.array_equal(s.getPressure(), p)
+    assert s.pisoStep() and o.piso_step() == 0
+    st = o.state()
+    assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"])
