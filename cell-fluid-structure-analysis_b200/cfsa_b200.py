@@ -24,7 +24,7 @@ LIB_PATH = _HERE / "lib" / "libcfsa.so"
 OK, NOT_CONVERGED, BREAKDOWN, NAN, CUDA_ERROR, BAD_ARG, NOT_INITIALIZED, UNSUPPORTED = range(8)
 
 MAT_MASS, MAT_STIFFNESS, MAT_GRAD_X, MAT_GRAD_Y, MAT_GRAD_Z, MAT_POISSON, MAT_MOMENTUM, MAT_POISSON_BC = range(8)
-KERNEL_MOMENTUM_SPMV, KERNEL_PRESSURE_SPMV, KERNEL_PRESSURE_SOLVE = 0, 1, 2
+KERNEL_MOMENTUM_SPMV, KERNEL_PRESSURE_SPMV, KERNEL_PRESSURE_SOLVE, KERNEL_MOMENTUM_SPMV_F32 = 0, 1, 2, 3
 KRYLOV_CG, KRYLOV_BICGSTAB, KRYLOV_CG1, KRYLOV_CG2L = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED, PRECISION_MIXED_FULL = 0, 1, 2
 NORM_REFERENCE, NORM_JACOBI = 0, 1

@@ -160,6 +160,7 @@ struct cfsa_ns {
   bool h_inlet_stale = false;  // h_inlet behind the device inlet (set from a device-side split)
   BicgState *bs_prof = nullptr;
   CgState *cs_prof = nullptr;
+  MixedState *ms_prof = nullptr;
   // persistent CG
   bool cg_persistent = true;
   int cg_grid = 0;
@@ -505,6 +506,7 @@ struct cfsa_ns {
 
     bs_prof = dalloc<BicgState>(1);
     cs_prof = dalloc<CgState>(1);
+    ms_prof = dalloc<MixedState>(1);
     // boundary faces
     nbf = m->nbf;
     if (nbf > 0) {
@@ -2141,9 +2143,24 @@ struct cfsa_ns {
 
   // Kernel timing on the live data with private Krylov states (solver state untouched).
   void profile_kernel(int which, int iters, double *avg_ms, double *alg_bytes) {
+    NvtxRange nvtx_("cfsa profile kernel");  // lets a profiler select these launches
     ensure_operators();
     CK(cudaStreamSynchronize(stream));
-    if (which == CFSA_KERNEL_MOMENTUM_SPMV) {
+    if (which == CFSA_KERNEL_MOMENTUM_SPMV_F32) {
+      MixedState hm{};
+      hm.active = 7;
+      CK(cudaMemcpyAsync(ms_prof, &hm, sizeof(hm), cudaMemcpyHostToDevice, stream));
+      MixedArgs a = mixed_args(ustar, nullptr);
+      a.ms = ms_prof;
+      a.p = fr;   // the FP32 Krylov vectors of the last mixed solve (any values serve the timing)
+      a.r0 = fr0;
+      a.v = ft;   // scratch output
+      k_mp_v<<<s2.nruns, kRunThreads, 0, stream>>>(a);  // warm-up
+      CK(cudaEventRecord(ev0, stream));
+      for (int k = 0; k < iters; ++k) k_mp_v<<<s2.nruns, kRunThreads, 0, stream>>>(a);
+      CK(cudaEventRecord(ev1, stream));
+      *alg_bytes = 8.0 * (double)nnz2 + 8.0 * s2.nrows_pad + 4.0 * (s2.nslices + 1) + 36.0 * (double)N2;
+    } else if (which == CFSA_KERNEL_MOMENTUM_SPMV) {
       BicgState hs{};
       hs.active = 7;
       hs.ncomp = 3;

@@ -131,6 +131,8 @@ typedef struct {
  * product and vector updates inside one kernel: avg_ms per solve, alg_bytes = iterations x bytes
  * per iteration (operator, row metadata, each vector read or written once, coarse inverse) */
 #define CFSA_KERNEL_PRESSURE_SOLVE 2
+/* the FP32 3-right-hand-side product of the mixed-precision momentum solve */
+#define CFSA_KERNEL_MOMENTUM_SPMV_F32 3
 
 /* NavierStokesSolver::initialize (include/FEM/NavierStokes.hpp:91-92; NavierStokes.cpp:10-68):
  * uploads the mesh, builds the CSR patterns, assembles M, K, G, L on the device and zeroes the

@@ -629,7 +629,8 @@ def test_profile_kernel_leaves_the_solver_state(cf, po):
     s, o = make_pair(cf, po, m, tol=1e-12, krylov=cf.KRYLOV_CG2L)
     assert s.pisoStep() and o.piso_step() == 0
     u, p = s.getVelocity().copy(), s.getPressure().copy()
-    for which in (cf.KERNEL_MOMENTUM_SPMV, cf.KERNEL_PRESSURE_SPMV, cf.KERNEL_PRESSURE_SOLVE):
+    for which in (cf.KERNEL_MOMENTUM_SPMV, cf.KERNEL_PRESSURE_SPMV, cf.KERNEL_PRESSURE_SOLVE,
+                  cf.KERNEL_MOMENTUM_SPMV_F32):
         ms, by = s.profileKernel(which, 3)
         assert ms > 0.0 and by > 0.0, which
     assert np.array_equal(s.getVelocity(), u) and np.array_equal(s.getPressure(), p)
