@@ -252,6 +252,23 @@ constexpr int kRunThreads = 1024;
 constexpr int kRunWarps = kRunThreads / 32;
 constexpr int kSlicesPerBlock = kBlock / kSellC;
 
+// Slice scheduling inside a run: warp w starts with slice s0 + w and then takes the next slice
+// nobody has claimed from a shared-memory counter. A static stride (w, w + 32, ...) gave a warp
+// the same position in every 256-row window (rows are sorted by length inside a window, so warps
+// 0, 8, 16, 24 always got the longest rows) and left the other warps waiting at the run's closing
+// barrier (ncu, 415k tets: 7.8 barrier stalls per issued instruction). Which warp computes a slice
+// does not matter for the results: each slice's sums go to its own slot of spart.
+__device__ __forceinline__ int run_first_slice(int *next, int s0) {
+  if (threadIdx.x == 0) *next = s0 + (int)(blockDim.x >> 5);
+  __syncthreads();
+  return s0 + (int)(threadIdx.x >> 5);
+}
+__device__ __forceinline__ int run_next_slice(int *next) {
+  int v = 0;
+  if ((threadIdx.x & 31) == 0) v = atomicAdd(next, 1);
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
 template <int NV>
 __device__ __forceinline__ void slice_partial(const double (&v)[NV], const SellView &S, int sl) {
 #pragma unroll

@@ -726,9 +726,11 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_bicg_v(BicgArgs A) {
   if (!active) return;
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
+  __shared__ int s_next;
+  const int sl0 = run_first_slice(&s_next, A.S.rfirst[blockIdx.x]);
   with_mask<NC>(active, [&](auto mk) {
     constexpr int MASK = decltype(mk)::value;
-    for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+    for (int sl = sl0; sl < s1; sl = run_next_slice(&s_next)) {
       const int r = sl * kSellC + (threadIdx.x & 31);
       const int i = A.S.perm[r];
       double part[NC];
@@ -788,9 +790,11 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_bicg_t(BicgArgs A) {
   if (!active) return;
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
+  __shared__ int s_next;
+  const int sl0 = run_first_slice(&s_next, A.S.rfirst[blockIdx.x]);
   with_mask<NC>(active, [&](auto mk) {
     constexpr int MASK = decltype(mk)::value;
-    for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+    for (int sl = sl0; sl < s1; sl = run_next_slice(&s_next)) {
       const int r = sl * kSellC + (threadIdx.x & 31);
       const int i = A.S.perm[r];
       double part[2 * NC];

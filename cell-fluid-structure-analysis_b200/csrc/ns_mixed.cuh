@@ -216,9 +216,11 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_v(MixedArgs A) {
   if (!act) return;
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
+  __shared__ int s_next;
+  const int sl0 = run_first_slice(&s_next, A.S.rfirst[blockIdx.x]);
   with_mask<3>(act, [&](auto mk) {
     constexpr int MASK = decltype(mk)::value;
-    for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+    for (int sl = sl0; sl < s1; sl = run_next_slice(&s_next)) {
       const int r = sl * kSellC + (threadIdx.x & 31);
       const int i = A.S.perm[r];
       double part[3] = {0.0, 0.0, 0.0};
@@ -277,9 +279,11 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_t(MixedArgs A) {
   if (!act) return;
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
+  __shared__ int s_next;
+  const int sl0 = run_first_slice(&s_next, A.S.rfirst[blockIdx.x]);
   with_mask<3>(act, [&](auto mk) {
     constexpr int MASK = decltype(mk)::value;
-    for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+    for (int sl = sl0; sl < s1; sl = run_next_slice(&s_next)) {
       const int r = sl * kSellC + (threadIdx.x & 31);
       const int i = A.S.perm[r];
       double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -424,9 +428,11 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_mp_residual(MixedArgs A) {
   if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[2] += 1;
   const int64_t n = A.n;
   const int s1 = A.S.rfirst[blockIdx.x + 1];
+  __shared__ int s_next;
+  const int sl0 = run_first_slice(&s_next, A.S.rfirst[blockIdx.x]);
   with_mask<3>(upd, [&](auto mk) {
     constexpr int MASK = decltype(mk)::value;
-    for (int sl = A.S.rfirst[blockIdx.x] + (threadIdx.x >> 5); sl < s1; sl += kRunWarps) {
+    for (int sl = sl0; sl < s1; sl = run_next_slice(&s_next)) {
       const int r = sl * kSellC + (threadIdx.x & 31);
       const int i = A.S.perm[r];
       double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
