@@ -203,7 +203,6 @@ struct cfsa_ns {
   // reliable-update trigger of the mixed-precision BiCGSTAB: the FP64 residual replaces the FP32
   // one when the latter has dropped by this factor since the previous update
   double mixed_delta = 1e-2;
-  int loop_unroll = 1;  // iterations per WHILE-body launch of the momentum Krylov loop
 
   // discrete adjoint (ns_adjoint.cuh): transposed P1 slots, vertex -> (boundary face, local
   // index in the face's tet) incidence, host vertex coordinates for objective patches
@@ -504,7 +503,6 @@ struct cfsa_ns {
     CK(cudaMallocHost(&h_pmx, sizeof(PMixState)));
     if (const char *e = std::getenv("CFSA_MIXED_P_TOL_IN")) mixed_p_tol_in = std::atof(e);
     if (const char *e = std::getenv("CFSA_MIXED_DELTA")) mixed_delta = std::atof(e);
-    if (const char *e = std::getenv("CFSA_LOOP_UNROLL")) loop_unroll = std::max(1, std::min(4, std::atoi(e)));
 
     bs_prof = dalloc<BicgState>(1);
     cs_prof = dalloc<CgState>(1);
@@ -1076,7 +1074,7 @@ struct cfsa_ns {
       BicgArgs b = a;
       b.cond = h;
       b.use_cond = use;
-      for (int k = 0; k < (use ? loop_unroll : 1); ++k) bicg_body<3>(b, s, s2, (int)N2);
+      bicg_body<3>(b, s, s2, (int)N2);
     };
     if (capture)
       capture_while(body);
