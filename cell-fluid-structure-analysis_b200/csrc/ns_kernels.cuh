@@ -443,9 +443,11 @@ __global__ void k_gather_div(int nv, const int *__restrict__ adj_ptr, const int 
 
 // One SELL row, NC right-hand sides sharing the matrix. Entries are fetched in chunks of U
 // (all column indices and values of a chunk first, then the U*NC gathers) so that many loads are
-// in flight per thread; the products are still accumulated in ascending column order, so the
-// result is bit-identical to the sequential CSR row sum. Matrix entries are streamed once per
-// product (evict-first), the gathered vector stays cacheable.
+// in flight per thread. The last len % U entries form one predicated chunk, so a row costs
+// ceil(len / U) dependent round trips (index and value, then gather) instead of one per leftover
+// entry: 82% of the P2 momentum rows have len % 4 == 3. The products are still accumulated in
+// ascending column order, so the result is bit-identical to the sequential CSR row sum. Matrix
+// entries are streamed once per product (evict-first), the gathered vector stays cacheable.
 template <int NC, int U = 8, int MASK = (1 << NC) - 1>
 __device__ __forceinline__ void sell_spmv_row(const SellView &S, const double *__restrict__ val,
                                               const double *__restrict__ x, int64_t n, int r,
@@ -475,13 +477,27 @@ __device__ __forceinline__ void sell_spmv_row(const SellView &S, const double *_
       for (int c = 0; c < NC; ++c)
         if ((MASK >> c) & 1) acc[c] += a[u] * xv[u][c];
   }
-  for (; k < len; ++k) {
-    const int pos = base + k * kSellC;
-    const int j = __ldcs(S.col + pos);
-    const double a = __ldcs(val + pos);
+  if (k < len) {  // the last len % U entries as one predicated chunk: one memory round trip
+    int j[U];
+    double a[U];
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
-      if ((MASK >> c) & 1) acc[c] += a * __ldg(x + c * n + j);
+    for (int u = 0; u < U; ++u) {
+      const int pos = base + (k + u) * kSellC;
+      const bool in = k + u < len;
+      j[u] = in ? __ldcs(S.col + pos) : 0;
+      a[u] = in ? __ldcs(val + pos) : 0.0;
+    }
+    double xv[U][NC];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        if ((MASK >> c) & 1) xv[u][c] = (k + u < len) ? __ldg(x + c * n + j[u]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        if (((MASK >> c) & 1) && k + u < len) acc[c] += a[u] * xv[u][c];
   }
 }
 
@@ -1269,7 +1285,7 @@ struct CgPersistentArgs {
 // a variant that stores p in a third phase behind one more grid barrier).
 constexpr int kCgChunk = 4;
 
-__global__ void __launch_bounds__(kBlock, 5) k_cg_persistent(CgPersistentArgs A) {
+__global__ void __launch_bounds__(kBlock, 4) k_cg_persistent(CgPersistentArgs A) {
   if (A.st && A.st->halt) return;
   if (!A.cs->active) return;
   const double tol2 = A.cs->tol2;
@@ -1307,12 +1323,25 @@ __global__ void __launch_bounds__(kBlock, 5) k_cg_persistent(CgPersistentArgs A)
 #pragma unroll
           for (int u = 0; u < kCgChunk; ++u) acc += a[u] * (fly ? zz[u] + beta * po[u] : po[u]);
         }
-        for (; k < len; ++k) {
-          const int pos = base + k * kSellC;
-          const int jj = __ldg(A.S.col + pos);
-          const double a = __ldg(A.Ls + pos);
-          const double pj = fly ? __ldcg(A.z + jj) + beta * __ldcg(pold + jj) : __ldcg(pold + jj);
-          acc += a * pj;
+        if (k < len) {  // the last len % kCgChunk entries as one predicated chunk
+          int jj[kCgChunk];
+          double a[kCgChunk], po[kCgChunk], zz[kCgChunk];
+#pragma unroll
+          for (int u = 0; u < kCgChunk; ++u) {
+            const int pos = base + (k + u) * kSellC;
+            const bool in = k + u < len;
+            jj[u] = in ? __ldg(A.S.col + pos) : 0;
+            a[u] = in ? __ldg(A.Ls + pos) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kCgChunk; ++u) {
+            const bool in = k + u < len;
+            po[u] = in ? __ldcg(pold + jj[u]) : 0.0;
+            zz[u] = (in && fly) ? __ldcg(A.z + jj[u]) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kCgChunk; ++u)
+            if (k + u < len) acc += a[u] * (fly ? zz[u] + beta * po[u] : po[u]);
         }
         const double pi = fly ? __ldcg(A.z + i) + beta * __ldcg(pold + i) : __ldcg(pold + i);
         __stcg(pnew + i, pi);
@@ -1524,12 +1553,25 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg_resident(CgResidentArgs
 #pragma unroll
           for (int u = 0; u < kCgChunk; ++u) acc += a[u] * (fly ? zz[u] + beta * po[u] : po[u]);
         }
-        for (; k < len; ++k) {
-          const int pos = base + k * kSellC;
-          const int jj = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
-          const double a = __ldg(A.Ls + pos);
-          const double pj = fly ? __ldcg(A.z + jj) + beta * __ldcg(pold + jj) : __ldcg(pold + jj);
-          acc += a * pj;
+        if (k < len) {  // the last len % kCgChunk entries as one predicated chunk
+          int jj[kCgChunk];
+          double a[kCgChunk], po[kCgChunk], zz[kCgChunk];
+#pragma unroll
+          for (int u = 0; u < kCgChunk; ++u) {
+            const int pos = base + (k + u) * kSellC;
+            const bool in = k + u < len;
+            jj[u] = !in ? 0 : staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+            a[u] = in ? __ldg(A.Ls + pos) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kCgChunk; ++u) {
+            const bool in = k + u < len;
+            po[u] = in ? __ldcg(pold + jj[u]) : 0.0;
+            zz[u] = (in && fly) ? __ldcg(A.z + jj[u]) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kCgChunk; ++u)
+            if (k + u < len) acc += a[u] * (fly ? zz[u] + beta * po[u] : po[u]);
         }
         const double pi = fly ? __ldcg(A.z + i) + beta * __ldcg(pold + i) : __ldcg(pold + i);
         __stcg(pnew + i, pi);
@@ -1710,12 +1752,30 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg1_resident(Cg1Args C) {
             acc += a[q] * (mm[q] * rj);
           }
         }
-        for (; k < len; ++k) {
-          const int pos = base + k * kSellC;
-          const int jj = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
-          const double sj = __ldcg(wo + jj) + beta * __ldcg(so + jj);
-          const double rj = __ldcg(ro + jj) - alpha * sj;
-          acc += __ldg(A.Ls + pos) * (__ldg(A.invL + jj) * rj);
+        if (k < len) {  // the last len % kCgChunk entries as one predicated chunk
+          int jj[kCgChunk];
+          double a[kCgChunk], rr_[kCgChunk], ww[kCgChunk], ss[kCgChunk], mm[kCgChunk];
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            const int pos = base + (k + q) * kSellC;
+            const bool in = k + q < len;
+            jj[q] = !in ? 0 : staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+            a[q] = in ? __ldg(A.Ls + pos) : 0.0;
+          }
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            const bool in = k + q < len;
+            rr_[q] = in ? __ldcg(ro + jj[q]) : 0.0;
+            ww[q] = in ? __ldcg(wo + jj[q]) : 0.0;
+            ss[q] = in ? __ldcg(so + jj[q]) : 0.0;
+            mm[q] = in ? __ldg(A.invL + jj[q]) : 0.0;
+          }
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            const double sj = ww[q] + beta * ss[q];
+            const double rj = rr_[q] - alpha * sj;
+            if (k + q < len) acc += a[q] * (mm[q] * rj);
+          }
         }
         // own row
         const double mi = __ldg(A.invL + i);
@@ -2126,12 +2186,31 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
             acc += a[q] * (mm[q] * rj + cnew[aj[q]]);
           }
         }
-        for (; k < len; ++k) {
-          const int pos = base + k * kSellC;
-          const int jj = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
-          const double sj = (double)__ldcg(wo + jj) + beta * (double)__ldcg(so + jj);
-          const double rj = (double)__ldcg(ro + jj) - alpha * sj;
-          acc += (double)__ldg(Lsv + pos) * ((double)__ldg(invLv + jj) * rj + cnew[__ldg(V.agg + jj)]);
+        if (k < len) {  // the last len % kCgChunk entries as one predicated chunk
+          int jj[kCgChunk], aj[kCgChunk];
+          double a[kCgChunk], rr_[kCgChunk], ww[kCgChunk], ss[kCgChunk], mm[kCgChunk];
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            const int pos = base + (k + q) * kSellC;
+            const bool in = k + q < len;
+            jj[q] = !in ? 0 : staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+            a[q] = in ? (double)__ldg(Lsv + pos) : 0.0;
+          }
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            const bool in = k + q < len;
+            rr_[q] = in ? (double)__ldcg(ro + jj[q]) : 0.0;
+            ww[q] = in ? (double)__ldcg(wo + jj[q]) : 0.0;
+            ss[q] = in ? (double)__ldcg(so + jj[q]) : 0.0;
+            mm[q] = in ? (double)__ldg(invLv + jj[q]) : 0.0;
+            aj[q] = in ? __ldg(V.agg + jj[q]) : 0;
+          }
+#pragma unroll
+          for (int q = 0; q < kCgChunk; ++q) {
+            const double sj = ww[q] + beta * ss[q];
+            const double rj = rr_[q] - alpha * sj;
+            if (k + q < len) acc += a[q] * (mm[q] * rj + cnew[aj[q]]);
+          }
         }
         acc = rnd(acc);
         // own row

@@ -90,13 +90,27 @@ __device__ __forceinline__ void sell_spmv_row_f32x3(const SellView &S, const flo
       for (int c = 0; c < 3; ++c)
         if ((MASK >> c) & 1) acc[c] += a[u] * xv[u][c];
   }
-  for (; k < len; ++k) {
-    const int pos = base + k * kSellC;
-    const int j = __ldcs(S.col + pos);
-    const float a = __ldcs(val + pos);
+  if (k < len) {  // the last len % U entries as one predicated chunk: one memory round trip
+    int j[U];
+    float a[U];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-      if ((MASK >> c) & 1) acc[c] += a * __ldg(x + c * n + j);
+    for (int u = 0; u < U; ++u) {
+      const int pos = base + (k + u) * kSellC;
+      const bool in = k + u < len;
+      j[u] = in ? __ldcs(S.col + pos) : 0;
+      a[u] = in ? __ldcs(val + pos) : 0.f;
+    }
+    float xv[U][3];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        if ((MASK >> c) & 1) xv[u][c] = (k + u < len) ? __ldg(x + c * n + j[u]) : 0.f;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        if (((MASK >> c) & 1) && k + u < len) acc[c] += a[u] * xv[u][c];
   }
 }
 
