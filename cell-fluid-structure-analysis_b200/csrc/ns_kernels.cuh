@@ -1452,37 +1452,43 @@ __device__ __forceinline__ void group_partial(double (&v)[NV], double *__restric
   group_sync(g);
 }
 
-// tree_total for a 1024-thread CTA: the first 256 threads form the 256 accumulators.
+// tree_total for a 1024-thread CTA: the 256-thread quarter j forms the 256 accumulators of value
+// j (same sums in the same order as tree_total), so the values are reduced side by side with eight
+// loads in flight per thread instead of one value after another.
 template <int NV>
 __device__ __forceinline__ void tree_total_cta(const double *__restrict__ partials, int nblk,
                                                double (&out)[NV], double (*sm)[kBlock / 32]) {
+  static_assert(NV * kBlock <= kCgResThreads, "one 256-thread quarter per value");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x < kBlock) {
+  const int j = threadIdx.x / kBlock, t = threadIdx.x & (kBlock - 1);
+  if (j < NV) {
+    // accumulator t of value j: blocks t, t + 256, ... in order, eight loads in flight
+    constexpr int kB = 8;
+    double s = 0.0;
+    int b = t;
+    for (; b + (kB - 1) * kBlock < nblk; b += kB * kBlock) {
+      double v[kB];
 #pragma unroll
-    for (int j = 0; j < NV; ++j) {
-      double s = 0.0;
-      int b = threadIdx.x;
-      for (; b + 3 * kBlock < nblk; b += 4 * kBlock) {
-        const double v0 = __ldcg(&partials[(size_t)b * kMaxRed + j]);
-        const double v1 = __ldcg(&partials[(size_t)(b + kBlock) * kMaxRed + j]);
-        const double v2 = __ldcg(&partials[(size_t)(b + 2 * kBlock) * kMaxRed + j]);
-        const double v3 = __ldcg(&partials[(size_t)(b + 3 * kBlock) * kMaxRed + j]);
-        s += v0;
-        s += v1;
-        s += v2;
-        s += v3;
-      }
-      for (; b < nblk; b += kBlock) s += __ldcg(&partials[(size_t)b * kMaxRed + j]);
-      s = warp_sum(s);
-      if (lane == 0) sm[j][warp] = s;
+      for (int q = 0; q < kB; ++q) v[q] = __ldcg(&partials[(size_t)(b + q * kBlock) * kMaxRed + j]);
+#pragma unroll
+      for (int q = 0; q < kB; ++q) s += v[q];
     }
+    double v[kB];
+#pragma unroll
+    for (int q = 0; q < kB; ++q)
+      v[q] = (b + q * kBlock < nblk) ? __ldcg(&partials[(size_t)(b + q * kBlock) * kMaxRed + j]) : 0.0;
+#pragma unroll
+    for (int q = 0; q < kB; ++q)
+      if (b + q * kBlock < nblk) s += v[q];
+    s = warp_sum(s);
+    if (lane == 0) sm[j][warp & (kBlock / 32 - 1)] = s;
   }
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < NV; ++j) {
+  for (int j2 = 0; j2 < NV; ++j2) {
     double s = 0.0;
-    for (int w = 0; w < kBlock / 32; ++w) s += sm[j][w];
-    out[j] = s;
+    for (int w = 0; w < kBlock / 32; ++w) s += sm[j2][w];
+    out[j2] = s;
   }
   __syncthreads();
 }
@@ -1914,43 +1920,54 @@ __device__ __forceinline__ double unfixed128(unsigned long long lo, unsigned lon
   return ((double)(long long)hi * 0x1p64 + (double)lo) * iscale;
 }
 
-// Sums of this CTA's staged values per own aggregate into global buffer `buf`: one warp per
-// aggregate segment. Each lane adds its values exactly as 128-bit integers offset by 2^100 (so
-// that they are non-negative); the lane sums are cut into five 26-bit limbs, each limb summed by a
-// warp reduction (32 x 2^26 < 2^32), and lane 0 re-assembles the total, removes count x 2^100 and
-// adds it to the global accumulator.
+// Sums of this CTA's staged values per own aggregate into global buffer `buf`. Each own
+// aggregate's segment of the staging is cut into pieces of kSegPiece positions, and the warps
+// take the pieces of all segments round robin, so a CTA whose rows fall into a few large
+// aggregates still spreads the work over all its warps. Each lane adds its values exactly as
+// 128-bit integers offset by 2^100 (so that they are non-negative); the lane sums are cut into five
+// 26-bit limbs, each limb summed by a warp reduction (32 x 2^26 < 2^32), and lane 0 re-assembles
+// the piece's total, removes count x 2^100 and adds it to the global accumulator. The sums are
+// exact, so how a segment is cut does not change the result.
+constexpr int kSegPiece = 64;
+
 template <int NV>
 __device__ __forceinline__ void seg_sums(const CoarseView &V, const double *__restrict__ stage,
                                          int buf, const int (&vi)[NV], double scale) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int q0 = __ldg(V.own_ptr + blockIdx.x), q1 = __ldg(V.own_ptr + blockIdx.x + 1);
-  for (int q = q0 + warp; q < q1; q += nw) {
+  int item = 0;  // pieces of the segments before q
+  for (int q = q0; q < q1; ++q) {
     const int p0 = __ldg(V.seg_lo + q), p1 = __ldg(V.seg_hi + q), m = __ldg(V.own + q);
+    const int np = (p1 - p0 + kSegPiece - 1) / kSegPiece;
+    for (int k = ((warp - item) % nw + nw) % nw; k < np; k += nw) {
+      const int a0 = p0 + k * kSegPiece, a1 = min(p1, a0 + kSegPiece);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      const double *sv = stage + (size_t)v * V.npos_max;
-      unsigned long long al = 0ull, ah = 0ull;
-      for (int p = p0 + lane; p < p1; p += 32) {
-        unsigned long long l, h;
-        fixed128(sv[p], scale, l, h);
-        h += 1ull << 36;  // + 2^100
-        al += l;
-        ah += h + ((al < l) ? 1ull : 0ull);
-      }
-      const unsigned m26 = (1u << 26) - 1u;
-      const unsigned long long s0 = __reduce_add_sync(0xffffffffu, (unsigned)(al & m26));
-      const unsigned long long s1 = __reduce_add_sync(0xffffffffu, (unsigned)((al >> 26) & m26));
-      const unsigned long long s2 = __reduce_add_sync(0xffffffffu, (unsigned)(((al >> 52) | (ah << 12)) & m26));
-      const unsigned long long s3 = __reduce_add_sync(0xffffffffu, (unsigned)((ah >> 14) & m26));
-      const unsigned long long s4 = __reduce_add_sync(0xffffffffu, (unsigned)((ah >> 40) & m26));
-      if (lane == 0) {
-        const unsigned long long l1 = s0 + (s1 << 26);
-        const unsigned long long l2 = l1 + (s2 << 52);
-        const unsigned long long h = (s2 >> 12) + (s3 << 14) + (s4 << 40) + ((l2 < l1) ? 1ull : 0ull) -
-                                     ((unsigned long long)(p1 - p0) << 36);
-        add128(V.gacc + 2 * ((size_t)(3 * buf + vi[v]) * V.nc + m), l2, h);
+      for (int v = 0; v < NV; ++v) {
+        const double *sv = stage + (size_t)v * V.npos_max;
+        unsigned long long al = 0ull, ah = 0ull;
+        for (int p = a0 + lane; p < a1; p += 32) {
+          unsigned long long l, h;
+          fixed128(sv[p], scale, l, h);
+          h += 1ull << 36;  // + 2^100
+          al += l;
+          ah += h + ((al < l) ? 1ull : 0ull);
+        }
+        const unsigned m26 = (1u << 26) - 1u;
+        const unsigned long long s0 = __reduce_add_sync(0xffffffffu, (unsigned)(al & m26));
+        const unsigned long long s1 = __reduce_add_sync(0xffffffffu, (unsigned)((al >> 26) & m26));
+        const unsigned long long s2 = __reduce_add_sync(0xffffffffu, (unsigned)(((al >> 52) | (ah << 12)) & m26));
+        const unsigned long long s3 = __reduce_add_sync(0xffffffffu, (unsigned)((ah >> 14) & m26));
+        const unsigned long long s4 = __reduce_add_sync(0xffffffffu, (unsigned)((ah >> 40) & m26));
+        if (lane == 0) {
+          const unsigned long long l1 = s0 + (s1 << 26);
+          const unsigned long long l2 = l1 + (s2 << 52);
+          const unsigned long long h = (s2 >> 12) + (s3 << 14) + (s4 << 40) + ((l2 < l1) ? 1ull : 0ull) -
+                                       ((unsigned long long)(a1 - a0) << 36);
+          add128(V.gacc + 2 * ((size_t)(3 * buf + vi[v]) * V.nc + m), l2, h);
+        }
       }
     }
+    item += np;
   }
 }
 
@@ -1972,9 +1989,9 @@ __device__ __forceinline__ void read_sums(const CoarseView &V, int buf, int v0, 
 }
 
 // c[m] = Z[m] . t for the aggregates this CTA reads: one warp per aggregate, lane l adding
-// k = l, l + 32, ... in order, then a warp butterfly.
-constexpr int kZBatch = 8;
-
+// k = l, l + 32, ... in order, then a warp butterfly. ZB entries of the Z row are loaded per lane
+// at a time (16: one round trip for up to 512 aggregates); the batch does not change the sums.
+template <int ZB>
 __device__ __forceinline__ void coarse_values(const CoarseView &V, const double *__restrict__ t,
                                               double *__restrict__ c) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -1984,12 +2001,12 @@ __device__ __forceinline__ void coarse_values(const CoarseView &V, const double 
     const int m = __ldg(V.need + q);
     const double *zr = V.Z + (size_t)m * nc;
     double sum = 0.0;
-    for (int k0 = lane; k0 < nc; k0 += 32 * kZBatch) {
-      double z[kZBatch];
+    for (int k0 = lane; k0 < nc; k0 += 32 * ZB) {
+      double z[ZB];
 #pragma unroll
-      for (int u = 0; u < kZBatch; ++u) z[u] = (k0 + 32 * u < nc) ? __ldg(zr + k0 + 32 * u) : 0.0;
+      for (int u = 0; u < ZB; ++u) z[u] = (k0 + 32 * u < nc) ? __ldg(zr + k0 + 32 * u) : 0.0;
 #pragma unroll
-      for (int u = 0; u < kZBatch; ++u)
+      for (int u = 0; u < ZB; ++u)
         if (k0 + 32 * u < nc) sum += z[u] * t[k0 + 32 * u];
     }
     sum = warp_sum(sum);
@@ -2012,6 +2029,7 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
   const CgPersistentArgs &A = R.P;
   const CoarseView &V = C.V;
   constexpr bool f32 = std::is_same<TS, float>::value;
+  constexpr int kZB = f32 ? 8 : 16;  // 16 spills in the float form
   const TS *Lsv, *invLv;
   TS *xv, *pv, *rv0, *rv1, *wv0, *wv1, *sv0, *sv1;
   if constexpr (f32) {
@@ -2085,7 +2103,7 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
     double *const dR[1] = {cR};
     read_sums<1>(V, 0, 0, iscale, dR);
     __syncthreads();
-    coarse_values(V, cR, cc[0]);
+    coarse_values<kZB>(V, cR, cc[0]);
     __syncthreads();
   }
   // phase 1 (buffer 1): w0 = A u0 with u0 = D^-1 b + c0[agg]; delta0 = w0.u0, gamma0 = b.u0
@@ -2149,7 +2167,7 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
         ct[m] = cR[m] - alpha * sm;
       }
       __syncthreads();
-      coarse_values(V, ct, cc[pc ^ 1]);
+      coarse_values<kZB>(V, ct, cc[pc ^ 1]);
       __syncthreads();
     }
     const double *cold = cc[pc], *cnew = cc[pc ^ 1];
