@@ -142,7 +142,7 @@ struct cfsa_ns {
   double *wb = nullptr, *wr = nullptr, *wr0 = nullptr, *wp = nullptr, *wv = nullptr, *ws = nullptr,
          *wt = nullptr;  // [3][N2]
   double *pb = nullptr, *pr = nullptr, *pz = nullptr, *pp = nullptr, *pq = nullptr, *ps = nullptr,
-         *pt = nullptr, *pv = nullptr;  // [nv]
+         *pt = nullptr, *pv = nullptr, *pu = nullptr;  // [nv]
   double *stash = nullptr;
   // boundary faces
   int *fverts = nullptr, *ftet = nullptr, *vf_ptr = nullptr, *vf = nullptr;
@@ -193,7 +193,7 @@ struct cfsa_ns {
   MixedState *ms = nullptr;
   MixedState *h_ms = nullptr;
   // mixed-precision pressure (two-level CG in float storage inside FP64 defect correction)
-  float *Ls32 = nullptr, *invL32 = nullptr, *px32 = nullptr, *pp32 = nullptr;
+  float *Ls32 = nullptr, *invL32 = nullptr, *px32 = nullptr, *pp32 = nullptr, *pu32 = nullptr;
   float *pr32[2] = {nullptr, nullptr}, *pw32[2] = {nullptr, nullptr}, *ps32[2] = {nullptr, nullptr};
   CgState *cs_in = nullptr;
   PMixState *pmx = nullptr;
@@ -203,6 +203,7 @@ struct cfsa_ns {
   // reliable-update trigger of the mixed-precision BiCGSTAB: the FP64 residual replaces the FP32
   // one when the latter has dropped by this factor since the previous update
   double mixed_delta = 1e-2;
+  bool cg2l_split = false;  // two-level CG iteration in two passes (u stored, one gather per entry)
 
   // discrete adjoint (ns_adjoint.cuh): transposed P1 slots, vertex -> (boundary face, local
   // index in the face's tet) incidence, host vertex coordinates for objective patches
@@ -457,7 +458,7 @@ struct cfsa_ns {
     p = dalloc<double>(nv);
     pc = dalloc<double>(nv);
     for (double **w : {&wb, &wr, &wr0, &wp, &wv, &ws, &wt}) *w = dalloc<double>(n3);
-    for (double **w : {&pb, &pr, &pz, &pp, &pq, &ps, &pt, &pv}) *w = dalloc<double>(nv);
+    for (double **w : {&pb, &pr, &pz, &pp, &pq, &ps, &pt, &pv, &pu}) *w = dalloc<double>(nv);
     ct = dalloc<double>((size_t)nt * 3);
     divt = dalloc<double>(nt);
     stash = dalloc<double>(1);
@@ -494,7 +495,7 @@ struct cfsa_ns {
     CK(cudaMemsetAsync(ms, 0, sizeof(MixedState), stream));
     Ls32 = dalloc<float>((size_t)s1.nentries);
     CK(cudaMemsetAsync(Ls32, 0, (size_t)s1.nentries * sizeof(float), stream));
-    for (float **w : {&invL32, &px32, &pp32, &pr32[0], &pr32[1], &pw32[0], &pw32[1], &ps32[0], &ps32[1]})
+    for (float **w : {&invL32, &px32, &pp32, &pu32, &pr32[0], &pr32[1], &pw32[0], &pw32[1], &ps32[0], &ps32[1]})
       *w = dalloc<float>((size_t)nv);
     cs_in = dalloc<CgState>(1);
     pmx = dalloc<PMixState>(1);
@@ -503,6 +504,7 @@ struct cfsa_ns {
     CK(cudaMallocHost(&h_pmx, sizeof(PMixState)));
     if (const char *e = std::getenv("CFSA_MIXED_P_TOL_IN")) mixed_p_tol_in = std::atof(e);
     if (const char *e = std::getenv("CFSA_MIXED_DELTA")) mixed_delta = std::atof(e);
+    if (const char *e = std::getenv("CFSA_CG2L_SPLIT")) cg2l_split = std::atoi(e) != 0;
 
     bs_prof = dalloc<BicgState>(1);
     cs_prof = dalloc<CgState>(1);
@@ -850,6 +852,15 @@ struct cfsa_ns {
         npos_max = std::max(npos_max, (int)rows.size());
       }
     }
+    // pieces of kSegPiece staging positions per segment, in segment order (seg_sums)
+    std::vector<int> own_pfirst(own.size() + 1, 0);
+    std::vector<int4> pieces;
+    for (size_t q = 0; q < own.size(); ++q) {
+      own_pfirst[q] = (int)pieces.size();
+      for (int a0 = seg_lo[q]; a0 < seg_hi[q]; a0 += kSegPiece)
+        pieces.push_back(make_int4(a0, std::min(seg_hi[q], a0 + kSegPiece), own[q], 0));
+    }
+    own_pfirst[own.size()] = (int)pieces.size();
     CoarseView V{};
     V.nc = nc;
     V.agg = cupload(agg);
@@ -859,15 +870,17 @@ struct cfsa_ns {
     V.own = cupload(own);
     V.seg_lo = cupload(seg_lo);
     V.seg_hi = cupload(seg_hi);
+    V.own_pfirst = cupload(own_pfirst);
+    V.pieces = cupload(pieces);
     V.need_ptr = cupload(need_ptr);
     V.need = cupload(need);
-    V.gacc = cupload(std::vector<unsigned long long>((size_t)18 * std::max(nc, 1), 0ull));
+    V.gacc = cupload(std::vector<unsigned long long>((size_t)27 * std::max(nc, 1), 0ull));
     V.npos_max = npos_max;
     // shared memory: coarse arrays, row staging, then as many column indices as fit
     int optin = 0;
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     cudaFuncAttributes fa{};
-    CK(cudaFuncGetAttributes(&fa, k_cg2l_resident<double>));
+    CK(cudaFuncGetAttributes(&fa, k_cg2l_resident<double, false>));
     const int64_t coarse_bytes = (int64_t)(6 * nc + 2 + 2 * npos_max) * (int64_t)sizeof(double);
     const int64_t row_bytes = (int64_t)3 * cg_res_bpc_sell * kBlock * (int64_t)sizeof(int);
     const int64_t avail = (int64_t)optin - (int64_t)fa.sharedSizeBytes - coarse_bytes - row_bytes;
@@ -880,7 +893,8 @@ struct cfsa_ns {
     cg2l_col_cap = (int)std::min<int64_t>(max_entries, avail / (int64_t)sizeof(int));
     cg2l_smem = (size_t)(coarse_bytes + row_bytes + (int64_t)cg2l_col_cap * (int64_t)sizeof(int));
     int per_sm = 1;
-    for (const void *fn : {(const void *)k_cg2l_resident<double>, (const void *)k_cg2l_resident<float>}) {
+    for (const void *fn : {(const void *)k_cg2l_resident<double, false>, (const void *)k_cg2l_resident<float, false>,
+                           (const void *)k_cg2l_resident<double, true>, (const void *)k_cg2l_resident<float, true>}) {
       cudaFuncAttributes fb{};
       CK(cudaFuncGetAttributes(&fb, fn));
       if (fb.sharedSizeBytes > fa.sharedSizeBytes)
@@ -1235,6 +1249,8 @@ struct cfsa_ns {
     c2.invL32 = invL32;
     c2.x32 = px32;
     c2.p32 = pp32;
+    c2.u = pu;
+    c2.u32 = pu32;
     for (int q = 0; q < 2; ++q) {
       c2.r32[q] = pr32[q];
       c2.w32[q] = pw32[q];
@@ -1249,7 +1265,7 @@ struct cfsa_ns {
     CK(cudaMemsetAsync(bar_count, 0, (1 + kBarrierGroups) * sizeof(unsigned int), s));
     CK(cudaMemsetAsync(bar_err, 0, sizeof(int), s));
     if (coarse_view.nc > 0)
-      CK(cudaMemsetAsync(coarse_view.gacc, 0, (size_t)18 * coarse_view.nc * sizeof(unsigned long long), s));
+      CK(cudaMemsetAsync(coarse_view.gacc, 0, (size_t)27 * coarse_view.nc * sizeof(unsigned long long), s));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned int)cg_res_grid);
     cfg.blockDim = dim3(kCgResThreads);
@@ -1261,9 +1277,9 @@ struct cfsa_ns {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     if (f32)
-      CK(cudaLaunchKernelEx(&cfg, k_cg2l_resident<float>, c2));
+      CK(cudaLaunchKernelEx(&cfg, cg2l_split ? k_cg2l_resident<float, true> : k_cg2l_resident<float, false>, c2));
     else
-      CK(cudaLaunchKernelEx(&cfg, k_cg2l_resident<double>, c2));
+      CK(cudaLaunchKernelEx(&cfg, cg2l_split ? k_cg2l_resident<double, true> : k_cg2l_resident<double, false>, c2));
   }
 
   // Mixed-precision pressure solve (ns_mixed.cuh): FP64 defect correction around the float

@@ -1430,10 +1430,11 @@ __device__ __forceinline__ void group_sync(int g) {
   asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kBlock) : "memory");
 }
 
-// block_partial for one 256-thread group of a larger CTA (named barrier 1 + g).
+// block_partial for one 256-thread group of a larger CTA (named barrier 1 + g); the values go to
+// slots j0, j0 + 1, ... of the block's partials.
 template <int NV, int NS>
 __device__ __forceinline__ void group_partial(double (&v)[NV], double *__restrict__ partials, int b,
-                                              int g, double (*sm)[NS][kBlock / 32]) {
+                                              int g, double (*sm)[NS][kBlock / 32], int j0 = 0) {
   const int lt = threadIdx.x & (kBlock - 1), warp = lt >> 5, lane = lt & 31;
 #pragma unroll
   for (int j = 0; j < NV; ++j) {
@@ -1446,7 +1447,7 @@ __device__ __forceinline__ void group_partial(double (&v)[NV], double *__restric
     for (int j = 0; j < NV; ++j) {
       double s = 0.0;
       for (int w = 0; w < kBlock / 32; ++w) s += sm[g][j][w];
-      partials[(size_t)b * kMaxRed + j] = s;
+      partials[(size_t)b * kMaxRed + j0 + j] = s;
     }
   }
   group_sync(g);
@@ -1861,13 +1862,15 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg1_resident(Cg1Args C) {
 // Aggregate sums are exact fixed-point sums, so their order does not matter and they cost a few
 // atomics instead of a reduction tree: each value x becomes the 128-bit integer floor(x 2^S)
 // (S = 80 - floor(log2(b.b) / 2), clamped to +-2^100). A CTA stages its rows' values in shared
-// memory sorted by aggregate, one warp per aggregate sums a segment exactly and adds it into a
-// global accumulator (two 64-bit atomics with the carry of the low word), and after the barrier a
+// memory sorted by aggregate, one warp per 64-position piece of a segment sums it exactly and adds
+// it into a global accumulator (three carry-free 64-bit words, red128), and after the barrier a
 // sum converts back as (hi 2^64 + lo) 2^-S.
 // Global accumulators rotate over three buffers; the buffer of the next phase is cleared while no
 // CTA can still read it. c[m] is a warp butterfly over lanes l of sum_{k = l mod 32} Z[m][k]
 // t[k]. Each CTA forms c only for the aggregates its rows and their neighbours belong to. The
 // oracle's cg2l() restates the same arithmetic, so GPU and oracle agree bit for bit.
+constexpr int kSegPiece = 64;  // staging positions per piece of an aggregate sum
+
 struct CoarseView {
   int nc;                       // aggregates (0: Jacobi only)
   const int *agg;               // [n] aggregate of each row; nc for rows without one
@@ -1876,8 +1879,10 @@ struct CoarseView {
                                 // order, -1 for rows without aggregate
   const int *own_ptr, *own;     // aggregates of each CTA's rows (ascending)
   const int *seg_lo, *seg_hi;   // staging positions of each own aggregate's rows
+  const int *own_pfirst;        // [own entries + 1] first piece of each own aggregate's segment
+  const int4 *pieces;           // (first, end staging position, aggregate, 0) per piece
   const int *need_ptr, *need;   // aggregates whose coarse value each CTA reads
-  unsigned long long *gacc;     // [3 buffers][3 vectors][nc][lo, hi] fixed-point sums
+  unsigned long long *gacc;     // [3 buffers][3 vectors][nc][3 words] fixed-point sums (red128)
   int npos_max;                 // largest staging list (shared-memory doubles per vector)
 };
 
@@ -1890,6 +1895,10 @@ struct Cg2lArgs {
   // inverse diagonal, solution and the same vectors (r32[0] = b, p32 = s32[0] = 0 on entry)
   const float *Ls32, *invL32;
   float *x32, *r32[2], *w32[2], *s32[2], *p32;
+  // u = D^-1 r + c[agg] of the current residual, stored by the split form (k_cg2l_resident with
+  // SPLIT) between its two passes
+  double *u;
+  float *u32;
 };
 
 // floor(x 2^S) as a two's-complement 128-bit integer (lo, hi); x 2^S is clamped to +-2^100 and a
@@ -1911,9 +1920,26 @@ __device__ __forceinline__ void fixed128(double x, double scale, unsigned long l
   }
 }
 
-__device__ __forceinline__ void add128(unsigned long long *p, unsigned long long lo, unsigned long long hi) {
-  const unsigned long long old = atomicAdd(p, lo);
-  atomicAdd(p + 1, hi + ((old + lo < old) ? 1ull : 0ull));
+// Exact 128-bit sums held in three 64-bit words of 42, 42 and 44 bits: every term adds its chunk
+// to each word with an atomic whose result is not used (a reduction the thread does not wait
+// for; no carry passes between the words, so no atomic depends on another). The two low words
+// stay exact for fewer than 2^22 terms, far above the pieces of one phase (at most 148 CTAs x a
+// few hundred); the top word only matters modulo 2^44.
+constexpr unsigned long long kMask42 = (1ull << 42) - 1ull;
+
+__device__ __forceinline__ void red128(unsigned long long *p, unsigned long long lo, unsigned long long hi) {
+  atomicAdd(p, lo & kMask42);
+  atomicAdd(p + 1, ((lo >> 42) | (hi << 22)) & kMask42);
+  atomicAdd(p + 2, hi >> 20);
+}
+
+// The 128-bit total (lo, hi) of three accumulated words: w0 + w1 2^42 + w2 2^84 modulo 2^128.
+__device__ __forceinline__ void words128(const unsigned long long *a, unsigned long long &lo,
+                                         unsigned long long &hi) {
+  const unsigned long long w0 = __ldcg(a), w1 = __ldcg(a + 1), w2 = __ldcg(a + 2);
+  const unsigned long long s = w1 << 42;
+  lo = w0 + s;
+  hi = (w1 >> 22) + (w2 << 20) + ((lo < s) ? 1ull : 0ull);
 }
 
 __device__ __forceinline__ double unfixed128(unsigned long long lo, unsigned long long hi, double iscale) {
@@ -1921,60 +1947,53 @@ __device__ __forceinline__ double unfixed128(unsigned long long lo, unsigned lon
 }
 
 // Sums of this CTA's staged values per own aggregate into global buffer `buf`. Each own
-// aggregate's segment of the staging is cut into pieces of kSegPiece positions, and the warps
-// take the pieces of all segments round robin, so a CTA whose rows fall into a few large
-// aggregates still spreads the work over all its warps. Each lane adds its values exactly as
-// 128-bit integers offset by 2^100 (so that they are non-negative); the lane sums are cut into five
-// 26-bit limbs, each limb summed by a warp reduction (32 x 2^26 < 2^32), and lane 0 re-assembles
-// the piece's total, removes count x 2^100 and adds it to the global accumulator. The sums are
-// exact, so how a segment is cut does not change the result.
-constexpr int kSegPiece = 64;
-
+// aggregate's segment of the staging is cut into pieces of kSegPiece positions (listed per CTA
+// on the host) and the warps take the CTA's pieces round robin, so a CTA whose rows fall into a
+// few large aggregates still spreads the work over all its warps. In a piece each lane adds its
+// values exactly as 128-bit integers offset by 2^100 (so that they are non-negative); the lane sums
+// are cut into five 26-bit limbs, each limb summed by a warp reduction (32 x 2^26 < 2^32), and
+// lane 0 re-assembles the piece's total, removes count x 2^100 and adds it to the global
+// accumulator (red128). The sums are exact, so how a segment is cut does not change the result.
 template <int NV>
 __device__ __forceinline__ void seg_sums(const CoarseView &V, const double *__restrict__ stage,
                                          int buf, const int (&vi)[NV], double scale) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const int q0 = __ldg(V.own_ptr + blockIdx.x), q1 = __ldg(V.own_ptr + blockIdx.x + 1);
-  int item = 0;  // pieces of the segments before q
-  for (int q = q0; q < q1; ++q) {
-    const int p0 = __ldg(V.seg_lo + q), p1 = __ldg(V.seg_hi + q), m = __ldg(V.own + q);
-    const int np = (p1 - p0 + kSegPiece - 1) / kSegPiece;
-    for (int k = ((warp - item) % nw + nw) % nw; k < np; k += nw) {
-      const int a0 = p0 + k * kSegPiece, a1 = min(p1, a0 + kSegPiece);
+  const int g0 = __ldg(V.own_pfirst + __ldg(V.own_ptr + blockIdx.x));
+  const int g1 = __ldg(V.own_pfirst + __ldg(V.own_ptr + blockIdx.x + 1));
+  for (int gp = g0 + warp; gp < g1; gp += nw) {
+    const int4 pc = __ldg(V.pieces + gp);  // x = first, y = end position, z = aggregate
 #pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        const double *sv = stage + (size_t)v * V.npos_max;
-        unsigned long long al = 0ull, ah = 0ull;
-        for (int p = a0 + lane; p < a1; p += 32) {
-          unsigned long long l, h;
-          fixed128(sv[p], scale, l, h);
-          h += 1ull << 36;  // + 2^100
-          al += l;
-          ah += h + ((al < l) ? 1ull : 0ull);
-        }
-        const unsigned m26 = (1u << 26) - 1u;
-        const unsigned long long s0 = __reduce_add_sync(0xffffffffu, (unsigned)(al & m26));
-        const unsigned long long s1 = __reduce_add_sync(0xffffffffu, (unsigned)((al >> 26) & m26));
-        const unsigned long long s2 = __reduce_add_sync(0xffffffffu, (unsigned)(((al >> 52) | (ah << 12)) & m26));
-        const unsigned long long s3 = __reduce_add_sync(0xffffffffu, (unsigned)((ah >> 14) & m26));
-        const unsigned long long s4 = __reduce_add_sync(0xffffffffu, (unsigned)((ah >> 40) & m26));
-        if (lane == 0) {
-          const unsigned long long l1 = s0 + (s1 << 26);
-          const unsigned long long l2 = l1 + (s2 << 52);
-          const unsigned long long h = (s2 >> 12) + (s3 << 14) + (s4 << 40) + ((l2 < l1) ? 1ull : 0ull) -
-                                       ((unsigned long long)(a1 - a0) << 36);
-          add128(V.gacc + 2 * ((size_t)(3 * buf + vi[v]) * V.nc + m), l2, h);
-        }
+    for (int v = 0; v < NV; ++v) {
+      const double *sv = stage + (size_t)v * V.npos_max;
+      unsigned long long al = 0ull, ah = 0ull;
+      for (int p = pc.x + lane; p < pc.y; p += 32) {
+        unsigned long long l, h;
+        fixed128(sv[p], scale, l, h);
+        h += 1ull << 36;  // + 2^100
+        al += l;
+        ah += h + ((al < l) ? 1ull : 0ull);
+      }
+      const unsigned m26 = (1u << 26) - 1u;
+      const unsigned long long s0 = __reduce_add_sync(0xffffffffu, (unsigned)(al & m26));
+      const unsigned long long s1 = __reduce_add_sync(0xffffffffu, (unsigned)((al >> 26) & m26));
+      const unsigned long long s2 = __reduce_add_sync(0xffffffffu, (unsigned)(((al >> 52) | (ah << 12)) & m26));
+      const unsigned long long s3 = __reduce_add_sync(0xffffffffu, (unsigned)((ah >> 14) & m26));
+      const unsigned long long s4 = __reduce_add_sync(0xffffffffu, (unsigned)((ah >> 40) & m26));
+      if (lane == 0) {
+        const unsigned long long l1 = s0 + (s1 << 26);
+        const unsigned long long l2 = l1 + (s2 << 52);
+        const unsigned long long h = (s2 >> 12) + (s3 << 14) + (s4 << 40) + ((l2 < l1) ? 1ull : 0ull) -
+                                     ((unsigned long long)(pc.y - pc.x) << 36);
+        red128(V.gacc + 3 * ((size_t)(3 * buf + vi[v]) * V.nc + pc.z), l2, h);
       }
     }
-    item += np;
   }
 }
 
 // Clears global buffer `buf` (every CTA a share).
 __device__ __forceinline__ void clear_acc(const CoarseView &V, int buf) {
-  unsigned long long *g = V.gacc + (size_t)2 * 3 * V.nc * buf;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 6 * V.nc; k += gridDim.x * blockDim.x) g[k] = 0ull;
+  unsigned long long *g = V.gacc + (size_t)9 * V.nc * buf;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 9 * V.nc; k += gridDim.x * blockDim.x) g[k] = 0ull;
 }
 
 // Aggregate sums of vectors [v0, v0 + NV) from global buffer `buf`.
@@ -1983,8 +2002,9 @@ __device__ __forceinline__ void read_sums(const CoarseView &V, int buf, int v0, 
                                           double *const (&dst)[NV]) {
   for (int idx = threadIdx.x; idx < NV * V.nc; idx += blockDim.x) {
     const int v = idx / V.nc, m = idx - v * V.nc;
-    const unsigned long long *a = V.gacc + 2 * ((size_t)(3 * buf + v0 + v) * V.nc + m);
-    dst[v][m] = unfixed128(__ldcg(a), __ldcg(a + 1), iscale);
+    unsigned long long lo, hi;
+    words128(V.gacc + 3 * ((size_t)(3 * buf + v0 + v) * V.nc + m), lo, hi);
+    dst[v][m] = unfixed128(lo, hi, iscale);
   }
 }
 
@@ -2014,13 +2034,17 @@ __device__ __forceinline__ void coarse_values(const CoarseView &V, const double 
   }
 }
 
+// Entries per chunk of the split form's product (one gather per entry, so twice the fused
+// form's chunk fits in the registers).
+constexpr int kCg2lChunk = 8;
+
 // TS: storage type of the operator values, inverse diagonal, solution and Krylov vectors. double:
 // the FP64 solve (bit-identical to the oracle's cg2l); float: the inner solve of the mixed-precision
 // pressure solve (half the bytes per entry). Arithmetic, dot products, aggregate sums and scalars
 // are FP64 in both; in the float form each updated vector entry is rounded to float once and the
 // rounded value is the one used in the dot products and aggregate sums, so they describe the
 // stored vectors.
-template <class TS>
+template <class TS, bool SPLIT>
 __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) {
   extern __shared__ double s_dbl[];
   __shared__ double s_grp[kCgResGroups][4][kBlock / 32];
@@ -2031,12 +2055,12 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
   constexpr bool f32 = std::is_same<TS, float>::value;
   constexpr int kZB = f32 ? 8 : 16;  // 16 spills in the float form
   const TS *Lsv, *invLv;
-  TS *xv, *pv, *rv0, *rv1, *wv0, *wv1, *sv0, *sv1;
+  TS *xv, *pv, *uv, *rv0, *rv1, *wv0, *wv1, *sv0, *sv1;
   if constexpr (f32) {
-    Lsv = C.Ls32, invLv = C.invL32, xv = C.x32, pv = C.p32;
+    Lsv = C.Ls32, invLv = C.invL32, xv = C.x32, pv = C.p32, uv = C.u32;
     rv0 = C.r32[0], rv1 = C.r32[1], wv0 = C.w32[0], wv1 = C.w32[1], sv0 = C.s32[0], sv1 = C.s32[1];
   } else {
-    Lsv = A.Ls, invLv = A.invL, xv = A.x, pv = C.p;
+    Lsv = A.Ls, invLv = A.invL, xv = A.x, pv = C.p, uv = C.u;
     rv0 = C.r[0], rv1 = C.r[1], wv0 = C.w[0], wv1 = C.w[1], sv0 = C.s[0], sv1 = C.s[1];
   }
   auto rnd = [](double v) { return (double)(TS)v; };  // storage rounding (identity for double)
@@ -2171,94 +2195,180 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
       __syncthreads();
     }
     const double *cold = cc[pc], *cnew = cc[pc ^ 1];
-    for (int b = b0 + g; b < b1; b += kCgResGroups) {
-      const int lp = (b - b0) * kBlock + lt;
-      const int i = s_row[lp];
-      double v[4] = {0.0, 0.0, 0.0, 0.0};
-      if (i >= 0) {
-        const int base = s_base[lp], len = s_len[lp];
-        const bool staged = b < bs;
-        double acc = 0.0;
-        int k = 0;
-        for (; k + kCgChunk <= len; k += kCgChunk) {
-          int jj[kCgChunk], aj[kCgChunk];
-          double a[kCgChunk], rr_[kCgChunk], ww[kCgChunk], ss[kCgChunk], mm[kCgChunk];
-#pragma unroll
-          for (int q = 0; q < kCgChunk; ++q) {
-            const int pos = base + (k + q) * kSellC;
-            jj[q] = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
-            a[q] = (double)__ldg(Lsv + pos);
-          }
-#pragma unroll
-          for (int q = 0; q < kCgChunk; ++q) {
-            rr_[q] = (double)__ldcg(ro + jj[q]);
-            ww[q] = (double)__ldcg(wo + jj[q]);
-            ss[q] = (double)__ldcg(so + jj[q]);
-            mm[q] = (double)__ldg(invLv + jj[q]);
-            aj[q] = __ldg(V.agg + jj[q]);
-          }
-#pragma unroll
-          for (int q = 0; q < kCgChunk; ++q) {
-            const double sj = ww[q] + beta * ss[q];
-            const double rj = rr_[q] - alpha * sj;
-            acc += a[q] * (mm[q] * rj + cnew[aj[q]]);
+    if constexpr (SPLIT) {
+      // pass 1: own-row updates and u = D^-1 r_new + c_new[agg]; slots 0-2 take r.u, r.r, r.D^-1 r
+      for (int b = b0 + g; b < b1; b += kCgResGroups) {
+        const int lp = (b - b0) * kBlock + lt;
+        const int i = s_row[lp];
+        double v[3] = {0.0, 0.0, 0.0};
+        if (i >= 0) {
+          const int ai = __ldg(V.agg + i);
+          const double mi = (double)__ldg(invLv + i);
+          const double roi = (double)__ldcg(ro + i);
+          const double woi = (double)__ldcg(wo + i), soi = (double)__ldcg(so + i);
+          const double poi = (double)__ldcg(pv + i), xoi = (double)__ldcg(xv + i);
+          const double uoi = mi * roi + cold[ai];
+          const double pi = rnd(uoi + beta * poi);
+          const double si = rnd(woi + beta * soi);
+          const double xi = xoi + alpha * pi;
+          const double ri = rnd(roi - alpha * si);
+          const double ui = rnd(mi * ri + cnew[ai]);
+          __stcg(pv + i, (TS)pi);
+          __stcg(sn + i, (TS)si);
+          __stcg(xv + i, (TS)xi);
+          __stcg(rn + i, (TS)ri);
+          __stcg(uv + i, (TS)ui);
+          v[0] = ri * ui;
+          v[1] = ri * ri;
+          v[2] = ri * (mi * ri);
+          if (nc > 0) {
+            const int ps = __ldg(V.row_pos + i);
+            if (ps >= 0) s_stage[ps] = ri;
           }
         }
-        if (k < len) {  // the last len % kCgChunk entries as one predicated chunk
-          int jj[kCgChunk], aj[kCgChunk];
-          double a[kCgChunk], rr_[kCgChunk], ww[kCgChunk], ss[kCgChunk], mm[kCgChunk];
-#pragma unroll
-          for (int q = 0; q < kCgChunk; ++q) {
-            const int pos = base + (k + q) * kSellC;
-            const bool in = k + q < len;
-            jj[q] = !in ? 0 : staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
-            a[q] = in ? (double)__ldg(Lsv + pos) : 0.0;
-          }
-#pragma unroll
-          for (int q = 0; q < kCgChunk; ++q) {
-            const bool in = k + q < len;
-            rr_[q] = in ? (double)__ldcg(ro + jj[q]) : 0.0;
-            ww[q] = in ? (double)__ldcg(wo + jj[q]) : 0.0;
-            ss[q] = in ? (double)__ldcg(so + jj[q]) : 0.0;
-            mm[q] = in ? (double)__ldg(invLv + jj[q]) : 0.0;
-            aj[q] = in ? __ldg(V.agg + jj[q]) : 0;
-          }
-#pragma unroll
-          for (int q = 0; q < kCgChunk; ++q) {
-            const double sj = ww[q] + beta * ss[q];
-            const double rj = rr_[q] - alpha * sj;
-            if (k + q < len) acc += a[q] * (mm[q] * rj + cnew[aj[q]]);
-          }
-        }
-        acc = rnd(acc);
-        // own row
-        const int ai = __ldg(V.agg + i);
-        const double mi = (double)__ldg(invLv + i);
-        const double roi = (double)__ldcg(ro + i);
-        const double uoi = mi * roi + cold[ai];
-        const double pi = rnd(uoi + beta * (double)__ldcg(pv + i));
-        const double si = rnd((double)__ldcg(wo + i) + beta * (double)__ldcg(so + i));
-        const double xi = (double)__ldcg(xv + i) + alpha * pi;
-        const double ri = rnd(roi - alpha * si);
-        const double ui = mi * ri + cnew[ai];
-        __stcg(pv + i, (TS)pi);
-        __stcg(sn + i, (TS)si);
-        __stcg(xv + i, (TS)xi);
-        __stcg(rn + i, (TS)ri);
-        __stcg(wn + i, (TS)acc);
-        v[0] = ri * ui;
-        v[1] = acc * ui;
-        v[2] = ri * ri;
-        v[3] = ri * (mi * ri);
-        if (nc > 0) {
-          const int ps = __ldg(V.row_pos + i);
-          if (ps >= 0) {
-            s_stage[ps] = ri;
-            s_stage[V.npos_max + ps] = acc;
-          }
-        }
+        group_partial<3>(v, part, b, g, s_grp);
       }
-      group_partial<4>(v, part, b, g, s_grp);
+      if (!grid_sync(A.bar)) return;
+      // pass 2: w = A u (one gather per entry); slot 3 takes w.u
+      for (int b = b0 + g; b < b1; b += kCgResGroups) {
+        const int lp = (b - b0) * kBlock + lt;
+        const int i = s_row[lp];
+        double v[1] = {0.0};
+        if (i >= 0) {
+          const int base = s_base[lp], len = s_len[lp];
+          const bool staged = b < bs;
+          double acc = 0.0;
+          int k = 0;
+          for (; k + kCg2lChunk <= len; k += kCg2lChunk) {
+            int jj[kCg2lChunk];
+            double a[kCg2lChunk], uu[kCg2lChunk];
+#pragma unroll
+            for (int q = 0; q < kCg2lChunk; ++q) {
+              const int pos = base + (k + q) * kSellC;
+              jj[q] = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+              a[q] = (double)__ldg(Lsv + pos);
+            }
+#pragma unroll
+            for (int q = 0; q < kCg2lChunk; ++q) uu[q] = (double)__ldcg(uv + jj[q]);
+#pragma unroll
+            for (int q = 0; q < kCg2lChunk; ++q) acc += a[q] * uu[q];
+          }
+          if (k < len) {  // the last len % kCg2lChunk entries as one predicated chunk
+            int jj[kCg2lChunk];
+            double a[kCg2lChunk], uu[kCg2lChunk];
+#pragma unroll
+            for (int q = 0; q < kCg2lChunk; ++q) {
+              const int pos = base + (k + q) * kSellC;
+              const bool in = k + q < len;
+              jj[q] = !in ? 0 : staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+              a[q] = in ? (double)__ldg(Lsv + pos) : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < kCg2lChunk; ++q) uu[q] = (k + q < len) ? (double)__ldcg(uv + jj[q]) : 0.0;
+#pragma unroll
+            for (int q = 0; q < kCg2lChunk; ++q)
+              if (k + q < len) acc += a[q] * uu[q];
+          }
+          acc = rnd(acc);
+          __stcg(wn + i, (TS)acc);
+          v[0] = acc * (double)__ldcg(uv + i);
+          if (nc > 0) {
+            const int ps = __ldg(V.row_pos + i);
+            if (ps >= 0) s_stage[V.npos_max + ps] = acc;
+          }
+        }
+        group_partial<1>(v, part, b, g, s_grp, 3);
+      }
+    } else {
+      for (int b = b0 + g; b < b1; b += kCgResGroups) {
+        const int lp = (b - b0) * kBlock + lt;
+        const int i = s_row[lp];
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+        if (i >= 0) {
+          const int base = s_base[lp], len = s_len[lp];
+          const bool staged = b < bs;
+          double acc = 0.0;
+          int k = 0;
+          for (; k + kCgChunk <= len; k += kCgChunk) {
+            int jj[kCgChunk], aj[kCgChunk];
+            double a[kCgChunk], rr_[kCgChunk], ww[kCgChunk], ss[kCgChunk], mm[kCgChunk];
+  #pragma unroll
+            for (int q = 0; q < kCgChunk; ++q) {
+              const int pos = base + (k + q) * kSellC;
+              jj[q] = staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+              a[q] = (double)__ldg(Lsv + pos);
+            }
+  #pragma unroll
+            for (int q = 0; q < kCgChunk; ++q) {
+              rr_[q] = (double)__ldcg(ro + jj[q]);
+              ww[q] = (double)__ldcg(wo + jj[q]);
+              ss[q] = (double)__ldcg(so + jj[q]);
+              mm[q] = (double)__ldg(invLv + jj[q]);
+              aj[q] = __ldg(V.agg + jj[q]);
+            }
+  #pragma unroll
+            for (int q = 0; q < kCgChunk; ++q) {
+              const double sj = ww[q] + beta * ss[q];
+              const double rj = rr_[q] - alpha * sj;
+              acc += a[q] * (mm[q] * rj + cnew[aj[q]]);
+            }
+          }
+          if (k < len) {  // the last len % kCgChunk entries as one predicated chunk
+            int jj[kCgChunk], aj[kCgChunk];
+            double a[kCgChunk], rr_[kCgChunk], ww[kCgChunk], ss[kCgChunk], mm[kCgChunk];
+  #pragma unroll
+            for (int q = 0; q < kCgChunk; ++q) {
+              const int pos = base + (k + q) * kSellC;
+              const bool in = k + q < len;
+              jj[q] = !in ? 0 : staged ? s_col[pos - e0] : __ldg(A.S.col + pos);
+              a[q] = in ? (double)__ldg(Lsv + pos) : 0.0;
+            }
+  #pragma unroll
+            for (int q = 0; q < kCgChunk; ++q) {
+              const bool in = k + q < len;
+              rr_[q] = in ? (double)__ldcg(ro + jj[q]) : 0.0;
+              ww[q] = in ? (double)__ldcg(wo + jj[q]) : 0.0;
+              ss[q] = in ? (double)__ldcg(so + jj[q]) : 0.0;
+              mm[q] = in ? (double)__ldg(invLv + jj[q]) : 0.0;
+              aj[q] = in ? __ldg(V.agg + jj[q]) : 0;
+            }
+  #pragma unroll
+            for (int q = 0; q < kCgChunk; ++q) {
+              const double sj = ww[q] + beta * ss[q];
+              const double rj = rr_[q] - alpha * sj;
+              if (k + q < len) acc += a[q] * (mm[q] * rj + cnew[aj[q]]);
+            }
+          }
+          acc = rnd(acc);
+          // own row
+          const int ai = __ldg(V.agg + i);
+          const double mi = (double)__ldg(invLv + i);
+          const double roi = (double)__ldcg(ro + i);
+          const double uoi = mi * roi + cold[ai];
+          const double pi = rnd(uoi + beta * (double)__ldcg(pv + i));
+          const double si = rnd((double)__ldcg(wo + i) + beta * (double)__ldcg(so + i));
+          const double xi = (double)__ldcg(xv + i) + alpha * pi;
+          const double ri = rnd(roi - alpha * si);
+          const double ui = mi * ri + cnew[ai];
+          __stcg(pv + i, (TS)pi);
+          __stcg(sn + i, (TS)si);
+          __stcg(xv + i, (TS)xi);
+          __stcg(rn + i, (TS)ri);
+          __stcg(wn + i, (TS)acc);
+          v[0] = ri * ui;
+          v[1] = acc * ui;
+          v[2] = ri * ri;
+          v[3] = ri * (mi * ri);
+          if (nc > 0) {
+            const int ps = __ldg(V.row_pos + i);
+            if (ps >= 0) {
+              s_stage[ps] = ri;
+              s_stage[V.npos_max + ps] = acc;
+            }
+          }
+        }
+        group_partial<4>(v, part, b, g, s_grp);
+      }
     }
     if (nc > 0) {
       __syncthreads();
@@ -2267,6 +2377,12 @@ __global__ void __launch_bounds__(kCgResThreads, 1) k_cg2l_resident(Cg2lArgs C) 
     if (!grid_sync(A.bar)) return;
     double t[4];
     tree_total_cta<4>(part, A.nblk_sell, t, s_tree);
+    if constexpr (SPLIT) {  // slots r.u, r.r, r.D^-1 r, w.u -> r.u, w.u, r.r, r.D^-1 r
+      const double wu = t[3];
+      t[3] = t[2];
+      t[2] = t[1];
+      t[1] = wu;
+    }
     if (nc > 0) {
       double *const d2[2] = {cR, cW};
       read_sums<2>(V, buf, 0, iscale, d2);
