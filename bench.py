@@ -96,6 +96,8 @@ def parse():
     ap.add_argument("--rings", type=int, default=GEOM["rings"])
     ap.add_argument("--layers", type=int, default=GEOM["layers"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--momentum-solver", default=MOMENTUM_SOLVER, choices=sorted(MOMENTUM),
+                    help="momentum Krylov method of the FP64 headline step")
     ap.add_argument("--no-oracle", action="store_true",
                     help="skip every oracle run (parity at 1M tets, config-2 CPU comparison, CPU baseline)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
@@ -142,12 +144,17 @@ def make_mesh(cf, rings, layers):
     return m
 
 
+MOMENTUM = {"bicgstab": 1, "cg": 0}  # --momentum-solver -> CFSA_KRYLOV_BICGSTAB / CFSA_KRYLOV_CG
+MOMENTUM_SOLVER = "bicgstab"
+
+
 def make_solver(cf, m, tol=TOL, norm=0):
     s = cf.NavierStokesSolver()
     s.setKrylovTolerances(tol, tol)
     s.setConvergenceNorm(norm)
     s.setMaxIterations(*MAXIT)
     s.setPressureSolver(cf.KRYLOV_CG2L)
+    s.setMomentumSolver(MOMENTUM[MOMENTUM_SOLVER])
     s.setDt(DT)
     s.initialize(m, cf.Fluid(*FLUID))  # from rest; inlet set after initialize (CLI order)
     profile = cf.parabolic_inlet(m.nodePositions(), INLET_PEAK, GEOM["radius"])
@@ -626,6 +633,8 @@ def main():
 
     import cfsa_b200 as cf
 
+    global MOMENTUM_SOLVER
+    MOMENTUM_SOLVER = args.momentum_solver
     m = make_mesh(cf, args.rings, args.layers)
     s, profile = make_solver(cf, m)
     nv, nt, ne, _, _ = m.sizes

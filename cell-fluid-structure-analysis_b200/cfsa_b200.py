@@ -177,6 +177,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "cfsa_ns_set_inlet_uniform": (i32, [vp, vp]),
         "cfsa_ns_set_inlet_profile": (i32, [vp, vp]),
         "cfsa_ns_set_pressure_solver": (i32, [vp, i32]),
+        "cfsa_ns_set_momentum_solver": (i32, [vp, i32]),
         "cfsa_ns_set_coarse_target": (i32, [vp, i32]),
         "cfsa_ns_save_state": (i32, [vp, C.c_char_p]),
         "cfsa_ns_load_state": (i32, [vp, C.c_char_p]),
@@ -398,6 +399,7 @@ class NavierStokesSolver:
         self.mean_inlet_velocity = np.zeros(3)
         self.inlet_profile = None
         self.krylov = KRYLOV_BICGSTAB  # the reference's pressure method; CG variants opt-in
+        self.momentum_krylov = KRYLOV_BICGSTAB  # the reference's momentum method; CG opt-in
         self.coarse_target = 256
         self.precision = PRECISION_FP64
         self.conv_norm = NORM_REFERENCE
@@ -431,6 +433,7 @@ class NavierStokesSolver:
         self._check(L.cfsa_ns_set_pressure_solver(h, int(self.krylov)))
         self._check(L.cfsa_ns_set_coarse_target(h, int(self.coarse_target)))
         self._check(L.cfsa_ns_set_precision(h, int(self.precision)))
+        self._check(L.cfsa_ns_set_momentum_solver(h, int(self.momentum_krylov)))
         self._check(L.cfsa_ns_set_convergence_norm(h, int(self.conv_norm)))
         self._push_inlet()
 
@@ -758,6 +761,13 @@ class NavierStokesSolver:
         self.maxit = (int(momentum), int(pressure))
         if self._h is not None:
             self._check(self._lib.cfsa_ns_set_max_iterations(self._h, *self.maxit))
+
+    def setMomentumSolver(self, krylov: int):
+        """Momentum Krylov method: KRYLOV_BICGSTAB (the reference's) or KRYLOV_CG (Jacobi CG on the
+        same symmetric positive definite system, one product per iteration; FP64 only)."""
+        self.momentum_krylov = int(krylov)
+        if self._h is not None:
+            self._check(self._lib.cfsa_ns_set_momentum_solver(self._h, self.momentum_krylov))
 
     def setPressureSolver(self, krylov: int):
         """Pressure Krylov method: KRYLOV_BICGSTAB (the reference's), KRYLOV_CG, KRYLOV_CG1

@@ -109,6 +109,7 @@ struct cfsa_ns {
   double outlet_pressure = 0.0;
   int ref_node = -1;
   int krylov = CFSA_KRYLOV_BICGSTAB;  // the reference's pressure method (NavierStokes.cpp:633)
+  int mom_krylov = CFSA_KRYLOV_BICGSTAB;  // the reference's momentum method (NavierStokes.cpp:498)
   int precision = CFSA_PRECISION_FP64;
   int conv_norm = CFSA_NORM_REFERENCE;
   double time = 0.0;
@@ -558,6 +559,8 @@ struct cfsa_ns {
         };
         q((const void *)k_bicg_xr<3>);
         q((const void *)k_bicg_xr<1>);
+        q((const void *)k_mcg_xr<3>);
+        q((const void *)k_mcg_init<3>);
         q((const void *)k_mp_xr);
         q((const void *)k_mp_init);
         q((const void *)k_pmx_prep);
@@ -638,7 +641,8 @@ struct cfsa_ns {
     if (mom_dirty) {
       k_momentum_diag<<<blocks_for(N2), kBlock, 0, stream>>>((int)N2, dt, dpos2, Mv, Kv, bc, diagA, invA);
       k_momentum_sell<<<blocks_for(nnz2), kBlock, 0, stream>>>(nnz2, dt, s2.posmap, rows2, ci2, Mv, Kv,
-                                                               bc, invA, At, Ms);
+                                                               bc, invA, At, Ms,
+                                                               mom_krylov == CFSA_KRYLOV_BICGSTAB ? 1 : 0);
       k_to_f32<<<blocks_for(s2.nentries), kBlock, 0, stream>>>(s2.nentries, At, At32);
       k_to_f32<<<blocks_for(N2), kBlock, 0, stream>>>(N2, invA, invA32);
       CK(cudaGetLastError());
@@ -1035,6 +1039,7 @@ struct cfsa_ns {
     a.st = s_out ? s_out : st;
     a.slot = 0;
     a.cw = (conv_norm == CFSA_NORM_JACOBI) ? invA : nullptr;
+    a.tol = tol_mom;
     return a;
   }
 
@@ -1084,11 +1089,23 @@ struct cfsa_ns {
       return;
     }
     BicgArgs a = momentum_args(x, s_out);
+    const bool cg = (mom_krylov == CFSA_KRYLOV_CG);
+    const unsigned int gp = blocks_for(N2);
+    if (cg) {
+      k_mcg_init<3><<<strided(k_mcg_init<3>, gp), kBlock, 0, stream>>>(a);
+      CK(cudaGetLastError());
+    }
     auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
       BicgArgs b = a;
       b.cond = h;
       b.use_cond = use;
-      bicg_body<3>(b, s, s2, (int)N2);
+      if (cg) {
+        k_mcg_q<3><<<s2.nruns, kRunThreads, 0, s>>>(b);
+        k_mcg_xr<3><<<strided(k_mcg_xr<3>, gp), kBlock, 0, s>>>(b);
+        k_mcg_p<3><<<gp, kBlock, 0, s>>>(b);
+      } else {
+        bicg_body<3>(b, s, s2, (int)N2);
+      }
     };
     if (capture)
       capture_while(body);
@@ -1655,8 +1672,11 @@ struct cfsa_ns {
     if (krylov == CFSA_KRYLOV_BICGSTAB) return 5;
     return (cg_persistent || krylov == CFSA_KRYLOV_CG1 || krylov == CFSA_KRYLOV_CG2L) ? 1 : 3;
   }
+  // Kernels of one momentum-solve body run (DevStatus::body_runs[0]): BiCGSTAB 5, CG 3.
+  bool momentum_cg() const { return !momentum_mixed() && mom_krylov == CFSA_KRYLOV_CG; }
+  int momentum_body_kernels() const { return momentum_cg() ? 3 : 5; }
   int mixed_fixed_kernels() const {
-    return (momentum_mixed() ? 1 : 0) + (pressure_mixed() ? 1 : 0);
+    return (momentum_mixed() ? 1 : 0) + (pressure_mixed() ? 1 : 0) + (momentum_cg() ? 1 : 0);
   }
 
   int finish_batch(int launched_steps) {
@@ -1668,7 +1688,8 @@ struct cfsa_ns {
     // mixed momentum: 5 kernels per iteration, 2 per reliable update (x update, residual) plus
     // the init kernel per step; mixed two-level CG pressure: 4 kernels per sweep plus its init
     batch_launches = (int64_t)launched_steps * (launches_per_step + mixed_fixed_kernels()) +
-                     5 * (int64_t)h_st->body_runs[0] + pressure_body * (int64_t)h_st->body_runs[1] +
+                     momentum_body_kernels() * (int64_t)h_st->body_runs[0] +
+                     pressure_body * (int64_t)h_st->body_runs[1] +
                      2 * (int64_t)h_st->body_runs[2];
     batch_iters[0] = (int64_t)h_st->iters[0];
     batch_iters[1] = (int64_t)h_st->iters[1];
@@ -1742,7 +1763,7 @@ struct cfsa_ns {
     const double d[] = {dt, tol_mom, tol_p, relax_u, relax_p, outlet_pressure, viscosity, density,
                         mixed_delta};
     const int64_t k[] = {maxit_mom, maxit_p, ncorr, outlet_type, ref_node, krylov, precision,
-                         conv_norm, geom_gen, (int64_t)cg_persistent};
+                         conv_norm, geom_gen, (int64_t)cg_persistent, mom_krylov};
     mix(d, sizeof(d));
     mix(k, sizeof(k));
     const std::vector<double> &hin = host_inlet();
@@ -2125,7 +2146,8 @@ struct cfsa_ns {
     adj_stats.pressure_iters = (int64_t)hs_adj.iters[1];
     adj_stats.backward_ms = ms;
     const int pressure_body = pressure_body_kernels();
-    adj_stats.kernel_launches = (int64_t)adj_steps * adj_launches_fixed + 5 * (int64_t)hs_adj.body_runs[0] +
+    adj_stats.kernel_launches = (int64_t)adj_steps * adj_launches_fixed +
+                                momentum_body_kernels() * (int64_t)hs_adj.body_runs[0] +
                                 pressure_body * (int64_t)hs_adj.body_runs[1] +
                                 2 * (int64_t)hs_adj.body_runs[2];
     if (h_st->code != CFSA_OK) {
@@ -2418,6 +2440,20 @@ int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov) {
   return CFSA_OK;
 }
 
+int cfsa_ns_set_momentum_solver(cfsa_ns *h, int krylov) {
+  if (!h) return CFSA_BAD_ARG;
+  if (krylov != CFSA_KRYLOV_CG && krylov != CFSA_KRYLOV_BICGSTAB)
+    return fail(h, CFSA_BAD_ARG, "momentum Krylov method must be CFSA_KRYLOV_BICGSTAB or CFSA_KRYLOV_CG");
+  if (krylov == CFSA_KRYLOV_CG && h->precision != CFSA_PRECISION_FP64)
+    return fail(h, CFSA_UNSUPPORTED, "the mixed-precision momentum solve is BiCGSTAB only");
+  if (krylov != h->mom_krylov) {
+    h->mom_dirty = true;  // the SELL values change between A D^-1 and A
+    h->graph_dirty = true;
+  }
+  h->mom_krylov = krylov;
+  return CFSA_OK;
+}
+
 int cfsa_ns_set_coarse_target(cfsa_ns *h, int target) {
   if (!h) return CFSA_BAD_ARG;
   if (target < 1 || target > 1024) return fail(h, CFSA_BAD_ARG, "coarse target outside [1, 1024]");
@@ -2440,6 +2476,8 @@ int cfsa_ns_set_precision(cfsa_ns *h, int precision) {
   if (precision != CFSA_PRECISION_FP64 && precision != CFSA_PRECISION_MIXED &&
       precision != CFSA_PRECISION_MIXED_FULL)
     return fail(h, CFSA_BAD_ARG, "unknown precision");
+  if (precision != CFSA_PRECISION_FP64 && h->mom_krylov == CFSA_KRYLOV_CG)
+    return fail(h, CFSA_UNSUPPORTED, "the mixed-precision momentum solve is BiCGSTAB only");
   if (precision != h->precision) h->graph_dirty = true;
   h->precision = precision;
   return CFSA_OK;

@@ -285,20 +285,21 @@ __global__ void k_momentum_diag(int n, double dt, const int *__restrict__ dpos,
   invA[i] = (d != 0.0) ? 1.0 / d : 1.0;
 }
 
-// Right-preconditioned momentum operator At = A * diag(invA) in SELL layout, and M in SELL.
+// Momentum operator in SELL layout: right-preconditioned At = A * diag(invA) for BiCGSTAB
+// (scale != 0) or A itself for CG; and M in SELL.
 __global__ void k_momentum_sell(int64_t nnz, double dt, const int *__restrict__ posmap,
                                 const int *__restrict__ rows, const int *__restrict__ ci,
                                 const double *__restrict__ Mv, const double *__restrict__ Kv,
                                 const signed char *__restrict__ bc,
                                 const double *__restrict__ invA, double *__restrict__ At,
-                                double *__restrict__ Ms) {
+                                double *__restrict__ Ms, int scale) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nnz) return;
   const int i = rows[k], j = ci[k];
   double a = Mv[k] / dt + Kv[k];
   if (i == j && (bc[i] == BC_INLET || bc[i] == BC_WALL)) a += kMomentumPenalty;
   const int pos = posmap[k];
-  At[pos] = a * invA[j];
+  At[pos] = scale ? a * invA[j] : a;
   Ms[pos] = Mv[k];
 }
 
@@ -681,6 +682,7 @@ struct BicgArgs {
   DevStatus *st;  // launch counters
   int slot;       // 0 momentum, 1 pressure
   const double *cw;  // convergence-norm weights, nullptr: unscaled ||r||
+  double tol;        // relative tolerance (read by the momentum CG's initialisation)
 };
 
 // K1: p = r + beta (p - omega v); on restart: r = b - A x, r0 = r, p = r, rho = |r|^2.
@@ -918,6 +920,209 @@ __global__ void k_bicg_xr(BicgArgs A) {
     }
     if (A.use_cond) cudaGraphSetConditional(A.cond, s->active ? 1u : 0u);
   }
+}
+
+// ------------------------------------------------------------------------------------------
+// Batched Jacobi-preconditioned CG for the momentum system (selectable; the reference solves it
+// with BiCGSTAB, NavierStokes.cpp:498-515). A = M/dt + K + 1e10 I_D is symmetric positive
+// definite (the convection term is explicit), so CG solves the same system with one product per
+// iteration instead of two. With this method the SELL values hold A itself, not A D^-1. Each
+// component keeps its own scalars and stops on its own, as in the BiCGSTAB batch:
+//   G0: z = D^-1 b, p = z, absnew = b.z; ||b|| in the convergence norm (r.r, or r.z)
+//   G1: q = A p, alpha = absnew / (p.q)
+//   G2: x += alpha p, r -= alpha q, z = D^-1 r; convergence test; beta = r.z / absnew
+//   G3: p = z + beta p
+// z is recomputed from r where it is needed (the same product, one stored vector less). The
+// reductions of G0 and G2 run over natural 256-position blocks, the one of G1 over the SELL runs.
+
+// G0, after k_momentum_rhs has written b, x = 0 and r = b.
+template <int NC>
+__global__ void k_mcg_init(BicgArgs A) {
+  if (A.st && A.st->halt) return;
+  __shared__ WarpSums<2 * NC> S;
+  const int nblk = (A.n + kBlock - 1) / kBlock;
+  const int64_t n = A.n;
+  int slot = 0;
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
+    const int i = b * kBlock + threadIdx.x;
+    double part[2 * NC];
+#pragma unroll
+    for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
+    if (i < A.n) {
+      const double dinv = A.invA[i];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const int64_t o = c * n + i;
+        const double bi = A.b[o];
+        const double zi = dinv * bi;
+        A.pk[o] = zi;
+        part[c] = bi * bi;
+        part[NC + c] = bi * zi;
+      }
+    }
+    warp_partial<2 * NC>(part, S, slot);
+  }
+  double tot[2 * NC];
+  if (grid_reduce_strided<2 * NC>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
+    BicgState *s = A.bs;
+    s->active = 0;
+    s->restart = 0;
+    s->ncomp = NC;
+    for (int c = 0; c < NC; ++c) {
+      const double bn = A.cw ? tot[NC + c] : tot[c];
+      s->bnorm2[c] = bn;
+      s->rnorm2[c] = bn;
+      s->tol2[c] = A.tol * A.tol * bn;
+      s->rho[c] = tot[NC + c];
+      s->alpha[c] = 0.0;
+      s->beta[c] = 0.0;
+      s->iters[c] = 0;
+      if (isnan(bn)) {
+        s->status[c] = KS_BREAKDOWN;
+      } else if (bn == 0.0 || bn <= s->tol2[c]) {
+        s->status[c] = KS_CONVERGED;
+      } else {
+        s->status[c] = KS_RUNNING;
+        s->active |= 1 << c;
+      }
+    }
+  }
+}
+
+// G1: q = A p (into v), alpha = absnew / (p . q)
+template <int NC>
+__global__ void __launch_bounds__(kRunThreads, 1) k_mcg_q(BicgArgs A) {
+  const int active = A.bs->active;
+  if (!active) return;
+  const int64_t n = A.n;
+  const int s1 = A.S.rfirst[blockIdx.x + 1];
+  __shared__ int s_next;
+  const int sl0 = run_first_slice(&s_next, A.S.rfirst[blockIdx.x]);
+  with_mask<NC>(active, [&](auto mk) {
+    constexpr int MASK = decltype(mk)::value;
+    for (int sl = sl0; sl < s1; sl = run_next_slice(&s_next)) {
+      const int r = sl * kSellC + (threadIdx.x & 31);
+      const int i = A.S.perm[r];
+      double part[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) part[c] = 0.0;
+      if (i >= 0) {
+        double acc[NC];
+        sell_spmv_row<NC, kU64, MASK>(A.S, A.At, A.pk, n, r, acc);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          if (!((MASK >> c) & 1)) continue;
+          const int64_t o = c * n + i;
+          A.v[o] = acc[c];
+          part[c] = A.pk[o] * acc[c];
+        }
+      }
+      slice_partial<NC>(part, A.S, sl);
+    }
+  });
+  double tot[NC];
+  if (grid_reduce_runs<NC>(A.S, A.red, tot) && threadIdx.x == 0) {
+    for (int c = 0; c < NC; ++c) {
+      if (!((active >> c) & 1)) continue;
+      if (tot[c] == 0.0) {
+        A.bs->status[c] = KS_BREAKDOWN;
+        A.bs->active &= ~(1 << c);
+      } else {
+        A.bs->alpha[c] = A.bs->rho[c] / tot[c];
+      }
+    }
+  }
+}
+
+// G2: x += alpha p, r -= alpha q, z = D^-1 r; r.r and r.z; convergence test and next beta.
+template <int NC>
+__global__ void k_mcg_xr(BicgArgs A) {
+  const int active = A.bs->active;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[A.slot] += 1;
+  if (!active) {
+    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0);
+    return;
+  }
+  __shared__ WarpSums<2 * NC> S;
+  const int nblk = (A.n + kBlock - 1) / kBlock;
+  const int64_t n = A.n;
+  double alpha_c[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) alpha_c[c] = A.bs->alpha[c];
+  int slot = 0;
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++slot) {
+    const int i = b * kBlock + threadIdx.x;
+    double part[2 * NC];
+#pragma unroll
+    for (int c = 0; c < 2 * NC; ++c) part[c] = 0.0;
+    if (i < A.n) {
+      const double dinv = A.invA[i];
+      double xv[NC], pv[NC], rv[NC], qv[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        if (!((active >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        xv[c] = A.x[o], pv[c] = A.pk[o], rv[c] = A.r[o], qv[c] = A.v[o];
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        if (!((active >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        A.x[o] = xv[c] + alpha_c[c] * pv[c];
+        const double ri = rv[c] - alpha_c[c] * qv[c];
+        A.r[o] = ri;
+        const double zi = dinv * ri;
+        part[c] = ri * ri;
+        part[NC + c] = ri * zi;
+      }
+    }
+    warp_partial<2 * NC>(part, S, slot);
+  }
+  double tot[2 * NC];
+  if (grid_reduce_strided<2 * NC>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
+    BicgState *s = A.bs;
+    for (int c = 0; c < NC; ++c) {
+      if (!((active >> c) & 1)) continue;
+      s->iters[c] += 1;
+      const double rr = tot[c], rz = tot[NC + c];
+      const double crit = A.cw ? rz : rr;
+      s->rnorm2[c] = crit;
+      if (isnan(rr) || isnan(rz)) {
+        s->status[c] = KS_BREAKDOWN;
+        s->active &= ~(1 << c);
+      } else if (crit <= s->tol2[c]) {
+        s->status[c] = KS_CONVERGED;
+        s->active &= ~(1 << c);
+      } else if (s->iters[c] >= s->maxit) {
+        s->status[c] = KS_MAXIT;
+        s->active &= ~(1 << c);
+      } else {
+        s->beta[c] = rz / s->rho[c];
+        s->rho[c] = rz;
+      }
+    }
+    if (A.use_cond) cudaGraphSetConditional(A.cond, s->active ? 1u : 0u);
+  }
+}
+
+// G3: p = z + beta p with z = D^-1 r
+template <int NC>
+__global__ void k_mcg_p(BicgArgs A) {
+  const int active = A.bs->active;
+  if (!active) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const int64_t n = A.n;
+  const double dinv = A.invA[i];
+  double beta[NC], rv[NC], pv[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    beta[c] = A.bs->beta[c];
+    if ((active >> c) & 1) rv[c] = A.r[c * n + i], pv[c] = A.pk[c * n + i];
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+    if ((active >> c) & 1) A.pk[c * n + i] = dinv * rv[c] + beta[c] * pv[c];
 }
 
 // After a Krylov loop: record a failure and halt the rest of the batch (pisoStep returns false

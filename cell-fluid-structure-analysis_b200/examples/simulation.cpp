@@ -86,6 +86,7 @@ int main(int argc, char **argv) {
   ns->setPrecision(N.precision == "mixed"        ? CFSA_PRECISION_MIXED
                    : N.precision == "mixed_full" ? CFSA_PRECISION_MIXED_FULL
                                                  : CFSA_PRECISION_FP64);
+  ns->setMomentumSolver(N.momentum_solver == "cg" ? CFSA_KRYLOV_CG : CFSA_KRYLOV_BICGSTAB);
   ns->setConvergenceNorm(N.convergence_norm == "jacobi" ? CFSA_NORM_JACOBI : CFSA_NORM_REFERENCE);
   ns->initialize(mesh, fluid);
   if (N.inlet_profile == "parabolic") {

@@ -55,6 +55,7 @@ void NavierStokesSolver::pushParameters() {
   status(cfsa_ns_set_pressure_solver(h_, krylov_), "setPressureSolver");
   status(cfsa_ns_set_coarse_target(h_, coarse_target_), "setCoarseTarget");
   status(cfsa_ns_set_precision(h_, precision_), "setPrecision");
+  status(cfsa_ns_set_momentum_solver(h_, mom_krylov_), "setMomentumSolver");
   status(cfsa_ns_set_convergence_norm(h_, conv_norm_), "setConvergenceNorm");
   pushInlet();
 }
@@ -359,6 +360,11 @@ void NavierStokesSolver::setMaxIterations(int momentum, int pressure) {
 void NavierStokesSolver::setPressureSolver(int krylov) {
   krylov_ = krylov;
   if (h_) status(cfsa_ns_set_pressure_solver(h_, krylov), "setPressureSolver");
+}
+
+void NavierStokesSolver::setMomentumSolver(int krylov) {
+  mom_krylov_ = krylov;
+  if (h_) status(cfsa_ns_set_momentum_solver(h_, krylov), "setMomentumSolver");
 }
 
 bool NavierStokesSolver::saveState(const std::string &path) {

@@ -31,6 +31,7 @@ class NavierStokesSolver {
   double relax_p_ = 1.0;
   double dt_ = 1e-4;
   int krylov_ = CFSA_KRYLOV_BICGSTAB;  // NavierStokes.cpp:633; the CG variants are opt-in
+  int mom_krylov_ = CFSA_KRYLOV_BICGSTAB;  // NavierStokes.cpp:498; Jacobi CG is opt-in
   int coarse_target_ = 256;
   int precision_ = CFSA_PRECISION_FP64;
   int conv_norm_ = CFSA_NORM_REFERENCE;
@@ -141,6 +142,7 @@ class NavierStokesSolver {
   void setKrylovTolerances(double momentum, double pressure);
   void setMaxIterations(int momentum, int pressure);
   void setPressureSolver(int krylov);  // CFSA_KRYLOV_CG, _BICGSTAB, _CG1 or _CG2L
+  void setMomentumSolver(int krylov);  // CFSA_KRYLOV_BICGSTAB or _CG (FP64 only)
   void setCoarseTarget(int target);    // aggregates of the CFSA_KRYLOV_CG2L coarse space (default 256)
   // new: binary restart file of u, p, time and step count (cfsa_ns_save_state / _load_state)
   bool saveState(const std::string &path);

@@ -234,6 +234,7 @@ SimulationConfig parseConfig(const std::string &text) {
       });
       opt(ns, "precision", [&](const Node *n, const std::string &k) { N.precision = n->scalar; one_of(N.precision, {"fp64", "mixed", "mixed_full"}, k); });
       opt(ns, "pressure_solver", [&](const Node *n, const std::string &k) { N.pressure_solver = n->scalar; one_of(N.pressure_solver, {"bicgstab", "cg", "cg1", "cg2l"}, k); });
+      opt(ns, "momentum_solver", [&](const Node *n, const std::string &k) { N.momentum_solver = n->scalar; one_of(N.momentum_solver, {"bicgstab", "cg"}, k); });
       opt(ns, "coarse_aggregates", [&](const Node *n, const std::string &k) {
         N.coarse_aggregates = as_int(n, k);
         if (N.coarse_aggregates < 1 || N.coarse_aggregates > 1024)
@@ -299,6 +300,7 @@ std::string describe(const SimulationConfig &c) {
     << " " << N.max_iterations[1] << "\nnavier_stokes.n_corrections = " << N.n_corrections
     << "\nnavier_stokes.precision = " << N.precision << "\nnavier_stokes.pressure_solver = " << N.pressure_solver
     << "\nnavier_stokes.coarse_aggregates = " << N.coarse_aggregates
+    << "\nnavier_stokes.momentum_solver = " << N.momentum_solver
     << "\nnavier_stokes.convergence_norm = " << N.convergence_norm << "\nnavier_stokes.inlet_profile = "
     << N.inlet_profile << "\noutput.prefix = " << c.output.output_prefix << "\noutput.total_steps = "
     << c.output.total_steps << "\noutput.output_frequency = " << c.output.output_frequency

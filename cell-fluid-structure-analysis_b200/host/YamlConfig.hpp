@@ -16,6 +16,7 @@
 //   navier_stokes.precision          fp64 | mixed | mixed_full
 //   navier_stokes.pressure_solver    bicgstab | cg | cg1 | cg2l (reference: bicgstab)
 //   navier_stokes.coarse_aggregates  aggregates of the cg2l coarse space (default 256)
+//   navier_stokes.momentum_solver    bicgstab | cg (reference: bicgstab; cg needs precision fp64)
 //   navier_stokes.convergence_norm   reference | jacobi
 //   navier_stokes.inlet_profile      uniform | parabolic (peak = |inlet_velocity|, radius = mesh radius)
 //   adjoint.enabled / objective (wall_shear | pressure_drop) / axis / lo / hi / checkpoint_every /
@@ -56,6 +57,7 @@ struct NavierStokesConfig {
   int max_iterations[2] = {1000, 1000};
   int n_corrections = 1;
   std::string precision = "fp64", pressure_solver = "bicgstab", convergence_norm = "reference";
+  std::string momentum_solver = "bicgstab";
   std::string inlet_profile = "uniform";
   int coarse_aggregates = 256;
 };

@@ -157,6 +157,12 @@ int cfsa_ns_set_reference_node(cfsa_ns *h, int node);                      /* se
 int cfsa_ns_set_inlet_uniform(cfsa_ns *h, const double u[3]);             /* setMeanInletVelocity */
 int cfsa_ns_set_inlet_profile(cfsa_ns *h, const double *u /*[N2][3]*/);   /* new: per-node inlet */
 int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov);                   /* new: CG or BiCGSTAB */
+/* new: momentum Krylov method, CFSA_KRYLOV_BICGSTAB (default; the reference's Jacobi BiCGSTAB,
+ * src/FEM/NavierStokes.cpp:498-515) or CFSA_KRYLOV_CG (Jacobi-preconditioned CG on the same
+ * system: M/dt + K + the 1e10 Dirichlet penalty is symmetric positive definite because the
+ * convection term is explicit; one sparse product per iteration instead of two; same stopping
+ * rule). CG with a mixed precision returns CFSA_UNSUPPORTED. */
+int cfsa_ns_set_momentum_solver(cfsa_ns *h, int krylov);
 /* new: aggregate count the CFSA_KRYLOV_CG2L coarse space aims for (default 256, 1..1024, others
  * are rejected with CFSA_BAD_ARG). The aggregates are boxes of a uniform grid, so the number
  * actually occupied can exceed the target (256 requested gives 432 on the 1M-tet cylinder); the

@@ -765,6 +765,7 @@ struct Oracle {
   int pressure_solver = 0;  // 0 = BiCGSTAB (reference), 1 = CG, 2 = CG with one reduction,
                             // 3 = the latter with the two-level preconditioner
   int conv_norm = 0;        // 0 = ||r|| (reference), 1 = ||D^-1/2 r||
+  int momentum_solver = 0;  // 0 = BiCGSTAB (reference), 1 = Jacobi CG on the same SPD system
   std::vector<V3> inlet;    // per P2-node inlet velocity (the reference: one mean vector)
   std::vector<V3> u, ustar;
   std::vector<double> p, pcorr, inv_lumped;
@@ -1068,6 +1069,16 @@ struct Oracle {
     return conv;
   }
 
+  // The momentum Krylov solve of one component: the reference's Jacobi BiCGSTAB
+  // (NavierStokes.cpp:498-515), or Jacobi CG on the same symmetric positive definite system. The
+  // device batches the three components; its reductions run over the SELL runs of the P2 pattern
+  // (order_p2: products, and the BiCGSTAB initialisation fused into the right-hand side) and over
+  // natural 256-position blocks (order_n2: vector updates, and the CG initialisation).
+  SolveInfo momentum_solve(const CSR &lhs, const std::vector<double> &rhs, std::vector<double> &x) const {
+    if (momentum_solver == 1) return cg(lhs, rhs, x, tol_mom, maxit_mom, order_p2, order_n2, conv_norm == 1);
+    return bicgstab(lhs, rhs, x, tol_mom, maxit_mom, order_p2, order_p2, order_n2, conv_norm == 1);
+  }
+
   // solveMomentumPredictor (NavierStokes.cpp:416-524)
   bool momentum() {
     const double t0 = now_s();
@@ -1094,7 +1105,7 @@ struct Oracle {
           rhs[i] += penalty * up;
         }
       }
-      SolveInfo si = bicgstab(lhs, rhs, x, tol_mom, maxit_mom, order_p2, order_p2, order_n2, conv_norm == 1);
+      SolveInfo si = momentum_solve(lhs, rhs, x);
       it_mom[comp] = si.iters;
       res_mom[comp] = si.rel_res;
       if (!si.converged) {
@@ -1541,8 +1552,7 @@ struct Oracle {
       // momentum solves (A symmetric)
       for (int a = 0; a < 3; ++a) {
         for (size_t i = 0; i < N2; ++i) lam[i] = lus[i][a];
-        SolveInfo si = bicgstab(A, lam, x, tol_mom, maxit_mom, order_p2, order_p2, order_n2,
-                                conv_norm == 1);
+        SolveInfo si = momentum_solve(A, lam, x);
         adj_it_mom = std::max(adj_it_mom, si.iters);
         if (!si.converged) return 1;
         for (size_t i = 0; i < N2; ++i) nu[i][a] = x[i];
@@ -1734,6 +1744,13 @@ int orc_solve_poisson_raw(void *h, const double *rhs, double *x, double tol, int
 
 // Target number of aggregates of the two-level pressure preconditioner (default 256). Returns 0,
 // or 1 (target unchanged) outside [1, 1024], the range the device solver accepts.
+// Momentum Krylov method: 0 BiCGSTAB (the reference's), 1 Jacobi CG.
+int orc_set_momentum_solver(void *h, int solver) {
+  if (solver != 0 && solver != 1) return 1;
+  static_cast<Oracle *>(h)->momentum_solver = solver;
+  return 0;
+}
+
 int orc_set_coarse_target(void *h, int target) {
   if (target < 1 || target > 1024) return 1;
   Oracle *o = static_cast<Oracle *>(h);

@@ -41,6 +41,7 @@ def lib() -> C.CDLL:
         "orc_set_params": (None, [vp, dbl, dbl, dbl, i32, i32, i32, dbl, dbl, i32, dbl, i32, i32, i32]),
         "orc_set_inlet": (None, [vp, vp]),
         "orc_set_coarse_target": (i32, [vp, i32]),
+        "orc_set_momentum_solver": (i32, [vp, i32]),
         "orc_coarse_size": (i32, [vp]),
         "orc_initialize": (None, [vp]),
         "orc_reference_node": (i32, [vp]),
@@ -155,6 +156,12 @@ class Oracle:
                               float(p["relax_u"]), float(p["relax_p"]), int(p["outlet_type"]),
                               float(p["outlet_pressure"]), int(p["reference_node"]),
                               int(p["pressure_solver"]), int(p["conv_norm"]))
+
+    def set_momentum_solver(self, solver: int):
+        """0: BiCGSTAB (the reference's), 1: Jacobi CG on the same system (as the device's
+        CFSA_KRYLOV_CG momentum method)."""
+        if self.L.orc_set_momentum_solver(self.h, int(solver)) != 0:
+            raise ValueError(f"unknown momentum solver {solver}")
 
     def set_coarse_target(self, target: int):
         """Aggregate count the two-level pressure preconditioner (pressure_solver 3) aims for,

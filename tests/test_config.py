@@ -75,7 +75,7 @@ def test_config_keys_resolved(tmp_path):
     assert float(d["navier_stokes.dt"]) == 0.005 and float(d["navier_stokes.relax_p"]) == 0.7
     assert float(d["navier_stokes.tolerance"]) == 1e-10 and d["navier_stokes.max_iterations"] == "4000 20000"
     assert d["navier_stokes.precision"] == "mixed" and d["navier_stokes.pressure_solver"] == "cg2l"
-    assert d["navier_stokes.coarse_aggregates"] == "128"
+    assert d["navier_stokes.coarse_aggregates"] == "128" and d["navier_stokes.momentum_solver"] == "bicgstab"
     assert d["navier_stokes.convergence_norm"] == "jacobi" and d["navier_stokes.inlet_profile"] == "parabolic"
     assert d["output.prefix"] == "run #1" and d["output.total_steps"] == "7" and d["output.output_frequency"] == "3"
     assert d["adjoint.enabled"] == "1" and d["adjoint.objective"] == "pressure_drop"

@@ -25,12 +25,14 @@ def make_mesh(cf, rings, layers):
     return m
 
 
-def gpu_solver(cf, m, prof, *, tol=1e-13, nu=NU, precision=0, krylov=0):
+def gpu_solver(cf, m, prof, *, tol=1e-13, nu=NU, precision=0, krylov=0, mom_cg=False):
     s = cf.NavierStokesSolver()
     s.setKrylovTolerances(tol, tol)
     s.setMaxIterations(20000, 50000)
     s.setPressureSolver(krylov)
     s.setPrecision(precision)
+    if mom_cg:
+        s.setMomentumSolver(cf.KRYLOV_CG)
     s.setConvergenceNorm(cf.NORM_JACOBI)
     s.setDt(DT)
     s.initialize(m, cf.Fluid(RHO, nu))
@@ -38,11 +40,13 @@ def gpu_solver(cf, m, prof, *, tol=1e-13, nu=NU, precision=0, krylov=0):
     return s
 
 
-def oracle(po, m, prof, *, tol=1e-13, nu=NU, krylov=0):
+def oracle(po, m, prof, *, tol=1e-13, nu=NU, krylov=0, mom_cg=False):
     o = po.Oracle(m.vertices(), m.tets())
     o.set_fluid(RHO, nu)
     o.set_params(dt=DT, tol_mom=tol, tol_p=tol, maxit_mom=20000, maxit_p=50000,
                  pressure_solver={0: 1, 1: 0, 2: 2, 3: 3}[krylov], conv_norm=1)
+    if mom_cg:
+        o.set_momentum_solver(1)
     o.initialize()
     o.set_inlet(prof)
     return o
@@ -77,6 +81,25 @@ def test_adjoint_bit_exact_vs_oracle(cf, po, small, obj, krylov):
     assert np.array_equal(g["grad_u0"], r["grad_u0"]), errs
     assert np.array_equal(g["grad_p0"], r["grad_p0"]), errs
     assert g["grad_viscosity"] == r["grad_viscosity"], errs
+
+
+@pytest.mark.parametrize("obj", [WSS, PDROP], ids=["wall_shear_patch", "pressure_drop"])
+def test_adjoint_momentum_cg_bit_exact_vs_oracle(cf, po, small, obj):
+    """With the momentum CG the forward steps and the reverse pass's momentum solves (A is
+    symmetric, so the adjoint solve is CG on A too) match the oracle bit for bit."""
+    m, prof = small
+    s = gpu_solver(cf, m, prof, krylov=3, mom_cg=True)
+    assert s.adjointForward(4)
+    g = s.adjointBackward(**obj)
+    o = oracle(po, m, prof, krylov=3, mom_cg=True)
+    assert o.adjoint_forward(4) == 0
+    J, su, sp, dnu = o.objective(**obj)
+    r = o.adjoint_backward(su, sp, dnu)
+    assert r["rc"] == 0
+    assert g["J"] == J
+    for k in ("grad_inlet", "grad_u0", "grad_p0"):
+        assert np.array_equal(g[k], r[k]), (k, rel_l2(g[k], r[k]))
+    assert g["grad_viscosity"] == r["grad_viscosity"]
 
 
 def test_adjoint_matches_gpu_central_fd(cf):

@@ -28,7 +28,7 @@ def make_mesh(cf, rings=3, layers=12, length=30.0, radius=2.0):
 
 
 def make_pair(cf, po, m, *, tol=1e-12, krylov=0, dt=0.01, inlet=0.5, profile=None, ncorr=1,
-              relax=(1.0, 1.0), outlet=0, outlet_p=0.0, maxit=(5000, 20000), norm=0):
+              relax=(1.0, 1.0), outlet=0, outlet_p=0.0, maxit=(5000, 20000), norm=0, mom_cg=False):
     """GPU solver and oracle configured identically (the reference's CLI order: initialize with
     a zero inlet, then set the inlet)."""
     s = cf.NavierStokesSolver()
@@ -41,6 +41,8 @@ def make_pair(cf, po, m, *, tol=1e-12, krylov=0, dt=0.01, inlet=0.5, profile=Non
     s.setRelaxP(relax[1])
     s.setOutletType(outlet)
     s.setConvergenceNorm(norm)
+    if mom_cg:
+        s.setMomentumSolver(cf.KRYLOV_CG)
     s.initialize(m, cf.Fluid(RHO, NU))
     s.setOutletPressure(outlet_p)
     o = po.Oracle(m.vertices(), m.tets())
@@ -49,6 +51,8 @@ def make_pair(cf, po, m, *, tol=1e-12, krylov=0, dt=0.01, inlet=0.5, profile=Non
                  n_corr=ncorr, relax_u=relax[0], relax_p=relax[1], outlet_type=outlet,
                  outlet_pressure=outlet_p, reference_node=s.reference_node,
                  pressure_solver={0: 1, 1: 0, 2: 2, 3: 3}[krylov], conv_norm=norm)
+    if mom_cg:
+        o.set_momentum_solver(1)
     o.initialize()
     if profile is not None:
         s.setInletVelocityProfile(profile)
@@ -392,6 +396,61 @@ def test_trajectory_bit_exact(cf, po, krylov):
         assert np.array_equal(s.getPressureCorrection(), st["pcorr"]), k
         assert np.array_equal(s.getVelocity(), st["u"]), k
         assert np.array_equal(s.getPressure(), st["p"]), k
+
+
+@pytest.mark.parametrize("krylov,norm", [(3, 0), (3, 1), (1, 0)], ids=["cg2l", "cg2l_jacobi_norm", "bicgstab"])
+def test_momentum_cg_trajectory_bit_exact(cf, po, krylov, norm):
+    """Momentum CG (CFSA_KRYLOV_CG) against the oracle's Jacobi CG on the same system: the batched
+    kernels reduce in the oracle's orders (products over the SELL runs, vector updates over natural
+    blocks), so the FP64 trajectories and iteration counts agree bit for bit."""
+    m = make_mesh(cf, 3, 12)
+    s, o = make_pair(cf, po, m, tol=1e-10, krylov=krylov, norm=norm, mom_cg=True)
+    for k in range(6):
+        assert s.pisoStep() and o.piso_step() == 0
+        assert s.stats()["momentum_iters"] == o.stats()["momentum_iters"], k
+        assert s.stats()["pressure_iters"] == o.stats()["pressure_iters"], k
+        st = o.state()
+        assert np.array_equal(s.getVelocityStar(), st["ustar"]), k
+        assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"]), k
+
+
+def test_momentum_cg_matches_bicgstab(cf, po):
+    """CG and BiCGSTAB solve the same momentum system: at a tight tolerance in the Jacobi-scaled norm
+    their trajectories agree to the FP64 bar, and CG needs fewer sparse products (one per
+    iteration against two)."""
+    m = make_mesh(cf, 4, 20)
+    out = []
+    for mom_cg in (False, True):
+        s, _ = make_pair(cf, po, m, tol=1e-13, krylov=3, norm=cf.NORM_JACOBI, mom_cg=mom_cg)
+        ok, done = s.pisoSteps(3)
+        assert ok and done == 3
+        out.append((s.getVelocity(), s.getPressure(), s.stats()["momentum_iters"]))
+    assert rel_l2(out[1][0], out[0][0]) <= 1e-8
+    assert rel_l2(out[1][1], out[0][1]) <= 1e-8
+    assert max(out[1][2]) < 2 * max(out[0][2])
+
+
+def test_momentum_cg_graph_equals_eager_and_failures(cf, po):
+    """Graph and eager stepping give the same bits with momentum CG; an iteration cap of one is
+    reported as a failed step (as the oracle's CG reports it), and CG cannot be combined with the
+    mixed-precision momentum solve."""
+    m = make_mesh(cf, 3, 12)
+    out = []
+    for eager in ("0", "1"):
+        os.environ["CFSA_NO_GRAPH"] = eager
+        try:
+            s, _ = make_pair(cf, po, m, tol=1e-10, krylov=3, mom_cg=True)
+            ok, done = s.pisoSteps(3)
+        finally:
+            os.environ.pop("CFSA_NO_GRAPH", None)
+        assert ok and done == 3
+        out.append((s.getVelocity(), s.getPressure()))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    s, o = make_pair(cf, po, m, tol=1e-10, krylov=3, maxit=(1, 20000), mom_cg=True)
+    assert not s.pisoStep()
+    assert o.piso_step() != 0
+    with pytest.raises(cf.CfsaError):
+        s.setPrecision(cf.PRECISION_MIXED)
 
 
 def test_persistent_cg_equals_loop_cg(cf, po):

@@ -76,11 +76,12 @@ def cyl(po):
     return g
 
 
-def run_oracle_cyl(po, g, solver, steps=3):
+def run_oracle_cyl(po, g, solver, steps=3, momentum_solver=0):
     o = po.Oracle(g["xyz"], g["tets"])
     o.set_fluid(1060.0, 0.004)
     o.set_params(dt=0.01, tol_mom=1e-14, tol_p=1e-14, maxit_mom=5000, maxit_p=5000,
                  pressure_solver=solver)
+    o.set_momentum_solver(momentum_solver)
     o.initialize()
     inl = np.zeros((o.N2, 3))
     inl[:, 0] = 0.5
@@ -100,11 +101,13 @@ def test_cylinder_tags_match_golden(po, cyl):
     assert np.array_equal(m["tet_edges"], cyl["te"])
 
 
-@pytest.mark.parametrize("solver", [0, 1], ids=["bicgstab", "cg"])
-def test_cylinder_piso_matches_golden(po, cyl, solver):
+@pytest.mark.parametrize("solver,momentum_solver", [(0, 0), (1, 0), (1, 1)],
+                         ids=["bicgstab", "cg", "cg_momentum_cg"])
+def test_cylinder_piso_matches_golden(po, cyl, solver, momentum_solver):
     """Three pisoSteps of the oracle (tight Krylov tolerance) against the direct-solve numpy
-    restatement: relative L2 <= 1e-8 on u, u*, p and p'."""
-    _, states = run_oracle_cyl(po, cyl, solver)
+    restatement: relative L2 <= 1e-8 on u, u*, p and p'. The momentum system is symmetric positive
+    definite, so its CG solve (momentum_solver 1) meets the same bar."""
+    _, states = run_oracle_cyl(po, cyl, solver, momentum_solver=momentum_solver)
     for k, s in enumerate(states):
         assert rel_l2(s["u"], cyl["u"][k]) < 1e-8
         assert rel_l2(s["ustar"], cyl["ustar"][k]) < 1e-8
