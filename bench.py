@@ -5,7 +5,8 @@ Workload (one "step" = one pisoStep): cylinder L=30, R=2 along x, ~1M tets (16 d
 axial prism layers -> 999,936 tets, N2 = 1,378,515 P2 nodes, nv = 178,106 pressure DOFs),
 rho = 1060, nu = 0.004, dt = 0.01, parabolic inlet u_x = 2*0.5*(1 - r^2/4), no-slip wall, p = 0
 outlet, FP64, two-level CG pressure (single-reduction CG with Jacobi plus an aggregation coarse
-correction) and batched BiCGSTAB momentum to 1e-10 relative residual, from rest. The CPU baseline is the oracle port of the reference algorithm (BiCGSTAB pressure).
+correction) and batched Jacobi CG momentum (the momentum system is symmetric positive definite; the
+reference solves it with BiCGSTAB, `--momentum-solver bicgstab`) to 1e-10 relative residual, from rest. The CPU baseline is the oracle port of the reference algorithm (BiCGSTAB pressure).
 The mesh is synthetic (the reference meshes with TetGen, which is not available here).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cfsa|reference]
@@ -132,8 +133,10 @@ def workload_desc(sizes, rings, layers, world):
     }
 
 
-GPU_SOLVER = ("two-level CG pressure (single-reduction CG, Jacobi + ~256-aggregate coarse correction) + "
-              "batched 3-component BiCGSTAB momentum, FP64, on the GPU")
+def gpu_solver_label():
+    mom = "Jacobi CG" if MOMENTUM_SOLVER == "cg" else "Jacobi BiCGSTAB"
+    return ("two-level CG pressure (single-reduction CG, Jacobi + ~256-aggregate coarse correction) + "
+            f"batched 3-component {mom} momentum, FP64, on the GPU")
 REF_SOLVER = ("reference algorithm (src/FEM/NavierStokes.cpp:416-668): Jacobi BiCGSTAB pressure + per-component "
               "Jacobi BiCGSTAB momentum, FP64, oracle port on the host cores")
 
@@ -145,7 +148,7 @@ def make_mesh(cf, rings, layers):
 
 
 MOMENTUM = {"bicgstab": 1, "cg": 0}  # --momentum-solver -> CFSA_KRYLOV_BICGSTAB / CFSA_KRYLOV_CG
-MOMENTUM_SOLVER = "bicgstab"
+MOMENTUM_SOLVER = "cg"
 
 
 def make_solver(cf, m, tol=TOL, norm=0):
@@ -494,9 +497,9 @@ def rel_l2(a, b) -> float:
     return float(norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0))
 
 
-def trajectory(cf, m, profile, precision, tol, norm, marks):
+def trajectory(cf, m, profile, precision, tol, norm, marks, momentum=None):
     """A solver from rest: device ms over all steps and (u, p, per-step stats) at each mark."""
-    s = make_solver_with(cf, m, profile, tol=tol, norm=norm, precision=precision)
+    s = make_solver_with(cf, m, profile, tol=tol, norm=norm, precision=precision, momentum=momentum)
     out, ms, done, ok = {}, 0.0, 0, True
     iters, upd = [0, 0], 0
     for k in marks:
@@ -511,13 +514,14 @@ def trajectory(cf, m, profile, precision, tol, norm, marks):
     return out, ms, ok, iters
 
 
-def make_solver_with(cf, m, profile, tol=TOL, norm=0, precision=0):
+def make_solver_with(cf, m, profile, tol=TOL, norm=0, precision=0, momentum=None):
     s = cf.NavierStokesSolver()
     s.setKrylovTolerances(tol, tol)
     s.setConvergenceNorm(norm)
     s.setMaxIterations(*MAXIT)
     s.setPressureSolver(cf.KRYLOV_CG2L)
     s.setPrecision(precision)
+    s.setMomentumSolver(MOMENTUM[momentum or MOMENTUM_SOLVER])
     s.setDt(DT)
     s.initialize(m, cf.Fluid(*FLUID))
     s.setInletVelocityProfile(profile)
@@ -525,8 +529,8 @@ def make_solver_with(cf, m, profile, tol=TOL, norm=0, precision=0):
 
 
 def mixed_section(cf, m, profile, marks):
-    """Config 2 on the headline mesh and inputs: FP64 and mixed precision (FP32 BiCGSTAB with FP64
-    reliable updates) from rest over marks[-1] steps, both under the Jacobi-scaled criterion at
+    """Config 2 on the headline mesh and inputs: FP64 and mixed precision (the headline's momentum
+    Krylov method in FP32 with FP64 reliable updates) from rest over marks[-1] steps, both under the Jacobi-scaled criterion at
     1e-10 (the reference's criterion is dominated by the 1e10 penalty rows and pins the interior
     only loosely), and an FP64 run at 1e-14 in the same norm as the converged solution; fields at
     every mark. Both paths run the two-level CG pressure solve in FP64."""
@@ -536,9 +540,10 @@ def mixed_section(cf, m, profile, marks):
     full, x_ms, x_ok, x_it = trajectory(cf, m, profile, cf.PRECISION_MIXED_FULL, TOL, J, marks)
     conv, _, c_ok, _ = trajectory(cf, m, profile, cf.PRECISION_FP64, 1e-14, J, marks)
     n = marks[-1]
-    res = {"workload": f"config 2: the headline mesh and inputs, {n} steps from rest; momentum BiCGSTAB with FP32 "
+    mom = "Jacobi CG" if MOMENTUM_SOLVER == "cg" else "BiCGSTAB"
+    res = {"workload": f"config 2: the headline mesh and inputs, {n} steps from rest; momentum {mom} with FP32 "
                        f"operator and Krylov vectors and FP64 reliable updates (true residual, solution, dots) vs "
-                       f"FP64 BiCGSTAB; two-level CG pressure in FP64 in both (CFSA_PRECISION_MIXED); "
+                       f"FP64 {mom}; two-level CG pressure in FP64 in both (CFSA_PRECISION_MIXED); "
                        f"Jacobi-scaled criterion 1e-10",
            "ok": bool(f_ok and m_ok and c_ok), "steps": n,
            "value": n / (m_ms / 1e3), "unit": UNIT, "fp64_value": n / (f_ms / 1e3),
@@ -561,6 +566,18 @@ def mixed_section(cf, m, profile, marks):
             "reliable_updates": mix[k][2]["momentum_outer"],
             "pressure_iters": mix[k][2]["pressure_iters"],
         }
+    if MOMENTUM_SOLVER == "cg":
+        # the same comparison with the reference's momentum method (BiCGSTAB in both precisions)
+        bf, bf_ms, bf_ok, bf_it = trajectory(cf, m, profile, cf.PRECISION_FP64, TOL, J, marks, "bicgstab")
+        bm, bm_ms, bm_ok, bm_it = trajectory(cf, m, profile, cf.PRECISION_MIXED, TOL, J, marks, "bicgstab")
+        res["bicgstab"] = {
+            "what": "momentum BiCGSTAB (the reference's method) in both precisions, same pressure and criterion",
+            "ok": bool(bf_ok and bm_ok), "value": n / (bm_ms / 1e3), "fp64_value": n / (bf_ms / 1e3),
+            "speedup_vs_fp64": bf_ms / bm_ms, "ms_per_step": bm_ms / n, "fp64_ms_per_step": bf_ms / n,
+            "krylov_iters_per_step": {"mixed": [bm_it[0] / n, bm_it[1] / n], "fp64": [bf_it[0] / n, bf_it[1] / n]},
+            "mixed_vs_fp64": {str(k): {"u": rel_l2(bm[k][0], bf[k][0]), "p": rel_l2(bm[k][1], bf[k][1])} for k in marks},
+            "mixed_vs_converged": {str(k): {"u": rel_l2(bm[k][0], conv[k][0]), "p": rel_l2(bm[k][1], conv[k][1])}
+                                   for k in marks}}
     first = marks[0]
     return res, {"mixed": mix[first][:2], "fp64": f64[first][:2]}
 
@@ -572,10 +589,12 @@ def cpu_section(args, gpu_headline, gpu_step1_jacobi):
     steps 1 and 3; (2) config 2's CPU comparison, FP64 in the Jacobi-scaled criterion, step 1;
     (3) the timed CPU baseline, the reference algorithm (BiCGSTAB pressure) on all host threads."""
     po, o = oracle_cylinder(args.rings, args.layers, pressure_solver=3)
+    o.set_momentum_solver(1 if MOMENTUM_SOLVER == "cg" else 0)
     threads = po.set_threads(os.cpu_count() or 1)
     zero_u, zero_p = np.zeros((o.N2, 3)), np.zeros(o.nv)
-    parity = {"workload": "headline FP64 step (two-level CG pressure, reference criterion 1e-10) from rest, "
-                          "GPU vs the oracle on the same mesh and inputs", "at_step": {}}
+    mom = "Jacobi CG" if MOMENTUM_SOLVER == "cg" else "BiCGSTAB"
+    parity = {"workload": f"headline FP64 step (two-level CG pressure, {mom} momentum, reference criterion 1e-10) "
+                          "from rest, GPU vs the oracle on the same mesh and inputs", "at_step": {}}
     t0 = time.perf_counter()
     for k in (1, 2, 3):
         if o.piso_step() != 0:
@@ -594,6 +613,7 @@ def cpu_section(args, gpu_headline, gpu_step1_jacobi):
         o.set_state(zero_u, zero_p)
         o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=3,
                      conv_norm=1)
+        o.set_momentum_solver(1 if MOMENTUM_SOLVER == "cg" else 0)  # config 2's FP64 path
         if o.piso_step() == 0:
             st = o.state()
             mixed_cpu = {"reference": "FP64 oracle (CPU), Jacobi-scaled criterion 1e-10, step 1 from rest"}
@@ -603,6 +623,7 @@ def cpu_section(args, gpu_headline, gpu_step1_jacobi):
     if not args.no_cpu_baseline:
         o.set_state(zero_u, zero_p)
         o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=0)
+        o.set_momentum_solver(0)  # the reference algorithm
         if o.piso_step() == 0:
             done, el, cores = time_oracle_steps(po, o, os.cpu_count() or 1, 5, 30.0)
             if done:
@@ -702,7 +723,8 @@ def main():
     peak, peak_kind = measured_peak()
     traffic = traffic_table()
     kernels = {}
-    for name, which, per_step in (("momentum_spmv_3rhs", cf.KERNEL_MOMENTUM_SPMV, 2 * st["krylov_iters"][0]),
+    products = 1 if MOMENTUM_SOLVER == "cg" else 2  # momentum products per Krylov iteration
+    for name, which, per_step in (("momentum_spmv_3rhs", cf.KERNEL_MOMENTUM_SPMV, products * st["krylov_iters"][0]),
                                   ("pressure_cg_solve", cf.KERNEL_PRESSURE_SOLVE, args.steps),
                                   ("momentum_spmv_3rhs_f32", cf.KERNEL_MOMENTUM_SPMV_F32, 0)):
         ms, by = s.profileKernel(which, 3 if which == cf.KERNEL_PRESSURE_SOLVE else 20)
@@ -772,7 +794,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": DATA,
             "config": workload_desc((nv, nt, ne), args.rings, args.layers, world),
-            "solver": GPU_SOLVER,
+            "solver": gpu_solver_label(),
             "dof_updates_per_s": value * (3 * N2 + nv),
             "krylov_iters_per_step": [st["krylov_iters"][0] / args.steps, st["krylov_iters"][1] / args.steps],
             "gpu_launches": int(st["kernel_launches"]),

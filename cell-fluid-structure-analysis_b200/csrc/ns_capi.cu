@@ -560,6 +560,8 @@ struct cfsa_ns {
         q((const void *)k_bicg_xr<3>);
         q((const void *)k_bicg_xr<1>);
         q((const void *)k_mcg_xr<3>);
+        q((const void *)k_mpc_xr);
+        q((const void *)k_mpc_init);
         q((const void *)k_mcg_init<3>);
         q((const void *)k_mp_xr);
         q((const void *)k_mp_init);
@@ -1147,6 +1149,10 @@ struct cfsa_ns {
   // is one iteration followed by an IF node holding the reliable update; eager: the update
   // kernels run after every iteration and return at once when no component asked for one.
   void enqueue_momentum_mixed(bool capture, double *x, DevStatus *s_out) {
+    if (mom_krylov == CFSA_KRYLOV_CG) {
+      enqueue_momentum_mixed_cg(capture, x, s_out);
+      return;
+    }
     const MixedArgs a = mixed_args(x, s_out);
     const unsigned int gp = blocks_for(N2);
     k_mp_init<<<strided(k_mp_init, gp), kBlock, 0, stream>>>(a, tol_mom, maxit_mom, mixed_delta);
@@ -1171,6 +1177,40 @@ struct cfsa_ns {
                           [&](cudaStream_t ss, cudaGraphConditionalHandle, int) { update_body(ss, b); });
       else
         update_body(s, b);
+    };
+    if (capture)
+      capture_while(body);
+    else
+      eager_while(body, [&] { return poll_mixed(); }, maxit_mom);
+    k_mp_check<<<1, 1, 0, stream>>>(ms, s_out);
+    CK(cudaGetLastError());
+  }
+
+  // FP32 CG with FP64 reliable updates (ns_mixed.cuh, k_mpc_*): per iteration the product, the
+  // x/r update and, after the reliable-update IF node, the direction update.
+  void enqueue_momentum_mixed_cg(bool capture, double *x, DevStatus *s_out) {
+    const MixedArgs a = mixed_args(x, s_out);
+    const unsigned int gp = blocks_for(N2);
+    k_mpc_init<<<strided(k_mpc_init, gp), kBlock, 0, stream>>>(a, tol_mom, maxit_mom, mixed_delta);
+    CK(cudaGetLastError());
+    auto update_body = [&](cudaStream_t s, MixedArgs b) {
+      k_mpc_xupdate<<<gp, kBlock, 0, s>>>(b);
+      k_mpc_residual<<<s2.nruns, kRunThreads, 0, s>>>(b);
+    };
+    auto body = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) {
+      MixedArgs b = a;
+      b.cond = h;
+      b.use_cond = use;
+      b.use_if = use;
+      if (b.use_if) b.cond_upd = new_cond_handle(s, 0);
+      k_mpc_q<<<s2.nruns, kRunThreads, 0, s>>>(b);
+      k_mpc_xr<<<strided(k_mpc_xr, gp), kBlock, 0, s>>>(b);
+      if (b.use_if)
+        capture_cond_with(s, body_stream2, b.cond_upd, cudaGraphCondTypeIf,
+                          [&](cudaStream_t ss, cudaGraphConditionalHandle, int) { update_body(ss, b); });
+      else
+        update_body(s, b);
+      k_mpc_p<<<gp, kBlock, 0, s>>>(b);
     };
     if (capture)
       capture_while(body);
@@ -1674,7 +1714,7 @@ struct cfsa_ns {
   }
   // Kernels of one momentum-solve body run (DevStatus::body_runs[0]): BiCGSTAB 5, CG 3.
   bool momentum_cg() const { return !momentum_mixed() && mom_krylov == CFSA_KRYLOV_CG; }
-  int momentum_body_kernels() const { return momentum_cg() ? 3 : 5; }
+  int momentum_body_kernels() const { return mom_krylov == CFSA_KRYLOV_CG ? 3 : 5; }
   int mixed_fixed_kernels() const {
     return (momentum_mixed() ? 1 : 0) + (pressure_mixed() ? 1 : 0) + (momentum_cg() ? 1 : 0);
   }
@@ -2190,12 +2230,17 @@ struct cfsa_ns {
       CK(cudaMemcpyAsync(ms_prof, &hm, sizeof(hm), cudaMemcpyHostToDevice, stream));
       MixedArgs a = mixed_args(ustar, nullptr);
       a.ms = ms_prof;
-      a.p = fr;   // the FP32 Krylov vectors of the last mixed solve (any values serve the timing)
-      a.r0 = fr0;
+      // input: the velocity rounded to float (nonzero wherever the flow is, so neither method's
+      // dot product vanishes; a zero p.q would end the CG product early); fs and ft are FP32 Krylov
+      // scratch that every mixed solve rewrites before reading
+      k_to_f32<<<blocks_for(3 * N2), kBlock, 0, stream>>>(3 * N2, u, fs);
+      a.p = fs;
+      a.r0 = fs;
       a.v = ft;   // scratch output
-      k_mp_v<<<s2.nruns, kRunThreads, 0, stream>>>(a);  // warm-up
+      auto *kern = (mom_krylov == CFSA_KRYLOV_CG) ? k_mpc_q : k_mp_v;  // the method's FP32 product
+      kern<<<s2.nruns, kRunThreads, 0, stream>>>(a);  // warm-up
       CK(cudaEventRecord(ev0, stream));
-      for (int k = 0; k < iters; ++k) k_mp_v<<<s2.nruns, kRunThreads, 0, stream>>>(a);
+      for (int k = 0; k < iters; ++k) kern<<<s2.nruns, kRunThreads, 0, stream>>>(a);
       CK(cudaEventRecord(ev1, stream));
       *alg_bytes = 8.0 * (double)nnz2 + 8.0 * s2.nrows_pad + 4.0 * (s2.nslices + 1) + 36.0 * (double)N2;
     } else if (which == CFSA_KERNEL_MOMENTUM_SPMV) {
@@ -2208,9 +2253,12 @@ struct cfsa_ns {
       a.bs = bs_prof;
       a.st = nullptr;
       a.v = ws;  // scratch output
-      k_bicg_v<3><<<s2.nruns, kRunThreads, 0, stream>>>(a);  // warm-up
+      // the product kernel of the selected momentum method (BiCGSTAB: v = At p with r0.v; CG:
+      // q = A p with p.q); same matrix stream, gathers and algorithmic bytes
+      auto *kern = (mom_krylov == CFSA_KRYLOV_CG) ? k_mcg_q<3> : k_bicg_v<3>;
+      kern<<<s2.nruns, kRunThreads, 0, stream>>>(a);  // warm-up
       CK(cudaEventRecord(ev0, stream));
-      for (int k = 0; k < iters; ++k) k_bicg_v<3><<<s2.nruns, kRunThreads, 0, stream>>>(a);
+      for (int k = 0; k < iters; ++k) kern<<<s2.nruns, kRunThreads, 0, stream>>>(a);
       CK(cudaEventRecord(ev1, stream));
       *alg_bytes = 12.0 * (double)nnz2 + 8.0 * s2.nrows_pad + 4.0 * (s2.nslices + 1) + 72.0 * (double)N2;
     } else if (which == CFSA_KERNEL_PRESSURE_SPMV) {
@@ -2444,8 +2492,6 @@ int cfsa_ns_set_momentum_solver(cfsa_ns *h, int krylov) {
   if (!h) return CFSA_BAD_ARG;
   if (krylov != CFSA_KRYLOV_CG && krylov != CFSA_KRYLOV_BICGSTAB)
     return fail(h, CFSA_BAD_ARG, "momentum Krylov method must be CFSA_KRYLOV_BICGSTAB or CFSA_KRYLOV_CG");
-  if (krylov == CFSA_KRYLOV_CG && h->precision != CFSA_PRECISION_FP64)
-    return fail(h, CFSA_UNSUPPORTED, "the mixed-precision momentum solve is BiCGSTAB only");
   if (krylov != h->mom_krylov) {
     h->mom_dirty = true;  // the SELL values change between A D^-1 and A
     h->graph_dirty = true;
@@ -2476,8 +2522,6 @@ int cfsa_ns_set_precision(cfsa_ns *h, int precision) {
   if (precision != CFSA_PRECISION_FP64 && precision != CFSA_PRECISION_MIXED &&
       precision != CFSA_PRECISION_MIXED_FULL)
     return fail(h, CFSA_BAD_ARG, "unknown precision");
-  if (precision != CFSA_PRECISION_FP64 && h->mom_krylov == CFSA_KRYLOV_CG)
-    return fail(h, CFSA_UNSUPPORTED, "the mixed-precision momentum solve is BiCGSTAB only");
   if (precision != h->precision) h->graph_dirty = true;
   h->precision = precision;
   return CFSA_OK;

@@ -530,6 +530,307 @@ __global__ void k_mp_check(const MixedState *__restrict__ m, DevStatus *st) {
 }
 
 // ------------------------------------------------------------------------------------------
+// Mixed-precision momentum CG (the CFSA_KRYLOV_CG momentum method with a mixed precision): one
+// batched Jacobi CG sequence in FP32 with FP64 reliable updates, the scheme of the BiCGSTAB above
+// applied to CG (residual replacement with group-wise solution updates, van der Vorst & Ye 2000).
+//   FP64: b, x (solution), r64 (true residual); FP32: r, p, q, dx; FP32 copy A32 of A
+//   every iteration (FP64 dot products and scalars):
+//     q = A32 p; alpha = rho / (p.q); dx += alpha p; r -= alpha q; z = D^-1 r; rho' = r.z
+//   reliable update of component c when its iterated residual has dropped below delta times the
+//   largest one since its last update, meets the tolerance or hits the cap:
+//     x += dx; dx = 0; r64 = b - A x (FP64 operator); r = (float) r64; rho' = r.z
+//   then p = z + (rho'/rho) p: the search direction carries on across updates. Convergence is
+//   decided on the FP64 true residual with the FP64 solve's criterion. An update that finds the
+//   true residual more than 10x the iterated one, or larger than at the previous update, restarts
+//   the direction (p = z).
+
+// Init (after k_momentum_rhs wrote b and x = 0): r = (float) b, p = z = D^-1 r, dx = 0; the FP64
+// ||b|| in the convergence norm and rho = r.z.
+__global__ void k_mpc_init(MixedArgs A, double tol, int maxit, double delta) {
+  if (A.st->halt) return;
+  const int64_t n = A.n;
+  __shared__ WarpSums<6> S;
+  const int nblk = (A.n + kBlock - 1) / kBlock;
+  int slot = 0;
+  for (int bk = blockIdx.x; bk < nblk; bk += gridDim.x, ++slot) {
+    const int i = bk * kBlock + threadIdx.x;
+    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (i < A.n) {
+      const double w = A.cw ? A.cw[i] : 1.0;
+      const float dinv = A.invA32[i];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int64_t o = c * n + i;
+        const double bi = A.b[o];
+        const float ri = (float)bi;
+        const float zi = dinv * ri;
+        A.r[o] = ri;
+        A.p[o] = zi;
+        A.dx[o] = 0.f;
+        part[c] = (bi * bi) * w;
+        part[3 + c] = (double)ri * (double)zi;
+      }
+    }
+    warp_partial<6>(part, S, slot);
+  }
+  double tot[6];
+  if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
+    MixedState *m = A.ms;
+    m->active = 0;
+    m->upd = 0;
+    m->restart = 0;
+    m->restart_next = 0;
+    m->force = 0;
+    m->maxit = maxit;
+    m->delta2 = delta * delta;
+    for (int c = 0; c < 3; ++c) {
+      m->bnorm2[c] = tot[c];
+      m->rnorm2[c] = tot[c];
+      m->rin2[c] = tot[c];
+      m->rmax2[c] = tot[c];
+      m->tol2[c] = tol * tol * tot[c];
+      m->rho[c] = tot[3 + c];
+      m->alpha[c] = 0.0;
+      m->beta[c] = 0.0;
+      m->iters[c] = 0;
+      m->updates[c] = 0;
+      m->restarts[c] = 0;
+      if (isnan(tot[c]) || isnan(tot[3 + c])) {
+        m->status[c] = KS_BREAKDOWN;
+      } else if (tot[c] == 0.0 || tot[c] <= m->tol2[c]) {
+        m->status[c] = KS_CONVERGED;
+      } else {
+        m->status[c] = KS_RUNNING;
+        m->active |= 1 << c;
+      }
+    }
+  }
+}
+
+// C1: q = A32 p (into v), alpha = rho / (p . q)
+__global__ void __launch_bounds__(kRunThreads, 1) k_mpc_q(MixedArgs A) {
+  const int act = A.ms->active;
+  if (!act) return;
+  const int64_t n = A.n;
+  const int s1 = A.S.rfirst[blockIdx.x + 1];
+  __shared__ int s_next;
+  const int sl0 = run_first_slice(&s_next, A.S.rfirst[blockIdx.x]);
+  with_mask<3>(act, [&](auto mk) {
+    constexpr int MASK = decltype(mk)::value;
+    for (int sl = sl0; sl < s1; sl = run_next_slice(&s_next)) {
+      const int r = sl * kSellC + (threadIdx.x & 31);
+      const int i = A.S.perm[r];
+      double part[3] = {0.0, 0.0, 0.0};
+      if (i >= 0) {
+        float acc[3];
+        sell_spmv_row_f32x3<8, MASK>(A.S, A.At32, A.p, n, r, acc);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (!((MASK >> c) & 1)) continue;
+          A.v[c * n + i] = acc[c];
+          part[c] = (double)A.p[c * n + i] * (double)acc[c];
+        }
+      }
+      slice_partial<3>(part, A.S, sl);
+    }
+  });
+  double tot[3];
+  if (grid_reduce_runs<3>(A.S, A.red, tot) && threadIdx.x == 0) {
+    for (int c = 0; c < 3; ++c) {
+      if (!((act >> c) & 1)) continue;
+      if (isnan(tot[c]) || tot[c] == 0.0) {
+        A.ms->status[c] = KS_BREAKDOWN;
+        A.ms->active &= ~(1 << c);
+      } else {
+        A.ms->alpha[c] = A.ms->rho[c] / tot[c];
+      }
+    }
+  }
+}
+
+// C2: dx += alpha p, r -= alpha q, z = D^-1 r; the iterated residual (convergence norm) and r.z;
+// which components take a reliable update at the end of this iteration (IF node); next beta for
+// the others.
+__global__ void k_mpc_xr(MixedArgs A) {
+  const int act = A.ms->active;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[0] += 1;
+  if (!act) {
+    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) {
+      if (A.use_if) cudaGraphSetConditional(A.cond_upd, 0);
+      cudaGraphSetConditional(A.cond, 0);
+    }
+    return;
+  }
+  const int64_t n = A.n;
+  __shared__ WarpSums<6> S;
+  const int nblk = (A.n + kBlock - 1) / kBlock;
+  float alpha_c[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) alpha_c[c] = (float)A.ms->alpha[c];
+  int slot = 0;
+  for (int bk = blockIdx.x; bk < nblk; bk += gridDim.x, ++slot) {
+    const int i = bk * kBlock + threadIdx.x;
+    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (i < A.n) {
+      const float dinv = A.invA32[i];
+      const double w = A.cw32 ? (double)A.cw32[i] : 1.0;
+      float pv[3], qv[3], rv[3], dxv[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (!((act >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        pv[c] = A.p[o], qv[c] = A.v[o], rv[c] = A.r[o], dxv[c] = A.dx[o];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (!((act >> c) & 1)) continue;
+        const int64_t o = c * n + i;
+        A.dx[o] = dxv[c] + alpha_c[c] * pv[c];
+        const float ri = rv[c] - alpha_c[c] * qv[c];
+        A.r[o] = ri;
+        const float zi = dinv * ri;
+        part[c] = ((double)ri * (double)ri) * w;
+        part[3 + c] = (double)ri * (double)zi;
+      }
+    }
+    warp_partial<6>(part, S, slot);
+  }
+  double tot[6];
+  if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
+    MixedState *m = A.ms;
+    int upd = 0;
+    for (int c = 0; c < 3; ++c) {
+      if (!((act >> c) & 1)) continue;
+      m->iters[c] += 1;
+      m->rin2[c] = tot[c];
+      if (isnan(tot[c]) || isnan(tot[3 + c])) {
+        m->status[c] = KS_BREAKDOWN;
+        m->active &= ~(1 << c);
+        continue;
+      }
+      if (tot[c] <= m->tol2[c] || m->iters[c] >= m->maxit || tot[c] < m->delta2 * m->rmax2[c]) {
+        upd |= 1 << c;  // the update replaces rho and beta from the true residual
+      } else {
+        m->beta[c] = tot[3 + c] / m->rho[c];
+        m->rho[c] = tot[3 + c];
+        m->rmax2[c] = fmax(m->rmax2[c], tot[c]);
+      }
+    }
+    m->upd = upd;
+    if (A.use_cond) {
+      if (A.use_if) cudaGraphSetConditional(A.cond_upd, upd ? 1u : 0u);
+      cudaGraphSetConditional(A.cond, m->active ? 1u : 0u);
+    }
+  }
+}
+
+// Reliable update, part 1: x += dx (FP64) and dx = 0 for the updated components.
+__global__ void k_mpc_xupdate(MixedArgs A) {
+  const int upd = A.ms->upd;
+  if (!upd) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const int64_t n = A.n;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (!((upd >> c) & 1)) continue;
+    const int64_t o = c * n + i;
+    A.x[o] = A.x[o] + (double)A.dx[o];
+    A.dx[o] = 0.f;
+  }
+}
+
+// Reliable update, part 2: r64 = b - A x (FP64 operator, rows in SELL order), r = (float) r64;
+// convergence on the true residual; rho = r.z and the next beta from the replaced residual (0 when
+// the direction restarts).
+__global__ void __launch_bounds__(kRunThreads, 1) k_mpc_residual(MixedArgs A) {
+  const int upd = A.ms->upd;
+  if (!upd) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.st) A.st->body_runs[2] += 1;
+  const int64_t n = A.n;
+  const int s1 = A.S.rfirst[blockIdx.x + 1];
+  __shared__ int s_next;
+  const int sl0 = run_first_slice(&s_next, A.S.rfirst[blockIdx.x]);
+  with_mask<3>(upd, [&](auto mk) {
+    constexpr int MASK = decltype(mk)::value;
+    for (int sl = sl0; sl < s1; sl = run_next_slice(&s_next)) {
+      const int r = sl * kSellC + (threadIdx.x & 31);
+      const int i = A.S.perm[r];
+      double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      if (i >= 0) {
+        double acc[3];
+        sell_spmv_row<3, kU64, MASK>(A.S, A.At64, A.x, n, r, acc);
+        const double w = A.cw ? A.cw[i] : 1.0;
+        const float dinv = A.invA32[i];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (!((MASK >> c) & 1)) continue;
+          const int64_t o = c * n + i;
+          const double ri = A.b[o] - acc[c];
+          A.r64[o] = ri;
+          const float rf = (float)ri;
+          A.r[o] = rf;
+          part[c] = (ri * ri) * w;
+          part[3 + c] = (double)rf * (double)(dinv * rf);
+        }
+      }
+      slice_partial<6>(part, A.S, sl);
+    }
+  });
+  double tot[6];
+  if (grid_reduce_runs<6>(A.S, A.red, tot) && threadIdx.x == 0) {
+    MixedState *m = A.ms;
+    for (int c = 0; c < 3; ++c) {
+      if (!((upd >> c) & 1)) continue;
+      m->updates[c] += 1;
+      const double prev2 = m->rnorm2[c];  // true residual at the previous update
+      m->rnorm2[c] = tot[c];
+      const double rz = tot[3 + c];
+      if (isnan(tot[c]) || isnan(rz)) {
+        m->status[c] = KS_BREAKDOWN;
+        m->active &= ~(1 << c);
+      } else if (tot[c] <= m->tol2[c]) {
+        m->status[c] = KS_CONVERGED;
+        m->active &= ~(1 << c);
+      } else if (m->iters[c] >= m->maxit) {
+        m->status[c] = KS_MAXIT;
+        m->active &= ~(1 << c);
+      } else {
+        // the FP32 recurrence drifted from the true residual, or convergence turned erratic:
+        // restart the direction from the replaced residual
+        const bool restart = tot[c] > kMixedDrift2 * m->rin2[c] || tot[c] > prev2;
+        m->beta[c] = restart ? 0.0 : rz / m->rho[c];
+        if (restart) m->restarts[c] += 1;
+        m->rho[c] = rz;
+        m->rin2[c] = tot[c];
+        m->rmax2[c] = tot[c];
+      }
+    }
+    m->upd = 0;
+    if (A.use_cond) cudaGraphSetConditional(A.cond, m->active ? 1u : 0u);
+  }
+}
+
+// C3: p = z + beta p with z = D^-1 r (after the update, which may have replaced r and beta)
+__global__ void k_mpc_p(MixedArgs A) {
+  const int act = A.ms->active;
+  if (!act) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const int64_t n = A.n;
+  const float dinv = A.invA32[i];
+  float beta[3], rv[3], pv[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    beta[c] = (float)A.ms->beta[c];
+    if ((act >> c) & 1) rv[c] = A.r[c * n + i], pv[c] = A.p[c * n + i];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    if ((act >> c) & 1) A.p[c * n + i] = dinv * rv[c] + beta[c] * pv[c];
+}
+
+// ------------------------------------------------------------------------------------------
 // Mixed-precision pressure solve: FP64 defect correction around the two-level CG with float
 // storage (k_cg2l_resident<float>: operator values, inverse diagonal and Krylov vectors in float,
 // arithmetic and reductions in FP64).

@@ -161,7 +161,7 @@ int cfsa_ns_set_pressure_solver(cfsa_ns *h, int krylov);                   /* ne
  * src/FEM/NavierStokes.cpp:498-515) or CFSA_KRYLOV_CG (Jacobi-preconditioned CG on the same
  * system: M/dt + K + the 1e10 Dirichlet penalty is symmetric positive definite because the
  * convection term is explicit; one sparse product per iteration instead of two; same stopping
- * rule). CG with a mixed precision returns CFSA_UNSUPPORTED. */
+ * rule). With a mixed precision the CG runs in FP32 with FP64 reliable updates, like BiCGSTAB. */
 int cfsa_ns_set_momentum_solver(cfsa_ns *h, int krylov);
 /* new: aggregate count the CFSA_KRYLOV_CG2L coarse space aims for (default 256, 1..1024, others
  * are rejected with CFSA_BAD_ARG). The aggregates are boxes of a uniform grid, so the number

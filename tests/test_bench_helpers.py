@@ -28,6 +28,7 @@ def test_cpu_section_parity_and_baseline_on_a_small_mesh():
 
     args = SimpleNamespace(rings=2, layers=6, no_cpu_baseline=False)
     _, o = bench.oracle_cylinder(2, 6, pressure_solver=3)
+    o.set_momentum_solver(1 if bench.MOMENTUM_SOLVER == "cg" else 0)  # the headline's method
     states = {}
     for k in (1, 2, 3):
         assert o.piso_step() == 0

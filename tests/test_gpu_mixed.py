@@ -152,3 +152,47 @@ def test_mixed_keeps_fp64_pressure(cf, po):
     out = run(cf, po, m, cf.PRECISION_MIXED, 2, 1e-12, krylov=cf.KRYLOV_CG2L)
     for _, _, st in out:
         assert st["pressure_outer"] == 0 and max(st["momentum_outer"]) >= 1
+
+
+@pytest.mark.parametrize("rings,layers", [(3, 12), (5, 68)])
+def test_mixed_momentum_cg_matches_converged_fp64(cf, po, rings, layers):
+    """The momentum CG in FP32 with FP64 reliable updates (CFSA_KRYLOV_CG with a mixed precision)
+    against a converged FP64 solution, Jacobi-scaled criterion: the same <= 1e-6 bar as the mixed
+    BiCGSTAB, with the true FP64 residual at the tolerance."""
+    m = make_mesh(cf, rings, layers)
+    ref = run(cf, po, m, cf.PRECISION_FP64, 10, 1e-14, norm=cf.NORM_JACOBI)
+    mix = run(cf, po, m, cf.PRECISION_MIXED, 10, 1e-12, norm=cf.NORM_JACOBI, mom_cg=True)
+    for k in (0, 4, 9):
+        eu, ep = rel_l2(mix[k][0], ref[k][0]), rel_l2(mix[k][1], ref[k][1])
+        print(f"step {k + 1}: mixed CG(1e-12) vs fp64(1e-14) rel L2 u {eu:.2e} p {ep:.2e}; "
+              f"iters {mix[k][2]['momentum_iters']} updates {mix[k][2]['momentum_outer']}")
+        assert eu <= 1e-6 and ep <= 1e-6, (k, eu, ep)
+    for _, _, st in mix:
+        assert max(st["momentum_residual"]) <= 1e-12
+        assert max(st["momentum_outer"]) >= 1
+
+
+def test_mixed_momentum_cg_graph_eager_and_failure(cf, po):
+    """Graph and eager stepping of the mixed momentum CG give the same bits; it stays as close to
+    the converged solution as FP64 CG at the configs' tolerance; an unreachable tolerance ends in a
+    failed step that does not advance time."""
+    m = make_mesh(cf, 3, 12)
+    res = []
+    for ng in ("0", "1"):
+        os.environ["CFSA_NO_GRAPH"] = ng
+        try:
+            out = run(cf, po, m, cf.PRECISION_MIXED, 3, 1e-12, mom_cg=True)
+        finally:
+            os.environ.pop("CFSA_NO_GRAPH", None)
+        res.append(out[-1])
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+    ref = run(cf, po, m, cf.PRECISION_FP64, 5, 1e-14)
+    f64 = run(cf, po, m, cf.PRECISION_FP64, 5, 1e-10, mom_cg=True)
+    mix = run(cf, po, m, cf.PRECISION_MIXED, 5, 1e-10, mom_cg=True)
+    e64, emx = rel_l2(f64[-1][0], ref[-1][0]), rel_l2(mix[-1][0], ref[-1][0])
+    print(f"5 steps at tol 1e-10: fp64 CG {e64:.2e}, mixed CG {emx:.2e} from the converged solution")
+    assert emx <= 1.5 * e64
+    s, _ = make_pair(cf, po, make_mesh(cf, 2, 6), tol=1e-20, mom_cg=True)
+    s.setPrecision(cf.PRECISION_MIXED)
+    assert not s.pisoStep()
+    assert s.getTime() == 0.0
