@@ -200,12 +200,16 @@ def test_reference_default_tolerances(cf, po):
 
 
 @pytest.mark.parametrize("case", ["neumann", "two_correctors", "relaxed", "parabolic", "outlet_p",
-                                  "neumann_cg2l"])
+                                  "neumann_cg2l", "neumann_momentum_cg", "two_correctors_relaxed_momentum_cg"])
 def test_variants_parity(cf, po, case):
     m = make_mesh(cf, 3, 12)
     kw = dict(tol=1e-13)
     if case == "neumann_cg2l":
         kw.update(outlet=1, krylov=cf.KRYLOV_CG2L)
+    elif case == "neumann_momentum_cg":
+        kw.update(outlet=1, krylov=cf.KRYLOV_CG2L, mom_cg=True)
+    elif case == "two_correctors_relaxed_momentum_cg":
+        kw.update(ncorr=2, relax=(0.7, 0.6), krylov=cf.KRYLOV_CG2L, mom_cg=True)
     if case == "neumann":
         kw.update(outlet=1)
     elif case == "two_correctors":
