@@ -178,6 +178,9 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "cfsa_ns_set_inlet_profile": (i32, [vp, vp]),
         "cfsa_ns_set_pressure_solver": (i32, [vp, i32]),
         "cfsa_ns_set_momentum_solver": (i32, [vp, i32]),
+        "cfsa_ns_get_velocity_async": (i32, [vp, vp]),
+        "cfsa_ns_get_pressure_async": (i32, [vp, vp]),
+        "cfsa_ns_wait_outputs": (i32, [vp]),
         "cfsa_ns_set_coarse_target": (i32, [vp, i32]),
         "cfsa_ns_save_state": (i32, [vp, C.c_char_p]),
         "cfsa_ns_load_state": (i32, [vp, C.c_char_p]),
@@ -552,6 +555,27 @@ class NavierStokesSolver:
         out = self._out((self.N2, 3), out)
         self._check(self._lib.cfsa_ns_get_velocity(self._h, _ptr(out)))
         return out
+
+    def getVelocityAsync(self, out: np.ndarray) -> np.ndarray:
+        """Stream-ordered read-back of u into `out` (C-contiguous float64 [N2, 3], ideally pinned):
+        returns at once, the copy overlaps later steps; `out` is complete after waitOutputs()."""
+        if out is None:
+            raise ValueError("getVelocityAsync needs a caller-owned output array")
+        out = self._out((self.N2, 3), out)
+        self._check(self._lib.cfsa_ns_get_velocity_async(self._h, _ptr(out)))
+        return out
+
+    def getPressureAsync(self, out: np.ndarray) -> np.ndarray:
+        """As getVelocityAsync for p ([nv])."""
+        if out is None:
+            raise ValueError("getPressureAsync needs a caller-owned output array")
+        out = self._out((self.nv,), out)
+        self._check(self._lib.cfsa_ns_get_pressure_async(self._h, _ptr(out)))
+        return out
+
+    def waitOutputs(self):
+        """Wait for every stream-ordered read-back issued so far."""
+        self._check(self._lib.cfsa_ns_wait_outputs(self._h))
 
     @staticmethod
     def _out(shape, out):

@@ -97,6 +97,11 @@ struct PinnedSet {
 struct cfsa_ns {
   int device = 0;
   cudaStream_t stream = nullptr, body_stream = nullptr, body_stream2 = nullptr;
+  // stream-ordered field read-back (cfsa_ns_get_*_async): device staging copies of u (node-major)
+  // and p taken on `stream`, copied to the caller's host arrays on copy_stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_u_ready = nullptr, ev_u_done = nullptr, ev_p_ready = nullptr, ev_p_done = nullptr;
+  double *out_u = nullptr, *out_p = nullptr;
   std::string err;
   std::vector<void *> allocs;
 
@@ -255,6 +260,12 @@ struct cfsa_ns {
   }
 
   ~cfsa_ns() {
+    if (copy_stream) {
+      cudaStreamSynchronize(copy_stream);  // async read-backs still in flight
+      cudaStreamDestroy(copy_stream);
+    }
+    for (cudaEvent_t e : {ev_u_ready, ev_u_done, ev_p_ready, ev_p_done})
+      if (e) cudaEventDestroy(e);
     if (adj_exec) cudaGraphExecDestroy(adj_exec);
     for (void *ptr : rec_allocs) cudaFree(ptr);
     for (void *ptr : coarse_allocs) cudaFree(ptr);
@@ -1774,6 +1785,34 @@ struct cfsa_ns {
     CK(cudaMemcpyAsync(out, d_vec3, (size_t)3 * N2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
   }
+  // Stream-ordered read-back of u (node-major [N2][3]) or p into a host array: the staging copy is
+  // taken on `stream` after the work enqueued so far, then copied to `out` on copy_stream. The
+  // next read-back of the same field first waits for this copy to finish with the staging buffer.
+  void readback_async(bool velocity, double *out) {
+    if (!copy_stream) {
+      CK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+      for (cudaEvent_t *e : {&ev_u_ready, &ev_u_done, &ev_p_ready, &ev_p_done})
+        CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+      out_u = dalloc<double>((size_t)3 * N2);
+      out_p = dalloc<double>((size_t)nv);
+    }
+    cudaEvent_t ready = velocity ? ev_u_ready : ev_p_ready, done = velocity ? ev_u_done : ev_p_done;
+    CK(cudaStreamWaitEvent(stream, done, 0));
+    size_t bytes;
+    if (velocity) {
+      k_vec3_interleave<<<blocks_for(3 * N2), kBlock, 0, stream>>>(N2, u, out_u);
+      CK(cudaGetLastError());
+      bytes = (size_t)3 * N2 * sizeof(double);
+    } else {
+      CK(cudaMemcpyAsync(out_p, p, (size_t)nv * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+      bytes = (size_t)nv * sizeof(double);
+    }
+    CK(cudaEventRecord(ready, stream));
+    CK(cudaStreamWaitEvent(copy_stream, ready, 0));
+    CK(cudaMemcpyAsync(out, velocity ? out_u : out_p, bytes, cudaMemcpyDeviceToHost, copy_stream));
+    CK(cudaEventRecord(done, copy_stream));
+  }
+
   void upload_vec3(const double *in, double *d) {
     CK(cudaMemcpyAsync(d_vec3, in, (size_t)3 * N2 * sizeof(double), cudaMemcpyHostToDevice, stream));
     k_vec3_split<<<blocks_for(3 * N2), kBlock, 0, stream>>>(N2, d_vec3, d);
@@ -2679,6 +2718,30 @@ int cfsa_ns_get_velocity(cfsa_ns *h, double *u) {
   if (!h || !u) return CFSA_BAD_ARG;
   return guarded(h, [&] {
     h->download_vec3(h->u, u);
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_get_velocity_async(cfsa_ns *h, double *u) {
+  if (!h || !u) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    h->readback_async(true, u);
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_get_pressure_async(cfsa_ns *h, double *p) {
+  if (!h || !p) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    h->readback_async(false, p);
+    return CFSA_OK;
+  });
+}
+
+int cfsa_ns_wait_outputs(cfsa_ns *h) {
+  if (!h) return CFSA_BAD_ARG;
+  return guarded(h, [&] {
+    if (h->copy_stream) CK(cudaStreamSynchronize(h->copy_stream));
     return CFSA_OK;
   });
 }

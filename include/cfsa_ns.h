@@ -212,6 +212,15 @@ int cfsa_ns_get_velocity(cfsa_ns *h, double *u /*[N2][3]*/);          /* getVelo
 int cfsa_ns_get_velocity_star(cfsa_ns *h, double *u /*[N2][3]*/);
 int cfsa_ns_get_pressure(cfsa_ns *h, double *p /*[nv]*/);             /* getPressure */
 int cfsa_ns_get_pressure_correction(cfsa_ns *h, double *p /*[nv]*/);
+/* new (the reference's getters are synchronous, getVelocity/getPressure): stream-ordered
+ * read-back of the current u ([N2][3]) or p ([nv]) into a host array. The call snapshots the field
+ * on the device after the work enqueued so far and returns at once; the copy to `u` / `p` runs
+ * while later steps compute. The host array must stay valid, and is complete, only after
+ * cfsa_ns_wait_outputs (or a later read-back of the same field, which waits for the previous one
+ * to release the snapshot first). Pinned host memory makes the copy truly asynchronous. */
+int cfsa_ns_get_velocity_async(cfsa_ns *h, double *u /*[N2][3]*/);
+int cfsa_ns_get_pressure_async(cfsa_ns *h, double *p /*[nv]*/);
+int cfsa_ns_wait_outputs(cfsa_ns *h);
 int cfsa_ns_set_fields(cfsa_ns *h, const double *u /*[N2][3] or NULL*/, const double *p /*[nv] or NULL*/);
 int cfsa_ns_get_time(const cfsa_ns *h, double *t);                    /* getTime */
 /* new: binary state file for restarts (the reference has none: its VTK output cannot be read

@@ -98,3 +98,40 @@ def test_yaml_cli_run_matches_api(cf, tmp_path):
     api = tmp_path / "api.vtk"
     s.exportToVtk(api, 1.0)
     assert (tmp_path / "run_2.vtk").read_text() == api.read_text()
+
+
+def test_async_readback_equals_synchronous_getters(cf):
+    """cfsa_ns_get_velocity_async / _pressure_async: each step's fields, read back into alternating
+    pinned host buffers while the next step runs, equal the synchronous getters of that step bit
+    for bit once cfsa_ns_wait_outputs returns; pageable buffers work too (the copy then completes
+    before the call returns)."""
+    import torch
+
+    m = cf.Mesh.cylinder(30.0, 2.0, 3, 12)
+    m.setupBoundaryConditions((1.0, 0.0, 0.0), 1.0)
+    s = cf.NavierStokesSolver()
+    s.setKrylovTolerances(1e-10, 1e-10)
+    s.setPressureSolver(cf.KRYLOV_CG2L)
+    s.setMomentumSolver(cf.KRYLOV_CG)
+    s.setDt(0.01)
+    s.initialize(m, cf.Fluid(1060.0, 0.004))
+    s.setMeanInletVelocity([0.5, 0.0, 0.0])
+    ub = [torch.empty((s.N2, 3), dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
+    pb = [torch.empty((s.nv,), dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
+    ref = []
+    for k in range(5):
+        assert s.pisoStep()
+        s.getVelocityAsync(ub[k % 2])
+        s.getPressureAsync(pb[k % 2])
+        ref.append((s.getVelocity().copy(), s.getPressure().copy()))
+    s.waitOutputs()
+    for k in (3, 4):
+        assert np.array_equal(ub[k % 2], ref[k][0]) and np.array_equal(pb[k % 2], ref[k][1]), k
+    u_pageable, p_pageable = np.empty((s.N2, 3)), np.empty(s.nv)
+    assert s.pisoStep()
+    s.getVelocityAsync(u_pageable)
+    s.getPressureAsync(p_pageable)
+    s.waitOutputs()
+    assert np.array_equal(u_pageable, s.getVelocity()) and np.array_equal(p_pageable, s.getPressure())
+    with pytest.raises(ValueError):
+        s.getVelocityAsync(None)
