@@ -752,8 +752,9 @@ def main():
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": dom["achieved_gbs"], "peak": peak,
                 "unit": "GB/s", "frac": dom["achieved_gbs"] / peak, "peak_kind": peak_kind,
                 "traffic": dom["traffic"],
-                "traffic_note": "ncu dram__bytes_read.sum + write.sum of one launch captured at 250k tets, "
-                                "scaled to this workload by the ratio of algorithmic bytes (profiles/)"}
+                "traffic_note": "scaled, not measured on this workload: ncu dram__bytes_read.sum + write.sum of "
+                                "the momentum product captured at 414,720 tets (k_mcg_q<3>), times the ratio of "
+                                "algorithmic bytes per launch (profiles/dram_traffic.json)"}
 
     # accuracy of the headline itself: the timed steps again from the same state with the Krylov
     # solves converged (1e-14 in the Jacobi-scaled criterion, which sees the interior rows)
