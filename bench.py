@@ -102,10 +102,10 @@ def parse():
     ap.add_argument("--no-oracle", action="store_true",
                     help="skip every oracle run (parity at 1M tets, config-2 CPU comparison, CPU baseline)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
-    ap.add_argument("--mixed-marks", default="1,50,200", help="steps at which config 2 compares fields")
+    ap.add_argument("--mixed-marks", default="1,50,200", help="steps at which the mixed-precision comparison reads the fields")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint run")
     ap.add_argument("--no-y-bifurcation", action="store_true",
-                    help="skip config 4 (Y-bifurcation, ~4M tets, mixed precision + adjoint)")
+                    help="skip the ~4M-tet Y-bifurcation run (mixed precision + adjoint)")
     ap.add_argument("--y-steps", type=int, default=20, help="steps of each config-4 run")
     ap.add_argument("--y-checkpoint", type=int, default=5, help="checkpoint interval of the config-4 adjoint")
     ap.add_argument("--y-cell", type=float, default=0.081, help="lattice edge of the Y-bifurcation mesh")
@@ -260,7 +260,7 @@ def adjoint_section(cf, args, barrier):
     p1, p2 = m.fluidBC()
     inlet = np.nonzero(np.concatenate([p1, p2]) == 1)[0]
     res = {
-        "workload": f"config 3: cylinder L=30 R=2, {nt} tets ({ADJ_GEOM['rings']} rings x "
+        "workload": f"discrete adjoint: cylinder L=30 R=2, {nt} tets ({ADJ_GEOM['rings']} rings x "
                     f"{ADJ_GEOM['layers']} layers), N2={nv + ne}; {ADJ_STEPS} FP64 PISO steps from rest, "
                     f"parabolic inlet peak 1.0, J = mean |WSS|^2 over wall vertices with 14<=x<=16, "
                     f"checkpoint every {ADJ_CHECKPOINT} steps; Krylov tol {ADJ_TOL:g} (Jacobi-scaled)",
@@ -317,7 +317,7 @@ Y_CELL = 0.081  # Kuhn lattice edge of the Y-bifurcation: ~4M tets (mean volume 
 
 
 def ybif_section(cf, args, barrier, peak):
-    """Config 4: Y-bifurcation (parent R=2 L=15, daughters R=1.5 L=12 at +-35 deg, blend 0.5),
+    """The ~4M-tet Y-bifurcation (parent R=2 L=15, daughters R=1.5 L=12 at +-35 deg, blend 0.5),
     ~4M tets, parabolic inlet peak 1.0, both outlets p=0, from rest; FP64 and mixed-precision
     forward runs (Jacobi-scaled criterion, tol 1e-10) over `--y-steps` steps (the configuration
     names 100; the default budget keeps the whole benchmark within minutes), the pressure solve's
@@ -335,7 +335,7 @@ def ybif_section(cf, args, barrier, peak):
     def solver(precision):
         return make_solver_with(cf, m, prof, tol=TOL, norm=cf.NORM_JACOBI, precision=precision)
 
-    out = {"workload": f"config 4: Y-bifurcation, {nt} tets, N2={nv + ne}, nv={nv} (Kuhn lattice cell "
+    out = {"workload": f"Y-bifurcation, mixed precision and adjoint: {nt} tets, N2={nv + ne}, nv={nv} (Kuhn lattice cell "
                        f"{args.y_cell}); {n} steps from rest (budget; the configuration names 100), parabolic "
                        f"inlet peak 1.0, both outlets p=0, Krylov tol {TOL:g} Jacobi-scaled, two-level CG pressure",
            "tets": nt, "p2_nodes": nv + ne, "pressure_dofs": nv, "inlet_vertices": int((p1 == 1).sum()),
@@ -529,7 +529,7 @@ def make_solver_with(cf, m, profile, tol=TOL, norm=0, precision=0, momentum=None
 
 
 def mixed_section(cf, m, profile, marks):
-    """Config 2 on the headline mesh and inputs: FP64 and mixed precision (the headline's momentum
+    """Mixed precision on the headline mesh and inputs: FP64 and mixed precision (the headline's momentum
     Krylov method in FP32 with FP64 reliable updates) from rest over marks[-1] steps, both under the Jacobi-scaled criterion at
     1e-10 (the reference's criterion is dominated by the 1e10 penalty rows and pins the interior
     only loosely), and an FP64 run at 1e-14 in the same norm as the converged solution; fields at
@@ -541,7 +541,7 @@ def mixed_section(cf, m, profile, marks):
     conv, _, c_ok, _ = trajectory(cf, m, profile, cf.PRECISION_FP64, 1e-14, J, marks)
     n = marks[-1]
     mom = "Jacobi CG" if MOMENTUM_SOLVER == "cg" else "BiCGSTAB"
-    res = {"workload": f"config 2: the headline mesh and inputs, {n} steps from rest; momentum {mom} with FP32 "
+    res = {"workload": f"mixed precision on the headline mesh and inputs, {n} steps from rest; momentum {mom} with FP32 "
                        f"operator and Krylov vectors and FP64 reliable updates (true residual, solution, dots) vs "
                        f"FP64 {mom}; two-level CG pressure in FP64 in both (CFSA_PRECISION_MIXED); "
                        f"Jacobi-scaled criterion 1e-10",
@@ -586,7 +586,8 @@ def cpu_section(args, gpu_headline, gpu_step1_jacobi):
     """Everything the oracle (test infrastructure) does in the GPU arm, on one oracle instance of
     the headline workload, after the GPU sections: (1) parity of the headline FP64 path, the same
     solver (two-level CG pressure, same coarse target, reference criterion 1e-10) from rest, at
-    steps 1 and 3; (2) config 2's CPU comparison, FP64 in the Jacobi-scaled criterion, step 1;
+    steps 1 and 3; (2) the mixed-precision section's CPU comparison, FP64 in the Jacobi-scaled
+    criterion, step 1;
     (3) the timed CPU baseline, the reference algorithm (BiCGSTAB pressure) on all host threads."""
     po, o = oracle_cylinder(args.rings, args.layers, pressure_solver=3)
     o.set_momentum_solver(1 if MOMENTUM_SOLVER == "cg" else 0)
@@ -613,7 +614,7 @@ def cpu_section(args, gpu_headline, gpu_step1_jacobi):
         o.set_state(zero_u, zero_p)
         o.set_params(dt=DT, tol_mom=TOL, tol_p=TOL, maxit_mom=MAXIT[0], maxit_p=MAXIT[1], pressure_solver=3,
                      conv_norm=1)
-        o.set_momentum_solver(1 if MOMENTUM_SOLVER == "cg" else 0)  # config 2's FP64 path
+        o.set_momentum_solver(1 if MOMENTUM_SOLVER == "cg" else 0)  # the mixed-precision section's FP64 path
         if o.piso_step() == 0:
             st = o.state()
             mixed_cpu = {"reference": "FP64 oracle (CPU), Jacobi-scaled criterion 1e-10, step 1 from rest"}
@@ -738,7 +739,7 @@ def main():
                          "launches_timed_region": int(per_step),
                          "time_share_est": None, "traffic": traffic.get(name)}
     kernels["momentum_spmv_3rhs_f32"]["note"] = (
-        "the FP32 product of the mixed-precision momentum solve (config 2), all three components active; "
+        "the FP32 product of the mixed-precision momentum solve, all three components active; "
         "not part of the FP64 headline step")
     kernels["pressure_cg_solve"]["note"] = (
         "one launch = one whole two-level CG solve (fused product, coarse correction and vector updates "

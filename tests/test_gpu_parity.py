@@ -158,8 +158,8 @@ def test_piso_matches_golden_fixture(cf):
         assert rel_l2(s.getPressureCorrection(), g["pcorr"][k]) < 1e-8
 
 
-def test_config0_parity_100_steps(cf, po):
-    """Config 0: cylinder L=30 R=2 (~30k tets), rho 1060, nu 0.004, plug inlet 0.5, p=0 outlet,
+def test_cylinder_30k_parity_100_steps(cf, po):
+    """The reference-runnable case: cylinder L=30 R=2 (~30k tets), rho 1060, nu 0.004, plug inlet 0.5, p=0 outlet,
     dt 0.01, 100 steps from rest, Krylov tolerance 1e-10 (CG pressure on both sides)."""
     m = make_mesh(cf, 5, 68)
     assert 29000 < m.nTets() < 32000
@@ -169,7 +169,7 @@ def test_config0_parity_100_steps(cf, po):
         assert o.piso_step() == 0, k
     st = o.state()
     eu, ep = rel_l2(s.getVelocity(), st["u"]), rel_l2(s.getPressure(), st["p"])
-    print(f"config0 100 steps: rel L2 u {eu:.3e} p {ep:.3e}")
+    print(f"30k-tet cylinder, 100 steps: rel L2 u {eu:.3e} p {ep:.3e}")
     assert eu < 1e-8 and ep < 1e-8
     assert np.array_equal(s.getVelocity(), st["u"]) and np.array_equal(s.getPressure(), st["p"])
 
