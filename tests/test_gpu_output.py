@@ -60,9 +60,11 @@ def test_vtk_export_matches_reference_format(cf, tmp_path):
     assert np.allclose(pf, s.computePressureForces(), rtol=1e-5, atol=1e-300)
 
 
-def test_yaml_cli_run_matches_api(cf, tmp_path):
+@pytest.mark.parametrize("momentum", ["bicgstab", "cg"])
+def test_yaml_cli_run_matches_api(cf, tmp_path, momentum):
     """`simulation config.yaml` (the reference CLI's fluid-only loop) writes the VTK files of the
-    same run through the API: identical text at the last output step."""
+    same run through the API: identical text at the last output step, with the reference's
+    momentum BiCGSTAB and with `momentum_solver: cg`."""
     import subprocess
 
     from conftest import PKG
@@ -75,6 +77,7 @@ def test_yaml_cli_run_matches_api(cf, tmp_path):
         "navier_stokes:\n  enabled: true\n  density: 1060.0\n  viscosity: 0.004\n"
         "  inlet_velocity: [0.5, 0.0, 0.0]\n  outlet_pressure: 0.0\n  dt: 0.01\n  relax_p: 0.5\n"
         "  relax_u: 0.5\n  tolerance: 1e-10\n  max_iterations: [5000, 50000]\n  pressure_solver: cg\n"
+        f"  momentum_solver: {momentum}\n"
         f"output:\n  prefix: {tmp_path / 'run'}\n  total_steps: 5\n  output_frequency: 2\n  vtk_scale: 1.0\n")
     r = subprocess.run([str(exe), str(cfg)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
@@ -86,6 +89,7 @@ def test_yaml_cli_run_matches_api(cf, tmp_path):
     s.setTolerance(1e-10)
     s.setMaxIterations(5000, 50000)
     s.setPressureSolver(cf.KRYLOV_CG)
+    s.setMomentumSolver(cf.KRYLOV_CG if momentum == "cg" else cf.KRYLOV_BICGSTAB)
     s.initialize(m, cf.Fluid(1060.0, 0.004))
     s.setMeanInletVelocity([0.5, 0.0, 0.0])
     s.setOutletType(cf.OutletType.DirichletPressure)
