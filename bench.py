@@ -151,6 +151,36 @@ MOMENTUM = {"bicgstab": 1, "cg": 0}  # --momentum-solver -> CFSA_KRYLOV_BICGSTAB
 MOMENTUM_SOLVER = "cg"
 
 
+def bicgstab_headline(cf, m, steps, warm, world):
+    """The headline workload with the momentum method the configuration names, the reference's
+    batched Jacobi BiCGSTAB, instead of the headline's Jacobi CG: same mesh, inputs, pressure
+    solver, criterion, warm-up and step count, timed with CUDA events on this rank. Any failure is
+    reported in the returned record instead of ending the run."""
+    global MOMENTUM_SOLVER
+    saved = MOMENTUM_SOLVER
+    try:
+        MOMENTUM_SOLVER = "bicgstab"
+        s, _ = make_solver(cf, m)
+    except Exception as e:  # noqa: BLE001 - a side measurement must not end the bench line
+        return {"ok": False, "error": str(e)}
+    finally:
+        MOMENTUM_SOLVER = saved
+    try:
+        ok, _ = s.pisoSteps(warm)
+        ok2, done = s.pisoSteps(steps)
+        st = s.stats()
+        ms = st["last_step_ms"]
+        return {"what": "the same FP64 headline with batched Jacobi BiCGSTAB momentum (the reference's method "
+                        "and the configuration's); device time of this rank",
+                "ok": bool(ok and ok2 and done == steps), "value": world * done / (ms / 1e3) if ms > 0 else 0.0,
+                "unit": UNIT, "ms_per_step": ms / max(done, 1),
+                "krylov_iters_per_step": [st["krylov_iters"][0] / max(done, 1), st["krylov_iters"][1] / max(done, 1)]}
+    except Exception as e:  # noqa: BLE001
+        return {"ok": False, "error": str(e)}
+    finally:
+        del s
+
+
 def make_solver(cf, m, tol=TOL, norm=0):
     s = cf.NavierStokesSolver()
     s.setKrylovTolerances(tol, tol)
@@ -771,6 +801,10 @@ def main():
                 "interior is solved loosely at the headline tolerance; this is the headline's own error"}
     del s
     torch.cuda.empty_cache()
+    momentum_bicgstab = None
+    if MOMENTUM_SOLVER == "cg":
+        momentum_bicgstab = bicgstab_headline(cf, m, args.steps, warm, world)
+        torch.cuda.empty_cache()
 
     mixed, step1 = None, None
     if not args.no_mixed:
@@ -814,6 +848,7 @@ def main():
                                 "fields copy to pinned host arrays while the next step computes",
                     "fields_match_device_timed": e2e_match},
             "cpu_baseline": cpu, "clocks": clk, "parity": parity, "headline_accuracy": headline_accuracy,
+            "momentum_bicgstab": momentum_bicgstab,
             "mixed": mixed, "adjoint": adjoint, "y_bifurcation": ybif,
         }
         print(json.dumps(line), flush=True)
