@@ -206,10 +206,9 @@ struct cfsa_ns {
   PMixState *h_pmx = nullptr;
   double mixed_p_tol_in = 1e-5;  // inner reduction per sweep
   int mixed_p_max_sweeps = 30;
-  // reliable-update trigger of the mixed-precision BiCGSTAB: the FP64 residual replaces the FP32
-  // one when the latter has dropped by this factor since the previous update
-  // reliable-update threshold of the mixed-precision momentum solve (0: the method's default).
-  // BiCGSTAB 1e-2: a larger drop between updates costs it extra iterations. CG 1e-4: its FP32
+  // reliable-update threshold of the mixed-precision momentum solve: the FP64 residual replaces the
+  // FP32 one when the latter has dropped by this factor since the previous update (0: the method's
+  // default). BiCGSTAB 1e-2: a larger drop between updates costs it extra iterations. CG 1e-4: its FP32
   // iterations follow the FP64 ones whatever the threshold (1.4% faster than 1e-2 at 1M tets,
   // mixed vs FP64 3.5e-8 after 85 steps), so fewer FP64 residual products are pure savings.
   double mixed_delta = 0.0;
@@ -1744,8 +1743,9 @@ struct cfsa_ns {
     CK(cudaStreamSynchronize(stream));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
     const int pressure_body = pressure_body_kernels();
-    // mixed momentum: 5 kernels per iteration, 2 per reliable update (x update, residual) plus
-    // the init kernel per step; mixed two-level CG pressure: 4 kernels per sweep plus its init
+    // momentum: 5 kernels per BiCGSTAB iteration, 3 per CG iteration; mixed momentum: 2 more per
+    // reliable update (x update, residual) and an init kernel per solve, as has FP64 CG; mixed
+    // two-level CG pressure: 4 kernels per sweep plus its init
     batch_launches = (int64_t)launched_steps * (launches_per_step + mixed_fixed_kernels()) +
                      momentum_body_kernels() * (int64_t)h_st->body_runs[0] +
                      pressure_body * (int64_t)h_st->body_runs[1] +
