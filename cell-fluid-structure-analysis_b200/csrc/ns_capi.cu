@@ -578,6 +578,8 @@ struct cfsa_ns {
         q((const void *)k_bicg_xr<3>);
         q((const void *)k_bicg_xr<1>);
         q((const void *)k_mcg_xr<3>);
+        q((const void *)k_momentum_rhs);
+        q((const void *)k_finish_step);
         q((const void *)k_mpc_xr);
         q((const void *)k_mpc_init);
         q((const void *)k_mcg_init<3>);
@@ -1096,7 +1098,7 @@ struct cfsa_ns {
     m.st = st;
     m.red = red;
     m.cw = (conv_norm == CFSA_NORM_JACOBI) ? invA : nullptr;
-    k_momentum_rhs<<<blocks_for(s2.nrows_pad), kBlock, 0, stream>>>(m);
+    k_momentum_rhs<<<strided(k_momentum_rhs, blocks_for(s2.nrows_pad)), kBlock, 0, stream>>>(m);
     CK(cudaGetLastError());
     enqueue_momentum_krylov(capture, ustar, st);
   }
@@ -1658,7 +1660,7 @@ struct cfsa_ns {
     f.nv = (int)nv;
     f.st = st;
     f.red = red;
-    k_finish_step<<<blocks_for(N2), kBlock, 0, stream>>>(f);
+    k_finish_step<<<strided(k_finish_step, blocks_for(N2)), kBlock, 0, stream>>>(f);
     CK(cudaGetLastError());
   }
 
@@ -2121,7 +2123,7 @@ struct cfsa_ns {
     m.cw = (conv_norm == CFSA_NORM_JACOBI) ? invA : nullptr;
     m.adj_mu = a_px;
     m.tpos = tpos1;
-    k_momentum_rhs<<<blocks_for(s2.nrows_pad), kBlock, 0, stream>>>(m);
+    k_momentum_rhs<<<strided(k_momentum_rhs, blocks_for(s2.nrows_pad)), kBlock, 0, stream>>>(m);
     CK(cudaGetLastError());
     enqueue_momentum_krylov(capture, a_x, st_adj);
     k_adj_conv_tet<<<blocks_for(nt), kBlock, 0, stream>>>((int)nt, N2, nv, tnode, grad, vol, a_x, a_un,

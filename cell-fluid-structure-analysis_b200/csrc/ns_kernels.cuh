@@ -578,66 +578,74 @@ struct MomentumRhsArgs {
 
 __global__ void k_momentum_rhs(MomentumRhsArgs A) {
   if (A.st->halt) return;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
-  if (i >= 0) {
-    const int64_t n = A.n;
-    const double w = A.cw ? A.cw[i] : 1.0;
-    double b[3];
-    if (A.adj_mu) {
+  // one resident wave; each CTA visits 256-position blocks blockIdx.x, blockIdx.x + gridDim.x, ...
+  // (the reduction tree is that of one CTA per block, with one ticket per CTA instead of per block)
+  __shared__ WarpSums<6> S;
+  const int nblk = (A.S.nrows_pad + kBlock - 1) / kBlock;
+  int slot = 0;
+  for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x, ++slot) {
+    const int r = blk * kBlock + threadIdx.x;
+    double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const int i = (r < A.S.nrows_pad) ? A.S.perm[r] : -1;
+    if (i >= 0) {
+      const int64_t n = A.n;
+      const double w = A.cw ? A.cw[i] : 1.0;
+      double b[3];
+      if (A.adj_mu) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) b[c] = A.b[c * n + i];
+        for (int c = 0; c < 3; ++c) b[c] = A.b[c * n + i];
+        if (i < A.nv) {
+          double g[3];
+          gt_row3(i, A.G.rp, A.G.ci, A.tpos, A.Gv, A.nnz1, A.adj_mu, A.adj_mu, A.adj_mu, g);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) b[c] = b[c] - g[c] / A.dt;
+        }
+      } else {
+      double mu[3];
+      sell_spmv_row<3>(A.S, A.Ms, A.u, n, r, mu);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) b[c] = 0.0 + mu[c] / A.dt;
       if (i < A.nv) {
-        double g[3];
-        gt_row3(i, A.G.rp, A.G.ci, A.tpos, A.Gv, A.nnz1, A.adj_mu, A.adj_mu, A.adj_mu, g);
+        double gp[3] = {0.0, 0.0, 0.0};
+        for (int k = A.G.rp[i]; k < A.G.rp[i + 1]; ++k) {
+          const double pj = A.p[A.G.ci[k]];
+          gp[0] += A.Gv[k] * pj;
+          gp[1] += A.Gv[A.nnz1 + k] * pj;
+          gp[2] += A.Gv[2 * A.nnz1 + k] * pj;
+        }
 #pragma unroll
-        for (int c = 0; c < 3; ++c) b[c] = b[c] - g[c] / A.dt;
+        for (int c = 0; c < 3; ++c) b[c] -= gp[c];
       }
-    } else {
-    double mu[3];
-    sell_spmv_row<3>(A.S, A.Ms, A.u, n, r, mu);
+      double conv[3];
+      gather_conv(i, A.nt, A.adj_ptr, A.adj, A.vol, A.ct, conv);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) b[c] = 0.0 + mu[c] / A.dt;
-    if (i < A.nv) {
-      double gp[3] = {0.0, 0.0, 0.0};
-      for (int k = A.G.rp[i]; k < A.G.rp[i + 1]; ++k) {
-        const double pj = A.p[A.G.ci[k]];
-        gp[0] += A.Gv[k] * pj;
-        gp[1] += A.Gv[A.nnz1 + k] * pj;
-        gp[2] += A.Gv[2 * A.nnz1 + k] * pj;
+      for (int c = 0; c < 3; ++c) b[c] += conv[c];
+      const int bcv = A.bc[i];
+      if (bcv == BC_INLET || bcv == BC_WALL) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double up = (bcv == BC_INLET) ? A.inlet[c * n + i] : 0.0;
+          b[c] += kMomentumPenalty * up;
+        }
       }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) b[c] -= gp[c];
-    }
-    double conv[3];
-    gather_conv(i, A.nt, A.adj_ptr, A.adj, A.vol, A.ct, conv);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) b[c] += conv[c];
-    const int bcv = A.bc[i];
-    if (bcv == BC_INLET || bcv == BC_WALL) {
+      }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const double up = (bcv == BC_INLET) ? A.inlet[c * n + i] : 0.0;
-        b[c] += kMomentumPenalty * up;
+        const int64_t o = c * n + i;
+        A.b[o] = b[c];
+        A.x[o] = 0.0;
+        A.r[o] = b[c];
+        A.r0[o] = b[c];
+        A.pk[o] = 0.0;
+        A.v[o] = 0.0;
+        part[c] = b[c] * b[c];
+        part[3 + c] = (b[c] * b[c]) * w;
       }
     }
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int64_t o = c * n + i;
-      A.b[o] = b[c];
-      A.x[o] = 0.0;
-      A.r[o] = b[c];
-      A.r0[o] = b[c];
-      A.pk[o] = 0.0;
-      A.v[o] = 0.0;
-      part[c] = b[c] * b[c];
-      part[3 + c] = (b[c] * b[c]) * w;
-    }
+    warp_partial<6>(part, S, slot);
   }
   double tot[6];
-  if (grid_reduce<6>(part, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_strided<6>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     BicgState *s = A.bs;
     s->active = 0;
     s->restart = 0;
@@ -2730,28 +2738,35 @@ struct FinishArgs {
 
 __global__ void k_finish_step(FinishArgs A) {
   if (A.st->halt) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double part[1] = {0.0};
-  if (i < A.n) {
-    const int64_t n = A.n;
-    const int bcv = A.bc[i];
-    bool nan = false;
-    for (int c = 0; c < 3; ++c) {
-      double ui = A.u[c * n + i];
-      if (bcv == BC_INLET) {
-        ui = A.inlet[c * n + i];
-        A.u[c * n + i] = ui;
-      } else if (bcv == BC_WALL) {
-        ui = 0.0;
-        A.u[c * n + i] = ui;
+  // one resident wave visiting 256-position blocks (one reduction ticket per CTA)
+  __shared__ WarpSums<1> S;
+  const int nblk = (A.n + kBlock - 1) / kBlock;
+  int slot = 0;
+  for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x, ++slot) {
+    const int i = blk * kBlock + threadIdx.x;
+    double part[1] = {0.0};
+    if (i < A.n) {
+      const int64_t n = A.n;
+      const int bcv = A.bc[i];
+      bool nan = false;
+      for (int c = 0; c < 3; ++c) {
+        double ui = A.u[c * n + i];
+        if (bcv == BC_INLET) {
+          ui = A.inlet[c * n + i];
+          A.u[c * n + i] = ui;
+        } else if (bcv == BC_WALL) {
+          ui = 0.0;
+          A.u[c * n + i] = ui;
+        }
+        nan |= isnan(ui) || isnan(A.ustar[c * n + i]);
       }
-      nan |= isnan(ui) || isnan(A.ustar[c * n + i]);
+      if (i < A.nv) nan |= isnan(A.p[i]) || isnan(A.pc[i]);
+      part[0] = nan ? 1.0 : 0.0;
     }
-    if (i < A.nv) nan |= isnan(A.p[i]) || isnan(A.pc[i]);
-    part[0] = nan ? 1.0 : 0.0;
+    warp_partial<1>(part, S, slot);
   }
   double tot[1];
-  if (grid_reduce<1>(part, A.red, tot) && threadIdx.x == 0) {
+  if (grid_reduce_strided<1>(S, slot, nblk, A.red, tot) && threadIdx.x == 0) {
     A.st->steps_done += 1;
     if (tot[0] > 0.0) {
       A.st->nan = 1;
