@@ -93,6 +93,7 @@ def test_config_defaults_are_the_references(tmp_path):
     assert d["navier_stokes.inlet_velocity"] == "0.10000000000000001 0 0"
     assert float(d["navier_stokes.dt"]) == 1e-3 and float(d["navier_stokes.relax_p"]) == 0.5
     assert d["navier_stokes.pressure_solver"] == "bicgstab" and d["navier_stokes.precision"] == "fp64"
+    assert d["navier_stokes.momentum_solver"] == "bicgstab"
     assert d["output.prefix"] == "output" and d["output.total_steps"] == "1000" and d["output.output_frequency"] == "20"
 
 
@@ -107,6 +108,7 @@ def test_config_defaults_are_the_references(tmp_path):
     ("mesh:\n  type: msh\n", "msh_file required"),
     ("mesh:\n  type: cylinder\nnavier_stokes:\n  enabled: true\n  precision: fp16\n", "unknown value 'fp16'"),
     ("mesh:\n  type: cylinder\nnavier_stokes:\n  enabled: true\n  coarse_aggregates: 0\n", "coarse_aggregates must be in"),
+    ("mesh:\n  type: cylinder\nnavier_stokes:\n  enabled: true\n  momentum_solver: gmres\n", "unknown value 'gmres'"),
 ])
 def test_config_errors(tmp_path, text, msg):
     r = dry_run(tmp_path, text)
